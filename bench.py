@@ -1,0 +1,356 @@
+#!/usr/bin/env python3
+"""Benchmark: global residual + Jacobian assembly of plane-stress Lagrange quads on B200.
+
+Default workload: 1024x1024 order-3 quads on a 10x10 square (+-0.2h interior
+perturbation, u in [-1e-3,1e-3], E=70e9, nu=0.3, 4x4 Gauss points; 18,886,658 DOF,
+235,960,321 2x2 blocks).  One step = one complete residual + Jacobian assembly.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+Prints one JSON line (rank 0).  `value` is elements/s of the fastest validated
+path with device-resident inputs; `e2e` is the same metric through the public
+API with a host->device copy of the state and a device->host copy of the
+residual inside every timed step.  Multi-GPU runs are independent replicas (the
+assembly of one mesh is not sharded).  --impl reference times the FP64 CPU
+oracle (restatement of the reference's CPU assembly, element/FEKernels.h:317-508)
+on a bounded sample of the same mesh with all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOADS = {
+    "square1024_p3": dict(kind="square", n=1024, p=3),
+    "square512_p3": dict(kind="square", n=512, p=3),
+    "square2048_p1": dict(kind="square", n=2048, p=1),
+    "square64_p1": dict(kind="square64"),
+    "annulus512x2048_p2": dict(kind="annulus"),
+}
+
+
+def make_mesh(fem, name):
+    w = WORKLOADS[name]
+    if w["kind"] == "square64":
+        return fem.square64_p1()
+    if w["kind"] == "annulus":
+        return fem.annulus512x2048_p2()
+    if w["p"] == 3:
+        return fem.square1024_p3(w["n"])
+    return fem.square_mesh(w["n"], w["n"], w["p"], 1.0, 1.0, 0.1, 1e-3, 70e9, 0.3, 1.0, 0x5EED0006,
+                           f"square{w['n']}_p{w['p']}")
+
+
+def algorithmic_bytes(mesh, nnzb):
+    """Minimal HBM bytes of one residual+Jacobian assembly: read coords and states,
+    read conn, write the residual and the BSR values once."""
+    return 16 * mesh.num_nodes * 2 + 4 * mesh.num_elements * mesh.nodes_per_element + 16 * mesh.num_nodes + 32 * nnzb
+
+
+def algorithmic_flops(mesh):
+    """Per-element FP64 flop convention n_q*(24n^2 + 24n + 40) with n = n_q = (p+1)^2."""
+    n = mesh.nodes_per_element
+    return mesh.num_elements * n * (24 * n * n + 24 * n + 40)
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.dev)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+        return False
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        load = [s for s in sm if s > 0.5 * (mx or max(sm))] or sm
+        return {"sm_mhz": statistics.median(load), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ----------------------------------------------------------------------------------------
+def run_reference(args):
+    """FP64 CPU oracle (restatement of the reference CPU assembly) on a bounded sample."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import fem_pkg
+    import oracle as orc
+    fem = fem_pkg.load()
+    mesh = make_mesh(fem, args.workload)
+    sample = min(mesh.num_elements, args.ref_elements)
+    sub = fem.submesh(mesh, 0, sample)
+    rowp, cols = fem.build_bsr_pattern(sub.num_nodes, sub.conn_ptr, sub.conn)
+    mp = fem.build_element_bsr_map(sub.conn_ptr, sub.conn, sub.nodes_per_element, rowp, cols)
+    threads = os.cpu_count() or 1
+    orc.set_threads(threads)
+    times = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        orc.assemble(sub, mp, cols.size, parallel=True)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(dt)
+    tot = sum(times)
+    value = sample * len(times) / tot
+    line = {
+        "impl": "reference", "metric": "assembled elements/s (res+Jac)", "value": value, "unit": "elements/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "sample_elements": sample, "order": mesh.order},
+        "cpu_baseline": {"value": value, "unit": "elements/s", "cores": threads, "kind": "port",
+                         "sample": f"first {sample} elements of {mesh.name} (OpenMP over elements, atomic scatter)"},
+        "e2e": {"value": value, "unit": "elements/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+    world, rank, local, pg = dist_setup(args)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    import fem_pkg
+    fem = fem_pkg.load()
+    mesh = make_mesh(fem, args.workload)
+    stream = torch.cuda.Stream(device=dev)
+    sptr = stream.cuda_stream
+    with torch.cuda.stream(stream):
+        d = fem.DeviceMesh(mesh, dev)
+        plan = fem.Plan(mesh.order, mesh.num_nodes, mesh.conn_ptr, mesh.conn)
+        nnzb = plan.nnzb
+        res = torch.empty(mesh.num_nodes * 2, dtype=torch.float64, device=dev)
+        mat = torch.empty(nnzb * 4, dtype=torch.float64, device=dev)
+    stream.synchronize()
+    E, nu, t = mesh.E, mesh.nu, mesh.t
+    nE = mesh.num_elements
+
+    def time_steps(fn, steps, warmup, launches_per_step):
+        for _ in range(warmup):
+            fn()
+        stream.synchronize()
+        if pg is not None:
+            pg.barrier()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(steps):
+            fn()
+        ev1.record(stream)
+        ev1.synchronize()
+        ms = ev0.elapsed_time(ev1) / steps
+        if pg is not None:
+            tt = torch.tensor([ms], device=dev)
+            pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+            ms = float(tt.item())
+        return ms, launches_per_step * steps
+
+    paths = {}
+    # plan path (overwrite, no zeroing), FP64 and mixed
+    for prec in ("fp64", "mixed"):
+        fn = (lambda prec=prec: plan.assemble(d.states, d.coords, E, nu, t, res, mat, precision=prec, stream=sptr))
+        ms, _ = time_steps(fn, max(2, args.steps // 2), args.warmup, plan.num_colours)
+        paths[f"plan_{prec}"] = {"ms": ms, "elements_per_s": nE / (ms * 1e-3)}
+    # error of the mixed plan path against the FP64 plan path (FP64 path is oracle-checked in tests)
+    with torch.cuda.stream(stream):
+        plan.assemble(d.states, d.coords, E, nu, t, res, mat, precision="fp64", stream=sptr)
+        res64, mat64 = res.clone(), mat.clone()
+        plan.assemble(d.states, d.coords, E, nu, t, res, mat, precision="mixed", stream=sptr)
+        err_res = float(torch.linalg.vector_norm(res - res64) / torch.linalg.vector_norm(res64))
+        err_mat = float(torch.linalg.vector_norm(mat - mat64) / torch.linalg.vector_norm(mat64))
+    stream.synchronize()
+    del res64, mat64
+    paths["plan_mixed"]["rel_frobenius_err"] = {"residual": err_res, "jacobian": err_mat}
+    # plain drop-in FP64 (reference contract: caller zeroes, kernel accumulates via map, atomics)
+    if not args.skip_dropin:
+        rowp_h, cols_h = plan.pattern()
+        mp = fem.build_element_bsr_map(mesh.conn_ptr, mesh.conn, mesh.nodes_per_element, rowp_h, cols_h)
+        with torch.cuda.stream(stream):
+            dmap = torch.from_numpy(mp).to(dev)
+        del mp, rowp_h, cols_h
+
+        def dropin(prec="fp64", zero=True):
+            if zero:
+                res.zero_()
+                mat.zero_()
+            fem.run_jacobian_kernel(mesh.order, d.conn_ptr, d.conn, nE, d.states, d.coords, E, nu, t, dmap, res, mat,
+                                    precision=prec, stream=sptr, timed=False)
+
+        with torch.cuda.stream(stream):
+            ms, _ = time_steps(lambda: dropin("fp64", True), max(2, args.steps // 2), args.warmup, 1)
+            paths["dropin_fp64_with_zeroing"] = {"ms": ms, "elements_per_s": nE / (ms * 1e-3)}
+            ms, _ = time_steps(lambda: dropin("fp64", False), max(2, args.steps // 2), args.warmup, 1)
+            paths["dropin_fp64_kernel_only"] = {"ms": ms, "elements_per_s": nE / (ms * 1e-3)}
+        del dmap
+    best = "plan_mixed" if (paths["plan_mixed"]["ms"] < paths["plan_fp64"]["ms"] and max(err_res, err_mat) <= 1e-6) \
+        else "plan_fp64"
+    prec = "mixed" if best == "plan_mixed" else "fp64"
+
+    def step():
+        plan.assemble(d.states, d.coords, E, nu, t, res, mat, precision=prec, stream=sptr)
+
+    with ClockSampler(local) as clk:
+        ms, launches = time_steps(step, args.steps, args.warmup, plan.num_colours)
+    value = world * nE / (ms * 1e-3)
+
+    # end to end through the public API: pinned host state -> device, assemble, residual -> pinned host
+    h_states = torch.from_numpy(np.ascontiguousarray(mesh.states)).pin_memory()
+    h_res = torch.empty(mesh.num_nodes * 2, dtype=torch.float64).pin_memory()
+
+    def e2e_step():
+        d.states.copy_(h_states, non_blocking=True)
+        plan.assemble(d.states, d.coords, E, nu, t, res, mat, precision=prec, stream=sptr)
+        h_res.copy_(res, non_blocking=True)
+
+    with torch.cuda.stream(stream):
+        ms_e2e, _ = time_steps(e2e_step, args.steps, args.warmup, plan.num_colours)
+    h2d, d2h = h_states.numel() * 8, h_res.numel() * 8
+
+    hbm, peak_kind = peaks()
+    abytes = algorithmic_bytes(mesh, nnzb)
+    achieved = abytes / (ms * 1e-3) / 1e9
+    line = {
+        "metric": "assembled elements/s (res+Jac)", "value": value, "unit": "elements/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if prec == "fp64" else "f32/f64", "data": "synthetic",
+        "config": {"workload": mesh.name, "order": mesh.order, "elements": nE, "dof": mesh.num_dof, "nnzb": nnzb,
+                   "path": best, "l2": "inputs and outputs larger than L2 (BSR values %.2f GB)" % (32 * nnzb / 1e9),
+                   "parallelism": f"replicas{world}"},
+        "dof_per_s": value * mesh.num_dof / nE,
+        "paths": paths,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": None, "peak_kind": peak_kind, "algorithmic_bytes_per_step": abytes,
+                     "kernel": f"assemble_kernel<{mesh.order}> x {plan.num_colours} colour launches per step"},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+        "e2e": {"value": world * nE / (ms_e2e * 1e-3), "unit": "elements/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(fem, mesh, args)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    plan.close()
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def cpu_baseline(fem, mesh, args):
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as orc
+    sample = min(mesh.num_elements, args.ref_elements)
+    sub = fem.submesh(mesh, 0, sample)
+    rowp, cols = fem.build_bsr_pattern(sub.num_nodes, sub.conn_ptr, sub.conn)
+    mp = fem.build_element_bsr_map(sub.conn_ptr, sub.conn, sub.nodes_per_element, rowp, cols)
+    threads = os.cpu_count() or 1
+    orc.set_threads(threads)
+    orc.assemble(sub, mp, cols.size, parallel=True)
+    t0 = time.perf_counter()
+    reps = 0
+    while True:
+        orc.assemble(sub, mp, cols.size, parallel=True)
+        reps += 1
+        if time.perf_counter() - t0 > args.cpu_seconds:
+            break
+    dt = (time.perf_counter() - t0) / reps
+    return {"value": sample / dt, "unit": "elements/s", "cores": threads, "kind": "port",
+            "sample": f"first {sample} elements of {mesh.name}, {reps} repeats (OpenMP, atomic scatter)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="square1024_p3", choices=sorted(WORKLOADS))
+    ap.add_argument("--ref-elements", type=int, default=131072)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--skip-dropin", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

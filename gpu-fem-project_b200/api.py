@@ -1,0 +1,197 @@
+"""Python host mirror of the reference's element-kernel API over the C ABI.
+
+`run_residual_kernel` / `run_jacobian_kernel` keep the argument order and
+meaning of runResidualKernel / runJacobianKernel (element/FEKernels.h:1030,1125):
+device arrays in, accumulate into the caller-zeroed outputs, elapsed seconds
+out.  Device arrays are torch CUDA tensors (or raw device pointers as ints).
+Errors raise FemError instead of exiting the process (GPUMacros.h:23-31).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import FEM_PRECISION_FP64, FEM_PRECISION_MIXED, check, lib
+
+_PRECISION = {"fp64": FEM_PRECISION_FP64, "mixed": FEM_PRECISION_MIXED}
+
+
+def _prec(p) -> int:
+    if isinstance(p, int):
+        return p
+    return _PRECISION[p]
+
+
+def _dptr(x, dtype=None, name="array"):
+    """Device pointer of a CUDA tensor (or an int pointer); None stays None."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    import torch
+    if not isinstance(x, torch.Tensor):
+        raise TypeError(f"{name}: expected a CUDA tensor or a device pointer, got {type(x).__name__}")
+    if not x.is_cuda:
+        raise ValueError(f"{name}: tensor is on {x.device}; the assembly path runs on the GPU only")
+    if not x.is_contiguous():
+        raise ValueError(f"{name}: tensor must be contiguous")
+    if dtype is not None and x.dtype != dtype:
+        raise TypeError(f"{name}: dtype {x.dtype}, expected {dtype}")
+    return x.data_ptr()
+
+
+def _stream(stream):
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+def _np(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+def run_residual_kernel(element_order, conn_ptr, conn, num_elements, states, node_coords, E, nu, t, residual, *,
+                        precision="fp64", stream=None, timed=True):
+    """runResidualKernel: adds element residuals into `residual`; returns seconds (timed) or None."""
+    import torch
+    el = C.c_double(0.0)
+    fn = lib.fem_run_residual if _prec(precision) == FEM_PRECISION_FP64 else lib.fem_run_residual_mixed
+    st = fn(int(element_order), _dptr(conn_ptr, torch.int32, "connPtr"), _dptr(conn, torch.int32, "conn"),
+            int(num_elements), _dptr(states, torch.float64, "states"), _dptr(node_coords, torch.float64, "nodeCoords"),
+            float(E), float(nu), float(t), _dptr(residual, torch.float64, "residual"), _stream(stream),
+            C.byref(el) if timed else None)
+    check(st, "fem_run_residual")
+    return el.value if timed else None
+
+
+def run_jacobian_kernel(element_order, conn_ptr, conn, num_elements, states, node_coords, E, nu, t,
+                        element_bcsr_map, residual, mat_entries, *, precision="fp64", stream=None, timed=True):
+    """runJacobianKernel: adds element matrices (and residuals when `residual` is
+    not None) into the caller-zeroed outputs; returns seconds (timed) or None."""
+    import torch
+    el = C.c_double(0.0)
+    fn = lib.fem_run_jacobian if _prec(precision) == FEM_PRECISION_FP64 else lib.fem_run_jacobian_mixed
+    st = fn(int(element_order), _dptr(conn_ptr, torch.int32, "connPtr"), _dptr(conn, torch.int32, "conn"),
+            int(num_elements), _dptr(states, torch.float64, "states"), _dptr(node_coords, torch.float64, "nodeCoords"),
+            float(E), float(nu), float(t), _dptr(element_bcsr_map, torch.int32, "elementBCSRMap"),
+            _dptr(residual, torch.float64, "residual"), _dptr(mat_entries, torch.float64, "matEntries"),
+            _stream(stream), C.byref(el) if timed else None)
+    check(st, "fem_run_jacobian")
+    return el.value if timed else None
+
+
+def build_bsr_pattern(num_nodes, conn_ptr, conn):
+    """(rowp int32[numNodes+1], cols int32[nnzb]) of the nodal adjacency (host)."""
+    cp, cn = _np(conn_ptr, np.int32), _np(conn, np.int32)
+    ne = cp.size - 1
+    rowp = np.zeros(int(num_nodes) + 1, np.int32)
+    nnzb = C.c_int64(0)
+    check(lib.fem_build_bsr_pattern(int(num_nodes), cp.ctypes.data, cn.ctypes.data, ne, rowp.ctypes.data, None,
+                                    C.byref(nnzb)), "fem_build_bsr_pattern")
+    cols = np.zeros(nnzb.value, np.int32)
+    check(lib.fem_build_bsr_pattern(int(num_nodes), cp.ctypes.data, cn.ctypes.data, ne, rowp.ctypes.data,
+                                    cols.ctypes.data, C.byref(nnzb)), "fem_build_bsr_pattern")
+    return rowp, cols
+
+
+def build_element_bsr_map(conn_ptr, conn, nodes_per_element, rowp, cols):
+    """generateElementBCSRMap: int32[numElements * n * n] of block offsets * 4 (host)."""
+    cp, cn = _np(conn_ptr, np.int32), _np(conn, np.int32)
+    rp, cl = _np(rowp, np.int32), _np(cols, np.int32)
+    ne = cp.size - 1
+    out = np.zeros(ne * int(nodes_per_element) ** 2, np.int32)
+    check(lib.fem_build_element_bsr_map(cp.ctypes.data, cn.ctypes.data, ne, int(nodes_per_element), rp.ctypes.data,
+                                        cl.ctypes.data, out.ctypes.data), "fem_build_element_bsr_map")
+    return out
+
+
+def colour_elements(num_nodes, conn_ptr, conn):
+    """(colour int32[numElements], numColours): greedy, element order, no shared nodes per colour."""
+    cp, cn = _np(conn_ptr, np.int32), _np(conn, np.int32)
+    ne = cp.size - 1
+    colour = np.zeros(ne, np.int32)
+    nc = C.c_int(0)
+    check(lib.fem_colour_elements(int(num_nodes), cp.ctypes.data, cn.ctypes.data, ne, colour.ctypes.data,
+                                  C.byref(nc)), "fem_colour_elements")
+    return colour, nc.value
+
+
+def bsr_spmv(rowp, cols, values, x, y, stream=None):
+    """y = A x on the device for the 2x2-block BSR matrix (rowp, cols, values)."""
+    import torch
+    n = int(rowp.numel()) - 1
+    check(lib.fem_bsr_spmv(n, _dptr(rowp, torch.int32), _dptr(cols, torch.int32), _dptr(values, torch.float64),
+                           _dptr(x, torch.float64), _dptr(y, torch.float64), _stream(stream)), "fem_bsr_spmv")
+
+
+class Plan:
+    """Device-resident assembly plan of one mesh (fem_plan_*): BSR pattern,
+    colouring and block codes.  `assemble` overwrites the outputs completely."""
+
+    def __init__(self, element_order, num_nodes, conn_ptr, conn):
+        cp, cn = _np(conn_ptr, np.int32), _np(conn, np.int32)
+        self._h = C.c_void_p()
+        check(lib.fem_plan_create(int(element_order), int(num_nodes), cp.ctypes.data, cn.ctypes.data, cp.size - 1,
+                                  C.byref(self._h)), "fem_plan_create")
+        self.order = int(element_order)
+        nn, ne, nc = C.c_int(), C.c_int(), C.c_int()
+        nnzb, nbytes = C.c_int64(), C.c_int64()
+        check(lib.fem_plan_info(self._h, C.byref(nn), C.byref(ne), C.byref(nnzb), C.byref(nc), C.byref(nbytes)),
+              "fem_plan_info")
+        self.num_nodes, self.num_elements, self.nnzb = nn.value, ne.value, nnzb.value
+        self.num_colours, self.device_bytes = nc.value, nbytes.value
+
+    @property
+    def handle(self) -> int:
+        return self._h.value
+
+    def pattern(self):
+        rowp = np.zeros(self.num_nodes + 1, np.int32)
+        cols = np.zeros(self.nnzb, np.int32)
+        check(lib.fem_plan_get_pattern(self._h, rowp.ctypes.data, cols.ctypes.data), "fem_plan_get_pattern")
+        return rowp, cols
+
+    def device_pattern(self):
+        """(rowp, cols) device pointers owned by the plan."""
+        r, c = C.c_void_p(), C.c_void_p()
+        check(lib.fem_plan_device_pattern(self._h, C.byref(r), C.byref(c)), "fem_plan_device_pattern")
+        return r.value, c.value
+
+    def assemble(self, states, node_coords, E, nu, t, residual=None, mat_entries=None, *, precision="fp64",
+                 stream=None, timed=False):
+        import torch
+        el = C.c_double(0.0)
+        check(lib.fem_plan_assemble(self._h, _dptr(states, torch.float64, "states"),
+                                    _dptr(node_coords, torch.float64, "nodeCoords"), float(E), float(nu), float(t),
+                                    _dptr(residual, torch.float64, "residual"),
+                                    _dptr(mat_entries, torch.float64, "matEntries"), _prec(precision),
+                                    _stream(stream), C.byref(el) if timed else None), "fem_plan_assemble")
+        return el.value if timed else None
+
+    def close(self):
+        if self._h and self._h.value:
+            lib.fem_plan_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class DeviceMesh:
+    """A Mesh uploaded to the GPU as torch tensors (int32 topology, float64 data)."""
+
+    def __init__(self, mesh, device="cuda"):
+        import torch
+        self.mesh = mesh
+        self.order = mesh.order
+        self.conn_ptr = torch.from_numpy(_np(mesh.conn_ptr, np.int32)).to(device)
+        self.conn = torch.from_numpy(_np(mesh.conn, np.int32)).to(device)
+        self.coords = torch.from_numpy(_np(mesh.coords, np.float64)).to(device)
+        self.states = torch.from_numpy(_np(mesh.states, np.float64)).to(device)

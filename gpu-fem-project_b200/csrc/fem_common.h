@@ -1,0 +1,38 @@
+// Shared internals of libfemb200: error reporting and small helpers.
+#pragma once
+
+#include <cstdint>
+#include <cstdio>
+#include <vector>
+
+#include "fem_b200.h"
+
+namespace fem {
+
+// Records a message for fem_last_error() on this host thread and returns `status`.
+int fail(int status, const char *fmt, ...);
+void clear_error();
+const char *last_error_cstr();
+
+inline bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+// Host builders (fem_host.cpp).
+int build_pattern(int numNodes, const int *connPtr, const int *conn, int numElements, int *rowp, int *cols,
+                  int64_t *nnzb);
+int colour_greedy(int numNodes, const int *connPtr, const int *conn, int numElements, int *colour,
+                  int *numColours);
+
+// Plan topology built on the host before upload (fem_host.cpp).
+struct HostPlan {
+  int order = 0, nn = 0, numNodes = 0, numElements = 0, numColours = 0;
+  int64_t nnzb = 0;
+  std::vector<int> rowp, cols;                // pattern
+  std::vector<int> elemList;            // elements in colour order
+  std::vector<int> colourPtr;           // numColours+1 offsets into elemList
+  std::vector<int> connList;            // conn in elemList order, nn per element
+  std::vector<uint8_t> blockCode;       // per (k, a, b): rank in row | 0x80 store flag
+  std::vector<uint8_t> nodeCode;        // per (k, a): 1 = store, 0 = add
+};
+int build_host_plan(int order, int numNodes, const int *connPtr, const int *conn, int numElements, HostPlan &hp);
+
+}  // namespace fem

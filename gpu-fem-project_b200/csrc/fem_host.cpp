@@ -1,0 +1,271 @@
+// Host-side topology work of libfemb200: BSR pattern, element -> block map,
+// element colouring and the compact per-element block codes of an assembly
+// plan.  All integer work, exact and deterministic (OpenMP only where the
+// result does not depend on the schedule).
+#include <algorithm>
+#include <climits>
+#include <cstdarg>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "fem_common.h"
+
+namespace fem {
+
+namespace {
+thread_local std::string g_last_error;
+
+int validate_mesh(int numNodes, const int *connPtr, const int *conn, int numElements) {
+  if (numNodes < 0 || numElements < 0) return fail(FEM_ERR_INVALID_ARGUMENT, "negative size");
+  if (numElements > 0 && (!connPtr || !conn)) return fail(FEM_ERR_INVALID_ARGUMENT, "connPtr/conn is NULL");
+  for (int e = 0; e < numElements; e++)
+    if (connPtr[e + 1] < connPtr[e]) return fail(FEM_ERR_INVALID_ARGUMENT, "connPtr decreases at element %d", e);
+  const int64_t total = numElements > 0 ? (int64_t)connPtr[numElements] : 0;
+  int64_t bad = -1;
+#pragma omp parallel for reduction(max : bad)
+  for (int64_t i = numElements > 0 ? connPtr[0] : 0; i < total; i++)
+    if (conn[i] < 0 || conn[i] >= numNodes) bad = std::max(bad, i);
+  if (bad >= 0) return fail(FEM_ERR_INVALID_ARGUMENT, "conn[%lld] = %d outside [0, %d)", (long long)bad, conn[bad], numNodes);
+  return FEM_SUCCESS;
+}
+
+// node -> incident elements (CSR), counting sort in element order.
+void node_elements(int numNodes, const int *connPtr, const int *conn, int numElements, std::vector<int64_t> &ptr,
+                   std::vector<int> &elems) {
+  ptr.assign((size_t)numNodes + 1, 0);
+  for (int e = 0; e < numElements; e++)
+    for (int i = connPtr[e]; i < connPtr[e + 1]; i++) ptr[(size_t)conn[i] + 1]++;
+  for (int r = 0; r < numNodes; r++) ptr[r + 1] += ptr[r];
+  elems.resize((size_t)ptr[numNodes]);
+  std::vector<int64_t> fill(ptr.begin(), ptr.end() - 1);
+  for (int e = 0; e < numElements; e++)
+    for (int i = connPtr[e]; i < connPtr[e + 1]; i++) elems[(size_t)fill[conn[i]]++] = e;
+}
+
+// Sorted unique neighbours of node r into buf.
+inline void row_neighbours(int r, const std::vector<int64_t> &nptr, const std::vector<int> &nelem,
+                           const int *connPtr, const int *conn, std::vector<int> &buf) {
+  buf.clear();
+  for (int64_t k = nptr[r]; k < nptr[r + 1]; k++) {
+    const int e = nelem[(size_t)k];
+    buf.insert(buf.end(), conn + connPtr[e], conn + connPtr[e + 1]);
+  }
+  std::sort(buf.begin(), buf.end());
+  buf.erase(std::unique(buf.begin(), buf.end()), buf.end());
+}
+}  // namespace
+
+int fail(int status, const char *fmt, ...) {
+  char msg[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(msg, sizeof msg, fmt, ap);
+  va_end(ap);
+  g_last_error = msg;
+  return status;
+}
+
+void clear_error() { g_last_error.clear(); }
+
+const char *last_error_cstr() { return g_last_error.c_str(); }
+
+int build_pattern(int numNodes, const int *connPtr, const int *conn, int numElements, int *rowp, int *cols,
+                  int64_t *nnzb) {
+  if (!rowp && !nnzb) return fail(FEM_ERR_INVALID_ARGUMENT, "rowp and nnzb are both NULL");
+  int st = validate_mesh(numNodes, connPtr, conn, numElements);
+  if (st) return st;
+  std::vector<int64_t> nptr;
+  std::vector<int> nelem;
+  node_elements(numNodes, connPtr, conn, numElements, nptr, nelem);
+  std::vector<int64_t> len((size_t)numNodes + 1, 0);
+#pragma omp parallel
+  {
+    std::vector<int> buf;
+#pragma omp for schedule(dynamic, 1024)
+    for (int r = 0; r < numNodes; r++) {
+      row_neighbours(r, nptr, nelem, connPtr, conn, buf);
+      len[(size_t)r + 1] = (int64_t)buf.size();
+    }
+  }
+  for (int r = 0; r < numNodes; r++) len[r + 1] += len[r];
+  const int64_t total = len[numNodes];
+  if (nnzb) *nnzb = total;
+  if (total > INT_MAX) return fail(FEM_ERR_OVERFLOW, "nnzb = %lld does not fit int32 row pointers", (long long)total);
+  if (rowp)
+    for (int r = 0; r <= numNodes; r++) rowp[r] = (int)len[r];
+  if (cols) {
+#pragma omp parallel
+    {
+      std::vector<int> buf;
+#pragma omp for schedule(dynamic, 1024)
+      for (int r = 0; r < numNodes; r++) {
+        row_neighbours(r, nptr, nelem, connPtr, conn, buf);
+        std::copy(buf.begin(), buf.end(), cols + len[r]);
+      }
+    }
+  }
+  return FEM_SUCCESS;
+}
+
+int colour_greedy(int numNodes, const int *connPtr, const int *conn, int numElements, int *colour,
+                  int *numColours) {
+  if (!colour || !numColours) return fail(FEM_ERR_INVALID_ARGUMENT, "colour/numColours is NULL");
+  int st = validate_mesh(numNodes, connPtr, conn, numElements);
+  if (st) return st;
+  std::vector<uint64_t> used((size_t)numNodes, 0);
+  int nc = 0;
+  for (int e = 0; e < numElements; e++) {
+    uint64_t m = 0;
+    for (int i = connPtr[e]; i < connPtr[e + 1]; i++) m |= used[conn[i]];
+    if (~m == 0) return fail(FEM_ERR_UNSUPPORTED, "element %d needs more than 64 colours", e);
+    const int c = __builtin_ctzll(~m);
+    colour[e] = c;
+    nc = std::max(nc, c + 1);
+    for (int i = connPtr[e]; i < connPtr[e + 1]; i++) used[conn[i]] |= (1ull << c);
+  }
+  *numColours = nc;
+  return FEM_SUCCESS;
+}
+
+int build_host_plan(int order, int numNodes, const int *connPtr, const int *conn, int numElements, HostPlan &hp) {
+  const int nn = (order + 1) * (order + 1);
+  int st = validate_mesh(numNodes, connPtr, conn, numElements);
+  if (st) return st;
+  for (int e = 0; e < numElements; e++)
+    if (connPtr[e + 1] - connPtr[e] != nn)
+      return fail(FEM_ERR_INVALID_ARGUMENT, "element %d has %d nodes, order %d needs %d", e,
+                  connPtr[e + 1] - connPtr[e], order, nn);
+  hp.order = order;
+  hp.nn = nn;
+  hp.numNodes = numNodes;
+  hp.numElements = numElements;
+  hp.rowp.resize((size_t)numNodes + 1);
+  st = build_pattern(numNodes, connPtr, conn, numElements, hp.rowp.data(), nullptr, &hp.nnzb);
+  if (st) return st;
+  hp.cols.resize((size_t)hp.nnzb);
+  st = build_pattern(numNodes, connPtr, conn, numElements, hp.rowp.data(), hp.cols.data(), &hp.nnzb);
+  if (st) return st;
+
+  std::vector<int> colour((size_t)numElements);
+  st = colour_greedy(numNodes, connPtr, conn, numElements, colour.data(), &hp.numColours);
+  if (st) return st;
+  hp.colourPtr.assign((size_t)hp.numColours + 1, 0);
+  for (int e = 0; e < numElements; e++) hp.colourPtr[colour[e] + 1]++;
+  for (int c = 0; c < hp.numColours; c++) hp.colourPtr[c + 1] += hp.colourPtr[c];
+  hp.elemList.resize((size_t)numElements);
+  {
+    std::vector<int> fill(hp.colourPtr.begin(), hp.colourPtr.end() - 1);
+    for (int e = 0; e < numElements; e++) hp.elemList[fill[colour[e]]++] = e;
+  }
+  hp.connList.resize((size_t)numElements * nn);
+  hp.blockCode.resize((size_t)numElements * nn * nn);
+  hp.nodeCode.resize((size_t)numElements * nn);
+  std::vector<uint8_t> blockWritten((size_t)hp.nnzb, 0), nodeWritten((size_t)numNodes, 0);
+  int bad = 0;
+  for (int c = 0; c < hp.numColours; c++) {
+    // Elements of one colour share no node, hence no block: the byte flags they
+    // touch are disjoint and the loop is race-free.
+#pragma omp parallel for schedule(static) reduction(| : bad)
+    for (int k = hp.colourPtr[c]; k < hp.colourPtr[c + 1]; k++) {
+      const int e = hp.elemList[k];
+      const int *en = conn + connPtr[e];
+      int *cl = &hp.connList[(size_t)k * nn];
+      for (int a = 0; a < nn; a++) cl[a] = en[a];
+      for (int a = 0; a < nn; a++) {
+        const int r = en[a];
+        uint8_t &nf = nodeWritten[r];
+        hp.nodeCode[(size_t)k * nn + a] = nf ? 0 : 1;
+        nf = 1;
+        const int *c0 = hp.cols.data() + hp.rowp[r], *c1 = hp.cols.data() + hp.rowp[r + 1];
+        for (int b = 0; b < nn; b++) {
+          const int *pos = std::lower_bound(c0, c1, en[b]);
+          const int64_t rank = pos - c0;
+          if (pos == c1 || *pos != en[b] || rank > 127) {
+            bad = 1;
+            continue;
+          }
+          uint8_t &bf = blockWritten[(size_t)(pos - hp.cols.data())];
+          hp.blockCode[((size_t)k * nn + a) * nn + b] = (uint8_t)(rank | (bf ? 0 : 0x80));
+          bf = 1;
+        }
+      }
+    }
+  }
+  if (bad) return fail(FEM_ERR_UNSUPPORTED, "a BSR row holds more than 128 blocks; use the map-based entry points");
+  return FEM_SUCCESS;
+}
+
+}  // namespace fem
+
+extern "C" {
+
+const char *fem_last_error(void) { return fem::last_error_cstr(); }
+
+const char *fem_status_string(int status) {
+  switch (status) {
+    case FEM_SUCCESS: return "success";
+    case FEM_ERR_INVALID_ORDER: return "element order must be 1..4";
+    case FEM_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case FEM_ERR_MISALIGNED: return "array not 16-byte aligned";
+    case FEM_ERR_CUDA: return "CUDA runtime error";
+    case FEM_ERR_OVERFLOW: return "index overflows int32";
+    case FEM_ERR_NOT_FOUND: return "element block missing from BSR pattern";
+    case FEM_ERR_UNSUPPORTED: return "unsupported input";
+    case FEM_ERR_BUDGET: return "device memory budget exhausted";
+    default: return "unknown status";
+  }
+}
+
+int fem_version(void) { return 100; }
+
+int fem_build_bsr_pattern(int numNodes, const int *connPtr, const int *conn, int numElements, int *rowp, int *cols,
+                          int64_t *nnzb) {
+  fem::clear_error();
+  return fem::build_pattern(numNodes, connPtr, conn, numElements, rowp, cols, nnzb);
+}
+
+int fem_build_element_bsr_map(const int *connPtr, const int *conn, int numElements, int nodesPerElement,
+                              const int *rowp, const int *cols, int *map) {
+  fem::clear_error();
+  if (numElements < 0 || nodesPerElement <= 0) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "bad sizes");
+  if (numElements == 0) return FEM_SUCCESS;
+  if (!connPtr || !conn || !rowp || !cols || !map) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "NULL array");
+  const int n = nodesPerElement;
+  int status = FEM_SUCCESS;
+#pragma omp parallel for schedule(static) reduction(max : status)
+  for (int e = 0; e < numElements; e++) {
+    const int *en = conn + connPtr[e];
+    for (int a = 0; a < n; a++) {
+      const int *c0 = cols + rowp[en[a]], *c1 = cols + rowp[en[a] + 1];
+      for (int b = 0; b < n; b++) {
+        const int *pos = std::lower_bound(c0, c1, en[b]);
+        if (pos == c1 || *pos != en[b]) {
+          status = std::max(status, (int)FEM_ERR_NOT_FOUND);
+          continue;
+        }
+        const int64_t off = (int64_t)(pos - cols) * 4;
+        if (off > INT_MAX) {
+          status = std::max(status, (int)FEM_ERR_OVERFLOW);
+          continue;
+        }
+        map[((int64_t)e * n + a) * n + b] = (int)off;
+      }
+    }
+  }
+  if (status == FEM_ERR_NOT_FOUND) return fem::fail(status, "an element block is not in the BSR pattern");
+  if (status == FEM_ERR_OVERFLOW) return fem::fail(status, "block offset*4 exceeds INT32_MAX");
+  return status;
+}
+
+int fem_colour_elements(int numNodes, const int *connPtr, const int *conn, int numElements, int *colour,
+                        int *numColours) {
+  fem::clear_error();
+  return fem::colour_greedy(numNodes, connPtr, conn, numElements, colour, numColours);
+}
+
+}  // extern "C"

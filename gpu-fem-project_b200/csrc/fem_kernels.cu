@@ -1,0 +1,731 @@
+// Element assembly kernels for plane-stress Lagrange quads (orders 1..4) on sm_100a.
+//
+// One CTA processes EPB elements per step of a grid-stride loop (persistent
+// grid sized from the occupancy of the instantiation):
+//   1. gather      node ids, coordinates and states of the EPB elements
+//                  (double2 loads through the read-only path) into shared memory;
+//   2. quad points one thread per (element, q): J, signed detJ, J^-1, the
+//                  real-space state gradient and the weak stress
+//                  S = w*detJ*t*sigma (FP64 always);
+//   3. gradients   one thread per (element, q, node): G = dN*J^-1 and the
+//                  scaled copy H = w*detJ*t*G in the element arithmetic type T;
+//   4. residual    one thread per (element, node): R_a = sum_q S G_a;
+//   5. stiffness   one thread per (element, row tile of p+1 nodes, column node b):
+//                  M_ij[a][b] = sum_q H_ai G_bj for the p+1 rows a of the tile,
+//                  then the 2x2 block
+//                    K_xx = (lam+2mu) M_xx + mu M_yy,  K_xy = lam M_xy + mu M_yx,
+//                    K_yx = lam M_yx + mu M_xy,        K_yy = (lam+2mu) M_yy + mu M_xx.
+// That is the closed form of the reference's per-column forward AD through
+// planeStressWeakRes (element/FEKernels.h:286-315, 884-976): the seed of DOF
+// (b,k) gives weakResDot = w detJ t sigma(e_k (x) G_b), and its transform onto
+// DOF (a,i) is Ke[(a,i),(b,k)] = lam' M_ik + mu M_ki + mu delta_ik (M_xx + M_yy).
+//
+// Scatter: the drop-in mode adds through the reference's element->block map with
+// FP64 atomics (element/FEKernels.h:730-780); the plan mode runs one colour per
+// launch and stores (first contributor) or read-modify-writes (later colours)
+// without atomics.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <mutex>
+#include <utility>
+
+#include "fem_common.h"
+
+namespace fem {
+namespace dev {
+
+// Gauss-Legendre points/weights (element/GaussQuadrature.h:47-100), p+1 per direction.
+__constant__ double kGX[5][5] = {
+    {0.0, 0, 0, 0, 0},
+    {-0.577350269189626, 0.577350269189626, 0, 0, 0},
+    {-0.774596669241483, 0.0, 0.774596669241483, 0, 0},
+    {-0.861136311594053, -0.339981043584856, 0.339981043584856, 0.861136311594053, 0},
+    {-0.906179845938664, -0.538469310105683, 0.0, 0.538469310105683, 0.906179845938664},
+};
+__constant__ double kGW[5][5] = {
+    {2.0, 0, 0, 0, 0},
+    {1.0, 1.0, 0, 0, 0},
+    {5.0 / 9.0, 8.0 / 9.0, 5.0 / 9.0, 0, 0},
+    {0.347854845137454, 0.652145154862546, 0.652145154862546, 0.347854845137454, 0},
+    {0.236926885056189, 0.478628670499366, 0.568888888888889, 0.478628670499366, 0.236926885056189},
+};
+// Cosine-knot Lagrange monomial coefficients, highest power first
+// (element/LagrangeShapeFuncs.h:131-216), [order][node][coefficient].
+__constant__ double kCoef[5][5][5] = {
+    {{0}},
+    {{-0.5, 0.5}, {0.5, 0.5}},
+    {{0.5, -0.5, 0.0}, {-1.0, 0.0, 1.0}, {0.5, 0.5, 0.0}},
+    {{-2.0 / 3.0, 2.0 / 3.0, 1.0 / 6.0, -1.0 / 6.0},
+     {4.0 / 3.0, -2.0 / 3.0, -4.0 / 3.0, 2.0 / 3.0},
+     {-4.0 / 3.0, -2.0 / 3.0, 4.0 / 3.0, 2.0 / 3.0},
+     {2.0 / 3.0, 2.0 / 3.0, -1.0 / 6.0, -1.0 / 6.0}},
+    {{1.0, -1.0, -0.5, 0.5, 0.0},
+     {-2.0, 1.41421356237310, 2.0, -1.41421356237310, 0.0},
+     {2.0, 0.0, -3., 0.0, 1.0},
+     {-2.0, -1.41421356237310, 2.0, 1.41421356237310, 0.0},
+     {1.0, 1.0, -0.5, -0.5, 0.0}},
+};
+
+// lagrangePoly1dDeriv<double,p> (element/LagrangeShapeFuncs.h:129-216) with the
+// rounding of every step pinned, so the table matches the host restatement bit for bit.
+__device__ __forceinline__ void lag1d(int p, double x, int k, double &N, double &dN) {
+  const double *c = kCoef[p][k];
+  if (p == 1) {
+    N = __fma_rn(c[0], x, c[1]);
+    dN = c[0];
+  } else if (p == 2) {
+    N = __fma_rn(c[0], __dmul_rn(x, x), __fma_rn(c[1], x, c[2]));
+    dN = __fma_rn(__dmul_rn(2.0, c[0]), x, c[1]);
+  } else if (p == 3) {
+    const double x2 = __dmul_rn(x, x), x3 = __dmul_rn(x2, x);
+    N = __fma_rn(c[0], x3, __fma_rn(c[1], x2, __fma_rn(c[2], x, c[3])));
+    dN = __fma_rn(__dmul_rn(3.0, c[0]), x2, __fma_rn(__dmul_rn(2.0, c[1]), x, c[2]));
+  } else {
+    const double x2 = __dmul_rn(x, x), x3 = __dmul_rn(x2, x), x4 = __dmul_rn(x2, x2);
+    N = __fma_rn(c[0], x4, __fma_rn(c[1], x3, __fma_rn(c[2], x2, __fma_rn(c[3], x, c[4]))));
+    dN = __fma_rn(__dmul_rn(4.0, c[0]), x3,
+                  __fma_rn(__dmul_rn(3.0, c[1]), x2, __fma_rn(__dmul_rn(2.0, c[2]), x, c[3])));
+  }
+}
+
+template <typename T>
+struct Vec2;
+template <>
+struct Vec2<double> {
+  using type = double2;
+};
+template <>
+struct Vec2<float> {
+  using type = float2;
+};
+
+enum : int { kRes = 1, kJac = 2, kPlan = 4 };
+
+struct AsmArgs {
+  const int *connPtr;      // drop-in: CSR offsets
+  const int *conn;         // drop-in: node ids
+  const int *map;          // drop-in: element block offsets (doubles)
+  const int *connList;     // plan: node ids of the listed elements, nn each
+  const uint8_t *blockCode;  // plan: rank-in-row | 0x80 store flag, nn*nn per listed element
+  const uint8_t *nodeCode;   // plan: 1 store / 0 add, nn per listed element
+  const int *rowp;           // plan: BSR row pointers
+  const double *states;
+  const double *coords;
+  double *residual;
+  double *mat;
+  double mu, lam, t;
+  int64_t begin, count;  // element (or list position) range of this launch
+};
+
+constexpr size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+
+template <int P, typename T, int EPB>
+struct Layout {
+  static constexpr int P1 = P + 1, NN = P1 * P1, NQ = NN;
+  static constexpr size_t T2B = 2 * sizeof(T);
+  static constexpr size_t tab = 0;                               // double2 [NQ][NN]
+  static constexpr size_t tabT = tab + 16 * NQ * NN;             // double2 [NN][NQ]
+  static constexpr size_t wq = tabT + 16 * NQ * NN;              // double  [NQ]
+  static constexpr size_t X = align16(wq + 8 * NQ);              // double2 [EPB][NN]
+  static constexpr size_t U = X + 16 * EPB * NN;                 // double2 [EPB][NN]
+  static constexpr size_t qd = U + 16 * EPB * NN;                // double  [EPB][NQ][8]
+  static constexpr size_t G = qd + 64 * EPB * NQ;                // T2      [EPB][NQ][NN]
+  static constexpr size_t H = G + T2B * EPB * NQ * NN;           // T2      [EPB][NQ][NN]
+  static constexpr size_t nid = align16(H + T2B * EPB * NQ * NN);  // int   [EPB][NN]
+  static constexpr size_t total = align16(nid + 4 * EPB * NN);
+};
+
+template <int P>
+struct Tune {
+  // Elements per CTA step: fills ~256 threads in the stiffness stage
+  // ((p+1)*(p+1)^2 threads per element).
+  static constexpr int EPB = P == 1 ? 32 : P == 2 ? 9 : P == 3 ? 4 : 2;
+  static constexpr int NT = 256;
+};
+
+template <int P, typename T, int MODE, int EPB, int NT>
+__global__ void __launch_bounds__(NT) assemble_kernel(const AsmArgs A) {
+  constexpr int P1 = P + 1, NN = P1 * P1, NQ = NN;
+  using L = Layout<P, T, EPB>;
+  using T2 = typename Vec2<T>::type;
+  extern __shared__ __align__(16) unsigned char smem[];
+  double2 *tab = reinterpret_cast<double2 *>(smem + L::tab);
+  double2 *tabT = reinterpret_cast<double2 *>(smem + L::tabT);
+  double *wq = reinterpret_cast<double *>(smem + L::wq);
+  double2 *X = reinterpret_cast<double2 *>(smem + L::X);
+  double2 *U = reinterpret_cast<double2 *>(smem + L::U);
+  double *qd = reinterpret_cast<double *>(smem + L::qd);
+  T2 *G = reinterpret_cast<T2 *>(smem + L::G);
+  T2 *H = reinterpret_cast<T2 *>(smem + L::H);
+  int *nid = reinterpret_cast<int *>(smem + L::nid);
+
+  const int tid = threadIdx.x;
+  for (int i = tid; i < NQ * NN; i += NT) {
+    const int q = i / NN, a = i - q * NN;
+    double Nx, dNx, Ny, dNy;
+    lag1d(P, kGX[P][q % P1], a % P1, Nx, dNx);
+    lag1d(P, kGX[P][q / P1], a / P1, Ny, dNy);
+    const double2 d = make_double2(__dmul_rn(Ny, dNx), __dmul_rn(Nx, dNy));
+    tab[i] = d;
+    tabT[a * NQ + q] = d;
+  }
+  for (int q = tid; q < NQ; q += NT) wq[q] = __dmul_rn(kGW[P][q % P1], kGW[P][q / P1]);
+
+  const double mu = A.mu, lam = A.lam;
+  const T cMu = T(mu), cLam = T(lam), cC11 = T(lam + 2.0 * mu);
+
+  const int64_t nb = (A.count + EPB - 1) / EPB;
+  for (int64_t batch = blockIdx.x; batch < nb; batch += gridDim.x) {
+    const int64_t k0 = A.begin + batch * EPB;
+    const int ne = (int)min((int64_t)EPB, A.begin + A.count - k0);
+    __syncthreads();  // tables ready / previous step done with shared memory
+
+    // 1. gather
+    for (int i = tid; i < ne * NN; i += NT) {
+      const int el = i / NN, a = i - el * NN;
+      const int64_t k = k0 + el;
+      int node;
+      if constexpr ((MODE & kPlan) != 0) {
+        node = __ldg(A.connList + k * NN + a);
+      } else {
+        node = __ldg(A.conn + __ldg(A.connPtr + k) + a);
+      }
+      nid[i] = node;
+      X[i] = __ldg(reinterpret_cast<const double2 *>(A.coords) + node);
+      U[i] = __ldg(reinterpret_cast<const double2 *>(A.states) + node);
+    }
+    __syncthreads();
+
+    // 2. quadrature-point data (FP64)
+    for (int i = tid; i < ne * NQ; i += NT) {
+      const int el = i / NQ, q = i - el * NQ;
+      double j00 = 0, j01 = 0, j10 = 0, j11 = 0, g00 = 0, g01 = 0, g10 = 0, g11 = 0;
+#pragma unroll
+      for (int a = 0; a < NN; a++) {
+        const double2 d = tabT[a * NQ + q];
+        const double2 x = X[el * NN + a], u = U[el * NN + a];
+        j00 = fma(x.x, d.x, j00);
+        j01 = fma(x.x, d.y, j01);
+        j10 = fma(x.y, d.x, j10);
+        j11 = fma(x.y, d.y, j11);
+        g00 = fma(u.x, d.x, g00);
+        g01 = fma(u.x, d.y, g01);
+        g10 = fma(u.y, d.x, g10);
+        g11 = fma(u.y, d.y, g11);
+      }
+      const double det = j00 * j11 - j01 * j10;
+      const double inv = 1.0 / det;
+      const double i00 = j11 * inv, i01 = -j01 * inv, i10 = -j10 * inv, i11 = j00 * inv;
+      const double uxx = g00 * i00 + g01 * i10, uxy = g00 * i01 + g01 * i11;
+      const double uyx = g10 * i00 + g11 * i10, uyy = g10 * i01 + g11 * i11;
+      const double st = wq[q] * det * A.t;
+      const double tr = uxx + uyy;
+      double *Q = qd + (el * NQ + q) * 8;
+      Q[0] = i00;
+      Q[1] = i01;
+      Q[2] = i10;
+      Q[3] = i11;
+      Q[4] = st * (2.0 * mu * uxx + lam * tr);
+      Q[5] = st * (mu * (uxy + uyx));
+      Q[6] = st * (2.0 * mu * uyy + lam * tr);
+      Q[7] = st;
+    }
+    __syncthreads();
+
+    // 3. real-space shape gradients (only the stiffness stage needs them stored)
+    if constexpr ((MODE & kJac) != 0) {
+      for (int i = tid; i < ne * NQ * NN; i += NT) {
+        const int el = i / (NQ * NN);
+        const int r = i - el * NQ * NN;
+        const int q = r / NN, a = r - q * NN;
+        const double2 d = tab[q * NN + a];
+        const double *Q = qd + (el * NQ + q) * 8;
+        const double gx = d.x * Q[0] + d.y * Q[2];
+        const double gy = d.x * Q[1] + d.y * Q[3];
+        T2 g, h;
+        g.x = T(gx);
+        g.y = T(gy);
+        h.x = T(Q[7] * gx);
+        h.y = T(Q[7] * gy);
+        G[i] = g;
+        H[i] = h;
+      }
+      __syncthreads();
+    }
+
+    // 4. residual R_a = sum_q S(q) G_a(q)
+    if constexpr ((MODE & kRes) != 0) {
+      for (int i = tid; i < ne * NN; i += NT) {
+        const int el = i / NN, a = i - el * NN;
+        T rx = 0, ry = 0;
+#pragma unroll 4
+        for (int q = 0; q < NQ; q++) {
+          const double *Q = qd + (el * NQ + q) * 8;
+          T gx, gy;
+          if constexpr ((MODE & kJac) != 0) {
+            const T2 g = G[(el * NQ + q) * NN + a];
+            gx = g.x;
+            gy = g.y;
+          } else {
+            const double2 d = tab[q * NN + a];
+            gx = T(d.x * Q[0] + d.y * Q[2]);
+            gy = T(d.x * Q[1] + d.y * Q[3]);
+          }
+          const T sxx = T(Q[4]), sxy = T(Q[5]), syy = T(Q[6]);
+          rx = fma(sxx, gx, fma(sxy, gy, rx));
+          ry = fma(sxy, gx, fma(syy, gy, ry));
+        }
+        double *dst = A.residual + 2 * (int64_t)nid[i];
+        if constexpr ((MODE & kPlan) != 0) {
+          const int64_t k = k0 + el;
+          if (__ldg(A.nodeCode + k * NN + a)) {
+            *reinterpret_cast<double2 *>(dst) = make_double2(double(rx), double(ry));
+          } else {
+            double2 v = *reinterpret_cast<double2 *>(dst);
+            v.x += double(rx);
+            v.y += double(ry);
+            *reinterpret_cast<double2 *>(dst) = v;
+          }
+        } else {
+          atomicAdd(dst, double(rx));
+          atomicAdd(dst + 1, double(ry));
+        }
+      }
+    }
+
+    // 5. element stiffness, one row tile of P1 nodes x one column node per thread
+    if constexpr ((MODE & kJac) != 0) {
+      for (int i = tid; i < ne * P1 * NN; i += NT) {
+        const int el = i / (P1 * NN);
+        const int r = i - el * P1 * NN;
+        const int at = r / NN, b = r - at * NN;
+        T m[P1][4];
+#pragma unroll
+        for (int ax = 0; ax < P1; ax++) m[ax][0] = m[ax][1] = m[ax][2] = m[ax][3] = T(0);
+        const T2 *Gb = G + el * NQ * NN + b;
+        const T2 *Ha = H + el * NQ * NN + at * P1;
+#pragma unroll 2
+        for (int q = 0; q < NQ; q++) {
+          const T2 g = Gb[q * NN];
+#pragma unroll
+          for (int ax = 0; ax < P1; ax++) {
+            const T2 h = Ha[q * NN + ax];
+            m[ax][0] = fma(h.x, g.x, m[ax][0]);
+            m[ax][1] = fma(h.x, g.y, m[ax][1]);
+            m[ax][2] = fma(h.y, g.x, m[ax][2]);
+            m[ax][3] = fma(h.y, g.y, m[ax][3]);
+          }
+        }
+        const int64_t k = k0 + el;
+#pragma unroll
+        for (int ax = 0; ax < P1; ax++) {
+          const int a = at * P1 + ax;
+          const T kxx = cC11 * m[ax][0] + cMu * m[ax][3];
+          const T kxy = cLam * m[ax][1] + cMu * m[ax][2];
+          const T kyx = cLam * m[ax][2] + cMu * m[ax][1];
+          const T kyy = cC11 * m[ax][3] + cMu * m[ax][0];
+          if constexpr ((MODE & kPlan) != 0) {
+            const uint8_t code = __ldg(A.blockCode + (k * NN + a) * NN + b);
+            const int row = nid[el * NN + a];
+            double *blk = A.mat + 4 * ((int64_t)__ldg(A.rowp + row) + (code & 0x7f));
+            double2 *b2 = reinterpret_cast<double2 *>(blk);
+            if (code & 0x80) {
+              b2[0] = make_double2(double(kxx), double(kxy));
+              b2[1] = make_double2(double(kyx), double(kyy));
+            } else {
+              double2 v0 = b2[0], v1 = b2[1];
+              v0.x += double(kxx);
+              v0.y += double(kxy);
+              v1.x += double(kyx);
+              v1.y += double(kyy);
+              b2[0] = v0;
+              b2[1] = v1;
+            }
+          } else {
+            double *blk = A.mat + __ldg(A.map + (k * NN + a) * NN + b);
+            atomicAdd(blk + 0, double(kxx));
+            atomicAdd(blk + 1, double(kxy));
+            atomicAdd(blk + 2, double(kyx));
+            atomicAdd(blk + 3, double(kyy));
+          }
+        }
+      }
+    }
+  }
+}
+
+// y = A x, 2x2 BSR, eight lanes per block row.
+__global__ void __launch_bounds__(256) bsr_spmv_kernel(int numRows, const int *__restrict__ rowp,
+                                                       const int *__restrict__ cols, const double *__restrict__ Av,
+                                                       const double *__restrict__ x, double *__restrict__ y) {
+  const int lane = threadIdx.x & 7;
+  const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+  if (row >= numRows) return;
+  double y0 = 0, y1 = 0;
+  const int b0 = __ldg(rowp + row), b1 = __ldg(rowp + row + 1);
+  for (int j = b0 + lane; j < b1; j += 8) {
+    const double2 *blk = reinterpret_cast<const double2 *>(Av) + 2 * (int64_t)j;
+    const double2 r0 = __ldg(blk), r1 = __ldg(blk + 1);
+    const double2 xv = __ldg(reinterpret_cast<const double2 *>(x) + __ldg(cols + j));
+    y0 = fma(r0.x, xv.x, fma(r0.y, xv.y, y0));
+    y1 = fma(r1.x, xv.x, fma(r1.y, xv.y, y1));
+  }
+#pragma unroll
+  for (int o = 4; o > 0; o >>= 1) {
+    y0 += __shfl_down_sync(0xffffffffu, y0, o, 8);
+    y1 += __shfl_down_sync(0xffffffffu, y1, o, 8);
+  }
+  if (lane == 0) reinterpret_cast<double2 *>(y)[row] = make_double2(y0, y1);
+}
+
+}  // namespace dev
+
+// ---------------------------------------------------------------------------------------
+// Host-side launch machinery
+// ---------------------------------------------------------------------------------------
+namespace {
+
+struct LaunchInfo {
+  int grid_per_sm = 0;
+  int num_sms = 0;
+};
+
+std::mutex g_mu;
+std::map<std::pair<const void *, int>, LaunchInfo> g_info;
+
+int cuda_fail(cudaError_t err, const char *what) {
+  return fail(FEM_ERR_CUDA, "%s: %s", what, cudaGetErrorString(err));
+}
+
+// Occupancy-sized persistent grid; sets the dynamic shared-memory opt-in once per device.
+template <typename K>
+int launch_info(K kernel, int nt, size_t smem, LaunchInfo &out) {
+  int dev = 0;
+  cudaError_t err = cudaGetDevice(&dev);
+  if (err != cudaSuccess) return cuda_fail(err, "cudaGetDevice");
+  std::lock_guard<std::mutex> lk(g_mu);
+  auto key = std::make_pair(reinterpret_cast<const void *>(kernel), dev);
+  auto it = g_info.find(key);
+  if (it != g_info.end()) {
+    out = it->second;
+    return FEM_SUCCESS;
+  }
+  err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (err != cudaSuccess) return cuda_fail(err, "cudaFuncSetAttribute");
+  LaunchInfo li;
+  err = cudaDeviceGetAttribute(&li.num_sms, cudaDevAttrMultiProcessorCount, dev);
+  if (err != cudaSuccess) return cuda_fail(err, "cudaDeviceGetAttribute");
+  err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&li.grid_per_sm, kernel, nt, smem);
+  if (err != cudaSuccess) return cuda_fail(err, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+  if (li.grid_per_sm < 1) return fail(FEM_ERR_CUDA, "kernel does not fit on an SM (smem %zu B)", smem);
+  g_info[key] = li;
+  out = li;
+  return FEM_SUCCESS;
+}
+
+template <int P, typename T, int MODE>
+int launch_p(const dev::AsmArgs &a, cudaStream_t s) {
+  constexpr int EPB = dev::Tune<P>::EPB, NT = dev::Tune<P>::NT;
+  auto kernel = dev::assemble_kernel<P, T, MODE, EPB, NT>;
+  const size_t smem = dev::Layout<P, T, EPB>::total;
+  LaunchInfo li;
+  int st = launch_info(kernel, NT, smem, li);
+  if (st) return st;
+  const int64_t nb = (a.count + EPB - 1) / EPB;
+  const int64_t cap = (int64_t)li.grid_per_sm * li.num_sms;
+  const int grid = (int)(nb < cap ? nb : cap);
+  if (grid <= 0) return FEM_SUCCESS;
+  kernel<<<grid, NT, smem, s>>>(a);
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return cuda_fail(err, "assemble_kernel launch");
+  return FEM_SUCCESS;
+}
+
+template <typename T, int MODE>
+int launch_mode(int order, const dev::AsmArgs &a, cudaStream_t s) {
+  switch (order) {
+    case 1: return launch_p<1, T, MODE>(a, s);
+    case 2: return launch_p<2, T, MODE>(a, s);
+    case 3: return launch_p<3, T, MODE>(a, s);
+    case 4: return launch_p<4, T, MODE>(a, s);
+    default: return fail(FEM_ERR_INVALID_ORDER, "element order %d (supported: 1..4)", order);
+  }
+}
+
+template <typename T>
+int launch_any(int order, int mode, const dev::AsmArgs &a, cudaStream_t s) {
+  using namespace dev;
+  switch (mode) {
+    case kRes: return launch_mode<T, kRes>(order, a, s);
+    case kJac: return launch_mode<T, kJac>(order, a, s);
+    case kRes | kJac: return launch_mode<T, kRes | kJac>(order, a, s);
+    case kPlan | kRes: return launch_mode<T, kPlan | kRes>(order, a, s);
+    case kPlan | kJac: return launch_mode<T, kPlan | kJac>(order, a, s);
+    case kPlan | kRes | kJac: return launch_mode<T, kPlan | kRes | kJac>(order, a, s);
+    default: return fail(FEM_ERR_INVALID_ARGUMENT, "bad kernel mode %d", mode);
+  }
+}
+
+int launch(int order, int precision, int mode, const dev::AsmArgs &a, cudaStream_t s) {
+  if (precision == FEM_PRECISION_FP64) return launch_any<double>(order, mode, a, s);
+  if (precision == FEM_PRECISION_MIXED) return launch_any<float>(order, mode, a, s);
+  return fail(FEM_ERR_INVALID_ARGUMENT, "precision %d", precision);
+}
+
+void set_material(dev::AsmArgs &a, double E, double nu, double t) {
+  // element/FEKernels.h:300-301
+  a.mu = 0.5 * E / (1.0 + nu);
+  a.lam = 2 * a.mu * nu / (1.0 - nu);
+  a.t = t;
+}
+
+// Runs `body` on `stream`; with elapsed != NULL brackets it with events and synchronises.
+template <typename F>
+int timed(cudaStream_t s, double *elapsed, F body) {
+  if (!elapsed) return body();
+  cudaEvent_t e0, e1;
+  cudaError_t err = cudaEventCreate(&e0);
+  if (err != cudaSuccess) return cuda_fail(err, "cudaEventCreate");
+  err = cudaEventCreate(&e1);
+  if (err != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return cuda_fail(err, "cudaEventCreate");
+  }
+  int st = FEM_SUCCESS;
+  err = cudaEventRecord(e0, s);
+  if (err != cudaSuccess) st = cuda_fail(err, "cudaEventRecord");
+  if (!st) st = body();
+  if (!st && (err = cudaEventRecord(e1, s)) != cudaSuccess) st = cuda_fail(err, "cudaEventRecord");
+  if (!st && (err = cudaEventSynchronize(e1)) != cudaSuccess) st = cuda_fail(err, "kernel execution");
+  float ms = 0.f;
+  if (!st && (err = cudaEventElapsedTime(&ms, e0, e1)) != cudaSuccess) st = cuda_fail(err, "cudaEventElapsedTime");
+  *elapsed = st ? 0.0 : ms * 1e-3;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return st;
+}
+
+int run_dropin(int precision, bool jac, int order, const int *connPtr, const int *conn, int numElements,
+               const double *states, const double *coords, double E, double nu, double t, const int *map,
+               double *residual, double *mat, void *stream, double *elapsed) {
+  clear_error();
+  if (elapsed) *elapsed = 0.0;
+  if (order < 1 || order > 4) return fail(FEM_ERR_INVALID_ORDER, "element order %d (supported: 1..4)", order);
+  if (numElements < 0) return fail(FEM_ERR_INVALID_ARGUMENT, "numElements < 0");
+  if (numElements == 0) return FEM_SUCCESS;
+  if (!connPtr || !conn || !states || !coords) return fail(FEM_ERR_INVALID_ARGUMENT, "NULL input array");
+  if (jac && (!map || !mat)) return fail(FEM_ERR_INVALID_ARGUMENT, "NULL map or matEntries");
+  if (!jac && !residual) return fail(FEM_ERR_INVALID_ARGUMENT, "NULL residual");
+  if (!aligned16(states) || !aligned16(coords) || (residual && !aligned16(residual)))
+    return fail(FEM_ERR_MISALIGNED, "states, nodeCoords and residual must be 16-byte aligned");
+  if (mat && (reinterpret_cast<uintptr_t>(mat) & 7u)) return fail(FEM_ERR_MISALIGNED, "matEntries not 8-byte aligned");
+  dev::AsmArgs a{};
+  a.connPtr = connPtr;
+  a.conn = conn;
+  a.map = map;
+  a.states = states;
+  a.coords = coords;
+  a.residual = residual;
+  a.mat = mat;
+  a.begin = 0;
+  a.count = numElements;
+  set_material(a, E, nu, t);
+  const int mode = (jac ? dev::kJac : 0) | (residual ? dev::kRes : 0);
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  return timed(s, elapsed, [&] { return launch(order, precision, mode, a, s); });
+}
+
+}  // namespace
+}  // namespace fem
+
+// ---------------------------------------------------------------------------------------
+// Plans
+// ---------------------------------------------------------------------------------------
+struct fem_plan {
+  int device = 0;
+  int order = 0, nn = 0, numNodes = 0, numElements = 0, numColours = 0;
+  int64_t nnzb = 0;
+  std::vector<int> colourPtr;
+  int *d_rowp = nullptr, *d_cols = nullptr, *d_connList = nullptr;
+  uint8_t *d_blockCode = nullptr, *d_nodeCode = nullptr;
+  int64_t deviceBytes = 0;
+};
+
+namespace {
+void plan_free(fem_plan *p) {
+  if (!p) return;
+  int cur = 0;
+  cudaGetDevice(&cur);
+  cudaSetDevice(p->device);
+  cudaFree(p->d_rowp);
+  cudaFree(p->d_cols);
+  cudaFree(p->d_connList);
+  cudaFree(p->d_blockCode);
+  cudaFree(p->d_nodeCode);
+  cudaSetDevice(cur);
+  delete p;
+}
+
+template <typename V>
+int upload(const std::vector<V> &h, V **d, int64_t &bytes) {
+  const size_t n = h.size() * sizeof(V);
+  cudaError_t err = cudaMalloc(reinterpret_cast<void **>(d), n ? n : 16);
+  if (err != cudaSuccess) return fem::fail(FEM_ERR_CUDA, "cudaMalloc(%zu): %s", n, cudaGetErrorString(err));
+  bytes += (int64_t)n;
+  if (n) {
+    err = cudaMemcpy(*d, h.data(), n, cudaMemcpyHostToDevice);
+    if (err != cudaSuccess) return fem::fail(FEM_ERR_CUDA, "cudaMemcpy: %s", cudaGetErrorString(err));
+  }
+  return FEM_SUCCESS;
+}
+}  // namespace
+
+extern "C" {
+
+int fem_run_residual(int elementOrder, const int *connPtr, const int *conn, int numElements, const double *states,
+                     const double *nodeCoords, double E, double nu, double t, double *residual, void *stream,
+                     double *elapsedSeconds) {
+  return fem::run_dropin(FEM_PRECISION_FP64, false, elementOrder, connPtr, conn, numElements, states, nodeCoords, E,
+                         nu, t, nullptr, residual, nullptr, stream, elapsedSeconds);
+}
+
+int fem_run_jacobian(int elementOrder, const int *connPtr, const int *conn, int numElements, const double *states,
+                     const double *nodeCoords, double E, double nu, double t, const int *elementBCSRMap,
+                     double *residual, double *matEntries, void *stream, double *elapsedSeconds) {
+  return fem::run_dropin(FEM_PRECISION_FP64, true, elementOrder, connPtr, conn, numElements, states, nodeCoords, E,
+                         nu, t, elementBCSRMap, residual, matEntries, stream, elapsedSeconds);
+}
+
+int fem_run_residual_mixed(int elementOrder, const int *connPtr, const int *conn, int numElements,
+                           const double *states, const double *nodeCoords, double E, double nu, double t,
+                           double *residual, void *stream, double *elapsedSeconds) {
+  return fem::run_dropin(FEM_PRECISION_MIXED, false, elementOrder, connPtr, conn, numElements, states, nodeCoords, E,
+                         nu, t, nullptr, residual, nullptr, stream, elapsedSeconds);
+}
+
+int fem_run_jacobian_mixed(int elementOrder, const int *connPtr, const int *conn, int numElements,
+                           const double *states, const double *nodeCoords, double E, double nu, double t,
+                           const int *elementBCSRMap, double *residual, double *matEntries, void *stream,
+                           double *elapsedSeconds) {
+  return fem::run_dropin(FEM_PRECISION_MIXED, true, elementOrder, connPtr, conn, numElements, states, nodeCoords, E,
+                         nu, t, elementBCSRMap, residual, matEntries, stream, elapsedSeconds);
+}
+
+int fem_bsr_spmv(int numRows, const int *rowp, const int *cols, const double *A, const double *x, double *y,
+                 void *stream) {
+  fem::clear_error();
+  if (numRows < 0) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "numRows < 0");
+  if (numRows == 0) return FEM_SUCCESS;
+  if (!rowp || !cols || !A || !x || !y) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "NULL array");
+  if (!fem::aligned16(A) || !fem::aligned16(x) || !fem::aligned16(y))
+    return fem::fail(FEM_ERR_MISALIGNED, "A, x, y must be 16-byte aligned");
+  const int64_t threads = (int64_t)numRows * 8;
+  const int grid = (int)((threads + 255) / 256);
+  fem::dev::bsr_spmv_kernel<<<grid, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(numRows, rowp, cols, A, x, y);
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return fem::cuda_fail(err, "bsr_spmv launch");
+  return FEM_SUCCESS;
+}
+
+int fem_plan_create(int elementOrder, int numNodes, const int *connPtr, const int *conn, int numElements,
+                    fem_plan **plan) {
+  fem::clear_error();
+  if (!plan) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "plan is NULL");
+  *plan = nullptr;
+  if (elementOrder < 1 || elementOrder > 4) return fem::fail(FEM_ERR_INVALID_ORDER, "element order %d", elementOrder);
+  fem::HostPlan hp;
+  int st = fem::build_host_plan(elementOrder, numNodes, connPtr, conn, numElements, hp);
+  if (st) return st;
+  fem_plan *p = new fem_plan();
+  cudaGetDevice(&p->device);
+  p->order = hp.order;
+  p->nn = hp.nn;
+  p->numNodes = hp.numNodes;
+  p->numElements = hp.numElements;
+  p->numColours = hp.numColours;
+  p->nnzb = hp.nnzb;
+  p->colourPtr = hp.colourPtr;
+  if ((st = upload(hp.rowp, &p->d_rowp, p->deviceBytes)) || (st = upload(hp.cols, &p->d_cols, p->deviceBytes)) ||
+      (st = upload(hp.connList, &p->d_connList, p->deviceBytes)) ||
+      (st = upload(hp.blockCode, &p->d_blockCode, p->deviceBytes)) ||
+      (st = upload(hp.nodeCode, &p->d_nodeCode, p->deviceBytes))) {
+    plan_free(p);
+    return st;
+  }
+  *plan = p;
+  return FEM_SUCCESS;
+}
+
+int fem_plan_destroy(fem_plan *plan) {
+  fem::clear_error();
+  plan_free(plan);
+  return FEM_SUCCESS;
+}
+
+int fem_plan_info(const fem_plan *plan, int *numNodes, int *numElements, int64_t *nnzb, int *numColours,
+                  int64_t *deviceBytes) {
+  fem::clear_error();
+  if (!plan) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "plan is NULL");
+  if (numNodes) *numNodes = plan->numNodes;
+  if (numElements) *numElements = plan->numElements;
+  if (nnzb) *nnzb = plan->nnzb;
+  if (numColours) *numColours = plan->numColours;
+  if (deviceBytes) *deviceBytes = plan->deviceBytes;
+  return FEM_SUCCESS;
+}
+
+int fem_plan_get_pattern(const fem_plan *plan, int *rowp, int *cols) {
+  fem::clear_error();
+  if (!plan || !rowp || !cols) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "NULL argument");
+  cudaError_t err = cudaMemcpy(rowp, plan->d_rowp, sizeof(int) * ((size_t)plan->numNodes + 1), cudaMemcpyDeviceToHost);
+  if (err == cudaSuccess) err = cudaMemcpy(cols, plan->d_cols, sizeof(int) * (size_t)plan->nnzb, cudaMemcpyDeviceToHost);
+  if (err != cudaSuccess) return fem::cuda_fail(err, "cudaMemcpy");
+  return FEM_SUCCESS;
+}
+
+int fem_plan_device_pattern(const fem_plan *plan, const int **rowp, const int **cols) {
+  fem::clear_error();
+  if (!plan) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "plan is NULL");
+  if (rowp) *rowp = plan->d_rowp;
+  if (cols) *cols = plan->d_cols;
+  return FEM_SUCCESS;
+}
+
+int fem_plan_assemble(const fem_plan *plan, const double *states, const double *nodeCoords, double E, double nu,
+                      double t, double *residual, double *matEntries, int precision, void *stream,
+                      double *elapsedSeconds) {
+  fem::clear_error();
+  if (elapsedSeconds) *elapsedSeconds = 0.0;
+  if (!plan) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "plan is NULL");
+  if (!states || !nodeCoords) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "NULL input array");
+  if (!residual && !matEntries) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "no output requested");
+  if (!fem::aligned16(states) || !fem::aligned16(nodeCoords) || (residual && !fem::aligned16(residual)) ||
+      (matEntries && !fem::aligned16(matEntries)))
+    return fem::fail(FEM_ERR_MISALIGNED, "all arrays must be 16-byte aligned");
+  if (plan->numElements == 0) return FEM_SUCCESS;
+  fem::dev::AsmArgs a{};
+  a.connList = plan->d_connList;
+  a.blockCode = plan->d_blockCode;
+  a.nodeCode = plan->d_nodeCode;
+  a.rowp = plan->d_rowp;
+  a.states = states;
+  a.coords = nodeCoords;
+  a.residual = residual;
+  a.mat = matEntries;
+  fem::set_material(a, E, nu, t);
+  const int mode = fem::dev::kPlan | (residual ? fem::dev::kRes : 0) | (matEntries ? fem::dev::kJac : 0);
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  return fem::timed(s, elapsedSeconds, [&] {
+    for (int c = 0; c < plan->numColours; c++) {
+      a.begin = plan->colourPtr[c];
+      a.count = plan->colourPtr[c + 1] - plan->colourPtr[c];
+      int st = fem::launch(plan->order, precision, mode, a, s);
+      if (st) return st;
+    }
+    return (int)FEM_SUCCESS;
+  });
+}
+
+}  // extern "C"

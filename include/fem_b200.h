@@ -1,0 +1,137 @@
+/*
+ * fem_b200.h -- C ABI of the B200 plane-stress quad assembly library (libfemb200.so).
+ *
+ * Global residual and 2x2-block BSR Jacobian assembly for 2D plane-stress
+ * Lagrange quadrilaterals of order 1..4, (p+1)x(p+1) Gauss points, linear
+ * strain.  All array arguments are plain pointers; no C++ or torch types cross
+ * this boundary.
+ *
+ * Conventions shared with A-CGray/GPU-FEM-Project (element/FEKernels.h):
+ *   - nodeCoords[node*2 + d] and states[node*2 + s]: node-major, 2 values per node.
+ *   - connPtr (CSR offsets) and conn (int32 node ids); element e's local node
+ *     a = ay*(p+1) + ax is conn[connPtr[e] + a] (tensor-product order).
+ *   - residual[node*2 + s]; BSR values are 2x2 row-major blocks:
+ *     matEntries[blk*4 + i*2 + j] couples DOF (row node, i) with (col node, j).
+ *   - elementBCSRMap[e*n*n + a*n + b] is the offset (in doubles, = block index*4)
+ *     of the block coupling local nodes a and b (verification/TACSHelpers.h:133-137).
+ *
+ * Every entry point returns a status (FEM_SUCCESS == 0) instead of exiting the
+ * process.  Device-side entry points take DEVICE pointers (as the reference's
+ * nvcc build does), must be 16-byte aligned for coordinate/state/output arrays,
+ * and are asynchronous on `stream` (a cudaStream_t, NULL = legacy default
+ * stream) unless elapsedSeconds is non-NULL, in which case the call records
+ * CUDA events around the launch, synchronises the stream and returns the
+ * device time in seconds (the reference always synchronised and returned seconds).
+ */
+#ifndef FEM_B200_H
+#define FEM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------------------- */
+#define FEM_SUCCESS 0
+#define FEM_ERR_INVALID_ORDER 1    /* element order outside 1..4 (reference: silent no-op)   */
+#define FEM_ERR_INVALID_ARGUMENT 2 /* NULL where data is required, negative sizes, ...      */
+#define FEM_ERR_MISALIGNED 3       /* a double array is not 16-byte aligned                 */
+#define FEM_ERR_CUDA 4             /* a CUDA runtime call failed; see fem_last_error()      */
+#define FEM_ERR_OVERFLOW 5         /* an index does not fit the int32 format                */
+#define FEM_ERR_NOT_FOUND 6        /* an element block is missing from the BSR pattern      */
+#define FEM_ERR_UNSUPPORTED 7      /* input outside what this entry point supports          */
+#define FEM_ERR_BUDGET 8           /* device-memory budget exhausted (serving admission)    */
+
+#define FEM_PRECISION_FP64 0  /* all element arithmetic in FP64                               */
+#define FEM_PRECISION_MIXED 1 /* FP64 J/detJ/J^-1 and FP64 accumulate, FP32 element products */
+
+const char *fem_status_string(int status);
+/* Message describing the last failure on the calling host thread ("" if none). */
+const char *fem_last_error(void);
+/* Library version: major*10000 + minor*100 + patch. */
+int fem_version(void);
+
+/* ---- drop-in entry points (device pointers, accumulate-into) -------------------------- */
+
+/* Replaces runResidualKernel (element/FEKernels.h:1030-1102).  Adds the element
+ * residuals into `residual` (the caller zeroes it first, as the reference's
+ * driver does, verification/TestKernels.cpp:237). */
+int fem_run_residual(int elementOrder, const int *connPtr, const int *conn, int numElements, const double *states,
+                     const double *nodeCoords, double E, double nu, double t, double *residual, void *stream,
+                     double *elapsedSeconds);
+
+/* Replaces runJacobianKernel (element/FEKernels.h:1125-1225).  Adds the element
+ * matrices into matEntries through elementBCSRMap and, when residual != NULL,
+ * the element residuals into residual (FEKernels.h:996). */
+int fem_run_jacobian(int elementOrder, const int *connPtr, const int *conn, int numElements, const double *states,
+                     const double *nodeCoords, double E, double nu, double t, const int *elementBCSRMap,
+                     double *residual, double *matEntries, void *stream, double *elapsedSeconds);
+
+/* Same contracts as the two above with FEM_PRECISION_MIXED element arithmetic
+ * (no reference counterpart: the reference is FP64 only). */
+int fem_run_residual_mixed(int elementOrder, const int *connPtr, const int *conn, int numElements,
+                           const double *states, const double *nodeCoords, double E, double nu, double t,
+                           double *residual, void *stream, double *elapsedSeconds);
+int fem_run_jacobian_mixed(int elementOrder, const int *connPtr, const int *conn, int numElements,
+                           const double *states, const double *nodeCoords, double E, double nu, double t,
+                           const int *elementBCSRMap, double *residual, double *matEntries, void *stream,
+                           double *elapsedSeconds);
+
+/* ---- host-side setup helpers (HOST pointers) ------------------------------------------- */
+
+/* BSR sparsity of the nodal adjacency: row r lists, ascending, every node that
+ * shares an element with node r (itself included).  This is the pattern TACS
+ * hands the reference driver (verification/TestKernels.cpp:105-115).  Call with
+ * cols == NULL to obtain *nnzb only; rowp has numNodes+1 entries. */
+int fem_build_bsr_pattern(int numNodes, const int *connPtr, const int *conn, int numElements, int *rowp, int *cols,
+                          int64_t *nnzb);
+
+/* Replaces generateElementBCSRMap (verification/TACSHelpers.h:138-182):
+ * map[e*n*n + a*n + b] = (position of conn[b] in row conn[a]) * 4.
+ * FEM_ERR_NOT_FOUND if a block is missing, FEM_ERR_OVERFLOW if an offset
+ * exceeds INT32_MAX. */
+int fem_build_element_bsr_map(const int *connPtr, const int *conn, int numElements, int nodesPerElement,
+                              const int *rowp, const int *cols, int *map);
+
+/* Deterministic greedy element colouring in element order: no two elements of
+ * one colour share a node.  colour has numElements entries.  (No reference
+ * counterpart: the reference scatters with atomics only.) */
+int fem_colour_elements(int numNodes, const int *connPtr, const int *conn, int numElements, int *colour,
+                        int *numColours);
+
+/* y = A x for a 2x2-block BSR matrix on the device (rowp/cols/A/x/y device
+ * pointers).  Consumer of the assembled Jacobian (the reference exports the
+ * same BCSR layout to TACS, verification/TestKernels.cpp:113-121). */
+int fem_bsr_spmv(int numRows, const int *rowp, const int *cols, const double *A, const double *x, double *y,
+                 void *stream);
+
+/* ---- assembly plans: overwrite semantics, colour-ordered, no map ---------------------- */
+/* A plan owns device copies of the mesh topology, its BSR pattern, an element
+ * colouring and compact per-element block codes.  fem_plan_assemble writes the
+ * COMPLETE residual and matrix (no zeroing by the caller and no atomics): within
+ * a colour no two elements share a node, and the first contributor to each
+ * block stores while later colours add.  (No reference counterpart.) */
+typedef struct fem_plan fem_plan;
+
+int fem_plan_create(int elementOrder, int numNodes, const int *connPtr, const int *conn, int numElements,
+                    fem_plan **plan);
+int fem_plan_destroy(fem_plan *plan);
+/* Sizes: numNodes, numElements, nnzb, numColours, device bytes held. */
+int fem_plan_info(const fem_plan *plan, int *numNodes, int *numElements, int64_t *nnzb, int *numColours,
+                  int64_t *deviceBytes);
+/* Copy the plan's BSR pattern to host arrays (rowp: numNodes+1, cols: nnzb). */
+int fem_plan_get_pattern(const fem_plan *plan, int *rowp, int *cols);
+/* Device pointers of the plan's rowp/cols (owned by the plan). */
+int fem_plan_device_pattern(const fem_plan *plan, const int **rowp, const int **cols);
+/* states/nodeCoords/residual/matEntries are device pointers; residual or
+ * matEntries may be NULL to skip that output.  precision: FEM_PRECISION_*. */
+int fem_plan_assemble(const fem_plan *plan, const double *states, const double *nodeCoords, double E, double nu,
+                      double t, double *residual, double *matEntries, int precision, void *stream,
+                      double *elapsedSeconds);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FEM_B200_H */

@@ -1,0 +1,151 @@
+"""ctypes wrapper of the FP64 CPU oracle (oracle/libfemoracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by the smoke check in
+__graft_entry__.py and by the CPU-baseline leg of bench.py, where it is the
+checker or the timed CPU reference -- never part of the product path.
+See fem_oracle.cpp for what is restated from which reference file:line and for
+the pinning status (tables pinned against the reference's own headers; element
+physics not pinned by reference outputs).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import pathlib
+import subprocess
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+LIB_PATH = HERE / "libfemoracle.so"
+
+
+def build() -> pathlib.Path:
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB_PATH
+
+
+def _load():
+    if not LIB_PATH.exists():
+        build()
+    lib = C.CDLL(str(LIB_PATH))
+    p, i, i64, d = C.c_void_p, C.c_int, C.c_int64, C.c_double
+    lib.oracle_tables.argtypes = [i, p, p, p]
+    lib.oracle_lagrange1d.argtypes = [i, i, p, p, p]
+    lib.oracle_element.argtypes = [i, p, p, d, d, d, p, p]
+    lib.oracle_assemble.argtypes = [i, p, p, i64, p, p, d, d, d, p, p, p]
+    lib.oracle_assemble_parallel.argtypes = [i, p, p, i64, p, p, d, d, d, p, p, p]
+    lib.oracle_bsr_pattern.argtypes = [i, p, p, i64, p, p]
+    lib.oracle_bsr_pattern.restype = i64
+    lib.oracle_element_bsr_map.argtypes = [p, p, i64, i, p, p, p]
+    lib.oracle_element_bsr_map.restype = i64
+    lib.oracle_check_colouring.argtypes = [i, p, p, i64, p, i]
+    lib.oracle_check_colouring.restype = i64
+    lib.oracle_bsr_spmv.argtypes = [i, p, p, p, p, p]
+    lib.oracle_set_num_threads.argtypes = [i]
+    return lib
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = _load()
+    return _lib
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+def _c(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+def set_threads(n: int) -> None:
+    lib().oracle_set_num_threads(int(n))
+
+
+def num_threads() -> int:
+    return int(lib().oracle_num_threads())
+
+
+def tables(p: int):
+    """(xi[p+1], w[p+1], dN[(p+1)^2, (p+1)^2, 2]) with q = qy*(p+1)+qx, a = ay*(p+1)+ax."""
+    n = (p + 1) ** 2
+    xi, w, dN = np.zeros(p + 1), np.zeros(p + 1), np.zeros((n, n, 2))
+    assert lib().oracle_tables(p, _ptr(xi), _ptr(w), _ptr(dN)) == 0
+    return xi, w, dN
+
+
+def lagrange1d(p: int, x):
+    x = _c(x, np.float64)
+    N = np.zeros((x.size, p + 1))
+    dN = np.zeros((x.size, p + 1))
+    assert lib().oracle_lagrange1d(p, x.size, _ptr(x), _ptr(N), _ptr(dN)) == 0
+    return N, dN
+
+
+def element(p: int, X, U, E: float, nu: float, t: float):
+    """Element residual [2n] and stiffness [2n, 2n] for node coords X [n,2], states U [n,2]."""
+    n = (p + 1) ** 2
+    X, U = _c(X, np.float64), _c(U, np.float64)
+    Re, Ke = np.zeros(2 * n), np.zeros((2 * n, 2 * n))
+    assert lib().oracle_element(p, _ptr(X), _ptr(U), E, nu, t, _ptr(Re), _ptr(Ke)) == 0
+    return Re, Ke
+
+
+def bsr_pattern(num_nodes: int, conn_ptr, conn):
+    conn_ptr, conn = _c(conn_ptr, np.int32), _c(conn, np.int32)
+    ne = conn_ptr.size - 1
+    nnz = lib().oracle_bsr_pattern(num_nodes, _ptr(conn_ptr), _ptr(conn), ne, None, None)
+    rowp = np.zeros(num_nodes + 1, np.int32)
+    cols = np.zeros(nnz, np.int32)
+    lib().oracle_bsr_pattern(num_nodes, _ptr(conn_ptr), _ptr(conn), ne, _ptr(rowp), _ptr(cols))
+    return rowp, cols
+
+
+def element_bsr_map(conn_ptr, conn, nodes_per_element: int, rowp, cols):
+    conn_ptr, conn = _c(conn_ptr, np.int32), _c(conn, np.int32)
+    rowp, cols = _c(rowp, np.int32), _c(cols, np.int32)
+    ne = conn_ptr.size - 1
+    m = np.zeros(ne * nodes_per_element ** 2, np.int32)
+    missing = lib().oracle_element_bsr_map(_ptr(conn_ptr), _ptr(conn), ne, nodes_per_element, _ptr(rowp), _ptr(cols),
+                                           _ptr(m))
+    assert missing == 0, f"{missing} blocks missing from pattern"
+    return m
+
+
+def check_colouring(num_nodes: int, conn_ptr, conn, colour, num_colours: int) -> int:
+    conn_ptr, conn, colour = _c(conn_ptr, np.int32), _c(conn, np.int32), _c(colour, np.int32)
+    return int(lib().oracle_check_colouring(num_nodes, _ptr(conn_ptr), _ptr(conn), conn_ptr.size - 1, _ptr(colour),
+                                            num_colours))
+
+
+def assemble(mesh, bsr_map=None, nnzb: int | None = None, residual: bool = True, jacobian: bool = True,
+             parallel: bool = False, num_elements: int | None = None):
+    """Residual [numNodes*2] and BSR values [nnzb*4] (zero-initialised, then
+    accumulated as runJacobianKernel does).  parallel=True uses the OpenMP
+    atomic-scatter variant (timed CPU baseline; summation order not fixed)."""
+    ne = mesh.num_elements if num_elements is None else num_elements
+    cp, cn = _c(mesh.conn_ptr, np.int32), _c(mesh.conn, np.int32)
+    st, xy = _c(mesh.states, np.float64), _c(mesh.coords, np.float64)
+    res = np.zeros(mesh.num_nodes * 2) if residual else None
+    mat = None
+    mp = None
+    if jacobian:
+        mp = _c(bsr_map, np.int32)
+        mat = np.zeros(int(nnzb) * 4)
+    fn = lib().oracle_assemble_parallel if parallel else lib().oracle_assemble
+    rc = fn(mesh.order, _ptr(cp), _ptr(cn), ne, _ptr(st), _ptr(xy), mesh.E, mesh.nu, mesh.t, _ptr(mp), _ptr(res),
+            _ptr(mat))
+    assert rc == 0
+    return res, mat
+
+
+def bsr_spmv(rowp, cols, A, x):
+    rowp, cols, A, x = _c(rowp, np.int32), _c(cols, np.int32), _c(A, np.float64), _c(x, np.float64)
+    y = np.zeros(x.size)
+    lib().oracle_bsr_spmv(rowp.size - 1, _ptr(rowp), _ptr(cols), _ptr(A), _ptr(x), _ptr(y))
+    return y
