@@ -222,22 +222,24 @@ def run_ours(args):
 
     paths = {}
     # plan path (overwrite, no zeroing), FP64 and mixed
-    for prec in ("fp64", "mixed"):
+    for prec in [x for x in ("fp64", "mixed") if f"plan_{x}" in args.paths]:
         fn = (lambda prec=prec: plan.assemble(d.states, d.coords, E, nu, t, res, mat, precision=prec, stream=sptr))
         ms, _ = time_steps(fn, max(2, args.steps // 2), args.warmup, plan.num_colours)
         paths[f"plan_{prec}"] = {"ms": ms, "elements_per_s": nE / (ms * 1e-3)}
     # error of the mixed plan path against the FP64 plan path (FP64 path is oracle-checked in tests)
-    with torch.cuda.stream(stream):
-        plan.assemble(d.states, d.coords, E, nu, t, res, mat, precision="fp64", stream=sptr)
-        res64, mat64 = res.clone(), mat.clone()
-        plan.assemble(d.states, d.coords, E, nu, t, res, mat, precision="mixed", stream=sptr)
-        err_res = float(torch.linalg.vector_norm(res - res64) / torch.linalg.vector_norm(res64))
-        err_mat = float(torch.linalg.vector_norm(mat - mat64) / torch.linalg.vector_norm(mat64))
+    err_res = err_mat = float("inf")
+    if "plan_mixed" in paths:
+        with torch.cuda.stream(stream):
+            plan.assemble(d.states, d.coords, E, nu, t, res, mat, precision="fp64", stream=sptr)
+            res64, mat64 = res.clone(), mat.clone()
+            plan.assemble(d.states, d.coords, E, nu, t, res, mat, precision="mixed", stream=sptr)
+            err_res = float(torch.linalg.vector_norm(res - res64) / torch.linalg.vector_norm(res64))
+            err_mat = float(torch.linalg.vector_norm(mat - mat64) / torch.linalg.vector_norm(mat64))
+            del res64, mat64
+        paths["plan_mixed"]["rel_frobenius_err"] = {"residual": err_res, "jacobian": err_mat}
     stream.synchronize()
-    del res64, mat64
-    paths["plan_mixed"]["rel_frobenius_err"] = {"residual": err_res, "jacobian": err_mat}
     # plain drop-in FP64 (reference contract: caller zeroes, kernel accumulates via map, atomics)
-    if not args.skip_dropin:
+    if any(x.startswith("dropin") for x in args.paths):
         rowp_h, cols_h = plan.pattern()
         mp = fem.build_element_bsr_map(mesh.conn_ptr, mesh.conn, mesh.nodes_per_element, rowp_h, cols_h)
         with torch.cuda.stream(stream):
@@ -252,13 +254,19 @@ def run_ours(args):
                                     precision=prec, stream=sptr, timed=False)
 
         with torch.cuda.stream(stream):
-            ms, _ = time_steps(lambda: dropin("fp64", True), max(2, args.steps // 2), args.warmup, 1)
-            paths["dropin_fp64_with_zeroing"] = {"ms": ms, "elements_per_s": nE / (ms * 1e-3)}
-            ms, _ = time_steps(lambda: dropin("fp64", False), max(2, args.steps // 2), args.warmup, 1)
-            paths["dropin_fp64_kernel_only"] = {"ms": ms, "elements_per_s": nE / (ms * 1e-3)}
+            if "dropin_fp64" in args.paths:
+                ms, _ = time_steps(lambda: dropin("fp64", True), max(2, args.steps // 2), args.warmup, 1)
+                paths["dropin_fp64_with_zeroing"] = {"ms": ms, "elements_per_s": nE / (ms * 1e-3)}
+                ms, _ = time_steps(lambda: dropin("fp64", False), max(2, args.steps // 2), args.warmup, 1)
+                paths["dropin_fp64_kernel_only"] = {"ms": ms, "elements_per_s": nE / (ms * 1e-3)}
+            if "dropin_mixed" in args.paths:
+                ms, _ = time_steps(lambda: dropin("mixed", False), max(2, args.steps // 2), args.warmup, 1)
+                paths["dropin_mixed_kernel_only"] = {"ms": ms, "elements_per_s": nE / (ms * 1e-3)}
         del dmap
-    best = "plan_mixed" if (paths["plan_mixed"]["ms"] < paths["plan_fp64"]["ms"] and max(err_res, err_mat) <= 1e-6) \
-        else "plan_fp64"
+    best = "plan_fp64"
+    if "plan_mixed" in paths and max(err_res, err_mat) <= 1e-6 and (
+            "plan_fp64" not in paths or paths["plan_mixed"]["ms"] < paths["plan_fp64"]["ms"]):
+        best = "plan_mixed"
     prec = "mixed" if best == "plan_mixed" else "fp64"
 
     def step():
@@ -342,9 +350,11 @@ def main():
     ap.add_argument("--workload", default="square1024_p3", choices=sorted(WORKLOADS))
     ap.add_argument("--ref-elements", type=int, default=131072)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
-    ap.add_argument("--skip-dropin", action="store_true")
+    ap.add_argument("--paths", default="plan_fp64,plan_mixed,dropin_fp64",
+                    help="comma list of plan_fp64, plan_mixed, dropin_fp64, dropin_mixed")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    args.paths = set(args.paths.split(","))
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     if args.impl == "reference":
         run_reference(args)

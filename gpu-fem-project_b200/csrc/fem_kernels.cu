@@ -21,9 +21,10 @@
 // DOF (a,i) is Ke[(a,i),(b,k)] = lam' M_ik + mu M_ki + mu delta_ik (M_xx + M_yy).
 //
 // Scatter: the drop-in mode adds through the reference's element->block map with
-// FP64 atomics (element/FEKernels.h:730-780); the plan mode runs one colour per
-// launch and stores (first contributor) or read-modify-writes (later colours)
-// without atomics.
+// FP64 atomics (element/FEKernels.h:730-780).  The plan mode runs one colour per
+// launch; the first contributor to a block writes it with one 256-bit store (no
+// zeroing, no read), later colours add with fire-and-forget reductions, and no
+// two elements of one colour touch the same block or residual row.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -90,6 +91,11 @@ __device__ __forceinline__ void lag1d(int p, double x, int k, double &N, double 
   }
 }
 
+// One 2x2 block (32 bytes, 32-byte aligned) with a single 256-bit store.
+__device__ __forceinline__ void store_block(double *p, double a, double b, double c, double d) {
+  asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(a), "d"(b), "d"(c), "d"(d) : "memory");
+}
+
 template <typename T>
 struct Vec2;
 template <>
@@ -121,48 +127,85 @@ struct AsmArgs {
 
 constexpr size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
-template <int P, typename T, int EPB>
-struct Layout {
-  static constexpr int P1 = P + 1, NN = P1 * P1, NQ = NN;
-  static constexpr size_t T2B = 2 * sizeof(T);
-  static constexpr size_t tab = 0;                               // double2 [NQ][NN]
-  static constexpr size_t tabT = tab + 16 * NQ * NN;             // double2 [NN][NQ]
-  static constexpr size_t wq = tabT + 16 * NQ * NN;              // double  [NQ]
-  static constexpr size_t X = align16(wq + 8 * NQ);              // double2 [EPB][NN]
-  static constexpr size_t U = X + 16 * EPB * NN;                 // double2 [EPB][NN]
-  static constexpr size_t qd = U + 16 * EPB * NN;                // double  [EPB][NQ][8]
-  static constexpr size_t G = qd + 64 * EPB * NQ;                // T2      [EPB][NQ][NN]
-  static constexpr size_t H = G + T2B * EPB * NQ * NN;           // T2      [EPB][NQ][NN]
-  static constexpr size_t nid = align16(H + T2B * EPB * NQ * NN);  // int   [EPB][NN]
-  static constexpr size_t total = align16(nid + 4 * EPB * NN);
+// Launch shape per order: GT threads per group, EPG elements per group step,
+// GPC independent groups per CTA (each synchronises on its own named barrier),
+// NPART threads per quadrature point in the Jacobian stage, MINB resident CTAs
+// per SM the register budget is sized for.  Stiffness-stage threads per element:
+// the (p+1)-row tiles on or above the diagonal, 6 / 18 / 40 / 75 for p = 1..4.
+template <int P>
+struct Shape;
+template <>
+struct Shape<1> {
+  static constexpr int GT = 64, EPG = 8, GPC = 4, NPART = 2, MINB = 4;
+};
+template <>
+struct Shape<2> {
+  static constexpr int GT = 64, EPG = 3, GPC = 4, NPART = 2, MINB = 4;
+};
+template <>
+struct Shape<3> {
+  static constexpr int GT = 64, EPG = 1, GPC = 4, NPART = 4, MINB = 4;
+};
+template <>
+struct Shape<4> {
+  static constexpr int GT = 128, EPG = 1, GPC = 2, NPART = 4, MINB = 3;
 };
 
 template <int P>
-struct Tune {
-  // Elements per CTA step: fills ~256 threads in the stiffness stage
-  // ((p+1)*(p+1)^2 threads per element).
-  static constexpr int EPB = P == 1 ? 32 : P == 2 ? 9 : P == 3 ? 4 : 2;
-  static constexpr int NT = 256;
+struct Dims {
+  static constexpr int P1 = P + 1, NN = P1 * P1, NQ = NN;
+  // upper-triangle row tiles: row tile `at` covers nodes at*P1 .. at*P1+P, columns b >= at*P1
+  static constexpr int NTILE = P1 * NN - P1 * P1 * (P1 - 1) / 2;
 };
 
-template <int P, typename T, int MODE, int EPB, int NT>
-__global__ void __launch_bounds__(NT) assemble_kernel(const AsmArgs A) {
-  constexpr int P1 = P + 1, NN = P1 * P1, NQ = NN;
-  using L = Layout<P, T, EPB>;
+// Shared memory: per-CTA tables, then GPC group regions.
+template <int P, typename T>
+struct Layout {
+  using S = Shape<P>;
+  static constexpr int NN = Dims<P>::NN, NQ = NN, EPG = S::EPG;
+  static constexpr size_t T2B = 2 * sizeof(T);
+  static constexpr size_t tab = 0;                      // double2 [NQ][NN]
+  static constexpr size_t tabT = tab + 16 * NQ * NN;    // double2 [NN][NQ]
+  static constexpr size_t wq = tabT + 16 * NQ * NN;     // double  [NQ]
+  static constexpr size_t groups = align16(wq + 8 * NQ);
+  // group-relative
+  static constexpr size_t X = 0;                               // double2 [EPG][NN]
+  static constexpr size_t U = X + 16 * EPG * NN;               // double2 [EPG][NN]
+  static constexpr size_t qd = U + 16 * EPG * NN;              // double  [8][EPG*NQ]  (SoA)
+  static constexpr size_t G = qd + 64 * EPG * NQ;              // T2      [EPG][NQ][NN]
+  static constexpr size_t H = G + T2B * EPG * NQ * NN;         // T2      [EPG][NQ][NN]
+  static constexpr size_t nid = H + T2B * EPG * NQ * NN;       // int     [EPG][NN]
+  static constexpr size_t group_bytes = align16(nid + 4 * EPG * NN);
+  static constexpr size_t total = groups + S::GPC * group_bytes;
+};
+
+__device__ __forceinline__ void group_sync(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+// FP64 stiffness tiles hold (p+1)*4 double accumulators: give p = 3 the
+// registers of 3 resident CTAs instead of 4 so the tile loop does not spill.
+template <int P, typename T>
+constexpr int min_blocks() {
+  return (P == 3 && sizeof(T) == 8) ? 3 : Shape<P>::MINB;
+}
+
+template <int P, typename T, int MODE>
+__global__ void __launch_bounds__(Shape<P>::GT *Shape<P>::GPC, min_blocks<P, T>()) assemble_kernel(const AsmArgs A) {
+  using S = Shape<P>;
+  using L = Layout<P, T>;
+  constexpr int P1 = P + 1, NN = Dims<P>::NN, NQ = NN, NTILE = Dims<P>::NTILE;
+  constexpr int GT = S::GT, EPG = S::EPG, NPART = S::NPART;
+  static_assert(EPG * NN <= GT, "one prefetched node per thread");
+  static_assert(GT % 32 == 0 && 32 % NPART == 0, "group/part shape");
   using T2 = typename Vec2<T>::type;
   extern __shared__ __align__(16) unsigned char smem[];
   double2 *tab = reinterpret_cast<double2 *>(smem + L::tab);
   double2 *tabT = reinterpret_cast<double2 *>(smem + L::tabT);
   double *wq = reinterpret_cast<double *>(smem + L::wq);
-  double2 *X = reinterpret_cast<double2 *>(smem + L::X);
-  double2 *U = reinterpret_cast<double2 *>(smem + L::U);
-  double *qd = reinterpret_cast<double *>(smem + L::qd);
-  T2 *G = reinterpret_cast<T2 *>(smem + L::G);
-  T2 *H = reinterpret_cast<T2 *>(smem + L::H);
-  int *nid = reinterpret_cast<int *>(smem + L::nid);
 
-  const int tid = threadIdx.x;
-  for (int i = tid; i < NQ * NN; i += NT) {
+  // Shape-function derivative tables at the Gauss points, once per CTA.
+  for (int i = threadIdx.x; i < NQ * NN; i += blockDim.x) {
     const int q = i / NN, a = i - q * NN;
     double Nx, dNx, Ny, dNy;
     lag1d(P, kGX[P][q % P1], a % P1, Nx, dNx);
@@ -171,122 +214,162 @@ __global__ void __launch_bounds__(NT) assemble_kernel(const AsmArgs A) {
     tab[i] = d;
     tabT[a * NQ + q] = d;
   }
-  for (int q = tid; q < NQ; q += NT) wq[q] = __dmul_rn(kGW[P][q % P1], kGW[P][q / P1]);
+  for (int q = threadIdx.x; q < NQ; q += blockDim.x) wq[q] = __dmul_rn(kGW[P][q % P1], kGW[P][q / P1]);
+  __syncthreads();
+
+  const int g = threadIdx.x / GT, tg = threadIdx.x - g * GT;
+  unsigned char *gs = smem + L::groups + g * L::group_bytes;
+  double2 *X = reinterpret_cast<double2 *>(gs + L::X);
+  double2 *U = reinterpret_cast<double2 *>(gs + L::U);
+  double *qd = reinterpret_cast<double *>(gs + L::qd);
+  T2 *G = reinterpret_cast<T2 *>(gs + L::G);
+  T2 *H = reinterpret_cast<T2 *>(gs + L::H);
+  int *nid = reinterpret_cast<int *>(gs + L::nid);
+  const int bar = 1 + g;
 
   const double mu = A.mu, lam = A.lam;
   const T cMu = T(mu), cLam = T(lam), cC11 = T(lam + 2.0 * mu);
+  const int64_t end = A.begin + A.count;
+  const int64_t nb = (A.count + EPG - 1) / EPG;
+  const int64_t stride = (int64_t)gridDim.x * S::GPC;
 
-  const int64_t nb = (A.count + EPB - 1) / EPB;
-  for (int64_t batch = blockIdx.x; batch < nb; batch += gridDim.x) {
-    const int64_t k0 = A.begin + batch * EPB;
-    const int ne = (int)min((int64_t)EPB, A.begin + A.count - k0);
-    __syncthreads();  // tables ready / previous step done with shared memory
-
-    // 1. gather
-    for (int i = tid; i < ne * NN; i += NT) {
-      const int el = i / NN, a = i - el * NN;
-      const int64_t k = k0 + el;
-      int node;
-      if constexpr ((MODE & kPlan) != 0) {
-        node = __ldg(A.connList + k * NN + a);
-      } else {
-        node = __ldg(A.conn + __ldg(A.connPtr + k) + a);
-      }
-      nid[i] = node;
-      X[i] = __ldg(reinterpret_cast<const double2 *>(A.coords) + node);
-      U[i] = __ldg(reinterpret_cast<const double2 *>(A.states) + node);
+  // Gather of the next batch, issued early so its latency overlaps the current batch.
+  int pf_node = 0;
+  double2 pf_x = make_double2(0, 0), pf_u = make_double2(0, 0);
+  auto prefetch = [&](int64_t batch) {
+    if (batch >= nb || tg >= EPG * NN) return;
+    const int el = tg / NN, a = tg - el * NN;
+    const int64_t k = A.begin + batch * EPG + el;
+    if (k >= end) return;
+    if constexpr ((MODE & kPlan) != 0) {
+      pf_node = __ldg(A.connList + k * NN + a);
+    } else {
+      pf_node = __ldg(A.conn + __ldg(A.connPtr + k) + a);
     }
-    __syncthreads();
+    pf_x = __ldg(reinterpret_cast<const double2 *>(A.coords) + pf_node);
+    pf_u = __ldg(reinterpret_cast<const double2 *>(A.states) + pf_node);
+  };
 
-    // 2. quadrature-point data (FP64)
-    for (int i = tid; i < ne * NQ; i += NT) {
-      const int el = i / NQ, q = i - el * NQ;
+  int64_t batch = (int64_t)blockIdx.x * S::GPC + g;
+  prefetch(batch);
+  for (; batch < nb; batch += stride) {
+    const int64_t k0 = A.begin + batch * EPG;
+    const int ne = (int)min((int64_t)EPG, end - k0);
+
+    // 0. commit the gathered element data
+    if (tg < ne * NN) {
+      X[tg] = pf_x;
+      U[tg] = pf_u;
+      nid[tg] = pf_node;
+    }
+    group_sync(bar, GT);
+
+    // 1. quadrature-point data: NPART lanes per (element, q) split the node sum
+    for (int base = 0; base < EPG * NQ * NPART; base += GT) {
+      const int i = base + tg;
+      const int iq = i / NPART, part = i - iq * NPART;
+      const int el = iq / NQ, q = iq - el * NQ;
+      const bool act = i < EPG * NQ * NPART && el < ne;
       double j00 = 0, j01 = 0, j10 = 0, j11 = 0, g00 = 0, g01 = 0, g10 = 0, g11 = 0;
+      if (act) {
+#pragma unroll 2
+        for (int a = part; a < NN; a += NPART) {
+          const double2 d = tabT[a * NQ + q];
+          const double2 x = X[el * NN + a], u = U[el * NN + a];
+          j00 = fma(x.x, d.x, j00);
+          j01 = fma(x.x, d.y, j01);
+          j10 = fma(x.y, d.x, j10);
+          j11 = fma(x.y, d.y, j11);
+          g00 = fma(u.x, d.x, g00);
+          g01 = fma(u.x, d.y, g01);
+          g10 = fma(u.y, d.x, g10);
+          g11 = fma(u.y, d.y, g11);
+        }
+      }
 #pragma unroll
-      for (int a = 0; a < NN; a++) {
-        const double2 d = tabT[a * NQ + q];
-        const double2 x = X[el * NN + a], u = U[el * NN + a];
-        j00 = fma(x.x, d.x, j00);
-        j01 = fma(x.x, d.y, j01);
-        j10 = fma(x.y, d.x, j10);
-        j11 = fma(x.y, d.y, j11);
-        g00 = fma(u.x, d.x, g00);
-        g01 = fma(u.x, d.y, g01);
-        g10 = fma(u.y, d.x, g10);
-        g11 = fma(u.y, d.y, g11);
+      for (int o = 1; o < NPART; o <<= 1) {
+        j00 += __shfl_xor_sync(0xffffffffu, j00, o);
+        j01 += __shfl_xor_sync(0xffffffffu, j01, o);
+        j10 += __shfl_xor_sync(0xffffffffu, j10, o);
+        j11 += __shfl_xor_sync(0xffffffffu, j11, o);
+        g00 += __shfl_xor_sync(0xffffffffu, g00, o);
+        g01 += __shfl_xor_sync(0xffffffffu, g01, o);
+        g10 += __shfl_xor_sync(0xffffffffu, g10, o);
+        g11 += __shfl_xor_sync(0xffffffffu, g11, o);
       }
-      const double det = j00 * j11 - j01 * j10;
-      const double inv = 1.0 / det;
-      const double i00 = j11 * inv, i01 = -j01 * inv, i10 = -j10 * inv, i11 = j00 * inv;
-      const double uxx = g00 * i00 + g01 * i10, uxy = g00 * i01 + g01 * i11;
-      const double uyx = g10 * i00 + g11 * i10, uyy = g10 * i01 + g11 * i11;
-      const double st = wq[q] * det * A.t;
-      const double tr = uxx + uyy;
-      double *Q = qd + (el * NQ + q) * 8;
-      Q[0] = i00;
-      Q[1] = i01;
-      Q[2] = i10;
-      Q[3] = i11;
-      Q[4] = st * (2.0 * mu * uxx + lam * tr);
-      Q[5] = st * (mu * (uxy + uyx));
-      Q[6] = st * (2.0 * mu * uyy + lam * tr);
-      Q[7] = st;
+      if (act && part == 0) {
+        const double det = j00 * j11 - j01 * j10;
+        const double inv = 1.0 / det;
+        const double i00 = j11 * inv, i01 = -j01 * inv, i10 = -j10 * inv, i11 = j00 * inv;
+        const double uxx = g00 * i00 + g01 * i10, uxy = g00 * i01 + g01 * i11;
+        const double uyx = g10 * i00 + g11 * i10, uyy = g10 * i01 + g11 * i11;
+        const double st = wq[q] * det * A.t;
+        const double tr = uxx + uyy;
+        constexpr int SQ = EPG * NQ;
+        qd[0 * SQ + iq] = i00;
+        qd[1 * SQ + iq] = i01;
+        qd[2 * SQ + iq] = i10;
+        qd[3 * SQ + iq] = i11;
+        qd[4 * SQ + iq] = st * (2.0 * mu * uxx + lam * tr);
+        qd[5 * SQ + iq] = st * (mu * (uxy + uyx));
+        qd[6 * SQ + iq] = st * (2.0 * mu * uyy + lam * tr);
+        qd[7 * SQ + iq] = st;
+      }
     }
-    __syncthreads();
+    group_sync(bar, GT);
 
-    // 3. real-space shape gradients (only the stiffness stage needs them stored)
+    // 2. real-space shape gradients G = dN J^-1 and H = w detJ t G
     if constexpr ((MODE & kJac) != 0) {
-      for (int i = tid; i < ne * NQ * NN; i += NT) {
-        const int el = i / (NQ * NN);
-        const int r = i - el * NQ * NN;
-        const int q = r / NN, a = r - q * NN;
+      constexpr int SQ = EPG * NQ;
+      for (int i = tg; i < ne * NQ * NN; i += GT) {
+        const int iq = i / NN, a = i - iq * NN;
+        const int q = iq % NQ;
         const double2 d = tab[q * NN + a];
-        const double *Q = qd + (el * NQ + q) * 8;
-        const double gx = d.x * Q[0] + d.y * Q[2];
-        const double gy = d.x * Q[1] + d.y * Q[3];
-        T2 g, h;
-        g.x = T(gx);
-        g.y = T(gy);
-        h.x = T(Q[7] * gx);
-        h.y = T(Q[7] * gy);
-        G[i] = g;
-        H[i] = h;
+        const double gx = d.x * qd[0 * SQ + iq] + d.y * qd[2 * SQ + iq];
+        const double gy = d.x * qd[1 * SQ + iq] + d.y * qd[3 * SQ + iq];
+        const double st = qd[7 * SQ + iq];
+        T2 gv, hv;
+        gv.x = T(gx);
+        gv.y = T(gy);
+        hv.x = T(st * gx);
+        hv.y = T(st * gy);
+        G[i] = gv;
+        H[i] = hv;
       }
-      __syncthreads();
     }
+    prefetch(batch + stride);
+    group_sync(bar, GT);
 
-    // 4. residual R_a = sum_q S(q) G_a(q)
+    // 3a. residual R_a = sum_q S(q) G_a(q)
     if constexpr ((MODE & kRes) != 0) {
-      for (int i = tid; i < ne * NN; i += NT) {
+      constexpr int SQ = EPG * NQ;
+      for (int i = tg; i < ne * NN; i += GT) {
         const int el = i / NN, a = i - el * NN;
         T rx = 0, ry = 0;
 #pragma unroll 4
         for (int q = 0; q < NQ; q++) {
-          const double *Q = qd + (el * NQ + q) * 8;
+          const int iq = el * NQ + q;
           T gx, gy;
           if constexpr ((MODE & kJac) != 0) {
-            const T2 g = G[(el * NQ + q) * NN + a];
-            gx = g.x;
-            gy = g.y;
+            const T2 gv = G[iq * NN + a];
+            gx = gv.x;
+            gy = gv.y;
           } else {
             const double2 d = tab[q * NN + a];
-            gx = T(d.x * Q[0] + d.y * Q[2]);
-            gy = T(d.x * Q[1] + d.y * Q[3]);
+            gx = T(d.x * qd[0 * SQ + iq] + d.y * qd[2 * SQ + iq]);
+            gy = T(d.x * qd[1 * SQ + iq] + d.y * qd[3 * SQ + iq]);
           }
-          const T sxx = T(Q[4]), sxy = T(Q[5]), syy = T(Q[6]);
+          const T sxx = T(qd[4 * SQ + iq]), sxy = T(qd[5 * SQ + iq]), syy = T(qd[6 * SQ + iq]);
           rx = fma(sxx, gx, fma(sxy, gy, rx));
           ry = fma(sxy, gx, fma(syy, gy, ry));
         }
         double *dst = A.residual + 2 * (int64_t)nid[i];
         if constexpr ((MODE & kPlan) != 0) {
-          const int64_t k = k0 + el;
-          if (__ldg(A.nodeCode + k * NN + a)) {
+          if (__ldg(A.nodeCode + (k0 + el) * NN + a)) {
             *reinterpret_cast<double2 *>(dst) = make_double2(double(rx), double(ry));
           } else {
-            double2 v = *reinterpret_cast<double2 *>(dst);
-            v.x += double(rx);
-            v.y += double(ry);
-            *reinterpret_cast<double2 *>(dst) = v;
+            atomicAdd(dst, double(rx));
+            atomicAdd(dst + 1, double(ry));
           }
         } else {
           atomicAdd(dst, double(rx));
@@ -295,12 +378,20 @@ __global__ void __launch_bounds__(NT) assemble_kernel(const AsmArgs A) {
       }
     }
 
-    // 5. element stiffness, one row tile of P1 nodes x one column node per thread
+    // 3b. element stiffness on and above the diagonal; the block below is its transpose
     if constexpr ((MODE & kJac) != 0) {
-      for (int i = tid; i < ne * P1 * NN; i += NT) {
-        const int el = i / (P1 * NN);
-        const int r = i - el * P1 * NN;
-        const int at = r / NN, b = r - at * NN;
+      for (int i = tg; i < ne * NTILE; i += GT) {
+        const int el = i / NTILE;
+        int r = i - el * NTILE, at = 0;
+#pragma unroll
+        for (int row = 0; row < P1; row++) {
+          const int len = NN - row * P1;
+          if (at == row && r >= len) {
+            r -= len;
+            at = row + 1;
+          }
+        }
+        const int b = at * P1 + r;
         T m[P1][4];
 #pragma unroll
         for (int ax = 0; ax < P1; ax++) m[ax][0] = m[ax][1] = m[ax][2] = m[ax][3] = T(0);
@@ -308,51 +399,69 @@ __global__ void __launch_bounds__(NT) assemble_kernel(const AsmArgs A) {
         const T2 *Ha = H + el * NQ * NN + at * P1;
 #pragma unroll 2
         for (int q = 0; q < NQ; q++) {
-          const T2 g = Gb[q * NN];
+          const T2 gv = Gb[q * NN];
 #pragma unroll
           for (int ax = 0; ax < P1; ax++) {
-            const T2 h = Ha[q * NN + ax];
-            m[ax][0] = fma(h.x, g.x, m[ax][0]);
-            m[ax][1] = fma(h.x, g.y, m[ax][1]);
-            m[ax][2] = fma(h.y, g.x, m[ax][2]);
-            m[ax][3] = fma(h.y, g.y, m[ax][3]);
+            const T2 hv = Ha[q * NN + ax];
+            m[ax][0] = fma(hv.x, gv.x, m[ax][0]);
+            m[ax][1] = fma(hv.x, gv.y, m[ax][1]);
+            m[ax][2] = fma(hv.y, gv.x, m[ax][2]);
+            m[ax][3] = fma(hv.y, gv.y, m[ax][3]);
           }
         }
         const int64_t k = k0 + el;
 #pragma unroll
         for (int ax = 0; ax < P1; ax++) {
           const int a = at * P1 + ax;
-          const T kxx = cC11 * m[ax][0] + cMu * m[ax][3];
-          const T kxy = cLam * m[ax][1] + cMu * m[ax][2];
-          const T kyx = cLam * m[ax][2] + cMu * m[ax][1];
-          const T kyy = cC11 * m[ax][3] + cMu * m[ax][0];
+          if (a > b) continue;
+          const double kxx = double(cC11 * m[ax][0] + cMu * m[ax][3]);
+          const double kxy = double(cLam * m[ax][1] + cMu * m[ax][2]);
+          const double kyx = double(cLam * m[ax][2] + cMu * m[ax][1]);
+          const double kyy = double(cC11 * m[ax][3] + cMu * m[ax][0]);
           if constexpr ((MODE & kPlan) != 0) {
-            const uint8_t code = __ldg(A.blockCode + (k * NN + a) * NN + b);
-            const int row = nid[el * NN + a];
-            double *blk = A.mat + 4 * ((int64_t)__ldg(A.rowp + row) + (code & 0x7f));
-            double2 *b2 = reinterpret_cast<double2 *>(blk);
-            if (code & 0x80) {
-              b2[0] = make_double2(double(kxx), double(kxy));
-              b2[1] = make_double2(double(kyx), double(kyy));
+            const int ra = nid[el * NN + a], rb = nid[el * NN + b];
+            const uint8_t c0 = __ldg(A.blockCode + (k * NN + a) * NN + b);
+            double *b0 = A.mat + 4 * ((int64_t)__ldg(A.rowp + ra) + (c0 & 0x7f));
+            if (c0 & 0x80) {
+              store_block(b0, kxx, kxy, kyx, kyy);
             } else {
-              double2 v0 = b2[0], v1 = b2[1];
-              v0.x += double(kxx);
-              v0.y += double(kxy);
-              v1.x += double(kyx);
-              v1.y += double(kyy);
-              b2[0] = v0;
-              b2[1] = v1;
+              // later colour: the first contributor's store is complete (previous
+              // launch) and no element of this colour shares the block
+              atomicAdd(b0 + 0, kxx);
+              atomicAdd(b0 + 1, kxy);
+              atomicAdd(b0 + 2, kyx);
+              atomicAdd(b0 + 3, kyy);
+            }
+            if (a != b) {
+              const uint8_t c1 = __ldg(A.blockCode + (k * NN + b) * NN + a);
+              double *b1 = A.mat + 4 * ((int64_t)__ldg(A.rowp + rb) + (c1 & 0x7f));
+              if (c1 & 0x80) {
+                store_block(b1, kxx, kyx, kxy, kyy);
+              } else {
+                atomicAdd(b1 + 0, kxx);
+                atomicAdd(b1 + 1, kyx);
+                atomicAdd(b1 + 2, kxy);
+                atomicAdd(b1 + 3, kyy);
+              }
             }
           } else {
-            double *blk = A.mat + __ldg(A.map + (k * NN + a) * NN + b);
-            atomicAdd(blk + 0, double(kxx));
-            atomicAdd(blk + 1, double(kxy));
-            atomicAdd(blk + 2, double(kyx));
-            atomicAdd(blk + 3, double(kyy));
+            double *b0 = A.mat + __ldg(A.map + (k * NN + a) * NN + b);
+            atomicAdd(b0 + 0, kxx);
+            atomicAdd(b0 + 1, kxy);
+            atomicAdd(b0 + 2, kyx);
+            atomicAdd(b0 + 3, kyy);
+            if (a != b) {
+              double *b1 = A.mat + __ldg(A.map + (k * NN + b) * NN + a);
+              atomicAdd(b1 + 0, kxx);
+              atomicAdd(b1 + 1, kyx);
+              atomicAdd(b1 + 2, kxy);
+              atomicAdd(b1 + 3, kyy);
+            }
           }
         }
       }
     }
+    group_sync(bar, GT);
   }
 }
 
@@ -427,15 +536,17 @@ int launch_info(K kernel, int nt, size_t smem, LaunchInfo &out) {
 
 template <int P, typename T, int MODE>
 int launch_p(const dev::AsmArgs &a, cudaStream_t s) {
-  constexpr int EPB = dev::Tune<P>::EPB, NT = dev::Tune<P>::NT;
-  auto kernel = dev::assemble_kernel<P, T, MODE, EPB, NT>;
-  const size_t smem = dev::Layout<P, T, EPB>::total;
+  using S = dev::Shape<P>;
+  constexpr int NT = S::GT * S::GPC;
+  auto kernel = dev::assemble_kernel<P, T, MODE>;
+  const size_t smem = dev::Layout<P, T>::total;
   LaunchInfo li;
   int st = launch_info(kernel, NT, smem, li);
   if (st) return st;
-  const int64_t nb = (a.count + EPB - 1) / EPB;
+  const int64_t groups = (a.count + S::EPG - 1) / S::EPG;
+  const int64_t need = (groups + S::GPC - 1) / S::GPC;
   const int64_t cap = (int64_t)li.grid_per_sm * li.num_sms;
-  const int grid = (int)(nb < cap ? nb : cap);
+  const int grid = (int)(need < cap ? need : cap);
   if (grid <= 0) return FEM_SUCCESS;
   kernel<<<grid, NT, smem, s>>>(a);
   cudaError_t err = cudaGetLastError();
@@ -701,9 +812,10 @@ int fem_plan_assemble(const fem_plan *plan, const double *states, const double *
   if (!plan) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "plan is NULL");
   if (!states || !nodeCoords) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "NULL input array");
   if (!residual && !matEntries) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "no output requested");
-  if (!fem::aligned16(states) || !fem::aligned16(nodeCoords) || (residual && !fem::aligned16(residual)) ||
-      (matEntries && !fem::aligned16(matEntries)))
-    return fem::fail(FEM_ERR_MISALIGNED, "all arrays must be 16-byte aligned");
+  if (!fem::aligned16(states) || !fem::aligned16(nodeCoords) || (residual && !fem::aligned16(residual)))
+    return fem::fail(FEM_ERR_MISALIGNED, "states, nodeCoords and residual must be 16-byte aligned");
+  if (matEntries && (reinterpret_cast<uintptr_t>(matEntries) & 31u))
+    return fem::fail(FEM_ERR_MISALIGNED, "matEntries must be 32-byte aligned (one 2x2 block per 256-bit store)");
   if (plan->numElements == 0) return FEM_SUCCESS;
   fem::dev::AsmArgs a{};
   a.connList = plan->d_connList;

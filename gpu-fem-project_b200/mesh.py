@@ -80,20 +80,38 @@ def _structured_conn(nx: int, ny: int, p: int, nodes_x: int, wrap_y: int = 0) ->
 def square_mesh(nx: int, ny: int, p: int, lx: float = 1.0, ly: float = 1.0, perturb: float = 0.0,
                 disp: float = 1e-3, E: float = 70e9, nu: float = 0.3, t: float = 1.0, seed: int = 0,
                 name: str = "square") -> Mesh:
-    """nx x ny order-p quads on [0,lx]x[0,ly]; nodes not on the domain boundary are
-    moved by U(-perturb*h, +perturb*h) per direction (h = element size along that
-    direction); nodal displacements U(-disp, disp)."""
+    """nx x ny order-p quads on [0,lx]x[0,ly]; nodal displacements U(-disp, disp).
+
+    Perturbation: element vertices not on the domain boundary move by
+    U(-perturb*h, +perturb*h) per direction (h = element size along it); every
+    higher-order node then sits at the cosine knots of its element's bilinear map
+    of the perturbed vertices, so elements stay valid (a node-by-node move of
+    +-0.2h would push the first interior knot, 0.25h from the edge at p=3 and
+    0.146h at p=4, past its neighbour and invert the element)."""
     rng = np.random.default_rng(seed)
     nxn, nyn = nx * p + 1, ny * p + 1
-    xs, ys = _axis(nx, p, lx), _axis(ny, p, ly)
-    X = np.empty((nyn, nxn, 2))
-    X[:, :, 0] = xs[None, :]
-    X[:, :, 1] = ys[:, None]
-    if perturb:
-        hx, hy = lx / nx, ly / ny
-        d = rng.uniform(-1.0, 1.0, size=(nyn - 2, nxn - 2, 2))
-        X[1:-1, 1:-1, 0] += perturb * hx * d[:, :, 0]
-        X[1:-1, 1:-1, 1] += perturb * hy * d[:, :, 1]
+    V = np.empty((ny + 1, nx + 1, 2))
+    V[:, :, 0] = np.linspace(0.0, lx, nx + 1)[None, :]
+    V[:, :, 1] = np.linspace(0.0, ly, ny + 1)[:, None]
+    if perturb and nx > 1 and ny > 1:
+        d = rng.uniform(-1.0, 1.0, size=(ny - 1, nx - 1, 2))
+        V[1:-1, 1:-1, 0] += perturb * (lx / nx) * d[:, :, 0]
+        V[1:-1, 1:-1, 1] += perturb * (ly / ny) * d[:, :, 1]
+    f = cosine_knots(p)
+
+    def split(n_el, n_nodes):
+        idx = np.arange(n_nodes)
+        e = np.minimum(idx // p, n_el - 1)
+        return e, f[idx - e * p]
+
+    ex, fx = split(nx, nxn)
+    ey, fy = split(ny, nyn)
+    fx, fy = fx[None, :, None], fy[:, None, None]
+    v00 = V[ey][:, ex]
+    v10 = V[ey][:, ex + 1]
+    v01 = V[ey + 1][:, ex]
+    v11 = V[ey + 1][:, ex + 1]
+    X = (1 - fx) * (1 - fy) * v00 + fx * (1 - fy) * v10 + (1 - fx) * fy * v01 + fx * fy * v11
     coords = np.ascontiguousarray(X.reshape(-1, 2))
     conn = _structured_conn(nx, ny, p, nxn)
     nn = (p + 1) ** 2

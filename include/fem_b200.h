@@ -109,9 +109,9 @@ int fem_bsr_spmv(int numRows, const int *rowp, const int *cols, const double *A,
 /* ---- assembly plans: overwrite semantics, colour-ordered, no map ---------------------- */
 /* A plan owns device copies of the mesh topology, its BSR pattern, an element
  * colouring and compact per-element block codes.  fem_plan_assemble writes the
- * COMPLETE residual and matrix (no zeroing by the caller and no atomics): within
- * a colour no two elements share a node, and the first contributor to each
- * block stores while later colours add.  (No reference counterpart.) */
+ * COMPLETE residual and matrix (the caller zeroes nothing): colours run in
+ * order, no two elements of one colour share a node, the first contributor to
+ * each block stores it and later colours add to it.  (No reference counterpart.) */
 typedef struct fem_plan fem_plan;
 
 int fem_plan_create(int elementOrder, int numNodes, const int *connPtr, const int *conn, int numElements,
@@ -125,7 +125,8 @@ int fem_plan_get_pattern(const fem_plan *plan, int *rowp, int *cols);
 /* Device pointers of the plan's rowp/cols (owned by the plan). */
 int fem_plan_device_pattern(const fem_plan *plan, const int **rowp, const int **cols);
 /* states/nodeCoords/residual/matEntries are device pointers; residual or
- * matEntries may be NULL to skip that output.  precision: FEM_PRECISION_*. */
+ * matEntries may be NULL to skip that output; matEntries must be 32-byte
+ * aligned.  precision: FEM_PRECISION_*. */
 int fem_plan_assemble(const fem_plan *plan, const double *states, const double *nodeCoords, double E, double nu,
                       double t, double *residual, double *matEntries, int precision, void *stream,
                       double *elapsedSeconds);
