@@ -341,6 +341,24 @@ def cpu_baseline(fem, mesh, args):
             "sample": f"first {sample} elements of {mesh.name}, {reps} repeats (OpenMP, atomic scatter)"}
 
 
+def measure_peaks():
+    """Arithmetic peaks of this GPU from the library's probe kernels (TFLOP/s)."""
+    import ctypes as C
+
+    import torch
+
+    import fem_pkg
+    fem = fem_pkg.load()
+    torch.cuda.init()
+    out = {}
+    for kind, name in ((0, "fp64_fma_tflops"), (1, "fp32_fma_tflops"), (2, "fp64_mma_tflops")):
+        v = C.c_double()
+        fem.check(fem.lib.fem_probe_peak(kind, C.byref(v)), "fem_probe_peak")
+        out[name] = v.value
+    out["gpu"] = torch.cuda.get_device_name(0)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -353,8 +371,12 @@ def main():
     ap.add_argument("--paths", default="plan_fp64,plan_mixed,dropin_fp64",
                     help="comma list of plan_fp64, plan_mixed, dropin_fp64, dropin_mixed")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--peaks", action="store_true", help="print measured FP64/FP32/FP64-MMA peaks and exit")
     args = ap.parse_args()
     args.paths = set(args.paths.split(","))
+    if args.peaks:
+        print(json.dumps(measure_peaks()))
+        return
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     if args.impl == "reference":
         run_reference(args)

@@ -52,6 +52,7 @@ SIGNATURES = {
     "fem_plan_get_pattern": (_i, [_p, _p, _p]),
     "fem_plan_device_pattern": (_i, [_p, C.POINTER(_p), C.POINTER(_p)]),
     "fem_plan_assemble": (_i, [_p, _p, _p, _d, _d, _d, _p, _p, _i, _p, _pd]),
+    "fem_probe_peak": (_i, [_i, _pd]),
     "fem_batch_create": (_i, [_i, _p, C.POINTER(_p)]),
     "fem_batch_destroy": (_i, [_p]),
     "fem_batch_info": (_i, [_p, _pi64, _pi64, _pi, _pi64]),

@@ -140,15 +140,15 @@ struct Shape<1> {
 };
 template <>
 struct Shape<2> {
-  static constexpr int GT = 64, EPG = 3, GPC = 4, NPART = 2, MINB = 4;
+  static constexpr int GT = 64, EPG = 2, GPC = 4, NPART = 2, MINB = 4;
 };
 template <>
 struct Shape<3> {
-  static constexpr int GT = 64, EPG = 1, GPC = 4, NPART = 4, MINB = 4;
+  static constexpr int GT = 64, EPG = 2, GPC = 2, NPART = 2, MINB = 4;
 };
 template <>
 struct Shape<4> {
-  static constexpr int GT = 128, EPG = 1, GPC = 2, NPART = 4, MINB = 3;
+  static constexpr int GT = 64, EPG = 1, GPC = 2, NPART = 2, MINB = 3;
 };
 
 template <int P>
@@ -156,25 +156,37 @@ struct Dims {
   static constexpr int P1 = P + 1, NN = P1 * P1, NQ = NN;
   // upper-triangle row tiles: row tile `at` covers nodes at*P1 .. at*P1+P, columns b >= at*P1
   static constexpr int NTILE = P1 * NN - P1 * P1 * (P1 - 1) / 2;
+  // FP64 tensor-core (m8n8k4) geometry of M = H^T G: rows/cols r = 2*node + component
+  // padded to NT8 tiles of 8, the quadrature (k) dimension padded to NQP = 4*KS,
+  // shared-memory row stride RS doubles with RS = 4 or 12 (mod 16): the four
+  // quadrature rows of a fragment load then cover every bank exactly twice, and
+  // the 16-byte gradient stores of the quadrature stage spread over all 8 bank groups.
+  static constexpr int NT8 = (2 * NN + 7) / 8;
+  static constexpr int KS = (NQ + 3) / 4, NQP = 4 * KS;
+  static constexpr int RS = 8 * NT8 + 4;  // 8*NT8 is 0 or 8 mod 16
 };
 
-// Shared memory: per-CTA tables, then GPC group regions.
+// Shared memory: per-CTA table, then GPC group regions.
+//   FP64 (tensor-core stiffness): G and H as [NQP][RS] doubles, row r = 2a + i.
+//   FP32 (CUDA-core stiffness):   G and H as [NQ][NN+1] float2, the padded row
+//   lets the quadrature stage store without bank conflicts.
 template <int P, typename T>
 struct Layout {
   using S = Shape<P>;
-  static constexpr int NN = Dims<P>::NN, NQ = NN, EPG = S::EPG;
-  static constexpr size_t T2B = 2 * sizeof(T);
-  static constexpr size_t tab = 0;                      // double2 [NQ][NN]
-  static constexpr size_t tabT = tab + 16 * NQ * NN;    // double2 [NN][NQ]
+  using D = Dims<P>;
+  static constexpr bool TC = sizeof(T) == 8;
+  static constexpr int NN = D::NN, NQ = NN, NNP = NN + 1, EPG = S::EPG;
+  static constexpr size_t GH_ELEM = TC ? 8 * D::NQP * D::RS : 2 * sizeof(T) * NQ * NNP;  // bytes per element
+  static constexpr size_t tabT = 0;                     // double2 [NN][NQ]
   static constexpr size_t wq = tabT + 16 * NQ * NN;     // double  [NQ]
   static constexpr size_t groups = align16(wq + 8 * NQ);
   // group-relative
   static constexpr size_t X = 0;                               // double2 [EPG][NN]
   static constexpr size_t U = X + 16 * EPG * NN;               // double2 [EPG][NN]
-  static constexpr size_t qd = U + 16 * EPG * NN;              // double  [8][EPG*NQ]  (SoA)
-  static constexpr size_t G = qd + 64 * EPG * NQ;              // T2      [EPG][NQ][NN]
-  static constexpr size_t H = G + T2B * EPG * NQ * NN;         // T2      [EPG][NQ][NN]
-  static constexpr size_t nid = H + T2B * EPG * NQ * NN;       // int     [EPG][NN]
+  static constexpr size_t S3 = U + 16 * EPG * NN;              // double  [3][EPG*NQ]  weak stress (SoA)
+  static constexpr size_t G = align16(S3 + 24 * EPG * NQ);     // [EPG] x GH_ELEM
+  static constexpr size_t H = align16(G + EPG * GH_ELEM);      // [EPG] x GH_ELEM
+  static constexpr size_t nid = align16(H + EPG * GH_ELEM);    // int [EPG][NN]
   static constexpr size_t group_bytes = align16(nid + 4 * EPG * NN);
   static constexpr size_t total = groups + S::GPC * group_bytes;
 };
@@ -183,49 +195,145 @@ __device__ __forceinline__ void group_sync(int id, int nthreads) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
 
-// FP64 stiffness tiles hold (p+1)*4 double accumulators: give p = 3 the
-// registers of 3 resident CTAs instead of 4 so the tile loop does not spill.
+__device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+// Writes the element block K(a,b) (and K(b,a) = K(a,b)^T when a != b) through the
+// plan codes or the reference map.  `which`: 0 = block (a,b), 1 = block (b,a).
+template <int NN, int MODE>
+__device__ __forceinline__ void write_block(const AsmArgs &A, int64_t k, const int *nid_el, int a, int b, int which,
+                                            double kxx, double kxy, double kyx, double kyy) {
+  const int r0 = which ? b : a, c0 = which ? a : b;
+  const double v0 = kxx, v1 = which ? kyx : kxy, v2 = which ? kxy : kyx, v3 = kyy;
+  if constexpr ((MODE & kPlan) != 0) {
+    const uint8_t code = __ldg(A.blockCode + (k * NN + r0) * NN + c0);
+    double *blk = A.mat + 4 * ((int64_t)__ldg(A.rowp + nid_el[r0]) + (code & 0x7f));
+    if (code & 0x80) {
+      store_block(blk, v0, v1, v2, v3);
+    } else {
+      // later colour: the first contributor's store is complete (previous launch)
+      // and no element of this colour shares the block
+      atomicAdd(blk + 0, v0);
+      atomicAdd(blk + 1, v1);
+      atomicAdd(blk + 2, v2);
+      atomicAdd(blk + 3, v3);
+    }
+  } else {
+    double *blk = A.mat + __ldg(A.map + (k * NN + r0) * NN + c0);
+    atomicAdd(blk + 0, v0);
+    atomicAdd(blk + 1, v1);
+    atomicAdd(blk + 2, v2);
+    atomicAdd(blk + 3, v3);
+  }
+}
+
+// One warp, tile rows [R0, R1) of the upper triangle of M = H^T G (FP64 MMA),
+// then the 2x2 stiffness blocks.  Lane l holds C[8ti + l/4][8tj + 2(l%4) + {0,1}]
+// = (M_i0, M_i1)[a][b] with a = (8ti + l/4)/2, i = (l/4)%2, b = 4tj + l%4; the
+// lane with the other i (l ^ 4) supplies the second row of the block.
+template <int P, int MODE, int R0, int R1>
+__device__ __forceinline__ void stiffness_mma(const AsmArgs &A, const double *Gm, const double *Hm, const int *nid_el,
+                                              int64_t k, double mu, double lam, int lane) {
+  using D = Dims<P>;
+  constexpr int NT8 = D::NT8, KS = D::KS, RS = D::RS, NN = D::NN;
+  constexpr int NR = R1 - R0;
+  double acc[NR][NT8][2];
+#pragma unroll
+  for (int r = 0; r < NR; r++)
+#pragma unroll
+    for (int c = 0; c < NT8; c++) acc[r][c][0] = acc[r][c][1] = 0.0;
+  const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int ks = 0; ks < KS; ks++) {
+    const int q = 4 * ks + t;
+    double af[NR], bf[NT8];
+#pragma unroll
+    for (int r = 0; r < NR; r++) af[r] = Hm[q * RS + 8 * (R0 + r) + g];
+#pragma unroll
+    for (int c = 0; c < NT8; c++)
+      if (c >= R0) bf[c] = Gm[q * RS + 8 * c + g];
+#pragma unroll
+    for (int r = 0; r < NR; r++)
+#pragma unroll
+      for (int c = 0; c < NT8; c++)
+        if (c >= R0 + r) dmma(acc[r][c][0], acc[r][c][1], af[r], bf[c]);
+  }
+  const double c11 = lam + 2.0 * mu;
+  const int i = g & 1;
+#pragma unroll
+  for (int r = 0; r < NR; r++) {
+    const int a = (8 * (R0 + r) + g) >> 1;
+#pragma unroll
+    for (int c = 0; c < NT8; c++) {
+      if (c < R0 + r) continue;
+      const double o0 = __shfl_xor_sync(0xffffffffu, acc[r][c][0], 4);
+      const double o1 = __shfl_xor_sync(0xffffffffu, acc[r][c][1], 4);
+      const double mxx = i ? o0 : acc[r][c][0], mxy = i ? o1 : acc[r][c][1];
+      const double myx = i ? acc[r][c][0] : o0, myy = i ? acc[r][c][1] : o1;
+      const int b = 4 * c + t;
+      if (a < NN && b < NN && a <= b && (i == 0 || a < b)) {
+        const double kxx = c11 * mxx + mu * myy;
+        const double kxy = lam * mxy + mu * myx;
+        const double kyx = lam * myx + mu * mxy;
+        const double kyy = c11 * myy + mu * mxx;
+        write_block<NN, MODE>(A, k, nid_el, a, b, i, kxx, kxy, kyx, kyy);
+      }
+    }
+  }
+}
+
 template <int P, typename T>
 constexpr int min_blocks() {
-  return (P == 3 && sizeof(T) == 8) ? 3 : Shape<P>::MINB;
+  return Shape<P>::MINB;
 }
 
 template <int P, typename T, int MODE>
 __global__ void __launch_bounds__(Shape<P>::GT *Shape<P>::GPC, min_blocks<P, T>()) assemble_kernel(const AsmArgs A) {
   using S = Shape<P>;
   using L = Layout<P, T>;
-  constexpr int P1 = P + 1, NN = Dims<P>::NN, NQ = NN, NTILE = Dims<P>::NTILE;
-  constexpr int GT = S::GT, EPG = S::EPG, NPART = S::NPART;
+  using D = Dims<P>;
+  constexpr bool TC = L::TC;
+  constexpr int P1 = P + 1, NN = D::NN, NQ = NN, NNP = L::NNP, NTILE = D::NTILE;
+  constexpr int NQP = D::NQP, RS = D::RS;
+  constexpr int GT = S::GT, EPG = S::EPG, NPART = S::NPART, SQ = EPG * NQ;
   static_assert(EPG * NN <= GT, "one prefetched node per thread");
   static_assert(GT % 32 == 0 && 32 % NPART == 0, "group/part shape");
   using T2 = typename Vec2<T>::type;
   extern __shared__ __align__(16) unsigned char smem[];
-  double2 *tab = reinterpret_cast<double2 *>(smem + L::tab);
   double2 *tabT = reinterpret_cast<double2 *>(smem + L::tabT);
   double *wq = reinterpret_cast<double *>(smem + L::wq);
 
-  // Shape-function derivative tables at the Gauss points, once per CTA.
+  // Shape-function derivative table at the Gauss points, once per CTA.
   for (int i = threadIdx.x; i < NQ * NN; i += blockDim.x) {
     const int q = i / NN, a = i - q * NN;
     double Nx, dNx, Ny, dNy;
     lag1d(P, kGX[P][q % P1], a % P1, Nx, dNx);
     lag1d(P, kGX[P][q / P1], a / P1, Ny, dNy);
-    const double2 d = make_double2(__dmul_rn(Ny, dNx), __dmul_rn(Nx, dNy));
-    tab[i] = d;
-    tabT[a * NQ + q] = d;
+    tabT[a * NQ + q] = make_double2(__dmul_rn(Ny, dNx), __dmul_rn(Nx, dNy));
   }
   for (int q = threadIdx.x; q < NQ; q += blockDim.x) wq[q] = __dmul_rn(kGW[P][q % P1], kGW[P][q / P1]);
-  __syncthreads();
 
   const int g = threadIdx.x / GT, tg = threadIdx.x - g * GT;
+  const int warp = tg >> 5, lane = tg & 31;
   unsigned char *gs = smem + L::groups + g * L::group_bytes;
   double2 *X = reinterpret_cast<double2 *>(gs + L::X);
   double2 *U = reinterpret_cast<double2 *>(gs + L::U);
-  double *qd = reinterpret_cast<double *>(gs + L::qd);
-  T2 *G = reinterpret_cast<T2 *>(gs + L::G);
-  T2 *H = reinterpret_cast<T2 *>(gs + L::H);
+  double *S3 = reinterpret_cast<double *>(gs + L::S3);
   int *nid = reinterpret_cast<int *>(gs + L::nid);
   const int bar = 1 + g;
+  if constexpr (TC) {
+    // zero the padded quadrature rows once: they feed the k dimension of the MMA
+    double *Gz = reinterpret_cast<double *>(gs + L::G), *Hz = reinterpret_cast<double *>(gs + L::H);
+    for (int i = tg; i < EPG * (NQP - NQ) * RS; i += GT) {
+      const int el = i / ((NQP - NQ) * RS), r = i - el * (NQP - NQ) * RS;
+      Gz[el * NQP * RS + NQ * RS + r] = 0.0;
+      Hz[el * NQP * RS + NQ * RS + r] = 0.0;
+    }
+  }
+  __syncthreads();
 
   const double mu = A.mu, lam = A.lam;
   const T cMu = T(mu), cLam = T(lam), cC11 = T(lam + 2.0 * mu);
@@ -263,8 +371,10 @@ __global__ void __launch_bounds__(Shape<P>::GT *Shape<P>::GPC, min_blocks<P, T>(
       nid[tg] = pf_node;
     }
     group_sync(bar, GT);
+    prefetch(batch + stride);
 
-    // 1. quadrature-point data: NPART lanes per (element, q) split the node sum
+    // 1. quadrature points: NPART lanes per (element, q) split the node sums,
+    //    every lane of the quad then forms J^-1 and the gradients of its nodes.
     for (int base = 0; base < EPG * NQ * NPART; base += GT) {
       const int i = base + tg;
       const int iq = i / NPART, part = i - iq * NPART;
@@ -297,166 +407,160 @@ __global__ void __launch_bounds__(Shape<P>::GT *Shape<P>::GPC, min_blocks<P, T>(
         g10 += __shfl_xor_sync(0xffffffffu, g10, o);
         g11 += __shfl_xor_sync(0xffffffffu, g11, o);
       }
-      if (act && part == 0) {
+      if (act) {
         const double det = j00 * j11 - j01 * j10;
         const double inv = 1.0 / det;
         const double i00 = j11 * inv, i01 = -j01 * inv, i10 = -j10 * inv, i11 = j00 * inv;
-        const double uxx = g00 * i00 + g01 * i10, uxy = g00 * i01 + g01 * i11;
-        const double uyx = g10 * i00 + g11 * i10, uyy = g10 * i01 + g11 * i11;
         const double st = wq[q] * det * A.t;
-        const double tr = uxx + uyy;
-        constexpr int SQ = EPG * NQ;
-        qd[0 * SQ + iq] = i00;
-        qd[1 * SQ + iq] = i01;
-        qd[2 * SQ + iq] = i10;
-        qd[3 * SQ + iq] = i11;
-        qd[4 * SQ + iq] = st * (2.0 * mu * uxx + lam * tr);
-        qd[5 * SQ + iq] = st * (mu * (uxy + uyx));
-        qd[6 * SQ + iq] = st * (2.0 * mu * uyy + lam * tr);
-        qd[7 * SQ + iq] = st;
-      }
-    }
-    group_sync(bar, GT);
-
-    // 2. real-space shape gradients G = dN J^-1 and H = w detJ t G
-    if constexpr ((MODE & kJac) != 0) {
-      constexpr int SQ = EPG * NQ;
-      for (int i = tg; i < ne * NQ * NN; i += GT) {
-        const int iq = i / NN, a = i - iq * NN;
-        const int q = iq % NQ;
-        const double2 d = tab[q * NN + a];
-        const double gx = d.x * qd[0 * SQ + iq] + d.y * qd[2 * SQ + iq];
-        const double gy = d.x * qd[1 * SQ + iq] + d.y * qd[3 * SQ + iq];
-        const double st = qd[7 * SQ + iq];
-        T2 gv, hv;
-        gv.x = T(gx);
-        gv.y = T(gy);
-        hv.x = T(st * gx);
-        hv.y = T(st * gy);
-        G[i] = gv;
-        H[i] = hv;
-      }
-    }
-    prefetch(batch + stride);
-    group_sync(bar, GT);
-
-    // 3a. residual R_a = sum_q S(q) G_a(q)
-    if constexpr ((MODE & kRes) != 0) {
-      constexpr int SQ = EPG * NQ;
-      for (int i = tg; i < ne * NN; i += GT) {
-        const int el = i / NN, a = i - el * NN;
-        T rx = 0, ry = 0;
-#pragma unroll 4
-        for (int q = 0; q < NQ; q++) {
-          const int iq = el * NQ + q;
-          T gx, gy;
-          if constexpr ((MODE & kJac) != 0) {
-            const T2 gv = G[iq * NN + a];
-            gx = gv.x;
-            gy = gv.y;
-          } else {
-            const double2 d = tab[q * NN + a];
-            gx = T(d.x * qd[0 * SQ + iq] + d.y * qd[2 * SQ + iq]);
-            gy = T(d.x * qd[1 * SQ + iq] + d.y * qd[3 * SQ + iq]);
-          }
-          const T sxx = T(qd[4 * SQ + iq]), sxy = T(qd[5 * SQ + iq]), syy = T(qd[6 * SQ + iq]);
-          rx = fma(sxx, gx, fma(sxy, gy, rx));
-          ry = fma(sxy, gx, fma(syy, gy, ry));
+        if (part == 0) {
+          const double uxx = g00 * i00 + g01 * i10, uxy = g00 * i01 + g01 * i11;
+          const double uyx = g10 * i00 + g11 * i10, uyy = g10 * i01 + g11 * i11;
+          const double tr = uxx + uyy;
+          S3[0 * SQ + iq] = st * (2.0 * mu * uxx + lam * tr);
+          S3[1 * SQ + iq] = st * (mu * (uxy + uyx));
+          S3[2 * SQ + iq] = st * (2.0 * mu * uyy + lam * tr);
         }
-        double *dst = A.residual + 2 * (int64_t)nid[i];
-        if constexpr ((MODE & kPlan) != 0) {
-          if (__ldg(A.nodeCode + (k0 + el) * NN + a)) {
-            *reinterpret_cast<double2 *>(dst) = make_double2(double(rx), double(ry));
+#pragma unroll 2
+        for (int a = part; a < NN; a += NPART) {
+          const double2 d = tabT[a * NQ + q];
+          const double gx = d.x * i00 + d.y * i10;
+          const double gy = d.x * i01 + d.y * i11;
+          if constexpr (TC) {
+            double *Gm = reinterpret_cast<double *>(gs + L::G) + (el * NQP + q) * RS;
+            *reinterpret_cast<double2 *>(Gm + 2 * a) = make_double2(gx, gy);
+            if constexpr ((MODE & kJac) != 0) {
+              double *Hm = reinterpret_cast<double *>(gs + L::H) + (el * NQP + q) * RS;
+              *reinterpret_cast<double2 *>(Hm + 2 * a) = make_double2(st * gx, st * gy);
+            }
+          } else {
+            T2 gv;
+            gv.x = T(gx);
+            gv.y = T(gy);
+            reinterpret_cast<T2 *>(gs + L::G)[iq * NNP + a] = gv;
+            if constexpr ((MODE & kJac) != 0) {
+              T2 hv;
+              hv.x = T(st * gx);
+              hv.y = T(st * gy);
+              reinterpret_cast<T2 *>(gs + L::H)[iq * NNP + a] = hv;
+            }
+          }
+        }
+      }
+    }
+    group_sync(bar, GT);
+
+    // 2a. residual R_a = sum_q S(q) G_a(q), NPART lanes per node split the q sum
+    if constexpr ((MODE & kRes) != 0) {
+      for (int base = 0; base < EPG * NN * NPART; base += GT) {
+        const int i = base + tg;
+        const int ia = i / NPART, part = i - ia * NPART;
+        const int el = ia / NN, a = ia - el * NN;
+        const bool act = i < EPG * NN * NPART && el < ne;
+        T rx = 0, ry = 0;
+        if (act) {
+#pragma unroll 2
+          for (int q = part; q < NQ; q += NPART) {
+            const int iq = el * NQ + q;
+            T gx, gy;
+            if constexpr (TC) {
+              const double2 gv = *reinterpret_cast<const double2 *>(reinterpret_cast<const double *>(gs + L::G) +
+                                                                     (el * NQP + q) * RS + 2 * a);
+              gx = gv.x;
+              gy = gv.y;
+            } else {
+              const T2 gv = reinterpret_cast<const T2 *>(gs + L::G)[iq * NNP + a];
+              gx = gv.x;
+              gy = gv.y;
+            }
+            const T sxx = T(S3[0 * SQ + iq]), sxy = T(S3[1 * SQ + iq]), syy = T(S3[2 * SQ + iq]);
+            rx = fma(sxx, gx, fma(sxy, gy, rx));
+            ry = fma(sxy, gx, fma(syy, gy, ry));
+          }
+        }
+#pragma unroll
+        for (int o = 1; o < NPART; o <<= 1) {
+          rx += __shfl_xor_sync(0xffffffffu, rx, o);
+          ry += __shfl_xor_sync(0xffffffffu, ry, o);
+        }
+        if (act && part == 0) {
+          double *dst = A.residual + 2 * (int64_t)nid[ia];
+          if constexpr ((MODE & kPlan) != 0) {
+            if (__ldg(A.nodeCode + (k0 + el) * NN + a)) {
+              *reinterpret_cast<double2 *>(dst) = make_double2(double(rx), double(ry));
+            } else {
+              atomicAdd(dst, double(rx));
+              atomicAdd(dst + 1, double(ry));
+            }
           } else {
             atomicAdd(dst, double(rx));
             atomicAdd(dst + 1, double(ry));
           }
-        } else {
-          atomicAdd(dst, double(rx));
-          atomicAdd(dst + 1, double(ry));
         }
       }
     }
 
-    // 3b. element stiffness on and above the diagonal; the block below is its transpose
+    // 2b. element stiffness
     if constexpr ((MODE & kJac) != 0) {
-      for (int i = tg; i < ne * NTILE; i += GT) {
-        const int el = i / NTILE;
-        int r = i - el * NTILE, at = 0;
-#pragma unroll
-        for (int row = 0; row < P1; row++) {
-          const int len = NN - row * P1;
-          if (at == row && r >= len) {
-            r -= len;
-            at = row + 1;
+      if constexpr (TC) {
+        // FP64 tensor cores: warps take (element, row range) work items
+        constexpr int WPE = (P == 4) ? 2 : 1;  // warps per element
+        constexpr int NW = GT / 32;
+        for (int w = warp; w < ne * WPE; w += NW) {
+          const int el = w / WPE, part = w - el * WPE;
+          const double *Gm = reinterpret_cast<const double *>(gs + L::G) + el * NQP * RS;
+          const double *Hm = reinterpret_cast<const double *>(gs + L::H) + el * NQP * RS;
+          if constexpr (WPE == 1) {
+            stiffness_mma<P, MODE, 0, D::NT8>(A, Gm, Hm, nid + el * NN, k0 + el, mu, lam, lane);
+          } else {
+            if (part == 0)
+              stiffness_mma<P, MODE, 0, 2>(A, Gm, Hm, nid + el * NN, k0 + el, mu, lam, lane);
+            else
+              stiffness_mma<P, MODE, 2, D::NT8>(A, Gm, Hm, nid + el * NN, k0 + el, mu, lam, lane);
           }
         }
-        const int b = at * P1 + r;
-        T m[P1][4];
+      } else {
+        // FP32 CUDA cores: one (p+1)-row tile x one column per thread, upper triangle
+        const T2 *G = reinterpret_cast<const T2 *>(gs + L::G);
+        const T2 *H = reinterpret_cast<const T2 *>(gs + L::H);
+        for (int i = tg; i < ne * NTILE; i += GT) {
+          const int el = i / NTILE;
+          int r = i - el * NTILE, at = 0;
 #pragma unroll
-        for (int ax = 0; ax < P1; ax++) m[ax][0] = m[ax][1] = m[ax][2] = m[ax][3] = T(0);
-        const T2 *Gb = G + el * NQ * NN + b;
-        const T2 *Ha = H + el * NQ * NN + at * P1;
+          for (int row = 0; row < P1; row++) {
+            const int len = NN - row * P1;
+            if (at == row && r >= len) {
+              r -= len;
+              at = row + 1;
+            }
+          }
+          const int b = at * P1 + r;
+          T m[P1][4];
+#pragma unroll
+          for (int ax = 0; ax < P1; ax++) m[ax][0] = m[ax][1] = m[ax][2] = m[ax][3] = T(0);
+          const T2 *Gb = G + el * NQ * NNP + b;
+          const T2 *Ha = H + el * NQ * NNP + at * P1;
 #pragma unroll 2
-        for (int q = 0; q < NQ; q++) {
-          const T2 gv = Gb[q * NN];
+          for (int q = 0; q < NQ; q++) {
+            const T2 gv = Gb[q * NNP];
+#pragma unroll
+            for (int ax = 0; ax < P1; ax++) {
+              const T2 hv = Ha[q * NNP + ax];
+              m[ax][0] = fma(hv.x, gv.x, m[ax][0]);
+              m[ax][1] = fma(hv.x, gv.y, m[ax][1]);
+              m[ax][2] = fma(hv.y, gv.x, m[ax][2]);
+              m[ax][3] = fma(hv.y, gv.y, m[ax][3]);
+            }
+          }
 #pragma unroll
           for (int ax = 0; ax < P1; ax++) {
-            const T2 hv = Ha[q * NN + ax];
-            m[ax][0] = fma(hv.x, gv.x, m[ax][0]);
-            m[ax][1] = fma(hv.x, gv.y, m[ax][1]);
-            m[ax][2] = fma(hv.y, gv.x, m[ax][2]);
-            m[ax][3] = fma(hv.y, gv.y, m[ax][3]);
-          }
-        }
-        const int64_t k = k0 + el;
-#pragma unroll
-        for (int ax = 0; ax < P1; ax++) {
-          const int a = at * P1 + ax;
-          if (a > b) continue;
-          const double kxx = double(cC11 * m[ax][0] + cMu * m[ax][3]);
-          const double kxy = double(cLam * m[ax][1] + cMu * m[ax][2]);
-          const double kyx = double(cLam * m[ax][2] + cMu * m[ax][1]);
-          const double kyy = double(cC11 * m[ax][3] + cMu * m[ax][0]);
-          if constexpr ((MODE & kPlan) != 0) {
-            const int ra = nid[el * NN + a], rb = nid[el * NN + b];
-            const uint8_t c0 = __ldg(A.blockCode + (k * NN + a) * NN + b);
-            double *b0 = A.mat + 4 * ((int64_t)__ldg(A.rowp + ra) + (c0 & 0x7f));
-            if (c0 & 0x80) {
-              store_block(b0, kxx, kxy, kyx, kyy);
-            } else {
-              // later colour: the first contributor's store is complete (previous
-              // launch) and no element of this colour shares the block
-              atomicAdd(b0 + 0, kxx);
-              atomicAdd(b0 + 1, kxy);
-              atomicAdd(b0 + 2, kyx);
-              atomicAdd(b0 + 3, kyy);
-            }
-            if (a != b) {
-              const uint8_t c1 = __ldg(A.blockCode + (k * NN + b) * NN + a);
-              double *b1 = A.mat + 4 * ((int64_t)__ldg(A.rowp + rb) + (c1 & 0x7f));
-              if (c1 & 0x80) {
-                store_block(b1, kxx, kyx, kxy, kyy);
-              } else {
-                atomicAdd(b1 + 0, kxx);
-                atomicAdd(b1 + 1, kyx);
-                atomicAdd(b1 + 2, kxy);
-                atomicAdd(b1 + 3, kyy);
-              }
-            }
-          } else {
-            double *b0 = A.mat + __ldg(A.map + (k * NN + a) * NN + b);
-            atomicAdd(b0 + 0, kxx);
-            atomicAdd(b0 + 1, kxy);
-            atomicAdd(b0 + 2, kyx);
-            atomicAdd(b0 + 3, kyy);
-            if (a != b) {
-              double *b1 = A.mat + __ldg(A.map + (k * NN + b) * NN + a);
-              atomicAdd(b1 + 0, kxx);
-              atomicAdd(b1 + 1, kyx);
-              atomicAdd(b1 + 2, kxy);
-              atomicAdd(b1 + 3, kyy);
-            }
+            const int a = at * P1 + ax;
+            if (a > b) continue;
+            const double kxx = double(cC11 * m[ax][0] + cMu * m[ax][3]);
+            const double kxy = double(cLam * m[ax][1] + cMu * m[ax][2]);
+            const double kyx = double(cLam * m[ax][2] + cMu * m[ax][1]);
+            const double kyy = double(cC11 * m[ax][3] + cMu * m[ax][0]);
+            write_block<NN, MODE>(A, k0 + el, nid + el * NN, a, b, 0, kxx, kxy, kyx, kyy);
+            if (a != b) write_block<NN, MODE>(A, k0 + el, nid + el * NN, a, b, 1, kxx, kxy, kyx, kyy);
           }
         }
       }

@@ -131,6 +131,13 @@ int fem_plan_assemble(const fem_plan *plan, const double *states, const double *
                       double t, double *residual, double *matEntries, int precision, void *stream,
                       double *elapsedSeconds);
 
+/* ---- calibration ---------------------------------------------------------------------- */
+/* Measured arithmetic peak of the current device in TFLOP/s, used as the
+ * roofline denominator of the element arithmetic: kind 0 = FP64 FMA pipe,
+ * 1 = FP32 FMA pipe, 2 = FP64 tensor-core MMA (m8n8k4).  Allocates a scratch
+ * buffer and synchronises the device.  (No reference counterpart.) */
+int fem_probe_peak(int kind, double *tflops);
+
 #ifdef __cplusplus
 }
 #endif
