@@ -319,6 +319,122 @@ def run_ours(args):
         pg.destroy_process_group()
 
 
+def mesh_bytes(spec, with_map=True):
+    """Device bytes of one batched mesh: plan topology, coordinates/states/residual,
+    BSR values and (for the single-mesh comparison) the reference element map."""
+    n = (spec.order + 1) ** 2
+    N, ne, nnzb = spec.num_nodes(), spec.num_elements, spec.nnzb()
+    plan = 4 * (N + 1) + 4 * nnzb + 4 * ne * n + ne * n * n + ne * n
+    data = 16 * N * 3 + 4 * ne * n + 4 * (ne + 1) + 32 * nnzb
+    return plan + data + (4 * ne * n * n if with_map else 0)
+
+
+def run_batch(args):
+    """Many meshes (log-uniform sizes 1e3..1e6 elements, orders 1..4) per graph launch,
+    in waves that fit the device-memory budget, against the single-mesh FP64 drop-in."""
+    import torch
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    import fem_pkg
+    fem = fem_pkg.load()
+    specs = fem.batch_specs(count=args.batch_meshes)
+    budget = args.budget_gb * 1e9
+    waves, cur, used = [], [], 0
+    for sp in specs:
+        b = mesh_bytes(sp)
+        if cur and used + b > budget:
+            waves.append(cur)
+            cur, used = [], 0
+        cur.append(sp)
+        used += b
+    if cur:
+        waves.append(cur)
+    stream = torch.cuda.Stream(device=dev)
+    sptr = stream.cuda_stream
+    tot_el, t_batch, t_plain, launches, graph_ms, errs, tiles = 0, 0.0, 0.0, 0, [], [], []
+
+    def ev_time(fn, reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps * 1e-3
+
+    for wave in waves:
+        meshes = [sp.build() for sp in wave]
+        plans = [fem.Plan(m.order, m.num_nodes, m.conn_ptr, m.conn) for m in meshes]
+        with torch.cuda.stream(stream):
+            devs = [fem.DeviceMesh(m, dev) for m in meshes]
+            res = [torch.empty(m.num_nodes * 2, dtype=torch.float64, device=dev) for m in meshes]
+            mat = [torch.empty(p.nnzb * 4, dtype=torch.float64, device=dev) for p in plans]
+        stream.synchronize()
+        batch = fem.Batch(plans)
+        for i, (m, d) in enumerate(zip(meshes, devs)):
+            batch.bind(i, d.states, d.coords, m.E, m.nu, m.t, res[i], mat[i])
+        prec = args.batch_precision
+        batch.tune(precision=prec, stream=sptr, reps=2)
+        tiles.append(batch.info()["tile_batches"])
+        batch.capture(precision=prec, stream=sptr)
+        for _ in range(args.warmup):
+            batch.replay(stream=sptr)
+        tb = ev_time(lambda: batch.replay(stream=sptr), args.steps)
+        launches += batch.info()["launches"] * args.steps
+        if prec == "mixed":
+            with torch.cuda.stream(stream):
+                keep = [(r.clone(), a.clone()) for r, a in zip(res[:8], mat[:8])]
+                batch.assemble(precision="fp64", stream=sptr)
+                for (r, a), r64, a64 in zip(keep, res[:8], mat[:8]):
+                    errs.append(max(float(torch.linalg.vector_norm(r - r64) / torch.linalg.vector_norm(r64)),
+                                    float(torch.linalg.vector_norm(a - a64) / torch.linalg.vector_norm(a64))))
+            del keep
+        # plain single-mesh FP64 drop-in (reference contract): zero outputs, one call per mesh
+        maps = []
+        for m, p in zip(meshes, plans):
+            rowp, cols = p.pattern()
+            mp = fem.build_element_bsr_map(m.conn_ptr, m.conn, m.nodes_per_element, rowp, cols)
+            maps.append(torch.from_numpy(mp).to(dev))
+
+        def plain():
+            for m, d, r, a, mp in zip(meshes, devs, res, mat, maps):
+                r.zero_()
+                a.zero_()
+                fem.run_jacobian_kernel(m.order, d.conn_ptr, d.conn, m.num_elements, d.states, d.coords, m.E, m.nu,
+                                        m.t, mp, r, a, stream=sptr, timed=False)
+
+        with torch.cuda.stream(stream):
+            plain()
+            tp = ev_time(plain, max(1, args.steps // 2))
+        tot_el += sum(m.num_elements for m in meshes)
+        t_batch += tb
+        t_plain += tp
+        graph_ms.append(tb * 1e3)
+        batch.close()
+        for p in plans:
+            p.close()
+        del meshes, plans, devs, res, mat, maps, batch
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+    value = tot_el / t_batch
+    line = {
+        "metric": "assembled elements/s (res+Jac)", "value": value, "unit": "elements/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_batch * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.batch_precision == "fp64" else "f32/f64",
+        "data": "synthetic",
+        "config": {"workload": f"batch{len(specs)}: element counts log-uniform in [1e3, 1e6], orders 1..4",
+                   "meshes": len(specs), "elements": tot_el, "waves": len(waves),
+                   "budget_gb": args.budget_gb, "precision": args.batch_precision,
+                   "l2": "per-wave inputs and outputs larger than L2"},
+        "plain_fp64_single_mesh": {"elements_per_s": tot_el / t_plain, "ms_per_step": t_plain * 1e3},
+        "batched_over_plain": t_plain / t_batch,
+        "wave_graph_ms": graph_ms, "tuned_tile_batches": tiles,
+        "mixed_rel_frobenius_err_max": max(errs) if errs else None,
+        "gpu_launches": launches,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def cpu_baseline(fem, mesh, args):
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as orc
@@ -365,7 +481,10 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="square1024_p3", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="square1024_p3", choices=sorted(WORKLOADS) + ["batch256"])
+    ap.add_argument("--batch-meshes", type=int, default=256)
+    ap.add_argument("--budget-gb", type=float, default=100.0, help="device bytes per batched wave")
+    ap.add_argument("--batch-precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--ref-elements", type=int, default=131072)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--paths", default="plan_fp64,plan_mixed,dropin_fp64",
@@ -380,6 +499,8 @@ def main():
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batch256":
+        run_batch(args)
     else:
         run_ours(args)
 

@@ -55,10 +55,13 @@ SIGNATURES = {
     "fem_probe_peak": (_i, [_i, _pd]),
     "fem_batch_create": (_i, [_i, _p, C.POINTER(_p)]),
     "fem_batch_destroy": (_i, [_p]),
+    "fem_batch_bind": (_i, [_p, _i, _p, _p, _d, _d, _d, _p, _p]),
     "fem_batch_info": (_i, [_p, _pi64, _pi64, _pi, _pi64]),
-    "fem_batch_assemble": (_i, [_p, _p, _p, _p, _p, _p, _i, _p, _pd]),
-    "fem_batch_tune": (_i, [_p, _p, _p, _p, _p, _p, _i, _p, _i, _pd]),
-    "fem_batch_capture": (_i, [_p, _p, _p, _p, _p, _p, _i, _p]),
+    "fem_batch_get_tiles": (_i, [_p, _p]),
+    "fem_batch_set_tiles": (_i, [_p, _p]),
+    "fem_batch_assemble": (_i, [_p, _i, _p, _pd]),
+    "fem_batch_tune": (_i, [_p, _i, _p, _i, _pd]),
+    "fem_batch_capture": (_i, [_p, _i, _p]),
     "fem_batch_replay": (_i, [_p, _p, _pd]),
 }
 

@@ -184,6 +184,69 @@ class Plan:
             pass
 
 
+class Batch:
+    """Many meshes assembled together (fem_batch_*): one persistent kernel per
+    (order, colour) pulls element tiles from a work queue; orders run concurrently.
+    The plans must stay alive as long as the batch (the batch keeps references)."""
+
+    def __init__(self, plans):
+        self.plans = list(plans)
+        arr = (C.c_void_p * len(self.plans))(*[p.handle for p in self.plans])
+        self._h = C.c_void_p()
+        check(lib.fem_batch_create(len(self.plans), arr, C.byref(self._h)), "fem_batch_create")
+
+    def bind(self, mesh, states, node_coords, E, nu, t, residual, mat_entries):
+        import torch
+        check(lib.fem_batch_bind(self._h, int(mesh), _dptr(states, torch.float64, "states"),
+                                 _dptr(node_coords, torch.float64, "nodeCoords"), float(E), float(nu), float(t),
+                                 _dptr(residual, torch.float64, "residual"),
+                                 _dptr(mat_entries, torch.float64, "matEntries")), "fem_batch_bind")
+
+    def info(self):
+        ne, nt, bytes_ = C.c_int64(), C.c_int64(), C.c_int64()
+        nl = C.c_int()
+        check(lib.fem_batch_info(self._h, C.byref(ne), C.byref(nt), C.byref(nl), C.byref(bytes_)), "fem_batch_info")
+        tiles = (C.c_int * 4)()
+        check(lib.fem_batch_get_tiles(self._h, tiles), "fem_batch_get_tiles")
+        return {"elements": ne.value, "tiles": nt.value, "launches": nl.value, "device_bytes": bytes_.value,
+                "tile_batches": list(tiles)}
+
+    def set_tiles(self, tile_batches):
+        arr = (C.c_int * 4)(*[int(x) for x in tile_batches])
+        check(lib.fem_batch_set_tiles(self._h, arr), "fem_batch_set_tiles")
+
+    def assemble(self, *, precision="fp64", stream=None, timed=False):
+        el = C.c_double(0.0)
+        check(lib.fem_batch_assemble(self._h, _prec(precision), _stream(stream), C.byref(el) if timed else None),
+              "fem_batch_assemble")
+        return el.value if timed else None
+
+    def tune(self, *, precision="fp64", stream=None, reps=3):
+        best = C.c_double(0.0)
+        check(lib.fem_batch_tune(self._h, _prec(precision), _stream(stream), int(reps), C.byref(best)),
+              "fem_batch_tune")
+        return best.value
+
+    def capture(self, *, precision="fp64", stream=None):
+        check(lib.fem_batch_capture(self._h, _prec(precision), _stream(stream)), "fem_batch_capture")
+
+    def replay(self, *, stream=None, timed=False):
+        el = C.c_double(0.0)
+        check(lib.fem_batch_replay(self._h, _stream(stream), C.byref(el) if timed else None), "fem_batch_replay")
+        return el.value if timed else None
+
+    def close(self):
+        if self._h and self._h.value:
+            lib.fem_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class DeviceMesh:
     """A Mesh uploaded to the GPU as torch tensors (int32 topology, float64 data)."""
 

@@ -5,6 +5,7 @@ in-tree so that it travels with the repository to the GPU machine.
 """
 from __future__ import annotations
 
+import concurrent.futures
 import os
 import pathlib
 import subprocess
@@ -16,7 +17,7 @@ CSRC = PKG / "csrc"
 INCLUDE = ROOT / "include"
 LIB = PKG / "libfemb200.so"
 
-SOURCES = ["fem_kernels.cu", "fem_host.cpp", "fem_probe.cu"]
+SOURCES = ["fem_kernels.cu", "fem_batch.cu", "fem_host.cpp", "fem_probe.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -37,10 +38,10 @@ def build(force: bool = False, verbose: bool = False) -> pathlib.Path:
     deps = srcs + list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
     if not force and not _stale(LIB, deps):
         return LIB
-    objs = []
     obj_dir = PKG / "_build"
     obj_dir.mkdir(exist_ok=True)
     common = [f"-I{INCLUDE}", f"-I{CSRC}", "-O3", "-std=c++17"]
+    cmds, objs = [], []
     for src in srcs:
         obj = obj_dir / (src.name + ".o")
         if src.suffix == ".cu":
@@ -49,8 +50,10 @@ def build(force: bool = False, verbose: bool = False) -> pathlib.Path:
                 cmd.insert(1, "-Xptxas=-v")
         else:
             cmd = ["g++", "-fPIC", "-fopenmp", *common, "-c", str(src), "-o", str(obj)]
-        _run(cmd)
+        cmds.append(cmd)
         objs.append(str(obj))
+    with concurrent.futures.ThreadPoolExecutor(max_workers=len(cmds)) as ex:
+        list(ex.map(_run, cmds))
     _run([_nvcc(), *ARCH, "-shared", "-Xcompiler", "-fopenmp", "-o", str(LIB), *objs, "-lgomp"])
     return LIB
 

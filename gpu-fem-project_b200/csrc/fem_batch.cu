@@ -1,0 +1,438 @@
+// Batched assembly of many meshes of mixed orders (fem_batch_*).
+//
+// Every mesh brings an assembly plan (colour-ordered elements, block codes).  The
+// batch cuts each mesh's colour ranges into tiles and keeps one work queue per
+// (order, colour): a tile list plus an atomic counter.  One persistent kernel per
+// (order, colour) lets its groups pull tiles until the queue is empty, so meshes
+// of very different sizes share the GPU without per-mesh launches.  Orders are
+// independent chains on their own streams (colours of one order run in sequence:
+// a later colour adds to blocks an earlier one stored); the whole fork/join
+// pattern is captured once into a CUDA graph and replayed with one launch.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <vector>
+
+#include "fem_common.h"
+#include "fem_device.cuh"
+#include "fem_launch.h"
+
+namespace {
+
+constexpr int kMaxColours = 64;
+constexpr int kOrders = 5;  // index 1..4
+
+int epg_of(int p) {
+  switch (p) {
+    case 1: return fem::dev::Shape<1>::EPG;
+    case 2: return fem::dev::Shape<2>::EPG;
+    case 3: return fem::dev::Shape<3>::EPG;
+    default: return fem::dev::Shape<4>::EPG;
+  }
+}
+
+template <int P, typename T>
+int launch_batched_p(const fem::dev::AsmArgs *meshes, const fem::dev::Tile *tiles, int ntiles, int *counter,
+                     cudaStream_t s) {
+  using S = fem::dev::Shape<P>;
+  constexpr int NT = S::GT * S::GPC;
+  constexpr int MODE = fem::dev::kPlan | fem::dev::kRes | fem::dev::kJac;
+  auto kernel = fem::dev::assemble_batched_kernel<P, T, MODE>;
+  const size_t smem = fem::dev::Layout<P, T>::total;
+  fem::LaunchInfo li;
+  int st = fem::launch_info(kernel, NT, smem, li);
+  if (st) return st;
+  const int64_t need = (ntiles + S::GPC - 1) / S::GPC;
+  const int64_t cap = (int64_t)li.grid_per_sm * li.num_sms;
+  const int grid = (int)std::min(need, cap);
+  if (grid <= 0) return FEM_SUCCESS;
+  kernel<<<grid, NT, smem, s>>>(meshes, tiles, ntiles, counter);
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return fem::cuda_fail(err, "assemble_batched_kernel launch");
+  return FEM_SUCCESS;
+}
+
+template <typename T>
+int launch_batched(int p, const fem::dev::AsmArgs *meshes, const fem::dev::Tile *tiles, int ntiles, int *counter,
+                   cudaStream_t s) {
+  switch (p) {
+    case 1: return launch_batched_p<1, T>(meshes, tiles, ntiles, counter, s);
+    case 2: return launch_batched_p<2, T>(meshes, tiles, ntiles, counter, s);
+    case 3: return launch_batched_p<3, T>(meshes, tiles, ntiles, counter, s);
+    case 4: return launch_batched_p<4, T>(meshes, tiles, ntiles, counter, s);
+    default: return fem::fail(FEM_ERR_INVALID_ORDER, "order %d", p);
+  }
+}
+
+}  // namespace
+
+struct fem_batch {
+  int device = 0;
+  std::vector<const fem_plan *> plans;
+  std::vector<fem::dev::AsmArgs> args;
+  std::vector<char> bound;
+  fem::dev::AsmArgs *d_args = nullptr;
+  bool args_dirty = true;
+  int maxColours = 0;
+  int tileBatches[kOrders] = {0, 16, 16, 16, 16};  // tile length in element batches, per order
+  std::vector<fem::dev::Tile> tiles;
+  std::vector<int> tileOff;  // [kOrders][maxColours + 1]
+  fem::dev::Tile *d_tiles = nullptr;
+  size_t d_tiles_cap = 0;
+  bool tiles_dirty = true;
+  int *d_counters = nullptr;  // [kOrders][kMaxColours]
+  cudaStream_t streams[kOrders] = {};  // [0]: capture stream, [1..4]: one per order
+  cudaEvent_t fork = nullptr, join[kOrders] = {};
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int graphPrecision = -1;
+  int64_t totalElements = 0;
+  int64_t deviceBytes = 0;
+};
+
+namespace {
+
+void drop_graph(fem_batch *b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+  b->graphPrecision = -1;
+}
+
+void batch_free(fem_batch *b) {
+  if (!b) return;
+  int cur = 0;
+  cudaGetDevice(&cur);
+  cudaSetDevice(b->device);
+  drop_graph(b);
+  cudaFree(b->d_args);
+  cudaFree(b->d_tiles);
+  cudaFree(b->d_counters);
+  for (int p = 0; p < kOrders; p++) {
+    if (b->streams[p]) cudaStreamDestroy(b->streams[p]);
+    if (b->join[p]) cudaEventDestroy(b->join[p]);
+  }
+  if (b->fork) cudaEventDestroy(b->fork);
+  cudaSetDevice(cur);
+  delete b;
+}
+
+int order_of(const fem_batch *b, int m) { return b->plans[m]->order; }
+
+void build_tiles(fem_batch *b) {
+  const int C = b->maxColours;
+  b->tiles.clear();
+  b->tileOff.assign((size_t)kOrders * (C + 1), 0);
+  for (int p = 1; p < kOrders; p++) {
+    const int64_t len = (int64_t)b->tileBatches[p] * epg_of(p);
+    for (int c = 0; c < C; c++) {
+      b->tileOff[p * (C + 1) + c] = (int)b->tiles.size();
+      for (size_t m = 0; m < b->plans.size(); m++) {
+        const fem_plan *pl = b->plans[m];
+        if (pl->order != p || c >= pl->numColours) continue;
+        for (int64_t k = pl->colourPtr[c]; k < pl->colourPtr[c + 1]; k += len) {
+          fem::dev::Tile t;
+          t.mesh = (int)m;
+          t.begin = k;
+          t.count = (int)std::min<int64_t>(len, pl->colourPtr[c + 1] - k);
+          b->tiles.push_back(t);
+        }
+      }
+    }
+    b->tileOff[p * (C + 1) + C] = (int)b->tiles.size();
+  }
+  b->tiles_dirty = true;
+}
+
+int sync_device_state(fem_batch *b) {
+  cudaError_t err;
+  if (b->args_dirty) {
+    err = cudaMemcpy(b->d_args, b->args.data(), sizeof(fem::dev::AsmArgs) * b->args.size(), cudaMemcpyHostToDevice);
+    if (err != cudaSuccess) return fem::cuda_fail(err, "cudaMemcpy(mesh table)");
+    b->args_dirty = false;
+  }
+  if (b->tiles_dirty) {
+    const size_t need = std::max<size_t>(b->tiles.size(), 1);
+    if (need > b->d_tiles_cap) {
+      cudaFree(b->d_tiles);
+      b->d_tiles = nullptr;
+      err = cudaMalloc(&b->d_tiles, sizeof(fem::dev::Tile) * need);
+      if (err != cudaSuccess) return fem::cuda_fail(err, "cudaMalloc(tiles)");
+      b->d_tiles_cap = need;
+    }
+    if (!b->tiles.empty()) {
+      err = cudaMemcpy(b->d_tiles, b->tiles.data(), sizeof(fem::dev::Tile) * b->tiles.size(),
+                       cudaMemcpyHostToDevice);
+      if (err != cudaSuccess) return fem::cuda_fail(err, "cudaMemcpy(tiles)");
+    }
+    b->tiles_dirty = false;
+  }
+  return FEM_SUCCESS;
+}
+
+// The colour chain of one order on stream s (counters reset by the caller).
+int enqueue_order(fem_batch *b, int p, int precision, cudaStream_t s) {
+  const int C = b->maxColours;
+  for (int c = 0; c < C; c++) {
+    const int t0 = b->tileOff[p * (C + 1) + c], t1 = b->tileOff[p * (C + 1) + c + 1];
+    if (t1 <= t0) continue;
+    int *counter = b->d_counters + p * kMaxColours + c;
+    int st = precision == FEM_PRECISION_FP64
+                 ? launch_batched<double>(p, b->d_args, b->d_tiles + t0, t1 - t0, counter, s)
+                 : launch_batched<float>(p, b->d_args, b->d_tiles + t0, t1 - t0, counter, s);
+    if (st) return st;
+  }
+  return FEM_SUCCESS;
+}
+
+bool order_has_work(const fem_batch *b, int p) {
+  const int C = b->maxColours;
+  return b->tileOff[p * (C + 1) + C] > b->tileOff[p * (C + 1)];
+}
+
+// Whole batch: reset queues, fork one stream per order, join back into s.
+int enqueue(fem_batch *b, int precision, cudaStream_t s) {
+  cudaError_t err = cudaMemsetAsync(b->d_counters, 0, sizeof(int) * kOrders * kMaxColours, s);
+  if (err != cudaSuccess) return fem::cuda_fail(err, "cudaMemsetAsync(counters)");
+  if ((err = cudaEventRecord(b->fork, s)) != cudaSuccess) return fem::cuda_fail(err, "cudaEventRecord");
+  for (int p = 1; p < kOrders; p++) {
+    if (!order_has_work(b, p)) continue;
+    if ((err = cudaStreamWaitEvent(b->streams[p], b->fork, 0)) != cudaSuccess)
+      return fem::cuda_fail(err, "cudaStreamWaitEvent");
+    int st = enqueue_order(b, p, precision, b->streams[p]);
+    if (st) return st;
+    if ((err = cudaEventRecord(b->join[p], b->streams[p])) != cudaSuccess)
+      return fem::cuda_fail(err, "cudaEventRecord");
+    if ((err = cudaStreamWaitEvent(s, b->join[p], 0)) != cudaSuccess)
+      return fem::cuda_fail(err, "cudaStreamWaitEvent");
+  }
+  return FEM_SUCCESS;
+}
+
+int check_ready(fem_batch *b, int precision) {
+  if (precision != FEM_PRECISION_FP64 && precision != FEM_PRECISION_MIXED)
+    return fem::fail(FEM_ERR_INVALID_ARGUMENT, "precision %d", precision);
+  for (size_t m = 0; m < b->bound.size(); m++)
+    if (!b->bound[m]) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "mesh %zu has no bound arrays", m);
+  return sync_device_state(b);
+}
+
+}  // namespace
+
+extern "C" {
+
+int fem_batch_create(int numMeshes, fem_plan *const *plans, fem_batch **batch) {
+  fem::clear_error();
+  if (!batch) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "batch is NULL");
+  *batch = nullptr;
+  if (numMeshes <= 0 || !plans) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "no meshes");
+  fem_batch *b = new fem_batch();
+  cudaGetDevice(&b->device);
+  for (int m = 0; m < numMeshes; m++) {
+    if (!plans[m]) {
+      delete b;
+      return fem::fail(FEM_ERR_INVALID_ARGUMENT, "plan %d is NULL", m);
+    }
+    if (plans[m]->numColours > kMaxColours) {
+      delete b;
+      return fem::fail(FEM_ERR_UNSUPPORTED, "plan %d has %d colours (max %d)", m, plans[m]->numColours, kMaxColours);
+    }
+    b->plans.push_back(plans[m]);
+    b->maxColours = std::max(b->maxColours, plans[m]->numColours);
+    b->totalElements += plans[m]->numElements;
+    fem::dev::AsmArgs a{};
+    a.connList = plans[m]->d_connList;
+    a.blockCode = plans[m]->d_blockCode;
+    a.nodeCode = plans[m]->d_nodeCode;
+    a.rowp = plans[m]->d_rowp;
+    b->args.push_back(a);
+  }
+  b->bound.assign(numMeshes, 0);
+  cudaError_t err = cudaMalloc(&b->d_args, sizeof(fem::dev::AsmArgs) * numMeshes);
+  if (err == cudaSuccess) err = cudaMalloc(&b->d_counters, sizeof(int) * kOrders * kMaxColours);
+  if (err == cudaSuccess) err = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+  for (int p = 0; p < kOrders && err == cudaSuccess; p++) {
+    err = cudaStreamCreateWithFlags(&b->streams[p], cudaStreamNonBlocking);
+    if (err == cudaSuccess) err = cudaEventCreateWithFlags(&b->join[p], cudaEventDisableTiming);
+  }
+  if (err != cudaSuccess) {
+    int st = fem::cuda_fail(err, "fem_batch_create");
+    batch_free(b);
+    return st;
+  }
+  b->deviceBytes = (int64_t)(sizeof(fem::dev::AsmArgs) * numMeshes + sizeof(int) * kOrders * kMaxColours);
+  build_tiles(b);
+  *batch = b;
+  return FEM_SUCCESS;
+}
+
+int fem_batch_destroy(fem_batch *batch) {
+  fem::clear_error();
+  batch_free(batch);
+  return FEM_SUCCESS;
+}
+
+int fem_batch_bind(fem_batch *b, int mesh, const double *states, const double *nodeCoords, double E, double nu,
+                   double t, double *residual, double *matEntries) {
+  fem::clear_error();
+  if (!b || mesh < 0 || mesh >= (int)b->plans.size()) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "bad mesh index");
+  if (!states || !nodeCoords || !residual || !matEntries)
+    return fem::fail(FEM_ERR_INVALID_ARGUMENT, "batched meshes need states, coordinates, residual and matrix");
+  if (!fem::aligned16(states) || !fem::aligned16(nodeCoords) || !fem::aligned16(residual) ||
+      (reinterpret_cast<uintptr_t>(matEntries) & 31u))
+    return fem::fail(FEM_ERR_MISALIGNED, "16-byte aligned vectors and a 32-byte aligned matrix are required");
+  fem::dev::AsmArgs &a = b->args[mesh];
+  a.states = states;
+  a.coords = nodeCoords;
+  a.residual = residual;
+  a.mat = matEntries;
+  fem::set_material(a, E, nu, t);
+  a.begin = 0;
+  a.count = b->plans[mesh]->numElements;
+  b->bound[mesh] = 1;
+  b->args_dirty = true;
+  return FEM_SUCCESS;
+}
+
+int fem_batch_info(const fem_batch *b, int64_t *totalElements, int64_t *numTiles, int *numLaunches,
+                   int64_t *deviceBytes) {
+  fem::clear_error();
+  if (!b) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "batch is NULL");
+  if (totalElements) *totalElements = b->totalElements;
+  if (numTiles) *numTiles = (int64_t)b->tiles.size();
+  if (numLaunches) {
+    int n = 0;
+    const int C = b->maxColours;
+    for (int p = 1; p < kOrders; p++)
+      for (int c = 0; c < C; c++) n += b->tileOff[p * (C + 1) + c + 1] > b->tileOff[p * (C + 1) + c];
+    *numLaunches = n;
+  }
+  if (deviceBytes) *deviceBytes = b->deviceBytes + (int64_t)(sizeof(fem::dev::Tile) * b->d_tiles_cap);
+  return FEM_SUCCESS;
+}
+
+int fem_batch_get_tiles(const fem_batch *b, int *tileBatches) {
+  fem::clear_error();
+  if (!b || !tileBatches) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "NULL argument");
+  for (int p = 1; p < kOrders; p++) tileBatches[p - 1] = b->tileBatches[p];
+  return FEM_SUCCESS;
+}
+
+int fem_batch_set_tiles(fem_batch *b, const int *tileBatches) {
+  fem::clear_error();
+  if (!b || !tileBatches) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "NULL argument");
+  for (int p = 1; p < kOrders; p++)
+    if (tileBatches[p - 1] < 1) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "tile length must be >= 1");
+  for (int p = 1; p < kOrders; p++) b->tileBatches[p] = tileBatches[p - 1];
+  build_tiles(b);
+  drop_graph(b);
+  return FEM_SUCCESS;
+}
+
+int fem_batch_assemble(fem_batch *b, int precision, void *stream, double *elapsedSeconds) {
+  fem::clear_error();
+  if (elapsedSeconds) *elapsedSeconds = 0;
+  if (!b) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "batch is NULL");
+  int st = check_ready(b, precision);
+  if (st) return st;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  return fem::timed(s, elapsedSeconds, [&] { return enqueue(b, precision, s); });
+}
+
+int fem_batch_capture(fem_batch *b, int precision, void *stream) {
+  fem::clear_error();
+  if (!b) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "batch is NULL");
+  int st = check_ready(b, precision);
+  if (st) return st;
+  // The warm-up run sets the kernels' shared-memory attributes (not capturable)
+  // after the caller's pending work on `stream`; the capture itself runs on the
+  // batch's own stream (the legacy default stream cannot be captured).
+  cudaStream_t user = reinterpret_cast<cudaStream_t>(stream);
+  cudaStream_t s = b->streams[0];
+  cudaError_t err = cudaEventRecord(b->join[0], user);
+  if (err == cudaSuccess) err = cudaStreamWaitEvent(s, b->join[0], 0);
+  if (err != cudaSuccess) return fem::cuda_fail(err, "ordering after the caller's stream");
+  st = enqueue(b, precision, s);
+  if (st) return st;
+  err = cudaStreamSynchronize(s);
+  if (err != cudaSuccess) return fem::cuda_fail(err, "warm-up before capture");
+  drop_graph(b);
+  err = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+  if (err != cudaSuccess) return fem::cuda_fail(err, "cudaStreamBeginCapture");
+  st = enqueue(b, precision, s);
+  cudaGraph_t g = nullptr;
+  err = cudaStreamEndCapture(s, &g);
+  if (st) {
+    if (g) cudaGraphDestroy(g);
+    return st;
+  }
+  if (err != cudaSuccess) return fem::cuda_fail(err, "cudaStreamEndCapture");
+  b->graph = g;
+  err = cudaGraphInstantiate(&b->exec, g, 0);
+  if (err != cudaSuccess) {
+    drop_graph(b);
+    return fem::cuda_fail(err, "cudaGraphInstantiate");
+  }
+  b->graphPrecision = precision;
+  return FEM_SUCCESS;
+}
+
+int fem_batch_replay(fem_batch *b, void *stream, double *elapsedSeconds) {
+  fem::clear_error();
+  if (elapsedSeconds) *elapsedSeconds = 0;
+  if (!b || !b->exec) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "no captured graph (call fem_batch_capture)");
+  int st = sync_device_state(b);
+  if (st) return st;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  return fem::timed(s, elapsedSeconds, [&] {
+    cudaError_t err = cudaGraphLaunch(b->exec, s);
+    return err == cudaSuccess ? (int)FEM_SUCCESS : fem::cuda_fail(err, "cudaGraphLaunch");
+  });
+}
+
+int fem_batch_tune(fem_batch *b, int precision, void *stream, int reps, double *bestSeconds) {
+  fem::clear_error();
+  if (!b) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "batch is NULL");
+  if (reps < 1) reps = 1;
+  int st = check_ready(b, precision);
+  if (st) return st;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  static const int cand[] = {1, 4, 16, 64, 256};
+  double total = 0;
+  for (int p = 1; p < kOrders; p++) {
+    if (!order_has_work(b, p)) continue;
+    double best = 1e30;
+    int bestLen = b->tileBatches[p];
+    for (int len : cand) {
+      b->tileBatches[p] = len;
+      build_tiles(b);
+      if ((st = sync_device_state(b))) return st;
+      double secs = 0;
+      for (int r = 0; r <= reps; r++) {  // first run warms up
+        double one = 0;
+        st = fem::timed(s, &one, [&] {
+          cudaError_t err = cudaMemsetAsync(b->d_counters, 0, sizeof(int) * kOrders * kMaxColours, s);
+          if (err != cudaSuccess) return fem::cuda_fail(err, "cudaMemsetAsync");
+          return enqueue_order(b, p, precision, s);
+        });
+        if (st) return st;
+        if (r > 0) secs += one;
+      }
+      secs /= reps;
+      if (secs < best) {
+        best = secs;
+        bestLen = len;
+      }
+    }
+    b->tileBatches[p] = bestLen;
+    total += best;
+  }
+  build_tiles(b);
+  drop_graph(b);
+  if (bestSeconds) *bestSeconds = total;
+  return sync_device_state(b);
+}
+
+}  // extern "C"

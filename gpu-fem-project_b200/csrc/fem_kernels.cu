@@ -28,546 +28,13 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
-#include <map>
-#include <mutex>
-#include <utility>
 
 #include "fem_common.h"
+#include "fem_device.cuh"
+#include "fem_launch.h"
 
 namespace fem {
 namespace dev {
-
-// Gauss-Legendre points/weights (element/GaussQuadrature.h:47-100), p+1 per direction.
-__constant__ double kGX[5][5] = {
-    {0.0, 0, 0, 0, 0},
-    {-0.577350269189626, 0.577350269189626, 0, 0, 0},
-    {-0.774596669241483, 0.0, 0.774596669241483, 0, 0},
-    {-0.861136311594053, -0.339981043584856, 0.339981043584856, 0.861136311594053, 0},
-    {-0.906179845938664, -0.538469310105683, 0.0, 0.538469310105683, 0.906179845938664},
-};
-__constant__ double kGW[5][5] = {
-    {2.0, 0, 0, 0, 0},
-    {1.0, 1.0, 0, 0, 0},
-    {5.0 / 9.0, 8.0 / 9.0, 5.0 / 9.0, 0, 0},
-    {0.347854845137454, 0.652145154862546, 0.652145154862546, 0.347854845137454, 0},
-    {0.236926885056189, 0.478628670499366, 0.568888888888889, 0.478628670499366, 0.236926885056189},
-};
-// Cosine-knot Lagrange monomial coefficients, highest power first
-// (element/LagrangeShapeFuncs.h:131-216), [order][node][coefficient].
-__constant__ double kCoef[5][5][5] = {
-    {{0}},
-    {{-0.5, 0.5}, {0.5, 0.5}},
-    {{0.5, -0.5, 0.0}, {-1.0, 0.0, 1.0}, {0.5, 0.5, 0.0}},
-    {{-2.0 / 3.0, 2.0 / 3.0, 1.0 / 6.0, -1.0 / 6.0},
-     {4.0 / 3.0, -2.0 / 3.0, -4.0 / 3.0, 2.0 / 3.0},
-     {-4.0 / 3.0, -2.0 / 3.0, 4.0 / 3.0, 2.0 / 3.0},
-     {2.0 / 3.0, 2.0 / 3.0, -1.0 / 6.0, -1.0 / 6.0}},
-    {{1.0, -1.0, -0.5, 0.5, 0.0},
-     {-2.0, 1.41421356237310, 2.0, -1.41421356237310, 0.0},
-     {2.0, 0.0, -3., 0.0, 1.0},
-     {-2.0, -1.41421356237310, 2.0, 1.41421356237310, 0.0},
-     {1.0, 1.0, -0.5, -0.5, 0.0}},
-};
-
-// lagrangePoly1dDeriv<double,p> (element/LagrangeShapeFuncs.h:129-216) with the
-// rounding of every step pinned, so the table matches the host restatement bit for bit.
-__device__ __forceinline__ void lag1d(int p, double x, int k, double &N, double &dN) {
-  const double *c = kCoef[p][k];
-  if (p == 1) {
-    N = __fma_rn(c[0], x, c[1]);
-    dN = c[0];
-  } else if (p == 2) {
-    N = __fma_rn(c[0], __dmul_rn(x, x), __fma_rn(c[1], x, c[2]));
-    dN = __fma_rn(__dmul_rn(2.0, c[0]), x, c[1]);
-  } else if (p == 3) {
-    const double x2 = __dmul_rn(x, x), x3 = __dmul_rn(x2, x);
-    N = __fma_rn(c[0], x3, __fma_rn(c[1], x2, __fma_rn(c[2], x, c[3])));
-    dN = __fma_rn(__dmul_rn(3.0, c[0]), x2, __fma_rn(__dmul_rn(2.0, c[1]), x, c[2]));
-  } else {
-    const double x2 = __dmul_rn(x, x), x3 = __dmul_rn(x2, x), x4 = __dmul_rn(x2, x2);
-    N = __fma_rn(c[0], x4, __fma_rn(c[1], x3, __fma_rn(c[2], x2, __fma_rn(c[3], x, c[4]))));
-    dN = __fma_rn(__dmul_rn(4.0, c[0]), x3,
-                  __fma_rn(__dmul_rn(3.0, c[1]), x2, __fma_rn(__dmul_rn(2.0, c[2]), x, c[3])));
-  }
-}
-
-// One 2x2 block (32 bytes, 32-byte aligned) with a single 256-bit store.
-__device__ __forceinline__ void store_block(double *p, double a, double b, double c, double d) {
-  asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(a), "d"(b), "d"(c), "d"(d) : "memory");
-}
-
-template <typename T>
-struct Vec2;
-template <>
-struct Vec2<double> {
-  using type = double2;
-};
-template <>
-struct Vec2<float> {
-  using type = float2;
-};
-
-enum : int { kRes = 1, kJac = 2, kPlan = 4 };
-
-struct AsmArgs {
-  const int *connPtr;      // drop-in: CSR offsets
-  const int *conn;         // drop-in: node ids
-  const int *map;          // drop-in: element block offsets (doubles)
-  const int *connList;     // plan: node ids of the listed elements, nn each
-  const uint8_t *blockCode;  // plan: rank-in-row | 0x80 store flag, nn*nn per listed element
-  const uint8_t *nodeCode;   // plan: 1 store / 0 add, nn per listed element
-  const int *rowp;           // plan: BSR row pointers
-  const double *states;
-  const double *coords;
-  double *residual;
-  double *mat;
-  double mu, lam, t;
-  int64_t begin, count;  // element (or list position) range of this launch
-};
-
-constexpr size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
-
-// Launch shape per order: GT threads per group, EPG elements per group step,
-// GPC independent groups per CTA (each synchronises on its own named barrier),
-// NPART threads per quadrature point in the Jacobian stage, MINB resident CTAs
-// per SM the register budget is sized for.  Stiffness-stage threads per element:
-// the (p+1)-row tiles on or above the diagonal, 6 / 18 / 40 / 75 for p = 1..4.
-template <int P>
-struct Shape;
-template <>
-struct Shape<1> {
-  static constexpr int GT = 64, EPG = 8, GPC = 4, NPART = 2, MINB = 4;
-};
-template <>
-struct Shape<2> {
-  static constexpr int GT = 64, EPG = 2, GPC = 4, NPART = 2, MINB = 4;
-};
-template <>
-struct Shape<3> {
-  static constexpr int GT = 64, EPG = 2, GPC = 2, NPART = 2, MINB = 4;
-};
-template <>
-struct Shape<4> {
-  static constexpr int GT = 64, EPG = 1, GPC = 2, NPART = 2, MINB = 3;
-};
-
-template <int P>
-struct Dims {
-  static constexpr int P1 = P + 1, NN = P1 * P1, NQ = NN;
-  // upper-triangle row tiles: row tile `at` covers nodes at*P1 .. at*P1+P, columns b >= at*P1
-  static constexpr int NTILE = P1 * NN - P1 * P1 * (P1 - 1) / 2;
-  // FP64 tensor-core (m8n8k4) geometry of M = H^T G: rows/cols r = 2*node + component
-  // padded to NT8 tiles of 8, the quadrature (k) dimension padded to NQP = 4*KS,
-  // shared-memory row stride RS doubles with RS = 4 or 12 (mod 16): the four
-  // quadrature rows of a fragment load then cover every bank exactly twice, and
-  // the 16-byte gradient stores of the quadrature stage spread over all 8 bank groups.
-  static constexpr int NT8 = (2 * NN + 7) / 8;
-  static constexpr int KS = (NQ + 3) / 4, NQP = 4 * KS;
-  static constexpr int RS = 8 * NT8 + 4;  // 8*NT8 is 0 or 8 mod 16
-};
-
-// Shared memory: per-CTA table, then GPC group regions.
-//   FP64 (tensor-core stiffness): G and H as [NQP][RS] doubles, row r = 2a + i.
-//   FP32 (CUDA-core stiffness):   G and H as [NQ][NN+1] float2, the padded row
-//   lets the quadrature stage store without bank conflicts.
-template <int P, typename T>
-struct Layout {
-  using S = Shape<P>;
-  using D = Dims<P>;
-  static constexpr bool TC = sizeof(T) == 8;
-  static constexpr int NN = D::NN, NQ = NN, NNP = NN + 1, EPG = S::EPG;
-  static constexpr size_t GH_ELEM = TC ? 8 * D::NQP * D::RS : 2 * sizeof(T) * NQ * NNP;  // bytes per element
-  static constexpr size_t tabT = 0;                     // double2 [NN][NQ]
-  static constexpr size_t wq = tabT + 16 * NQ * NN;     // double  [NQ]
-  static constexpr size_t groups = align16(wq + 8 * NQ);
-  // group-relative
-  static constexpr size_t X = 0;                               // double2 [EPG][NN]
-  static constexpr size_t U = X + 16 * EPG * NN;               // double2 [EPG][NN]
-  static constexpr size_t S3 = U + 16 * EPG * NN;              // double  [3][EPG*NQ]  weak stress (SoA)
-  static constexpr size_t G = align16(S3 + 24 * EPG * NQ);     // [EPG] x GH_ELEM
-  static constexpr size_t H = align16(G + EPG * GH_ELEM);      // [EPG] x GH_ELEM
-  static constexpr size_t nid = align16(H + EPG * GH_ELEM);    // int [EPG][NN]
-  static constexpr size_t group_bytes = align16(nid + 4 * EPG * NN);
-  static constexpr size_t total = groups + S::GPC * group_bytes;
-};
-
-__device__ __forceinline__ void group_sync(int id, int nthreads) {
-  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
-}
-
-__device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
-               : "+d"(c0), "+d"(c1)
-               : "d"(a), "d"(b));
-}
-
-// Writes the element block K(a,b) (and K(b,a) = K(a,b)^T when a != b) through the
-// plan codes or the reference map.  `which`: 0 = block (a,b), 1 = block (b,a).
-template <int NN, int MODE>
-__device__ __forceinline__ void write_block(const AsmArgs &A, int64_t k, const int *nid_el, int a, int b, int which,
-                                            double kxx, double kxy, double kyx, double kyy) {
-  const int r0 = which ? b : a, c0 = which ? a : b;
-  const double v0 = kxx, v1 = which ? kyx : kxy, v2 = which ? kxy : kyx, v3 = kyy;
-  if constexpr ((MODE & kPlan) != 0) {
-    const uint8_t code = __ldg(A.blockCode + (k * NN + r0) * NN + c0);
-    double *blk = A.mat + 4 * ((int64_t)__ldg(A.rowp + nid_el[r0]) + (code & 0x7f));
-    if (code & 0x80) {
-      store_block(blk, v0, v1, v2, v3);
-    } else {
-      // later colour: the first contributor's store is complete (previous launch)
-      // and no element of this colour shares the block
-      atomicAdd(blk + 0, v0);
-      atomicAdd(blk + 1, v1);
-      atomicAdd(blk + 2, v2);
-      atomicAdd(blk + 3, v3);
-    }
-  } else {
-    double *blk = A.mat + __ldg(A.map + (k * NN + r0) * NN + c0);
-    atomicAdd(blk + 0, v0);
-    atomicAdd(blk + 1, v1);
-    atomicAdd(blk + 2, v2);
-    atomicAdd(blk + 3, v3);
-  }
-}
-
-// One warp, tile rows [R0, R1) of the upper triangle of M = H^T G (FP64 MMA),
-// then the 2x2 stiffness blocks.  Lane l holds C[8ti + l/4][8tj + 2(l%4) + {0,1}]
-// = (M_i0, M_i1)[a][b] with a = (8ti + l/4)/2, i = (l/4)%2, b = 4tj + l%4; the
-// lane with the other i (l ^ 4) supplies the second row of the block.
-template <int P, int MODE, int R0, int R1>
-__device__ __forceinline__ void stiffness_mma(const AsmArgs &A, const double *Gm, const double *Hm, const int *nid_el,
-                                              int64_t k, double mu, double lam, int lane) {
-  using D = Dims<P>;
-  constexpr int NT8 = D::NT8, KS = D::KS, RS = D::RS, NN = D::NN;
-  constexpr int NR = R1 - R0;
-  double acc[NR][NT8][2];
-#pragma unroll
-  for (int r = 0; r < NR; r++)
-#pragma unroll
-    for (int c = 0; c < NT8; c++) acc[r][c][0] = acc[r][c][1] = 0.0;
-  const int g = lane >> 2, t = lane & 3;
-#pragma unroll
-  for (int ks = 0; ks < KS; ks++) {
-    const int q = 4 * ks + t;
-    double af[NR], bf[NT8];
-#pragma unroll
-    for (int r = 0; r < NR; r++) af[r] = Hm[q * RS + 8 * (R0 + r) + g];
-#pragma unroll
-    for (int c = 0; c < NT8; c++)
-      if (c >= R0) bf[c] = Gm[q * RS + 8 * c + g];
-#pragma unroll
-    for (int r = 0; r < NR; r++)
-#pragma unroll
-      for (int c = 0; c < NT8; c++)
-        if (c >= R0 + r) dmma(acc[r][c][0], acc[r][c][1], af[r], bf[c]);
-  }
-  const double c11 = lam + 2.0 * mu;
-  const int i = g & 1;
-#pragma unroll
-  for (int r = 0; r < NR; r++) {
-    const int a = (8 * (R0 + r) + g) >> 1;
-#pragma unroll
-    for (int c = 0; c < NT8; c++) {
-      if (c < R0 + r) continue;
-      const double o0 = __shfl_xor_sync(0xffffffffu, acc[r][c][0], 4);
-      const double o1 = __shfl_xor_sync(0xffffffffu, acc[r][c][1], 4);
-      const double mxx = i ? o0 : acc[r][c][0], mxy = i ? o1 : acc[r][c][1];
-      const double myx = i ? acc[r][c][0] : o0, myy = i ? acc[r][c][1] : o1;
-      const int b = 4 * c + t;
-      if (a < NN && b < NN && a <= b && (i == 0 || a < b)) {
-        const double kxx = c11 * mxx + mu * myy;
-        const double kxy = lam * mxy + mu * myx;
-        const double kyx = lam * myx + mu * mxy;
-        const double kyy = c11 * myy + mu * mxx;
-        write_block<NN, MODE>(A, k, nid_el, a, b, i, kxx, kxy, kyx, kyy);
-      }
-    }
-  }
-}
-
-template <int P, typename T>
-constexpr int min_blocks() {
-  return Shape<P>::MINB;
-}
-
-template <int P, typename T, int MODE>
-__global__ void __launch_bounds__(Shape<P>::GT *Shape<P>::GPC, min_blocks<P, T>()) assemble_kernel(const AsmArgs A) {
-  using S = Shape<P>;
-  using L = Layout<P, T>;
-  using D = Dims<P>;
-  constexpr bool TC = L::TC;
-  constexpr int P1 = P + 1, NN = D::NN, NQ = NN, NNP = L::NNP, NTILE = D::NTILE;
-  constexpr int NQP = D::NQP, RS = D::RS;
-  constexpr int GT = S::GT, EPG = S::EPG, NPART = S::NPART, SQ = EPG * NQ;
-  static_assert(EPG * NN <= GT, "one prefetched node per thread");
-  static_assert(GT % 32 == 0 && 32 % NPART == 0, "group/part shape");
-  using T2 = typename Vec2<T>::type;
-  extern __shared__ __align__(16) unsigned char smem[];
-  double2 *tabT = reinterpret_cast<double2 *>(smem + L::tabT);
-  double *wq = reinterpret_cast<double *>(smem + L::wq);
-
-  // Shape-function derivative table at the Gauss points, once per CTA.
-  for (int i = threadIdx.x; i < NQ * NN; i += blockDim.x) {
-    const int q = i / NN, a = i - q * NN;
-    double Nx, dNx, Ny, dNy;
-    lag1d(P, kGX[P][q % P1], a % P1, Nx, dNx);
-    lag1d(P, kGX[P][q / P1], a / P1, Ny, dNy);
-    tabT[a * NQ + q] = make_double2(__dmul_rn(Ny, dNx), __dmul_rn(Nx, dNy));
-  }
-  for (int q = threadIdx.x; q < NQ; q += blockDim.x) wq[q] = __dmul_rn(kGW[P][q % P1], kGW[P][q / P1]);
-
-  const int g = threadIdx.x / GT, tg = threadIdx.x - g * GT;
-  const int warp = tg >> 5, lane = tg & 31;
-  unsigned char *gs = smem + L::groups + g * L::group_bytes;
-  double2 *X = reinterpret_cast<double2 *>(gs + L::X);
-  double2 *U = reinterpret_cast<double2 *>(gs + L::U);
-  double *S3 = reinterpret_cast<double *>(gs + L::S3);
-  int *nid = reinterpret_cast<int *>(gs + L::nid);
-  const int bar = 1 + g;
-  if constexpr (TC) {
-    // zero the padded quadrature rows once: they feed the k dimension of the MMA
-    double *Gz = reinterpret_cast<double *>(gs + L::G), *Hz = reinterpret_cast<double *>(gs + L::H);
-    for (int i = tg; i < EPG * (NQP - NQ) * RS; i += GT) {
-      const int el = i / ((NQP - NQ) * RS), r = i - el * (NQP - NQ) * RS;
-      Gz[el * NQP * RS + NQ * RS + r] = 0.0;
-      Hz[el * NQP * RS + NQ * RS + r] = 0.0;
-    }
-  }
-  __syncthreads();
-
-  const double mu = A.mu, lam = A.lam;
-  const T cMu = T(mu), cLam = T(lam), cC11 = T(lam + 2.0 * mu);
-  const int64_t end = A.begin + A.count;
-  const int64_t nb = (A.count + EPG - 1) / EPG;
-  const int64_t stride = (int64_t)gridDim.x * S::GPC;
-
-  // Gather of the next batch, issued early so its latency overlaps the current batch.
-  int pf_node = 0;
-  double2 pf_x = make_double2(0, 0), pf_u = make_double2(0, 0);
-  auto prefetch = [&](int64_t batch) {
-    if (batch >= nb || tg >= EPG * NN) return;
-    const int el = tg / NN, a = tg - el * NN;
-    const int64_t k = A.begin + batch * EPG + el;
-    if (k >= end) return;
-    if constexpr ((MODE & kPlan) != 0) {
-      pf_node = __ldg(A.connList + k * NN + a);
-    } else {
-      pf_node = __ldg(A.conn + __ldg(A.connPtr + k) + a);
-    }
-    pf_x = __ldg(reinterpret_cast<const double2 *>(A.coords) + pf_node);
-    pf_u = __ldg(reinterpret_cast<const double2 *>(A.states) + pf_node);
-  };
-
-  int64_t batch = (int64_t)blockIdx.x * S::GPC + g;
-  prefetch(batch);
-  for (; batch < nb; batch += stride) {
-    const int64_t k0 = A.begin + batch * EPG;
-    const int ne = (int)min((int64_t)EPG, end - k0);
-
-    // 0. commit the gathered element data
-    if (tg < ne * NN) {
-      X[tg] = pf_x;
-      U[tg] = pf_u;
-      nid[tg] = pf_node;
-    }
-    group_sync(bar, GT);
-    prefetch(batch + stride);
-
-    // 1. quadrature points: NPART lanes per (element, q) split the node sums,
-    //    every lane of the quad then forms J^-1 and the gradients of its nodes.
-    for (int base = 0; base < EPG * NQ * NPART; base += GT) {
-      const int i = base + tg;
-      const int iq = i / NPART, part = i - iq * NPART;
-      const int el = iq / NQ, q = iq - el * NQ;
-      const bool act = i < EPG * NQ * NPART && el < ne;
-      double j00 = 0, j01 = 0, j10 = 0, j11 = 0, g00 = 0, g01 = 0, g10 = 0, g11 = 0;
-      if (act) {
-#pragma unroll 2
-        for (int a = part; a < NN; a += NPART) {
-          const double2 d = tabT[a * NQ + q];
-          const double2 x = X[el * NN + a], u = U[el * NN + a];
-          j00 = fma(x.x, d.x, j00);
-          j01 = fma(x.x, d.y, j01);
-          j10 = fma(x.y, d.x, j10);
-          j11 = fma(x.y, d.y, j11);
-          g00 = fma(u.x, d.x, g00);
-          g01 = fma(u.x, d.y, g01);
-          g10 = fma(u.y, d.x, g10);
-          g11 = fma(u.y, d.y, g11);
-        }
-      }
-#pragma unroll
-      for (int o = 1; o < NPART; o <<= 1) {
-        j00 += __shfl_xor_sync(0xffffffffu, j00, o);
-        j01 += __shfl_xor_sync(0xffffffffu, j01, o);
-        j10 += __shfl_xor_sync(0xffffffffu, j10, o);
-        j11 += __shfl_xor_sync(0xffffffffu, j11, o);
-        g00 += __shfl_xor_sync(0xffffffffu, g00, o);
-        g01 += __shfl_xor_sync(0xffffffffu, g01, o);
-        g10 += __shfl_xor_sync(0xffffffffu, g10, o);
-        g11 += __shfl_xor_sync(0xffffffffu, g11, o);
-      }
-      if (act) {
-        const double det = j00 * j11 - j01 * j10;
-        const double inv = 1.0 / det;
-        const double i00 = j11 * inv, i01 = -j01 * inv, i10 = -j10 * inv, i11 = j00 * inv;
-        const double st = wq[q] * det * A.t;
-        if (part == 0) {
-          const double uxx = g00 * i00 + g01 * i10, uxy = g00 * i01 + g01 * i11;
-          const double uyx = g10 * i00 + g11 * i10, uyy = g10 * i01 + g11 * i11;
-          const double tr = uxx + uyy;
-          S3[0 * SQ + iq] = st * (2.0 * mu * uxx + lam * tr);
-          S3[1 * SQ + iq] = st * (mu * (uxy + uyx));
-          S3[2 * SQ + iq] = st * (2.0 * mu * uyy + lam * tr);
-        }
-#pragma unroll 2
-        for (int a = part; a < NN; a += NPART) {
-          const double2 d = tabT[a * NQ + q];
-          const double gx = d.x * i00 + d.y * i10;
-          const double gy = d.x * i01 + d.y * i11;
-          if constexpr (TC) {
-            double *Gm = reinterpret_cast<double *>(gs + L::G) + (el * NQP + q) * RS;
-            *reinterpret_cast<double2 *>(Gm + 2 * a) = make_double2(gx, gy);
-            if constexpr ((MODE & kJac) != 0) {
-              double *Hm = reinterpret_cast<double *>(gs + L::H) + (el * NQP + q) * RS;
-              *reinterpret_cast<double2 *>(Hm + 2 * a) = make_double2(st * gx, st * gy);
-            }
-          } else {
-            T2 gv;
-            gv.x = T(gx);
-            gv.y = T(gy);
-            reinterpret_cast<T2 *>(gs + L::G)[iq * NNP + a] = gv;
-            if constexpr ((MODE & kJac) != 0) {
-              T2 hv;
-              hv.x = T(st * gx);
-              hv.y = T(st * gy);
-              reinterpret_cast<T2 *>(gs + L::H)[iq * NNP + a] = hv;
-            }
-          }
-        }
-      }
-    }
-    group_sync(bar, GT);
-
-    // 2a. residual R_a = sum_q S(q) G_a(q), NPART lanes per node split the q sum
-    if constexpr ((MODE & kRes) != 0) {
-      for (int base = 0; base < EPG * NN * NPART; base += GT) {
-        const int i = base + tg;
-        const int ia = i / NPART, part = i - ia * NPART;
-        const int el = ia / NN, a = ia - el * NN;
-        const bool act = i < EPG * NN * NPART && el < ne;
-        T rx = 0, ry = 0;
-        if (act) {
-#pragma unroll 2
-          for (int q = part; q < NQ; q += NPART) {
-            const int iq = el * NQ + q;
-            T gx, gy;
-            if constexpr (TC) {
-              const double2 gv = *reinterpret_cast<const double2 *>(reinterpret_cast<const double *>(gs + L::G) +
-                                                                     (el * NQP + q) * RS + 2 * a);
-              gx = gv.x;
-              gy = gv.y;
-            } else {
-              const T2 gv = reinterpret_cast<const T2 *>(gs + L::G)[iq * NNP + a];
-              gx = gv.x;
-              gy = gv.y;
-            }
-            const T sxx = T(S3[0 * SQ + iq]), sxy = T(S3[1 * SQ + iq]), syy = T(S3[2 * SQ + iq]);
-            rx = fma(sxx, gx, fma(sxy, gy, rx));
-            ry = fma(sxy, gx, fma(syy, gy, ry));
-          }
-        }
-#pragma unroll
-        for (int o = 1; o < NPART; o <<= 1) {
-          rx += __shfl_xor_sync(0xffffffffu, rx, o);
-          ry += __shfl_xor_sync(0xffffffffu, ry, o);
-        }
-        if (act && part == 0) {
-          double *dst = A.residual + 2 * (int64_t)nid[ia];
-          if constexpr ((MODE & kPlan) != 0) {
-            if (__ldg(A.nodeCode + (k0 + el) * NN + a)) {
-              *reinterpret_cast<double2 *>(dst) = make_double2(double(rx), double(ry));
-            } else {
-              atomicAdd(dst, double(rx));
-              atomicAdd(dst + 1, double(ry));
-            }
-          } else {
-            atomicAdd(dst, double(rx));
-            atomicAdd(dst + 1, double(ry));
-          }
-        }
-      }
-    }
-
-    // 2b. element stiffness
-    if constexpr ((MODE & kJac) != 0) {
-      if constexpr (TC) {
-        // FP64 tensor cores: warps take (element, row range) work items
-        constexpr int WPE = (P == 4) ? 2 : 1;  // warps per element
-        constexpr int NW = GT / 32;
-        for (int w = warp; w < ne * WPE; w += NW) {
-          const int el = w / WPE, part = w - el * WPE;
-          const double *Gm = reinterpret_cast<const double *>(gs + L::G) + el * NQP * RS;
-          const double *Hm = reinterpret_cast<const double *>(gs + L::H) + el * NQP * RS;
-          if constexpr (WPE == 1) {
-            stiffness_mma<P, MODE, 0, D::NT8>(A, Gm, Hm, nid + el * NN, k0 + el, mu, lam, lane);
-          } else {
-            if (part == 0)
-              stiffness_mma<P, MODE, 0, 2>(A, Gm, Hm, nid + el * NN, k0 + el, mu, lam, lane);
-            else
-              stiffness_mma<P, MODE, 2, D::NT8>(A, Gm, Hm, nid + el * NN, k0 + el, mu, lam, lane);
-          }
-        }
-      } else {
-        // FP32 CUDA cores: one (p+1)-row tile x one column per thread, upper triangle
-        const T2 *G = reinterpret_cast<const T2 *>(gs + L::G);
-        const T2 *H = reinterpret_cast<const T2 *>(gs + L::H);
-        for (int i = tg; i < ne * NTILE; i += GT) {
-          const int el = i / NTILE;
-          int r = i - el * NTILE, at = 0;
-#pragma unroll
-          for (int row = 0; row < P1; row++) {
-            const int len = NN - row * P1;
-            if (at == row && r >= len) {
-              r -= len;
-              at = row + 1;
-            }
-          }
-          const int b = at * P1 + r;
-          T m[P1][4];
-#pragma unroll
-          for (int ax = 0; ax < P1; ax++) m[ax][0] = m[ax][1] = m[ax][2] = m[ax][3] = T(0);
-          const T2 *Gb = G + el * NQ * NNP + b;
-          const T2 *Ha = H + el * NQ * NNP + at * P1;
-#pragma unroll 2
-          for (int q = 0; q < NQ; q++) {
-            const T2 gv = Gb[q * NNP];
-#pragma unroll
-            for (int ax = 0; ax < P1; ax++) {
-              const T2 hv = Ha[q * NNP + ax];
-              m[ax][0] = fma(hv.x, gv.x, m[ax][0]);
-              m[ax][1] = fma(hv.x, gv.y, m[ax][1]);
-              m[ax][2] = fma(hv.y, gv.x, m[ax][2]);
-              m[ax][3] = fma(hv.y, gv.y, m[ax][3]);
-            }
-          }
-#pragma unroll
-          for (int ax = 0; ax < P1; ax++) {
-            const int a = at * P1 + ax;
-            if (a > b) continue;
-            const double kxx = double(cC11 * m[ax][0] + cMu * m[ax][3]);
-            const double kxy = double(cLam * m[ax][1] + cMu * m[ax][2]);
-            const double kyx = double(cLam * m[ax][2] + cMu * m[ax][1]);
-            const double kyy = double(cC11 * m[ax][3] + cMu * m[ax][0]);
-            write_block<NN, MODE>(A, k0 + el, nid + el * NN, a, b, 0, kxx, kxy, kyx, kyy);
-            if (a != b) write_block<NN, MODE>(A, k0 + el, nid + el * NN, a, b, 1, kxx, kxy, kyx, kyy);
-          }
-        }
-      }
-    }
-    group_sync(bar, GT);
-  }
-}
 
 // y = A x, 2x2 BSR, eight lanes per block row.
 __global__ void __launch_bounds__(256) bsr_spmv_kernel(int numRows, const int *__restrict__ rowp,
@@ -594,134 +61,10 @@ __global__ void __launch_bounds__(256) bsr_spmv_kernel(int numRows, const int *_
 }
 
 }  // namespace dev
+}  // namespace fem
 
-// ---------------------------------------------------------------------------------------
-// Host-side launch machinery
-// ---------------------------------------------------------------------------------------
+namespace fem {
 namespace {
-
-struct LaunchInfo {
-  int grid_per_sm = 0;
-  int num_sms = 0;
-};
-
-std::mutex g_mu;
-std::map<std::pair<const void *, int>, LaunchInfo> g_info;
-
-int cuda_fail(cudaError_t err, const char *what) {
-  return fail(FEM_ERR_CUDA, "%s: %s", what, cudaGetErrorString(err));
-}
-
-// Occupancy-sized persistent grid; sets the dynamic shared-memory opt-in once per device.
-template <typename K>
-int launch_info(K kernel, int nt, size_t smem, LaunchInfo &out) {
-  int dev = 0;
-  cudaError_t err = cudaGetDevice(&dev);
-  if (err != cudaSuccess) return cuda_fail(err, "cudaGetDevice");
-  std::lock_guard<std::mutex> lk(g_mu);
-  auto key = std::make_pair(reinterpret_cast<const void *>(kernel), dev);
-  auto it = g_info.find(key);
-  if (it != g_info.end()) {
-    out = it->second;
-    return FEM_SUCCESS;
-  }
-  err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (err != cudaSuccess) return cuda_fail(err, "cudaFuncSetAttribute");
-  LaunchInfo li;
-  err = cudaDeviceGetAttribute(&li.num_sms, cudaDevAttrMultiProcessorCount, dev);
-  if (err != cudaSuccess) return cuda_fail(err, "cudaDeviceGetAttribute");
-  err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&li.grid_per_sm, kernel, nt, smem);
-  if (err != cudaSuccess) return cuda_fail(err, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-  if (li.grid_per_sm < 1) return fail(FEM_ERR_CUDA, "kernel does not fit on an SM (smem %zu B)", smem);
-  g_info[key] = li;
-  out = li;
-  return FEM_SUCCESS;
-}
-
-template <int P, typename T, int MODE>
-int launch_p(const dev::AsmArgs &a, cudaStream_t s) {
-  using S = dev::Shape<P>;
-  constexpr int NT = S::GT * S::GPC;
-  auto kernel = dev::assemble_kernel<P, T, MODE>;
-  const size_t smem = dev::Layout<P, T>::total;
-  LaunchInfo li;
-  int st = launch_info(kernel, NT, smem, li);
-  if (st) return st;
-  const int64_t groups = (a.count + S::EPG - 1) / S::EPG;
-  const int64_t need = (groups + S::GPC - 1) / S::GPC;
-  const int64_t cap = (int64_t)li.grid_per_sm * li.num_sms;
-  const int grid = (int)(need < cap ? need : cap);
-  if (grid <= 0) return FEM_SUCCESS;
-  kernel<<<grid, NT, smem, s>>>(a);
-  cudaError_t err = cudaGetLastError();
-  if (err != cudaSuccess) return cuda_fail(err, "assemble_kernel launch");
-  return FEM_SUCCESS;
-}
-
-template <typename T, int MODE>
-int launch_mode(int order, const dev::AsmArgs &a, cudaStream_t s) {
-  switch (order) {
-    case 1: return launch_p<1, T, MODE>(a, s);
-    case 2: return launch_p<2, T, MODE>(a, s);
-    case 3: return launch_p<3, T, MODE>(a, s);
-    case 4: return launch_p<4, T, MODE>(a, s);
-    default: return fail(FEM_ERR_INVALID_ORDER, "element order %d (supported: 1..4)", order);
-  }
-}
-
-template <typename T>
-int launch_any(int order, int mode, const dev::AsmArgs &a, cudaStream_t s) {
-  using namespace dev;
-  switch (mode) {
-    case kRes: return launch_mode<T, kRes>(order, a, s);
-    case kJac: return launch_mode<T, kJac>(order, a, s);
-    case kRes | kJac: return launch_mode<T, kRes | kJac>(order, a, s);
-    case kPlan | kRes: return launch_mode<T, kPlan | kRes>(order, a, s);
-    case kPlan | kJac: return launch_mode<T, kPlan | kJac>(order, a, s);
-    case kPlan | kRes | kJac: return launch_mode<T, kPlan | kRes | kJac>(order, a, s);
-    default: return fail(FEM_ERR_INVALID_ARGUMENT, "bad kernel mode %d", mode);
-  }
-}
-
-int launch(int order, int precision, int mode, const dev::AsmArgs &a, cudaStream_t s) {
-  if (precision == FEM_PRECISION_FP64) return launch_any<double>(order, mode, a, s);
-  if (precision == FEM_PRECISION_MIXED) return launch_any<float>(order, mode, a, s);
-  return fail(FEM_ERR_INVALID_ARGUMENT, "precision %d", precision);
-}
-
-void set_material(dev::AsmArgs &a, double E, double nu, double t) {
-  // element/FEKernels.h:300-301
-  a.mu = 0.5 * E / (1.0 + nu);
-  a.lam = 2 * a.mu * nu / (1.0 - nu);
-  a.t = t;
-}
-
-// Runs `body` on `stream`; with elapsed != NULL brackets it with events and synchronises.
-template <typename F>
-int timed(cudaStream_t s, double *elapsed, F body) {
-  if (!elapsed) return body();
-  cudaEvent_t e0, e1;
-  cudaError_t err = cudaEventCreate(&e0);
-  if (err != cudaSuccess) return cuda_fail(err, "cudaEventCreate");
-  err = cudaEventCreate(&e1);
-  if (err != cudaSuccess) {
-    cudaEventDestroy(e0);
-    return cuda_fail(err, "cudaEventCreate");
-  }
-  int st = FEM_SUCCESS;
-  err = cudaEventRecord(e0, s);
-  if (err != cudaSuccess) st = cuda_fail(err, "cudaEventRecord");
-  if (!st) st = body();
-  if (!st && (err = cudaEventRecord(e1, s)) != cudaSuccess) st = cuda_fail(err, "cudaEventRecord");
-  if (!st && (err = cudaEventSynchronize(e1)) != cudaSuccess) st = cuda_fail(err, "kernel execution");
-  float ms = 0.f;
-  if (!st && (err = cudaEventElapsedTime(&ms, e0, e1)) != cudaSuccess) st = cuda_fail(err, "cudaEventElapsedTime");
-  *elapsed = st ? 0.0 : ms * 1e-3;
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  return st;
-}
-
 int run_dropin(int precision, bool jac, int order, const int *connPtr, const int *conn, int numElements,
                const double *states, const double *coords, double E, double nu, double t, const int *map,
                double *residual, double *mat, void *stream, double *elapsed) {
@@ -758,15 +101,6 @@ int run_dropin(int precision, bool jac, int order, const int *connPtr, const int
 // ---------------------------------------------------------------------------------------
 // Plans
 // ---------------------------------------------------------------------------------------
-struct fem_plan {
-  int device = 0;
-  int order = 0, nn = 0, numNodes = 0, numElements = 0, numColours = 0;
-  int64_t nnzb = 0;
-  std::vector<int> colourPtr;
-  int *d_rowp = nullptr, *d_cols = nullptr, *d_connList = nullptr;
-  uint8_t *d_blockCode = nullptr, *d_nodeCode = nullptr;
-  int64_t deviceBytes = 0;
-};
 
 namespace {
 void plan_free(fem_plan *p) {

@@ -1,0 +1,150 @@
+// Host-side launch helpers shared by the single-mesh and batched entry points.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <mutex>
+#include <utility>
+#include <vector>
+
+#include "fem_common.h"
+#include "fem_device.cuh"
+
+namespace fem {
+
+struct LaunchInfo {
+  int grid_per_sm = 0;
+  int num_sms = 0;
+};
+
+inline std::mutex g_mu;
+inline std::map<std::pair<const void *, int>, LaunchInfo> g_info;
+
+inline int cuda_fail(cudaError_t err, const char *what) {
+  return fail(FEM_ERR_CUDA, "%s: %s", what, cudaGetErrorString(err));
+}
+
+// Occupancy-sized persistent grid; sets the dynamic shared-memory opt-in once per device.
+template <typename K>
+int launch_info(K kernel, int nt, size_t smem, LaunchInfo &out) {
+  int dev = 0;
+  cudaError_t err = cudaGetDevice(&dev);
+  if (err != cudaSuccess) return cuda_fail(err, "cudaGetDevice");
+  std::lock_guard<std::mutex> lk(g_mu);
+  auto key = std::make_pair(reinterpret_cast<const void *>(kernel), dev);
+  auto it = g_info.find(key);
+  if (it != g_info.end()) {
+    out = it->second;
+    return FEM_SUCCESS;
+  }
+  err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (err != cudaSuccess) return cuda_fail(err, "cudaFuncSetAttribute");
+  LaunchInfo li;
+  err = cudaDeviceGetAttribute(&li.num_sms, cudaDevAttrMultiProcessorCount, dev);
+  if (err != cudaSuccess) return cuda_fail(err, "cudaDeviceGetAttribute");
+  err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&li.grid_per_sm, kernel, nt, smem);
+  if (err != cudaSuccess) return cuda_fail(err, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+  if (li.grid_per_sm < 1) return fail(FEM_ERR_CUDA, "kernel does not fit on an SM (smem %zu B)", smem);
+  g_info[key] = li;
+  out = li;
+  return FEM_SUCCESS;
+}
+
+template <int P, typename T, int MODE>
+int launch_p(const dev::AsmArgs &a, cudaStream_t s) {
+  using S = dev::Shape<P>;
+  constexpr int NT = S::GT * S::GPC;
+  auto kernel = dev::assemble_kernel<P, T, MODE>;
+  const size_t smem = dev::Layout<P, T>::total;
+  LaunchInfo li;
+  int st = launch_info(kernel, NT, smem, li);
+  if (st) return st;
+  const int64_t groups = (a.count + S::EPG - 1) / S::EPG;
+  const int64_t need = (groups + S::GPC - 1) / S::GPC;
+  const int64_t cap = (int64_t)li.grid_per_sm * li.num_sms;
+  const int grid = (int)(need < cap ? need : cap);
+  if (grid <= 0) return FEM_SUCCESS;
+  kernel<<<grid, NT, smem, s>>>(a);
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return cuda_fail(err, "assemble_kernel launch");
+  return FEM_SUCCESS;
+}
+
+template <typename T, int MODE>
+int launch_mode(int order, const dev::AsmArgs &a, cudaStream_t s) {
+  switch (order) {
+    case 1: return launch_p<1, T, MODE>(a, s);
+    case 2: return launch_p<2, T, MODE>(a, s);
+    case 3: return launch_p<3, T, MODE>(a, s);
+    case 4: return launch_p<4, T, MODE>(a, s);
+    default: return fail(FEM_ERR_INVALID_ORDER, "element order %d (supported: 1..4)", order);
+  }
+}
+
+template <typename T>
+int launch_any(int order, int mode, const dev::AsmArgs &a, cudaStream_t s) {
+  using namespace dev;
+  switch (mode) {
+    case kRes: return launch_mode<T, kRes>(order, a, s);
+    case kJac: return launch_mode<T, kJac>(order, a, s);
+    case kRes | kJac: return launch_mode<T, kRes | kJac>(order, a, s);
+    case kPlan | kRes: return launch_mode<T, kPlan | kRes>(order, a, s);
+    case kPlan | kJac: return launch_mode<T, kPlan | kJac>(order, a, s);
+    case kPlan | kRes | kJac: return launch_mode<T, kPlan | kRes | kJac>(order, a, s);
+    default: return fail(FEM_ERR_INVALID_ARGUMENT, "bad kernel mode %d", mode);
+  }
+}
+
+inline int launch(int order, int precision, int mode, const dev::AsmArgs &a, cudaStream_t s) {
+  if (precision == FEM_PRECISION_FP64) return launch_any<double>(order, mode, a, s);
+  if (precision == FEM_PRECISION_MIXED) return launch_any<float>(order, mode, a, s);
+  return fail(FEM_ERR_INVALID_ARGUMENT, "precision %d", precision);
+}
+
+inline void set_material(dev::AsmArgs &a, double E, double nu, double t) {
+  // element/FEKernels.h:300-301
+  a.mu = 0.5 * E / (1.0 + nu);
+  a.lam = 2 * a.mu * nu / (1.0 - nu);
+  a.t = t;
+}
+
+// Runs `body` on `stream`; with elapsed != NULL brackets it with events and synchronises.
+template <typename F>
+int timed(cudaStream_t s, double *elapsed, F body) {
+  if (!elapsed) return body();
+  cudaEvent_t e0, e1;
+  cudaError_t err = cudaEventCreate(&e0);
+  if (err != cudaSuccess) return cuda_fail(err, "cudaEventCreate");
+  err = cudaEventCreate(&e1);
+  if (err != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return cuda_fail(err, "cudaEventCreate");
+  }
+  int st = FEM_SUCCESS;
+  err = cudaEventRecord(e0, s);
+  if (err != cudaSuccess) st = cuda_fail(err, "cudaEventRecord");
+  if (!st) st = body();
+  if (!st && (err = cudaEventRecord(e1, s)) != cudaSuccess) st = cuda_fail(err, "cudaEventRecord");
+  if (!st && (err = cudaEventSynchronize(e1)) != cudaSuccess) st = cuda_fail(err, "kernel execution");
+  float ms = 0.f;
+  if (!st && (err = cudaEventElapsedTime(&ms, e0, e1)) != cudaSuccess) st = cuda_fail(err, "cudaEventElapsedTime");
+  *elapsed = st ? 0.0 : ms * 1e-3;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return st;
+}
+
+}  // namespace fem
+
+// Device-resident topology of one mesh (see fem_plan_create).
+struct fem_plan {
+  int device = 0;
+  int order = 0, nn = 0, numNodes = 0, numElements = 0, numColours = 0;
+  int64_t nnzb = 0;
+  std::vector<int> colourPtr;
+  int *d_rowp = nullptr, *d_cols = nullptr, *d_connList = nullptr;
+  uint8_t *d_blockCode = nullptr, *d_nodeCode = nullptr;
+  int64_t deviceBytes = 0;
+};

@@ -131,6 +131,40 @@ int fem_plan_assemble(const fem_plan *plan, const double *states, const double *
                       double t, double *residual, double *matEntries, int precision, void *stream,
                       double *elapsedSeconds);
 
+/* ---- batched assembly of many meshes (config: 256 meshes, mixed orders) --------------- */
+/* A batch references existing plans (they must outlive it) and assembles all of
+ * their meshes with one persistent kernel per (order, colour) whose thread groups
+ * pull element tiles from that launch's work queue; the orders run concurrently on
+ * internal streams.  Outputs follow fem_plan_assemble (complete overwrite).
+ * (No reference counterpart: the reference assembles one mesh per call.) */
+typedef struct fem_batch fem_batch;
+
+int fem_batch_create(int numMeshes, fem_plan *const *plans, fem_batch **batch);
+int fem_batch_destroy(fem_batch *batch);
+/* Device arrays and material of mesh `mesh`; all four arrays are required
+ * (vectors 16-byte, matEntries 32-byte aligned).  Rebinding is allowed at any
+ * time before the next assemble/replay. */
+int fem_batch_bind(fem_batch *batch, int mesh, const double *states, const double *nodeCoords, double E, double nu,
+                   double t, double *residual, double *matEntries);
+/* Total elements, queue tiles, kernel launches per assembly, device bytes held by the batch. */
+int fem_batch_info(const fem_batch *batch, int64_t *totalElements, int64_t *numTiles, int *numLaunches,
+                   int64_t *deviceBytes);
+/* Tile length per order (index 0..3 = order 1..4), in element batches of the
+ * order's kernel shape. */
+int fem_batch_get_tiles(const fem_batch *batch, int *tileBatches);
+int fem_batch_set_tiles(fem_batch *batch, const int *tileBatches);
+/* One assembly of every mesh, stream-ordered on `stream`. */
+int fem_batch_assemble(fem_batch *batch, int precision, void *stream, double *elapsedSeconds);
+/* Autotuner: per order, times the order's launches for each candidate tile
+ * length (reps repetitions after a warm-up) and keeps the fastest. */
+int fem_batch_tune(fem_batch *batch, int precision, void *stream, int reps, double *bestSeconds);
+/* Captures one complete assembly into a CUDA graph (after one uncaptured warm-up
+ * run on `stream`); fem_batch_replay launches it.  Rebinding arrays does not
+ * require a new capture (the graph reads the mesh table from device memory);
+ * changing tiles does. */
+int fem_batch_capture(fem_batch *batch, int precision, void *stream);
+int fem_batch_replay(fem_batch *batch, void *stream, double *elapsedSeconds);
+
 /* ---- calibration ---------------------------------------------------------------------- */
 /* Measured arithmetic peak of the current device in TFLOP/s, used as the
  * roofline denominator of the element arithmetic: kind 0 = FP64 FMA pipe,
