@@ -245,7 +245,6 @@ int fem_batch_create(int numMeshes, fem_plan *const *plans, fem_batch **batch) {
     fem::dev::AsmArgs a{};
     a.connList = plans[m]->d_connList;
     a.blockCode = plans[m]->d_blockCode;
-    a.nodeCode = plans[m]->d_nodeCode;
     a.rowp = plans[m]->d_rowp;
     b->args.push_back(a);
   }

@@ -30,8 +30,12 @@ struct HostPlan {
   std::vector<int> elemList;            // elements in colour order
   std::vector<int> colourPtr;           // numColours+1 offsets into elemList
   std::vector<int> connList;            // conn in elemList order, nn per element
-  std::vector<uint8_t> blockCode;       // per (k, a, b): rank in row | 0x80 store flag
-  std::vector<uint8_t> nodeCode;        // per (k, a): 1 = store, 0 = add
+  // Per listed element k a record of codeStride bytes: [a*nn + b] = rank of the
+  // block (a, b) in row conn[a] | 0x80 when this element stores it first, then
+  // [nn*nn + a] = 1 when this element writes node a's residual first; zero padding
+  // to a multiple of 16 bytes (records are copied to shared memory in 16-byte chunks).
+  int codeStride = 0;
+  std::vector<uint8_t> blockCode;
 };
 int build_host_plan(int order, int numNodes, const int *connPtr, const int *conn, int numElements, HostPlan &hp);
 

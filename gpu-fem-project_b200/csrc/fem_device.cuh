@@ -111,8 +111,7 @@ struct AsmArgs {
   const int *conn;         // drop-in: node ids
   const int *map;          // drop-in: element block offsets (doubles)
   const int *connList;     // plan: node ids of the listed elements, nn each
-  const uint8_t *blockCode;  // plan: rank-in-row | 0x80 store flag, nn*nn per listed element
-  const uint8_t *nodeCode;   // plan: 1 store / 0 add, nn per listed element
+  const uint8_t *blockCode;  // plan: per listed element a Dims<P>::CS-byte code record
   const int *rowp;           // plan: BSR row pointers
   const double *states;
   const double *coords;
@@ -122,22 +121,29 @@ struct AsmArgs {
   int64_t begin, count;  // element (or list position) range of this launch
 };
 
-// The output-side pointers of one mesh, copied into registers once per batch so
-// that the block writes do not re-read the argument block.
+// The output side of one batch: global outputs (registers) and the batch's
+// staged block codes / element map in shared memory.
 struct Out {
   double *mat;
   double *residual;
-  const int *rowp;
-  const uint8_t *blockCode;
-  const uint8_t *nodeCode;
-  const int *map;
+  const uint8_t *codes;  // plan: code records of the batch's elements (shared memory)
+  const int *rbase;      // plan: rowp[node] per (element, node) (shared memory)
+  const int *map;        // drop-in: element map rows of the batch (shared memory)
 };
 
-__device__ __forceinline__ Out load_out(const AsmArgs &A) {
-  return Out{A.mat, A.residual, A.rowp, A.blockCode, A.nodeCode, A.map};
+// Asynchronous global -> shared copies (no registers held while in flight).
+__device__ __forceinline__ void cp_async16(void *sdst, const void *gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gsrc) : "memory");
 }
+__device__ __forceinline__ void cp_async4(void *sdst, const void *gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-constexpr size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+__host__ __device__ constexpr size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
 // Launch shape per order: GT threads per group, EPG elements per group step,
 // GPC independent groups per CTA (each synchronises on its own named barrier),
@@ -176,6 +182,8 @@ struct Dims {
   static constexpr int NT8 = (2 * NN + 7) / 8;
   static constexpr int KS = (NQ + 3) / 4, NQP = 4 * KS;
   static constexpr int RS = 8 * NT8 + 4;  // 8*NT8 is 0 or 8 mod 16
+  // plan code record per element: NN*NN block codes + NN node codes, 16-byte padded
+  static constexpr int CS = (NN * NN + NN + 15) / 16 * 16;
 };
 
 // Shared memory: per-CTA table, then GPC group regions.
@@ -199,7 +207,12 @@ struct Layout {
   static constexpr size_t G = align16(S3 + 24 * EPG * NQ);     // [EPG] x GH_ELEM
   static constexpr size_t H = align16(G + EPG * GH_ELEM);      // [EPG] x GH_ELEM
   static constexpr size_t nid = align16(H + EPG * GH_ELEM);    // int [EPG][NN]
-  static constexpr size_t group_bytes = align16(nid + 4 * EPG * NN);
+  static constexpr size_t rbase = align16(nid + 4 * EPG * NN);  // int [EPG][NN]
+  // staged codes (plan) or element map rows (drop-in), double-buffered
+  static constexpr size_t STAGE = (size_t(EPG) * D::CS > size_t(EPG) * NN * NN * 4) ? size_t(EPG) * D::CS
+                                                                                      : size_t(EPG) * NN * NN * 4;
+  static constexpr size_t stage = align16(rbase + 4 * EPG * NN);  // [2][STAGE] bytes
+  static constexpr size_t group_bytes = align16(stage + 2 * align16(STAGE));
   static constexpr size_t total = groups + S::GPC * group_bytes;
 };
 
@@ -215,14 +228,15 @@ __device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b)
 
 // Writes the element block K(a,b) (and K(b,a) = K(a,b)^T when a != b) through the
 // plan codes or the reference map.  `which`: 0 = block (a,b), 1 = block (b,a).
-template <int NN, int MODE>
-__device__ __forceinline__ void write_block(const Out &A, int64_t k, const int *nid_el, int a, int b, int which,
-                                            double kxx, double kxy, double kyx, double kyy) {
+template <int P, int MODE>
+__device__ __forceinline__ void write_block(const Out &A, int el, int a, int b, int which, double kxx, double kxy,
+                                            double kyx, double kyy) {
+  constexpr int NN = Dims<P>::NN, CS = Dims<P>::CS;
   const int r0 = which ? b : a, c0 = which ? a : b;
   const double v0 = kxx, v1 = which ? kyx : kxy, v2 = which ? kxy : kyx, v3 = kyy;
   if constexpr ((MODE & kPlan) != 0) {
-    const uint8_t code = __ldg(A.blockCode + (k * NN + r0) * NN + c0);
-    double *blk = A.mat + 4 * ((int64_t)__ldg(A.rowp + nid_el[r0]) + (code & 0x7f));
+    const uint8_t code = A.codes[el * CS + r0 * NN + c0];
+    double *blk = A.mat + 4 * ((int64_t)A.rbase[el * NN + r0] + (code & 0x7f));
     if (code & 0x80) {
       store_block(blk, v0, v1, v2, v3);
     } else {
@@ -234,7 +248,7 @@ __device__ __forceinline__ void write_block(const Out &A, int64_t k, const int *
       atomicAdd(blk + 3, v3);
     }
   } else {
-    double *blk = A.mat + __ldg(A.map + (k * NN + r0) * NN + c0);
+    double *blk = A.mat + A.map[(el * NN + r0) * NN + c0];
     atomicAdd(blk + 0, v0);
     atomicAdd(blk + 1, v1);
     atomicAdd(blk + 2, v2);
@@ -247,8 +261,8 @@ __device__ __forceinline__ void write_block(const Out &A, int64_t k, const int *
 // = (M_i0, M_i1)[a][b] with a = (8ti + l/4)/2, i = (l/4)%2, b = 4tj + l%4; the
 // lane with the other i (l ^ 4) supplies the second row of the block.
 template <int P, int MODE, int R0, int R1>
-__device__ __forceinline__ void stiffness_mma(const Out &A, const double *Gm, const double *Hm, const int *nid_el,
-                                              int64_t k, double mu, double lam, int lane) {
+__device__ __forceinline__ void stiffness_mma(const Out &A, const double *Gm, const double *Hm, int el, double mu,
+                                              double lam, int lane) {
   using D = Dims<P>;
   constexpr int NT8 = D::NT8, KS = D::KS, RS = D::RS, NN = D::NN;
   constexpr int NR = R1 - R0;
@@ -291,7 +305,7 @@ __device__ __forceinline__ void stiffness_mma(const Out &A, const double *Gm, co
         const double kxy = lam * mxy + mu * myx;
         const double kyx = lam * myx + mu * mxy;
         const double kyy = c11 * myy + mu * mxx;
-        write_block<NN, MODE>(A, k, nid_el, a, b, i, kxx, kxy, kyx, kyy);
+        write_block<P, MODE>(A, el, a, b, i, kxx, kxy, kyx, kyy);
       }
     }
   }
@@ -302,26 +316,23 @@ constexpr int min_blocks() {
   return Shape<P>::MINB;
 }
 
-// A group's current batch: EPG (or fewer) consecutive elements k0.. of one mesh.
+// A group's current batch: EPG (or fewer) consecutive elements k0.. of mesh `mesh`
+// (always 0 for the single-mesh kernel); ne == 0 ends the loop.
 struct Cursor {
-  const AsmArgs *A;
-  int64_t k0;
+  int mesh;
   int ne;
+  int64_t k0;
 };
 
-// Work source of the single-mesh kernel: batches of A's element range, strided
+// Work source of the single-mesh kernel: batches of [begin, begin+count), strided
 // over all groups of the grid.
 struct StrideSource {
-  const AsmArgs *A;
-  int64_t batch, stride, nb;
+  static constexpr bool kBatched = false;
+  int64_t begin, end, batch, stride;
   int epg;
   __device__ Cursor make(int64_t b) const {
-    Cursor c{nullptr, 0, 0};
-    if (b < nb) {
-      c.A = A;
-      c.k0 = A->begin + b * epg;
-      c.ne = (int)min((int64_t)epg, A->begin + A->count - c.k0);
-    }
+    Cursor c{0, 0, begin + b * epg};
+    if (c.k0 < end) c.ne = (int)min((int64_t)epg, end - c.k0);
     return c;
   }
   __device__ Cursor first(int, int) { return make(batch); }
@@ -343,20 +354,18 @@ struct Tile {
 // Work source of the batched kernel: groups pull tiles from a per-launch queue
 // (one atomic counter per launch) and walk their batches.
 struct QueueSource {
-  const AsmArgs *meshes;
+  static constexpr bool kBatched = true;
   const Tile *tiles;
   int ntiles;
   int *counter;
   int *slot;  // one int in the group's shared memory
   int bar, gt, epg;
-  int tile;
   int64_t kend;
   __device__ Cursor from_tile(int t) {
-    Cursor c{nullptr, 0, 0};
-    tile = t;
+    Cursor c{0, 0, 0};
     if (t < ntiles) {
       const Tile tl = tiles[t];
-      c.A = meshes + tl.mesh;
+      c.mesh = tl.mesh;
       c.k0 = tl.begin;
       kend = tl.begin + tl.count;
       c.ne = (int)min((int64_t)epg, kend - c.k0);
@@ -412,9 +421,12 @@ __device__ __forceinline__ void cta_prologue(unsigned char *smem) {
   __syncthreads();
 }
 
-// One group's assembly loop over the batches its work source yields.
+// One group's assembly loop over the batches its work source yields.  `single`
+// is the single-mesh kernel's argument block (read straight from the parameter
+// bank); batched sources read `meshes[cursor.mesh]` from global memory.
 template <int P, typename T, int MODE, typename Src>
-__device__ __forceinline__ void group_loop(unsigned char *smem, Src &src) {
+__device__ __forceinline__ void group_loop(unsigned char *smem, Src &src, const AsmArgs &single,
+                                           const AsmArgs *__restrict__ meshes) {
   using S = Shape<P>;
   using L = Layout<P, T>;
   using D = Dims<P>;
@@ -435,43 +447,79 @@ __device__ __forceinline__ void group_loop(unsigned char *smem, Src &src) {
   double2 *U = reinterpret_cast<double2 *>(gs + L::U);
   double *S3 = reinterpret_cast<double *>(gs + L::S3);
   int *nid = reinterpret_cast<int *>(gs + L::nid);
+  int *rbase = reinterpret_cast<int *>(gs + L::rbase);
+  unsigned char *stage = gs + L::stage;
+  constexpr size_t STAGE = align16(L::STAGE);
   const int bar = 1 + g;
 
   // Gather of the next batch, issued early so its latency overlaps the current batch.
-  int pf_node = 0;
+  int pf_node = 0, pf_rb = 0;
   double2 pf_x = make_double2(0, 0), pf_u = make_double2(0, 0);
+  auto args = [&](const Cursor &c) -> const AsmArgs & {
+    if constexpr (Src::kBatched) {
+      return meshes[c.mesh];
+    } else {
+      return single;
+    }
+  };
   auto prefetch = [&](const Cursor &c) {
-    if (!c.A || tg >= c.ne * NN) return;
+    if (tg >= c.ne * NN) return;
+    const AsmArgs &M = args(c);
     const int el = tg / NN, a = tg - el * NN;
     const int64_t k = c.k0 + el;
     if constexpr ((MODE & kPlan) != 0) {
-      pf_node = __ldg(c.A->connList + k * NN + a);
+      pf_node = __ldg(M.connList + k * NN + a);
     } else {
-      pf_node = __ldg(c.A->conn + __ldg(c.A->connPtr + k) + a);
+      pf_node = __ldg(M.conn + __ldg(M.connPtr + k) + a);
     }
-    pf_x = __ldg(reinterpret_cast<const double2 *>(c.A->coords) + pf_node);
-    pf_u = __ldg(reinterpret_cast<const double2 *>(c.A->states) + pf_node);
+    pf_x = __ldg(reinterpret_cast<const double2 *>(M.coords) + pf_node);
+    pf_u = __ldg(reinterpret_cast<const double2 *>(M.states) + pf_node);
+    if constexpr ((MODE & (kPlan | kJac)) == (kPlan | kJac) || (MODE & (kPlan | kRes)) == (kPlan | kRes)) {
+      pf_rb = __ldg(M.rowp + pf_node);
+    }
+  };
+  // The batch's code records (plan) or element map rows (drop-in Jacobian), copied
+  // asynchronously into stage buffer `buf`.
+  auto stage_codes = [&](const Cursor &c, int buf) {
+    if (c.ne <= 0) return;
+    const AsmArgs &M = args(c);
+    unsigned char *dst = stage + buf * STAGE;
+    if constexpr ((MODE & kPlan) != 0) {
+      constexpr int CS = D::CS;
+      const unsigned char *src_ = M.blockCode + c.k0 * CS;
+      for (int i = tg; i < c.ne * CS / 16; i += GT) cp_async16(dst + 16 * i, src_ + 16 * i);
+    } else if constexpr ((MODE & kJac) != 0) {
+      const int *src_ = M.map + c.k0 * NN * NN;
+      for (int i = tg; i < c.ne * NN * NN; i += GT) cp_async4(dst + 4 * i, src_ + i);
+    }
+    cp_async_commit();
   };
 
   Cursor cur = src.first(tg, bar);
   prefetch(cur);
-  while (cur.A) {
-    const Out A = load_out(*cur.A);
+  stage_codes(cur, 0);
+  int buf = 0;
+  while (cur.ne > 0) {
+    const AsmArgs &M = args(cur);
     const int64_t k0 = cur.k0;
     const int ne = cur.ne;
-    const double mu = cur.A->mu, lam = cur.A->lam, thick = cur.A->t;
+    const double mu = M.mu, lam = M.lam, thick = M.t;
     const T cMu = T(mu), cLam = T(lam), cC11 = T(lam + 2.0 * mu);
+    const Out A{M.mat, M.residual, stage + buf * STAGE, rbase, reinterpret_cast<const int *>(stage + buf * STAGE)};
 
     // 0. commit the gathered element data
     if (tg < ne * NN) {
       X[tg] = pf_x;
       U[tg] = pf_u;
       nid[tg] = pf_node;
+      rbase[tg] = pf_rb;
     }
+    cp_async_wait_all();
     src.request(cur, tg);
     group_sync(bar, GT);
     const Cursor nxt = src.next(cur);
     prefetch(nxt);
+    stage_codes(nxt, buf ^ 1);
 
     // 1. quadrature points: NPART lanes per (element, q) split the node sums,
     //    every lane of the quad then forms J^-1 and the gradients of its nodes.
@@ -585,7 +633,7 @@ __device__ __forceinline__ void group_loop(unsigned char *smem, Src &src) {
         if (act && part == 0) {
           double *dst = A.residual + 2 * (int64_t)nid[ia];
           if constexpr ((MODE & kPlan) != 0) {
-            if (__ldg(A.nodeCode + (k0 + el) * NN + a)) {
+            if (A.codes[el * D::CS + NN * NN + a]) {
               *reinterpret_cast<double2 *>(dst) = make_double2(double(rx), double(ry));
             } else {
               atomicAdd(dst, double(rx));
@@ -610,12 +658,12 @@ __device__ __forceinline__ void group_loop(unsigned char *smem, Src &src) {
           const double *Gm = reinterpret_cast<const double *>(gs + L::G) + el * NQP * RS;
           const double *Hm = reinterpret_cast<const double *>(gs + L::H) + el * NQP * RS;
           if constexpr (WPE == 1) {
-            stiffness_mma<P, MODE, 0, D::NT8>(A, Gm, Hm, nid + el * NN, k0 + el, mu, lam, lane);
+            stiffness_mma<P, MODE, 0, D::NT8>(A, Gm, Hm, el, mu, lam, lane);
           } else {
             if (part == 0)
-              stiffness_mma<P, MODE, 0, 2>(A, Gm, Hm, nid + el * NN, k0 + el, mu, lam, lane);
+              stiffness_mma<P, MODE, 0, 2>(A, Gm, Hm, el, mu, lam, lane);
             else
-              stiffness_mma<P, MODE, 2, D::NT8>(A, Gm, Hm, nid + el * NN, k0 + el, mu, lam, lane);
+              stiffness_mma<P, MODE, 2, D::NT8>(A, Gm, Hm, el, mu, lam, lane);
           }
         }
       } else {
@@ -659,15 +707,17 @@ __device__ __forceinline__ void group_loop(unsigned char *smem, Src &src) {
             const double kxy = double(cLam * m[ax][1] + cMu * m[ax][2]);
             const double kyx = double(cLam * m[ax][2] + cMu * m[ax][1]);
             const double kyy = double(cC11 * m[ax][3] + cMu * m[ax][0]);
-            write_block<NN, MODE>(A, k0 + el, nid + el * NN, a, b, 0, kxx, kxy, kyx, kyy);
-            if (a != b) write_block<NN, MODE>(A, k0 + el, nid + el * NN, a, b, 1, kxx, kxy, kyx, kyy);
+            write_block<P, MODE>(A, el, a, b, 0, kxx, kxy, kyx, kyy);
+            if (a != b) write_block<P, MODE>(A, el, a, b, 1, kxx, kxy, kyx, kyy);
           }
         }
       }
     }
     group_sync(bar, GT);
     cur = nxt;
+    buf ^= 1;
   }
+  cp_async_wait_all();
 }
 
 // Single mesh: A.count elements from A.begin, persistent grid-stride over batches.
@@ -678,9 +728,9 @@ __global__ void __launch_bounds__(Shape<P>::GT *Shape<P>::GPC, min_blocks<P, T>(
   extern __shared__ __align__(16) unsigned char smem[];
   cta_prologue<P, T>(smem);
   const int g = threadIdx.x / S::GT;
-  StrideSource src{&A, (int64_t)blockIdx.x * S::GPC + g, (int64_t)gridDim.x * S::GPC,
-                   (A.count + S::EPG - 1) / S::EPG, S::EPG};
-  group_loop<P, T, MODE>(smem, src);
+  StrideSource src{A.begin, A.begin + A.count, (int64_t)blockIdx.x * S::GPC + g, (int64_t)gridDim.x * S::GPC,
+                   S::EPG};
+  group_loop<P, T, MODE>(smem, src, A, nullptr);
 }
 
 // Many meshes of one order: groups pull tiles from the launch's queue.
@@ -693,8 +743,8 @@ __global__ void __launch_bounds__(Shape<P>::GT *Shape<P>::GPC, min_blocks<P, T>(
   __shared__ int slots[S::GPC];
   cta_prologue<P, T>(smem);
   const int g = threadIdx.x / S::GT;
-  QueueSource src{meshes, tiles, ntiles, counter, &slots[g], 1 + g, S::GT, S::EPG, 0, 0};
-  group_loop<P, T, MODE>(smem, src);
+  QueueSource src{tiles, ntiles, counter, &slots[g], 1 + g, S::GT, S::EPG, 0};
+  group_loop<P, T, MODE>(smem, src, meshes[0], meshes);
 }
 
 }  // namespace dev

@@ -163,8 +163,8 @@ int build_host_plan(int order, int numNodes, const int *connPtr, const int *conn
     for (int e = 0; e < numElements; e++) hp.elemList[fill[colour[e]]++] = e;
   }
   hp.connList.resize((size_t)numElements * nn);
-  hp.blockCode.resize((size_t)numElements * nn * nn);
-  hp.nodeCode.resize((size_t)numElements * nn);
+  hp.codeStride = (nn * nn + nn + 15) / 16 * 16;
+  hp.blockCode.assign((size_t)numElements * hp.codeStride, 0);
   std::vector<uint8_t> blockWritten((size_t)hp.nnzb, 0), nodeWritten((size_t)numNodes, 0);
   int bad = 0;
   for (int c = 0; c < hp.numColours; c++) {
@@ -179,7 +179,8 @@ int build_host_plan(int order, int numNodes, const int *connPtr, const int *conn
       for (int a = 0; a < nn; a++) {
         const int r = en[a];
         uint8_t &nf = nodeWritten[r];
-        hp.nodeCode[(size_t)k * nn + a] = nf ? 0 : 1;
+        uint8_t *rec = &hp.blockCode[(size_t)k * hp.codeStride];
+        rec[nn * nn + a] = nf ? 0 : 1;
         nf = 1;
         const int *c0 = hp.cols.data() + hp.rowp[r], *c1 = hp.cols.data() + hp.rowp[r + 1];
         for (int b = 0; b < nn; b++) {
@@ -190,7 +191,7 @@ int build_host_plan(int order, int numNodes, const int *connPtr, const int *conn
             continue;
           }
           uint8_t &bf = blockWritten[(size_t)(pos - hp.cols.data())];
-          hp.blockCode[((size_t)k * nn + a) * nn + b] = (uint8_t)(rank | (bf ? 0 : 0x80));
+          rec[a * nn + b] = (uint8_t)(rank | (bf ? 0 : 0x80));
           bf = 1;
         }
       }

@@ -112,7 +112,6 @@ void plan_free(fem_plan *p) {
   cudaFree(p->d_cols);
   cudaFree(p->d_connList);
   cudaFree(p->d_blockCode);
-  cudaFree(p->d_nodeCode);
   cudaSetDevice(cur);
   delete p;
 }
@@ -198,8 +197,7 @@ int fem_plan_create(int elementOrder, int numNodes, const int *connPtr, const in
   p->colourPtr = hp.colourPtr;
   if ((st = upload(hp.rowp, &p->d_rowp, p->deviceBytes)) || (st = upload(hp.cols, &p->d_cols, p->deviceBytes)) ||
       (st = upload(hp.connList, &p->d_connList, p->deviceBytes)) ||
-      (st = upload(hp.blockCode, &p->d_blockCode, p->deviceBytes)) ||
-      (st = upload(hp.nodeCode, &p->d_nodeCode, p->deviceBytes))) {
+      (st = upload(hp.blockCode, &p->d_blockCode, p->deviceBytes))) {
     plan_free(p);
     return st;
   }
@@ -258,7 +256,6 @@ int fem_plan_assemble(const fem_plan *plan, const double *states, const double *
   fem::dev::AsmArgs a{};
   a.connList = plan->d_connList;
   a.blockCode = plan->d_blockCode;
-  a.nodeCode = plan->d_nodeCode;
   a.rowp = plan->d_rowp;
   a.states = states;
   a.coords = nodeCoords;

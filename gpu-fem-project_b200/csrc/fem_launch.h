@@ -145,6 +145,6 @@ struct fem_plan {
   int64_t nnzb = 0;
   std::vector<int> colourPtr;
   int *d_rowp = nullptr, *d_cols = nullptr, *d_connList = nullptr;
-  uint8_t *d_blockCode = nullptr, *d_nodeCode = nullptr;
+  uint8_t *d_blockCode = nullptr;  // per-element code records (Dims<P>::CS bytes each)
   int64_t deviceBytes = 0;
 };
