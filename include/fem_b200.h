@@ -165,6 +165,41 @@ int fem_batch_tune(fem_batch *batch, int precision, void *stream, int reps, doub
 int fem_batch_capture(fem_batch *batch, int precision, void *stream);
 int fem_batch_replay(fem_batch *batch, void *stream, double *elapsedSeconds);
 
+/* ---- batched drop-in assembly without device allocation --------------------------------- */
+/* One mesh in the reference's drop-in format (all arrays are the caller's device
+ * memory, laid out as for fem_run_jacobian; residual is required here). */
+typedef struct {
+  int elementOrder;
+  int numElements;
+  const int *connPtr;
+  const int *conn;
+  const double *states;
+  const double *nodeCoords;
+  double E, nu, t;
+  const int *elementBCSRMap;
+  double *residual;
+  double *matEntries;
+} fem_dropin_mesh;
+
+/* Bytes of the library's file-scope device scratch array (the argument table of
+ * up to 256 meshes, up to 16384 work-queue tiles and the queue counters). */
+#define FEM_STATIC_SCRATCH_BYTES 294912
+
+/* fem_run_jacobian for up to 256 meshes of mixed orders in one batched pass
+ * (one persistent launch per order present), for callers that cannot allocate
+ * device memory: it calls no cudaMalloc, cudaFree or other allocating routine.
+ * What the batched kernel needs besides the caller's arrays lives in a
+ * file-scope __device__ array of FEM_STATIC_SCRATCH_BYTES that every GPU using
+ * the library holds until the process exits.  The first call on a device looks
+ * up that array's device address (make it before any stream capture).  Calls
+ * share the array, so calls that overlap on the GPU race; each call clears the
+ * queue counters it uses.  Accumulates into caller-zeroed residual and
+ * matEntries like fem_run_jacobian; asynchronous on `stream` (the host staging
+ * of the mesh table is copied out before the call returns).  More than 256
+ * meshes or more work than the tile capacity returns FEM_ERR_UNSUPPORTED.
+ * (No counterpart in the reference: it assembles one mesh per call.) */
+int fem_run_jacobian_batched_static(int numMeshes, const fem_dropin_mesh *meshes, void *stream);
+
 /* ---- calibration ---------------------------------------------------------------------- */
 /* Measured arithmetic peak of the current device in TFLOP/s, used as the
  * roofline denominator of the element arithmetic: kind 0 = FP64 FMA pipe,
