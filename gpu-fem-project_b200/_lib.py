@@ -53,6 +53,15 @@ SIGNATURES = {
     "fem_plan_device_pattern": (_i, [_p, C.POINTER(_p), C.POINTER(_p)]),
     "fem_plan_assemble": (_i, [_p, _p, _p, _d, _d, _d, _p, _p, _i, _p, _pd]),
     "fem_probe_peak": (_i, [_i, _pd]),
+    "fem_server_create": (_i, [_i64, _i, _i, C.POINTER(_p)]),
+    "fem_server_destroy": (_i, [_p]),
+    "fem_server_add_mesh": (_i, [_p, _i, _i, _p, _p, _i, _p, _d, _d, _d, _pi]),
+    "fem_server_remove_mesh": (_i, [_p, _i]),
+    "fem_server_mesh_outputs": (_i, [_p, _i, C.POINTER(_p), C.POINTER(_p), C.POINTER(_p), C.POINTER(_p), _pi64]),
+    "fem_server_submit": (_i, [_p, _i, _p, _p, _pi64]),
+    "fem_server_wait": (_i, [_p, _i64, _i, _pd]),
+    "fem_server_stats": (_i, [_p, _pi64, _pi64, _pi64, _pi64, _pi64]),
+    "fem_run_jacobian_batched_static": (_i, [_i, _p, _p]),
     "fem_batch_create": (_i, [_i, _p, C.POINTER(_p)]),
     "fem_batch_destroy": (_i, [_p]),
     "fem_batch_bind": (_i, [_p, _i, _p, _p, _d, _d, _d, _p, _p]),

@@ -247,6 +247,84 @@ class Batch:
             pass
 
 
+def _hptr(x):
+    """Host pointer of a numpy array or a (pinned) CPU tensor."""
+    if x is None:
+        return None
+    if isinstance(x, np.ndarray):
+        if not x.flags.c_contiguous or x.dtype != np.float64:
+            raise ValueError("host arrays must be contiguous float64")
+        return x.ctypes.data
+    import torch
+    if isinstance(x, torch.Tensor):
+        if x.is_cuda or x.dtype != torch.float64 or not x.is_contiguous():
+            raise ValueError("host tensors must be contiguous float64 CPU tensors")
+        return x.data_ptr()
+    raise TypeError(type(x).__name__)
+
+
+class Server:
+    """Continuous-batching assembly server over device-resident meshes (fem_server_*)."""
+
+    def __init__(self, budget_bytes, *, precision="fp64", max_batch=64):
+        self._h = C.c_void_p()
+        check(lib.fem_server_create(int(budget_bytes), _prec(precision), int(max_batch), C.byref(self._h)),
+              "fem_server_create")
+        self._inflight = {}
+
+    def add_mesh(self, mesh):
+        cp, cn = _np(mesh.conn_ptr, np.int32), _np(mesh.conn, np.int32)
+        xy = _np(mesh.coords, np.float64)
+        mid = C.c_int()
+        check(lib.fem_server_add_mesh(self._h, mesh.order, mesh.num_nodes, cp.ctypes.data, cn.ctypes.data, cp.size - 1,
+                                      xy.ctypes.data, float(mesh.E), float(mesh.nu), float(mesh.t), C.byref(mid)),
+              "fem_server_add_mesh")
+        return mid.value
+
+    def remove_mesh(self, mesh_id):
+        check(lib.fem_server_remove_mesh(self._h, int(mesh_id)), "fem_server_remove_mesh")
+
+    def outputs(self, mesh_id):
+        r, a, rp, cl = C.c_void_p(), C.c_void_p(), C.c_void_p(), C.c_void_p()
+        nnzb = C.c_int64()
+        check(lib.fem_server_mesh_outputs(self._h, int(mesh_id), C.byref(r), C.byref(a), C.byref(rp), C.byref(cl),
+                                          C.byref(nnzb)), "fem_server_mesh_outputs")
+        return {"residual": r.value, "mat": a.value, "rowp": rp.value, "cols": cl.value, "nnzb": nnzb.value}
+
+    def submit(self, mesh_id, host_states, host_residual=None):
+        tk = C.c_int64()
+        check(lib.fem_server_submit(self._h, int(mesh_id), _hptr(host_states), _hptr(host_residual), C.byref(tk)),
+              "fem_server_submit")
+        self._inflight[tk.value] = (host_states, host_residual)
+        return tk.value
+
+    def wait(self, ticket, timeout_ms=120000):
+        lat = C.c_double()
+        try:
+            check(lib.fem_server_wait(self._h, int(ticket), int(timeout_ms), C.byref(lat)), "fem_server_wait")
+        finally:
+            self._inflight.pop(ticket, None)
+        return lat.value
+
+    def stats(self):
+        w, c, e, u, b = (C.c_int64() for _ in range(5))
+        check(lib.fem_server_stats(self._h, C.byref(w), C.byref(c), C.byref(e), C.byref(u), C.byref(b)),
+              "fem_server_stats")
+        return {"waves": w.value, "completed": c.value, "elements": e.value, "used_bytes": u.value,
+                "budget_bytes": b.value}
+
+    def close(self):
+        if self._h and self._h.value:
+            lib.fem_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class DeviceMesh:
     """A Mesh uploaded to the GPU as torch tensors (int32 topology, float64 data)."""
 

@@ -23,48 +23,6 @@ namespace {
 constexpr int kMaxColours = 64;
 constexpr int kOrders = 5;  // index 1..4
 
-int epg_of(int p) {
-  switch (p) {
-    case 1: return fem::dev::Shape<1>::EPG;
-    case 2: return fem::dev::Shape<2>::EPG;
-    case 3: return fem::dev::Shape<3>::EPG;
-    default: return fem::dev::Shape<4>::EPG;
-  }
-}
-
-template <int P, typename T>
-int launch_batched_p(const fem::dev::AsmArgs *meshes, const fem::dev::Tile *tiles, int ntiles, int *counter,
-                     cudaStream_t s) {
-  using S = fem::dev::Shape<P>;
-  constexpr int NT = S::GT * S::GPC;
-  constexpr int MODE = fem::dev::kPlan | fem::dev::kRes | fem::dev::kJac;
-  auto kernel = fem::dev::assemble_batched_kernel<P, T, MODE>;
-  const size_t smem = fem::dev::Layout<P, T>::total;
-  fem::LaunchInfo li;
-  int st = fem::launch_info(kernel, NT, smem, li);
-  if (st) return st;
-  const int64_t need = (ntiles + S::GPC - 1) / S::GPC;
-  const int64_t cap = (int64_t)li.grid_per_sm * li.num_sms;
-  const int grid = (int)std::min(need, cap);
-  if (grid <= 0) return FEM_SUCCESS;
-  kernel<<<grid, NT, smem, s>>>(meshes, tiles, ntiles, counter);
-  cudaError_t err = cudaGetLastError();
-  if (err != cudaSuccess) return fem::cuda_fail(err, "assemble_batched_kernel launch");
-  return FEM_SUCCESS;
-}
-
-template <typename T>
-int launch_batched(int p, const fem::dev::AsmArgs *meshes, const fem::dev::Tile *tiles, int ntiles, int *counter,
-                   cudaStream_t s) {
-  switch (p) {
-    case 1: return launch_batched_p<1, T>(meshes, tiles, ntiles, counter, s);
-    case 2: return launch_batched_p<2, T>(meshes, tiles, ntiles, counter, s);
-    case 3: return launch_batched_p<3, T>(meshes, tiles, ntiles, counter, s);
-    case 4: return launch_batched_p<4, T>(meshes, tiles, ntiles, counter, s);
-    default: return fem::fail(FEM_ERR_INVALID_ORDER, "order %d", p);
-  }
-}
-
 }  // namespace
 
 struct fem_batch {
@@ -126,7 +84,7 @@ void build_tiles(fem_batch *b) {
   b->tiles.clear();
   b->tileOff.assign((size_t)kOrders * (C + 1), 0);
   for (int p = 1; p < kOrders; p++) {
-    const int64_t len = (int64_t)b->tileBatches[p] * epg_of(p);
+    const int64_t len = (int64_t)b->tileBatches[p] * fem::epg_of(p);
     for (int c = 0; c < C; c++) {
       b->tileOff[p * (C + 1) + c] = (int)b->tiles.size();
       for (size_t m = 0; m < b->plans.size(); m++) {
@@ -180,8 +138,8 @@ int enqueue_order(fem_batch *b, int p, int precision, cudaStream_t s) {
     if (t1 <= t0) continue;
     int *counter = b->d_counters + p * kMaxColours + c;
     int st = precision == FEM_PRECISION_FP64
-                 ? launch_batched<double>(p, b->d_args, b->d_tiles + t0, t1 - t0, counter, s)
-                 : launch_batched<float>(p, b->d_args, b->d_tiles + t0, t1 - t0, counter, s);
+                 ? fem::launch_batched<double>(p, b->d_args, b->d_tiles + t0, t1 - t0, counter, s)
+                 : fem::launch_batched<float>(p, b->d_args, b->d_tiles + t0, t1 - t0, counter, s);
     if (st) return st;
   }
   return FEM_SUCCESS;

@@ -136,6 +136,49 @@ int timed(cudaStream_t s, double *elapsed, F body) {
   return st;
 }
 
+inline int epg_of(int p) {
+  switch (p) {
+    case 1: return dev::Shape<1>::EPG;
+    case 2: return dev::Shape<2>::EPG;
+    case 3: return dev::Shape<3>::EPG;
+    default: return dev::Shape<4>::EPG;
+  }
+}
+
+// One persistent batched launch of order P over the tile queue `tiles` (plan mode,
+// residual and Jacobian).
+template <int P, typename T>
+int launch_batched_p(const dev::AsmArgs *meshes, const dev::Tile *tiles, int ntiles, int *counter, cudaStream_t s) {
+  using S = dev::Shape<P>;
+  constexpr int NT = S::GT * S::GPC;
+  constexpr int MODE = dev::kPlan | dev::kRes | dev::kJac;
+  auto kernel = dev::assemble_batched_kernel<P, T, MODE>;
+  const size_t smem = dev::Layout<P, T>::total;
+  LaunchInfo li;
+  int st = launch_info(kernel, NT, smem, li);
+  if (st) return st;
+  const int64_t need = (ntiles + S::GPC - 1) / S::GPC;
+  const int64_t cap = (int64_t)li.grid_per_sm * li.num_sms;
+  const int grid = (int)(need < cap ? need : cap);
+  if (grid <= 0) return FEM_SUCCESS;
+  kernel<<<grid, NT, smem, s>>>(meshes, tiles, ntiles, counter);
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return cuda_fail(err, "assemble_batched_kernel launch");
+  return FEM_SUCCESS;
+}
+
+template <typename T>
+int launch_batched(int p, const dev::AsmArgs *meshes, const dev::Tile *tiles, int ntiles, int *counter,
+                   cudaStream_t s) {
+  switch (p) {
+    case 1: return launch_batched_p<1, T>(meshes, tiles, ntiles, counter, s);
+    case 2: return launch_batched_p<2, T>(meshes, tiles, ntiles, counter, s);
+    case 3: return launch_batched_p<3, T>(meshes, tiles, ntiles, counter, s);
+    case 4: return launch_batched_p<4, T>(meshes, tiles, ntiles, counter, s);
+    default: return fail(FEM_ERR_INVALID_ORDER, "order %d", p);
+  }
+}
+
 }  // namespace fem
 
 // Device-resident topology of one mesh (see fem_plan_create).

@@ -165,6 +165,34 @@ int fem_batch_tune(fem_batch *batch, int precision, void *stream, int reps, doub
 int fem_batch_capture(fem_batch *batch, int precision, void *stream);
 int fem_batch_replay(fem_batch *batch, void *stream, double *elapsedSeconds);
 
+/* ---- serving: continuous batching over device-resident meshes ------------------------- */
+/* A server keeps client meshes resident (plan, coordinates, state, residual and
+ * matrix) within a device-memory budget and assembles submitted requests in
+ * waves: whenever one of its two lanes is free, everything pending (up to
+ * maxBatch requests) is copied in, assembled by the batched persistent kernels
+ * and its residuals copied back, while the other lane may still be running.
+ * (No reference counterpart.) */
+typedef struct fem_server fem_server;
+
+int fem_server_create(int64_t budgetBytes, int precision, int maxBatch, fem_server **server);
+int fem_server_destroy(fem_server *server);
+/* Registers a mesh (host topology and coordinates); FEM_ERR_BUDGET when its
+ * device bytes do not fit the remaining budget (retry after a removal). */
+int fem_server_add_mesh(fem_server *server, int elementOrder, int numNodes, const int *connPtr, const int *conn,
+                        int numElements, const double *nodeCoords, double E, double nu, double t, int *meshId);
+int fem_server_remove_mesh(fem_server *server, int meshId);
+/* Device pointers of a mesh's resident outputs and pattern (valid until removal). */
+int fem_server_mesh_outputs(fem_server *server, int meshId, const double **residual, const double **matEntries,
+                            const int **rowp, const int **cols, int64_t *nnzb);
+/* One request: hostStates (numNodes*2 doubles, read when the wave is issued) and
+ * an optional hostResidual to receive the residual.  One request per mesh may be
+ * in flight.  Pinned host buffers let the copies overlap. */
+int fem_server_submit(fem_server *server, int meshId, const double *hostStates, double *hostResidual, int64_t *ticket);
+/* Waits up to timeoutMs for a ticket; returns its submit-to-completion latency. */
+int fem_server_wait(fem_server *server, int64_t ticket, int timeoutMs, double *latencySeconds);
+int fem_server_stats(fem_server *server, int64_t *waves, int64_t *completed, int64_t *elements, int64_t *usedBytes,
+                     int64_t *budgetBytes);
+
 /* ---- batched drop-in assembly without device allocation --------------------------------- */
 /* One mesh in the reference's drop-in format (all arrays are the caller's device
  * memory, laid out as for fem_run_jacobian; residual is required here). */
