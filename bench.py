@@ -35,6 +35,8 @@ WORKLOADS = {
     "square1024_p3": dict(kind="square", n=1024, p=3),
     "square512_p3": dict(kind="square", n=512, p=3),
     "square2048_p1": dict(kind="square", n=2048, p=1),
+    "square1024_p2": dict(kind="square", n=1024, p=2),
+    "square512_p4": dict(kind="square", n=512, p=4),
     "square64_p1": dict(kind="square64"),
     "annulus512x2048_p2": dict(kind="annulus"),
 }
@@ -435,6 +437,135 @@ def run_batch(args):
     print(json.dumps(line), flush=True)
 
 
+def run_serve(args):
+    """64 Newton-solve clients with device-resident meshes (drawn like the batched
+    workload, at most 4M DOF each) issue requests as one Poisson stream at each
+    swept aggregate rate; the server admits meshes under the HBM budget and
+    batches concurrent requests.  Latency is measured from each request's arrival
+    (so it includes waiting behind the client's previous request)."""
+    import threading
+
+    import torch
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    import fem_pkg
+    fem = fem_pkg.load()
+    specs = fem.batch_specs(count=args.clients, seed=fem.mesh.SEEDS["serve64"], max_dof=4e6)
+    meshes = [sp.build() for sp in specs]
+    srv = fem.Server(int(args.budget_gb * 1e9), precision=args.batch_precision, max_batch=args.max_batch)
+    ids, admitted = [], []
+    for i, m in enumerate(meshes):
+        try:
+            ids.append(srv.add_mesh(m))
+            admitted.append(i)
+        except fem.FemError as e:
+            if e.status != fem.FEM_ERR_BUDGET:
+                raise
+    meshes = [meshes[i] for i in admitted]
+    rng = np.random.default_rng(12345)
+    states = []
+    for m in meshes:
+        s0 = torch.from_numpy(np.ascontiguousarray(m.states)).pin_memory()
+        s1 = torch.from_numpy(np.ascontiguousarray(m.states * 1.01 + 1e-6)).pin_memory()
+        states.append((s0, s1))
+    outs = [torch.empty(m.num_nodes * 2, dtype=torch.float64).pin_memory() for m in meshes]
+    for i in range(len(meshes)):  # warm-up: one request per client
+        srv.wait(srv.submit(ids[i], states[i][0], outs[i]))
+    sweep = []
+    for rate in args.rates:
+        n_req = max(50, int(rate * args.serve_seconds))
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n_req))
+        who = rng.integers(0, len(meshes), size=n_req)
+        per_client = [[] for _ in meshes]
+        for t, c in zip(arrivals, who):
+            per_client[c].append(t)
+        lat, srv_lat, elems = [], [], [0]
+        lock = threading.Lock()
+        t0 = time.perf_counter() + 0.05
+        st0 = srv.stats()
+
+        def client(c):
+            k = 0
+            for t in per_client[c]:
+                delay = t0 + t - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                tk = srv.submit(ids[c], states[c][k & 1], outs[c])
+                sl = srv.wait(tk)
+                done = time.perf_counter()
+                k += 1
+                with lock:
+                    lat.append(done - (t0 + t))
+                    srv_lat.append(sl)
+                    elems[0] += meshes[c].num_elements
+
+        threads = [threading.Thread(target=client, args=(c,)) for c in range(len(meshes)) if per_client[c]]
+        for th in threads:
+            th.start()
+        for th in threads:
+            th.join()
+        wall = time.perf_counter() - t0
+        st1 = srv.stats()
+        lat_ms = np.array(lat) * 1e3
+        sweep.append({"rate_req_s": rate, "requests": len(lat), "elements_per_s": elems[0] / wall,
+                      "p50_ms": float(np.percentile(lat_ms, 50)), "p99_ms": float(np.percentile(lat_ms, 99)),
+                      "server_p50_ms": float(np.percentile(np.array(srv_lat) * 1e3, 50)),
+                      "server_p99_ms": float(np.percentile(np.array(srv_lat) * 1e3, 99)),
+                      "waves": st1["waves"] - st0["waves"], "wall_s": wall})
+    used = srv.stats()["used_bytes"]
+    srv.close()
+    # plain single-mesh FP64 drop-in for a sample of the same requests: H2D state,
+    # zero the outputs, fem_run_jacobian, D2H residual, one request at a time
+    sample = rng.integers(0, len(meshes), size=min(64, len(meshes)))
+    stream = torch.cuda.Stream(device=dev)
+    plain_el, plain_t = 0, 0.0
+    for c in sorted(set(sample.tolist())):
+        m = meshes[c]
+        rowp, cols = fem.build_bsr_pattern(m.num_nodes, m.conn_ptr, m.conn)
+        mp = fem.build_element_bsr_map(m.conn_ptr, m.conn, m.nodes_per_element, rowp, cols)
+        with torch.cuda.stream(stream):
+            d = fem.DeviceMesh(m, dev)
+            dmap = torch.from_numpy(mp).to(dev)
+            r = torch.empty(m.num_nodes * 2, dtype=torch.float64, device=dev)
+            a = torch.empty(cols.size * 4, dtype=torch.float64, device=dev)
+        reps = int((sample == c).sum())
+
+        def one():
+            d.states.copy_(states[c][0], non_blocking=True)
+            r.zero_()
+            a.zero_()
+            fem.run_jacobian_kernel(m.order, d.conn_ptr, d.conn, m.num_elements, d.states, d.coords, m.E, m.nu, m.t,
+                                    dmap, r, a, stream=stream.cuda_stream, timed=False)
+            outs[c].copy_(r, non_blocking=True)
+
+        with torch.cuda.stream(stream):
+            one()
+            stream.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                one()
+            e1.record(stream)
+            e1.synchronize()
+        plain_t += e0.elapsed_time(e1) * 1e-3
+        plain_el += reps * m.num_elements
+        del d, dmap, r, a
+        torch.cuda.empty_cache()
+    best = max(sweep, key=lambda x: x["elements_per_s"])
+    line = {
+        "metric": "assembled elements/s (res+Jac); serve p50/p99 ms", "value": best["elements_per_s"],
+        "unit": "elements/s", "n_gpus": 1, "steps": sum(x["requests"] for x in sweep), "warmup": len(meshes),
+        "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.batch_precision == "fp64" else "f32/f64", "data": "synthetic",
+        "config": {"workload": f"serve{args.clients}: Newton clients, meshes <= 4M DOF, Poisson arrivals",
+                   "clients_admitted": len(meshes), "budget_gb": args.budget_gb, "device_bytes_used": used,
+                   "max_batch": args.max_batch, "precision": args.batch_precision},
+        "sweep": sweep,
+        "plain_fp64_single_mesh": {"elements_per_s": plain_el / plain_t, "requests": int(len(sample))},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def cpu_baseline(fem, mesh, args):
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as orc
@@ -481,7 +612,11 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="square1024_p3", choices=sorted(WORKLOADS) + ["batch256"])
+    ap.add_argument("--workload", default="square1024_p3", choices=sorted(WORKLOADS) + ["batch256", "serve64"])
+    ap.add_argument("--clients", type=int, default=64)
+    ap.add_argument("--rates", type=lambda v: [float(x) for x in v.split(",")], default=[100, 500, 1000, 2500, 5000])
+    ap.add_argument("--serve-seconds", type=float, default=3.0)
+    ap.add_argument("--max-batch", type=int, default=64)
     ap.add_argument("--batch-meshes", type=int, default=256)
     ap.add_argument("--budget-gb", type=float, default=100.0, help="device bytes per batched wave")
     ap.add_argument("--batch-precision", default="fp64", choices=["fp64", "mixed"])
@@ -501,6 +636,8 @@ def main():
         run_reference(args)
     elif args.workload == "batch256":
         run_batch(args)
+    elif args.workload == "serve64":
+        run_serve(args)
     else:
         run_ours(args)
 

@@ -166,7 +166,18 @@ struct Shape<3> {
 };
 template <>
 struct Shape<4> {
-  static constexpr int GT = 64, EPG = 1, GPC = 2, NPART = 2, MINB = 3;
+  static constexpr int GT = 128, EPG = 1, GPC = 1, NPART = 4, MINB = 4;
+};
+
+// Warps that share one element's stiffness MMA and the tile rows [R[w], R[w+1])
+// each takes (p = 4: 7 + 6 + 9 + 6 of the 28 upper tiles of the 7x7 tile grid).
+template <int P>
+struct RowSplit {
+  static constexpr int WPE = 1;
+};
+template <>
+struct RowSplit<4> {
+  static constexpr int WPE = 4;
 };
 
 template <int P>
@@ -190,7 +201,7 @@ struct Dims {
 //   FP64 (tensor-core stiffness): G and H as [NQP][RS] doubles, row r = 2a + i.
 //   FP32 (CUDA-core stiffness):   G and H as [NQ][NN+1] float2, the padded row
 //   lets the quadrature stage store without bank conflicts.
-template <int P, typename T>
+template <int P, typename T, int MODE>
 struct Layout {
   using S = Shape<P>;
   using D = Dims<P>;
@@ -208,9 +219,10 @@ struct Layout {
   static constexpr size_t H = align16(G + EPG * GH_ELEM);      // [EPG] x GH_ELEM
   static constexpr size_t nid = align16(H + EPG * GH_ELEM);    // int [EPG][NN]
   static constexpr size_t rbase = align16(nid + 4 * EPG * NN);  // int [EPG][NN]
-  // staged codes (plan) or element map rows (drop-in), double-buffered
-  static constexpr size_t STAGE = (size_t(EPG) * D::CS > size_t(EPG) * NN * NN * 4) ? size_t(EPG) * D::CS
-                                                                                      : size_t(EPG) * NN * NN * 4;
+  // staged code records (plan) or element map rows (drop-in Jacobian), double-buffered
+  static constexpr size_t STAGE = (MODE & kPlan) ? size_t(EPG) * D::CS
+                                  : (MODE & kJac) ? size_t(EPG) * NN * NN * 4
+                                                  : 16;
   static constexpr size_t stage = align16(rbase + 4 * EPG * NN);  // [2][STAGE] bytes
   static constexpr size_t group_bytes = align16(stage + 2 * align16(STAGE));
   static constexpr size_t total = groups + S::GPC * group_bytes;
@@ -392,10 +404,10 @@ struct QueueSource {
 };
 
 // The per-CTA prologue: derivative table and weights, zeroed MMA padding rows.
-template <int P, typename T>
+template <int P, typename T, int MODE>
 __device__ __forceinline__ void cta_prologue(unsigned char *smem) {
   using S = Shape<P>;
-  using L = Layout<P, T>;
+  using L = Layout<P, T, MODE>;
   using D = Dims<P>;
   constexpr int P1 = P + 1, NN = D::NN, NQ = NN, NQP = D::NQP, RS = D::RS, EPG = S::EPG;
   double2 *tabT = reinterpret_cast<double2 *>(smem + L::tabT);
@@ -428,7 +440,7 @@ template <int P, typename T, int MODE, typename Src>
 __device__ __forceinline__ void group_loop(unsigned char *smem, Src &src, const AsmArgs &single,
                                            const AsmArgs *__restrict__ meshes) {
   using S = Shape<P>;
-  using L = Layout<P, T>;
+  using L = Layout<P, T, MODE>;
   using D = Dims<P>;
   constexpr bool TC = L::TC;
   constexpr int P1 = P + 1, NN = D::NN, NQ = NN, NNP = L::NNP, NTILE = D::NTILE;
@@ -651,7 +663,7 @@ __device__ __forceinline__ void group_loop(unsigned char *smem, Src &src, const 
     if constexpr ((MODE & kJac) != 0) {
       if constexpr (TC) {
         // FP64 tensor cores: warps take (element, row range) work items
-        constexpr int WPE = (P == 4) ? 2 : 1;  // warps per element
+        constexpr int WPE = RowSplit<P>::WPE;  // warps per element
         constexpr int NW = GT / 32;
         for (int w = warp; w < ne * WPE; w += NW) {
           const int el = w / WPE, part = w - el * WPE;
@@ -660,10 +672,15 @@ __device__ __forceinline__ void group_loop(unsigned char *smem, Src &src, const 
           if constexpr (WPE == 1) {
             stiffness_mma<P, MODE, 0, D::NT8>(A, Gm, Hm, el, mu, lam, lane);
           } else {
+            static_assert(P != 4 || D::NT8 == 7, "row split of the 7x7 tile grid");
             if (part == 0)
-              stiffness_mma<P, MODE, 0, 2>(A, Gm, Hm, el, mu, lam, lane);
+              stiffness_mma<P, MODE, 0, 1>(A, Gm, Hm, el, mu, lam, lane);
+            else if (part == 1)
+              stiffness_mma<P, MODE, 1, 2>(A, Gm, Hm, el, mu, lam, lane);
+            else if (part == 2)
+              stiffness_mma<P, MODE, 2, 4>(A, Gm, Hm, el, mu, lam, lane);
             else
-              stiffness_mma<P, MODE, 2, D::NT8>(A, Gm, Hm, el, mu, lam, lane);
+              stiffness_mma<P, MODE, 4, D::NT8>(A, Gm, Hm, el, mu, lam, lane);
           }
         }
       } else {
@@ -726,7 +743,7 @@ __global__ void __launch_bounds__(Shape<P>::GT *Shape<P>::GPC, min_blocks<P, T>(
     assemble_kernel(const __grid_constant__ AsmArgs A) {
   using S = Shape<P>;
   extern __shared__ __align__(16) unsigned char smem[];
-  cta_prologue<P, T>(smem);
+  cta_prologue<P, T, MODE>(smem);
   const int g = threadIdx.x / S::GT;
   StrideSource src{A.begin, A.begin + A.count, (int64_t)blockIdx.x * S::GPC + g, (int64_t)gridDim.x * S::GPC,
                    S::EPG};
@@ -741,7 +758,7 @@ __global__ void __launch_bounds__(Shape<P>::GT *Shape<P>::GPC, min_blocks<P, T>(
   using S = Shape<P>;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int slots[S::GPC];
-  cta_prologue<P, T>(smem);
+  cta_prologue<P, T, MODE>(smem);
   const int g = threadIdx.x / S::GT;
   QueueSource src{tiles, ntiles, counter, &slots[g], 1 + g, S::GT, S::EPG, 0};
   group_loop<P, T, MODE>(smem, src, meshes[0], meshes);

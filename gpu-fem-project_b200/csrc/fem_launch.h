@@ -57,7 +57,7 @@ int launch_p(const dev::AsmArgs &a, cudaStream_t s) {
   using S = dev::Shape<P>;
   constexpr int NT = S::GT * S::GPC;
   auto kernel = dev::assemble_kernel<P, T, MODE>;
-  const size_t smem = dev::Layout<P, T>::total;
+  const size_t smem = dev::Layout<P, T, MODE>::total;
   LaunchInfo li;
   int st = launch_info(kernel, NT, smem, li);
   if (st) return st;
@@ -153,7 +153,7 @@ int launch_batched_p(const dev::AsmArgs *meshes, const dev::Tile *tiles, int nti
   constexpr int NT = S::GT * S::GPC;
   constexpr int MODE = dev::kPlan | dev::kRes | dev::kJac;
   auto kernel = dev::assemble_batched_kernel<P, T, MODE>;
-  const size_t smem = dev::Layout<P, T>::total;
+  const size_t smem = dev::Layout<P, T, MODE>::total;
   LaunchInfo li;
   int st = launch_info(kernel, NT, smem, li);
   if (st) return st;

@@ -73,7 +73,7 @@ int launch_static_p(const fem::dev::AsmArgs *meshes, const fem::dev::Tile *tiles
   constexpr int NT = S::GT * S::GPC;
   constexpr int MODE = fem::dev::kRes | fem::dev::kJac;
   auto kernel = fem::dev::assemble_batched_kernel<P, double, MODE>;
-  const size_t smem = fem::dev::Layout<P, double>::total;
+  const size_t smem = fem::dev::Layout<P, double, MODE>::total;
   fem::LaunchInfo li;
   int st = fem::launch_info(kernel, NT, smem, li);
   if (st) return st;

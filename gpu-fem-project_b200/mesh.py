@@ -198,10 +198,12 @@ class MeshSpec:
 
 
 def batch_specs(count: int = 256, lo: float = 1e3, hi: float = 1e6, seed: int | None = None,
-                perturb: float = 0.15, max_elements: float | None = None) -> list[MeshSpec]:
+                perturb: float = 0.15, max_elements: float | None = None, max_dof: float | None = None
+                ) -> list[MeshSpec]:
     """Independent meshes: element counts log-uniform in [lo, hi], order uniform in
     {1,2,3,4}, element aspect ratio (hx/hy) uniform in [1,4], perturbation +-0.15h,
-    E in U[50e9, 210e9], nu in U[0.25, 0.35], all drawn from one seed."""
+    E in U[50e9, 210e9], nu in U[0.25, 0.35], all drawn from one seed.  With
+    max_dof, the element count is capped so that 2*(p*nx+1)*(p*ny+1) <= max_dof."""
     rng = np.random.default_rng(SEEDS["batch256"] if seed is None else seed)
     out = []
     for i in range(count):
@@ -209,6 +211,8 @@ def batch_specs(count: int = 256, lo: float = 1e3, hi: float = 1e6, seed: int | 
         if max_elements is not None:
             ne = min(ne, max_elements)
         order = int(rng.integers(1, 5))
+        if max_dof is not None:
+            ne = min(ne, 0.98 * (math.sqrt(max_dof / 2.0) - 1.0) ** 2 / (order * order))
         aspect = float(rng.uniform(1.0, 4.0))
         E = float(rng.uniform(50e9, 210e9))
         nu = float(rng.uniform(0.25, 0.35))
