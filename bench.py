@@ -122,18 +122,10 @@ class ClockSampler:
 
 
 def dist_setup(args):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    pg = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        backend = "nccl" if args.impl == "ours" else "gloo"
-        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
-        pg = dist
-    return world, rank, local, pg
+    """Replica ranks from the torchrun environment (one mesh per GPU, no sharding)."""
+    import fem_pkg
+    rep = fem_pkg.load_module("replicas")
+    return rep.init_from_env("nccl" if args.impl == "ours" else "gloo")
 
 
 def peaks():
@@ -216,10 +208,7 @@ def run_ours(args):
         ev1.record(stream)
         ev1.synchronize()
         ms = ev0.elapsed_time(ev1) / steps
-        if pg is not None:
-            tt = torch.tensor([ms], device=dev)
-            pg.all_reduce(tt, op=pg.ReduceOp.MAX)
-            ms = float(tt.item())
+        ms = fem_pkg.load_module("replicas").max_over_ranks(ms, pg, dev)
         return ms, launches_per_step * steps
 
     paths = {}

@@ -32,3 +32,16 @@ def load_builder():
     mod = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(mod)
     return mod
+
+
+def load_module(name: str):
+    """A single module of the package directory that needs no compiled library
+    (e.g. `replicas`), importable on machines without the built .so."""
+    full = f"{NAME}_{name}"
+    if full in sys.modules:
+        return sys.modules[full]
+    spec = importlib.util.spec_from_file_location(full, PKG_DIR / f"{name}.py")
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[full] = mod
+    spec.loader.exec_module(mod)
+    return mod

@@ -185,3 +185,61 @@ def test_error_statuses(fem, cuda):
     assert fem.run_jacobian_kernel(1, d.conn_ptr, d.conn, 0, d.states, d.coords, m.E, m.nu, m.t, d.map, res,
                                    mat) == 0.0
     assert float(res.abs().max()) == 0.0 and float(mat.abs().max()) == 0.0
+
+
+def _scramble(fem, m, seed):
+    """Same mesh with node ids and element order permuted (unstructured numbering)."""
+    rng = np.random.default_rng(seed)
+    perm = rng.permutation(m.num_nodes)          # new id of old node
+    inv = np.argsort(perm)
+    n = m.nodes_per_element
+    conn = perm[m.conn.reshape(-1, n)]
+    order = rng.permutation(m.num_elements)
+    conn = np.ascontiguousarray(conn[order].reshape(-1)).astype(np.int32)
+    return fem.Mesh(m.order, np.ascontiguousarray(m.coords[inv]), m.conn_ptr.copy(), conn,
+                    np.ascontiguousarray(m.states[inv]), m.E, m.nu, m.t, m.name + "_scrambled", m.seed)
+
+
+@pytest.mark.parametrize("p", [1, 2, 3, 4])
+def test_scrambled_numbering(fem, orc, cuda, p):
+    """Unstructured node numbering and element order: more colours, scattered rows."""
+    import torch
+    m = _scramble(fem, fem.square_mesh(9, 7, p, 1.0, 1.0, 0.15, seed=40 + p), seed=p)
+    d = _dev(fem, m, cuda)
+    R0, A0 = orc.assemble(m, d.map_h, d.nnzb)
+    res = torch.zeros(m.num_nodes * 2, dtype=torch.float64, device=cuda)
+    mat = torch.zeros(d.nnzb * 4, dtype=torch.float64, device=cuda)
+    fem.run_jacobian_kernel(m.order, d.conn_ptr, d.conn, m.num_elements, d.states, d.coords, m.E, m.nu, m.t, d.map,
+                            res, mat)
+    assert _rel(res.cpu().numpy(), R0) <= FP64_TOL
+    assert _rel(mat.cpu().numpy(), A0) <= FP64_TOL
+    plan = fem.Plan(m.order, m.num_nodes, m.conn_ptr, m.conn)
+    assert plan.num_colours >= 4
+    res.fill_(9.0)
+    mat.fill_(9.0)
+    plan.assemble(d.states, d.coords, m.E, m.nu, m.t, res, mat)
+    torch.cuda.synchronize()
+    assert _rel(res.cpu().numpy(), R0) <= FP64_TOL
+    assert _rel(mat.cpu().numpy(), A0) <= FP64_TOL
+    plan.close()
+
+
+def test_connptr_offsets_are_honoured(fem, orc, cuda):
+    """The drop-in path reads conn[connPtr[e] + a]: a conn array with unused gaps
+    between elements gives the same result."""
+    import torch
+    m = fem.square_mesh(5, 4, 2, seed=51)
+    d = _dev(fem, m, cuda)
+    R0, A0 = orc.assemble(m, d.map_h, d.nnzb)
+    n = m.nodes_per_element
+    gap = 3
+    conn_g = np.full(m.num_elements * (n + gap), -1, np.int32)
+    ptr_g = (np.arange(m.num_elements + 1) * (n + gap)).astype(np.int32)
+    for e in range(m.num_elements):
+        conn_g[ptr_g[e]:ptr_g[e] + n] = m.conn[e * n:(e + 1) * n]
+    res = torch.zeros(m.num_nodes * 2, dtype=torch.float64, device=cuda)
+    mat = torch.zeros(d.nnzb * 4, dtype=torch.float64, device=cuda)
+    fem.run_jacobian_kernel(m.order, torch.from_numpy(ptr_g).to(cuda), torch.from_numpy(conn_g).to(cuda),
+                            m.num_elements, d.states, d.coords, m.E, m.nu, m.t, d.map, res, mat)
+    assert _rel(res.cpu().numpy(), R0) <= FP64_TOL
+    assert _rel(mat.cpu().numpy(), A0) <= FP64_TOL

@@ -127,3 +127,23 @@ def test_concurrent_clients(fem, cuda):
         srv.submit(ids[0], st)
     srv.wait(tk)
     srv.close()
+
+
+def test_bad_requests_and_abandoned_clients(fem, cuda):
+    """A request for an unknown mesh is refused; a client that submits and never
+    waits does not hold back the others."""
+    import torch
+    meshes = _meshes(fem)[:4]
+    srv = fem.Server(4 << 30, max_batch=8)
+    ids = [srv.add_mesh(m) for m in meshes]
+    st = [torch.from_numpy(np.ascontiguousarray(m.states)).pin_memory() for m in meshes]
+    with pytest.raises(fem.FemError) as ei:
+        srv.submit(99, st[0])
+    assert ei.value.status == fem.FEM_ERR_INVALID_ARGUMENT
+    srv.submit(ids[0], st[0])  # abandoned: never waited for
+    for _ in range(3):
+        for i in (1, 2, 3):
+            srv.wait(srv.submit(ids[i], st[i]), timeout_ms=20000)
+    with pytest.raises(fem.FemError):
+        srv.wait(123456789, timeout_ms=10)
+    srv.close()
