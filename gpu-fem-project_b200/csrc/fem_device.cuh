@@ -154,11 +154,11 @@ template <int P>
 struct Shape;
 template <>
 struct Shape<1> {
-  static constexpr int GT = 64, EPG = 8, GPC = 4, NPART = 2, MINB = 4;
+  static constexpr int GT = 64, EPG = 8, GPC = 4, NPART = 2, MINB = 3;
 };
 template <>
 struct Shape<2> {
-  static constexpr int GT = 64, EPG = 2, GPC = 4, NPART = 2, MINB = 4;
+  static constexpr int GT = 64, EPG = 2, GPC = 4, NPART = 2, MINB = 3;
 };
 template <>
 struct Shape<3> {
@@ -207,7 +207,9 @@ struct Layout {
   using D = Dims<P>;
   static constexpr bool TC = sizeof(T) == 8;
   static constexpr int NN = D::NN, NQ = NN, NNP = NN + 1, EPG = S::EPG;
+  // FP64: one scaled-gradient array per element (G-hat, below); FP32: G and H
   static constexpr size_t GH_ELEM = TC ? 8 * D::NQP * D::RS : 2 * sizeof(T) * NQ * NNP;  // bytes per element
+  static constexpr size_t H_ELEM = TC ? 0 : GH_ELEM;
   static constexpr size_t tabT = 0;                     // double2 [NN][NQ]
   static constexpr size_t wq = tabT + 16 * NQ * NN;     // double  [NQ]
   static constexpr size_t groups = align16(wq + 8 * NQ);
@@ -216,8 +218,9 @@ struct Layout {
   static constexpr size_t U = X + 16 * EPG * NN;               // double2 [EPG][NN]
   static constexpr size_t S3 = U + 16 * EPG * NN;              // double  [3][EPG*NQ]  weak stress (SoA)
   static constexpr size_t G = align16(S3 + 24 * EPG * NQ);     // [EPG] x GH_ELEM
-  static constexpr size_t H = align16(G + EPG * GH_ELEM);      // [EPG] x GH_ELEM
-  static constexpr size_t nid = align16(H + EPG * GH_ELEM);    // int [EPG][NN]
+  static constexpr size_t H = align16(G + EPG * GH_ELEM);      // [EPG] x H_ELEM
+  static constexpr size_t SG = align16(H + EPG * H_ELEM);      // double [EPG][NQP]: sign of w detJ t (FP64)
+  static constexpr size_t nid = align16(SG + (TC ? 8 * EPG * D::NQP : 0));  // int [EPG][NN]
   static constexpr size_t rbase = align16(nid + 4 * EPG * NN);  // int [EPG][NN]
   // staged code records (plan) or element map rows (drop-in Jacobian), double-buffered
   static constexpr size_t STAGE = (MODE & kPlan) ? size_t(EPG) * D::CS
@@ -272,8 +275,11 @@ __device__ __forceinline__ void write_block(const Out &A, int el, int a, int b, 
 // then the 2x2 stiffness blocks.  Lane l holds C[8ti + l/4][8tj + 2(l%4) + {0,1}]
 // = (M_i0, M_i1)[a][b] with a = (8ti + l/4)/2, i = (l/4)%2, b = 4tj + l%4; the
 // lane with the other i (l ^ 4) supplies the second row of the block.
+// M = H^T G with H = s G (s = w detJ t per quadrature point) is formed from the
+// one array G-hat = sqrt|s| G: A fragments are G-hat rows times sign(s), B
+// fragments G-hat rows, so sum_q A B = sum_q s G G.
 template <int P, int MODE, int R0, int R1>
-__device__ __forceinline__ void stiffness_mma(const Out &A, const double *Gm, const double *Hm, int el, double mu,
+__device__ __forceinline__ void stiffness_mma(const Out &A, const double *Gm, const double *SGm, int el, double mu,
                                               double lam, int lane) {
   using D = Dims<P>;
   constexpr int NT8 = D::NT8, KS = D::KS, RS = D::RS, NN = D::NN;
@@ -287,9 +293,10 @@ __device__ __forceinline__ void stiffness_mma(const Out &A, const double *Gm, co
 #pragma unroll
   for (int ks = 0; ks < KS; ks++) {
     const int q = 4 * ks + t;
+    const double sg = SGm[q];
     double af[NR], bf[NT8];
 #pragma unroll
-    for (int r = 0; r < NR; r++) af[r] = Hm[q * RS + 8 * (R0 + r) + g];
+    for (int r = 0; r < NR; r++) af[r] = sg * Gm[q * RS + 8 * (R0 + r) + g];
 #pragma unroll
     for (int c = 0; c < NT8; c++)
       if (c >= R0) bf[c] = Gm[q * RS + 8 * c + g];
@@ -427,7 +434,11 @@ __device__ __forceinline__ void cta_prologue(unsigned char *smem) {
       const int g = i / (EPG * PAD), r = i - g * EPG * PAD, el = r / PAD, o = r - el * PAD;
       unsigned char *gs = smem + L::groups + g * L::group_bytes;
       reinterpret_cast<double *>(gs + L::G)[el * NQP * RS + NQ * RS + o] = 0.0;
-      reinterpret_cast<double *>(gs + L::H)[el * NQP * RS + NQ * RS + o] = 0.0;
+    }
+    for (int i = threadIdx.x; i < S::GPC * EPG * (NQP - NQ); i += blockDim.x) {
+      const int g = i / (EPG * (NQP - NQ)), r = i - g * EPG * (NQP - NQ), el = r / (NQP - NQ), o = r - el * (NQP - NQ);
+      unsigned char *gs = smem + L::groups + g * L::group_bytes;
+      reinterpret_cast<double *>(gs + L::SG)[el * NQP + NQ + o] = 0.0;
     }
   }
   __syncthreads();
@@ -534,17 +545,23 @@ __device__ __forceinline__ void group_loop(unsigned char *smem, Src &src, const 
     stage_codes(nxt, buf ^ 1);
 
     // 1. quadrature points: NPART lanes per (element, q) split the node sums,
-    //    every lane of the quad then forms J^-1 and the gradients of its nodes.
+    //    every lane of the quad then forms J^-1 and the gradients of its nodes
+    //    (their table entries stay in registers between the two loops).
+    constexpr int MAXJ = (NN + NPART - 1) / NPART;
     for (int base = 0; base < EPG * NQ * NPART; base += GT) {
       const int i = base + tg;
       const int iq = i / NPART, part = i - iq * NPART;
       const int el = iq / NQ, q = iq - el * NQ;
       const bool act = i < EPG * NQ * NPART && el < ne;
       double j00 = 0, j01 = 0, j10 = 0, j11 = 0, g00 = 0, g01 = 0, g10 = 0, g11 = 0;
-      if (act) {
-#pragma unroll 2
-        for (int a = part; a < NN; a += NPART) {
+      double2 dt[MAXJ];
+#pragma unroll
+      for (int j = 0; j < MAXJ; j++) {
+        const int a = part + j * NPART;
+        dt[j] = make_double2(0.0, 0.0);
+        if (act && a < NN) {
           const double2 d = tabT[a * NQ + q];
+          dt[j] = d;
           const double2 x = X[el * NN + a], u = U[el * NN + a];
           j00 = fma(x.x, d.x, j00);
           j01 = fma(x.x, d.y, j01);
@@ -572,26 +589,29 @@ __device__ __forceinline__ void group_loop(unsigned char *smem, Src &src, const 
         const double inv = 1.0 / det;
         const double i00 = j11 * inv, i01 = -j01 * inv, i10 = -j10 * inv, i11 = j00 * inv;
         const double st = wq[q] * det * thick;
+        // FP64: gradients scaled by sqrt|st| (G-hat), the weak stress by st/sqrt|st|
+        const double rs = TC ? sqrt(fabs(st)) : 1.0;
+        const double sg = st < 0.0 ? -1.0 : 1.0;
+        const double sw = TC ? sg * rs : st;
         if (part == 0) {
           const double uxx = g00 * i00 + g01 * i10, uxy = g00 * i01 + g01 * i11;
           const double uyx = g10 * i00 + g11 * i10, uyy = g10 * i01 + g11 * i11;
           const double tr = uxx + uyy;
-          S3[0 * SQ + iq] = st * (2.0 * mu * uxx + lam * tr);
-          S3[1 * SQ + iq] = st * (mu * (uxy + uyx));
-          S3[2 * SQ + iq] = st * (2.0 * mu * uyy + lam * tr);
+          S3[0 * SQ + iq] = sw * (2.0 * mu * uxx + lam * tr);
+          S3[1 * SQ + iq] = sw * (mu * (uxy + uyx));
+          S3[2 * SQ + iq] = sw * (2.0 * mu * uyy + lam * tr);
+          if constexpr (TC) reinterpret_cast<double *>(gs + L::SG)[el * NQP + q] = sg;
         }
-#pragma unroll 2
-        for (int a = part; a < NN; a += NPART) {
-          const double2 d = tabT[a * NQ + q];
+#pragma unroll
+        for (int j = 0; j < MAXJ; j++) {
+          const int a = part + j * NPART;
+          if (a >= NN) continue;
+          const double2 d = dt[j];
           const double gx = d.x * i00 + d.y * i10;
           const double gy = d.x * i01 + d.y * i11;
           if constexpr (TC) {
             double *Gm = reinterpret_cast<double *>(gs + L::G) + (el * NQP + q) * RS;
-            *reinterpret_cast<double2 *>(Gm + 2 * a) = make_double2(gx, gy);
-            if constexpr ((MODE & kJac) != 0) {
-              double *Hm = reinterpret_cast<double *>(gs + L::H) + (el * NQP + q) * RS;
-              *reinterpret_cast<double2 *>(Hm + 2 * a) = make_double2(st * gx, st * gy);
-            }
+            *reinterpret_cast<double2 *>(Gm + 2 * a) = make_double2(rs * gx, rs * gy);
           } else {
             T2 gv;
             gv.x = T(gx);
@@ -668,7 +688,7 @@ __device__ __forceinline__ void group_loop(unsigned char *smem, Src &src, const 
         for (int w = warp; w < ne * WPE; w += NW) {
           const int el = w / WPE, part = w - el * WPE;
           const double *Gm = reinterpret_cast<const double *>(gs + L::G) + el * NQP * RS;
-          const double *Hm = reinterpret_cast<const double *>(gs + L::H) + el * NQP * RS;
+          const double *Hm = reinterpret_cast<const double *>(gs + L::SG) + el * NQP;
           if constexpr (WPE == 1) {
             stiffness_mma<P, MODE, 0, D::NT8>(A, Gm, Hm, el, mu, lam, lane);
           } else {
