@@ -162,7 +162,7 @@ struct Shape<2> {
 };
 template <>
 struct Shape<3> {
-  static constexpr int GT = 64, EPG = 2, GPC = 2, NPART = 2, MINB = 4;
+  static constexpr int GT = 64, EPG = 2, GPC = 2, NPART = 2, MINB = 5;
 };
 template <>
 struct Shape<4> {
@@ -174,6 +174,10 @@ struct Shape<4> {
 template <int P>
 struct RowSplit {
   static constexpr int WPE = 1;
+};
+template <>
+struct RowSplit<3> {
+  static constexpr int WPE = 2;
 };
 template <>
 struct RowSplit<4> {
@@ -692,15 +696,23 @@ __device__ __forceinline__ void group_loop(unsigned char *smem, Src &src, const 
           if constexpr (WPE == 1) {
             stiffness_mma<P, MODE, 0, D::NT8>(A, Gm, Hm, el, mu, lam, lane);
           } else {
-            static_assert(P != 4 || D::NT8 == 7, "row split of the 7x7 tile grid");
-            if (part == 0)
-              stiffness_mma<P, MODE, 0, 1>(A, Gm, Hm, el, mu, lam, lane);
-            else if (part == 1)
-              stiffness_mma<P, MODE, 1, 2>(A, Gm, Hm, el, mu, lam, lane);
-            else if (part == 2)
-              stiffness_mma<P, MODE, 2, 4>(A, Gm, Hm, el, mu, lam, lane);
-            else
-              stiffness_mma<P, MODE, 4, D::NT8>(A, Gm, Hm, el, mu, lam, lane);
+            if constexpr (WPE == 2) {
+              // p = 3: tile row 0 (4 tiles) | rows 1..3 (3 + 2 + 1 tiles)
+              if (part == 0)
+                stiffness_mma<P, MODE, 0, 1>(A, Gm, Hm, el, mu, lam, lane);
+              else
+                stiffness_mma<P, MODE, 1, D::NT8>(A, Gm, Hm, el, mu, lam, lane);
+            } else {
+              static_assert(P != 4 || D::NT8 == 7, "row split of the 7x7 tile grid");
+              if (part == 0)
+                stiffness_mma<P, MODE, 0, 1>(A, Gm, Hm, el, mu, lam, lane);
+              else if (part == 1)
+                stiffness_mma<P, MODE, 1, 2>(A, Gm, Hm, el, mu, lam, lane);
+              else if (part == 2)
+                stiffness_mma<P, MODE, 2, 4>(A, Gm, Hm, el, mu, lam, lane);
+              else
+                stiffness_mma<P, MODE, 4, D::NT8>(A, Gm, Hm, el, mu, lam, lane);
+            }
           }
         }
       } else {
