@@ -25,7 +25,11 @@
 // computes for GreenStrainType::LINEAR: weakRes = w*detJ*t*sigma, with
 // sigma = 2*mu*eps + lambda*tr(eps)*I, mu = E/(2(1+nu)), lambda = 2*mu*nu/(1-nu),
 // and the forward-mode Jacobian column is the same linear map applied to the
-// seeded state gradient.
+// seeded state gradient.  For GreenStrainType::NONLINEAR (a template option of
+// the reference kernels, FEKernels.h:286,317,379,589,786, that its dispatch
+// never selects) E = 1/2 (g + g^T + g^T g), S = 2 mu E + lambda tr(E) I,
+// weakRes = w*detJ*t*(I + g) S, and the Jacobian column is its forward
+// derivative along the seed, written out by hand (weakResDot).
 //
 // Pinning: the quadrature and shape-function tables are checked against the
 // reference's own headers compiled from their source (oracle/_ref, recipe in
@@ -122,32 +126,106 @@ inline void lagrange2dDeriv(int p, const double xi[2], int ax, int ay, double d[
   d[1] = Nx * dNy;
 }
 
+// strain: 0 = GreenStrainType::LINEAR (the reference's default), 1 = NONLINEAR.
 struct Material {
   double mu, lambda, t;
+  int strain;
 };
 
-inline Material makeMaterial(double E, double nu, double t) {
+inline Material makeMaterial(double E, double nu, double t, int strain = 0) {
   // element/FEKernels.h:300-301
   Material m;
   m.mu = 0.5 * E / (1.0 + nu);
   m.lambda = 2 * m.mu * nu / (1.0 - nu);
   m.t = t;
+  m.strain = strain;
   return m;
 }
 
-// planeStressWeakRes<LINEAR> closed form (element/FEKernels.h:286-315):
-// out = scale * t * sigma(sym(g)).  Linear in g, so it also gives the forward seed.
+// Green strain E = 1/2 (g + g^T + g^T g) (A2D MatGreenStrain<NONLINEAR>), stored
+// [E00, E01, E11]; g[i*2+j] = du_i/dx_j.
+inline void greenStrain(const double g[4], double e[3]) {
+  e[0] = 0.5 * (2 * g[0] + g[0] * g[0] + g[2] * g[2]);
+  e[1] = 0.5 * (g[1] + g[2] + g[0] * g[1] + g[2] * g[3]);
+  e[2] = 0.5 * (2 * g[3] + g[1] * g[1] + g[3] * g[3]);
+}
+
+// Forward derivative of the Green strain along the seed gd.
+inline void greenStrainDot(const double g[4], const double gd[4], double e[3]) {
+  e[0] = 0.5 * (2 * gd[0] + 2 * (gd[0] * g[0] + gd[2] * g[2]));
+  e[1] = 0.5 * (gd[1] + gd[2] + gd[0] * g[1] + g[0] * gd[1] + gd[2] * g[3] + g[2] * gd[3]);
+  e[2] = 0.5 * (2 * gd[3] + 2 * (gd[1] * g[1] + gd[3] * g[3]));
+}
+
+// SymIsotropic: S = 2 mu E + lambda tr(E) I, [S00, S01, S11].
+inline void isotropic(const Material &m, const double e[3], double s[3]) {
+  const double tr = e[0] + e[2];
+  s[0] = 2 * m.mu * e[0] + m.lambda * tr;
+  s[1] = 2 * m.mu * e[1];
+  s[2] = 2 * m.mu * e[2] + m.lambda * tr;
+}
+
+// planeStressWeakRes<strainType> closed form (element/FEKernels.h:286-315): the
+// gradient of W = 1/2 scale t S:E with respect to g.
+//   LINEAR:    E = sym(g), out = scale * t * sigma (symmetric).
+//   NONLINEAR: E = 1/2 (g + g^T + g^T g), out = scale * t * (I + g) S.
 inline void weakRes(const Material &m, double scale, const double g[4], double out[4]) {
-  const double e00 = g[0], e11 = g[3], e01 = 0.5 * (g[1] + g[2]);
-  const double tr = e00 + e11;
   const double f = scale * m.t;
-  const double s00 = 2 * m.mu * e00 + m.lambda * tr;
-  const double s11 = 2 * m.mu * e11 + m.lambda * tr;
-  const double s01 = 2 * m.mu * e01;
-  out[0] = f * s00;
-  out[1] = f * s01;
-  out[2] = f * s01;
-  out[3] = f * s11;
+  if (m.strain == 0) {
+    const double e00 = g[0], e11 = g[3], e01 = 0.5 * (g[1] + g[2]);
+    const double tr = e00 + e11;
+    const double s00 = 2 * m.mu * e00 + m.lambda * tr;
+    const double s11 = 2 * m.mu * e11 + m.lambda * tr;
+    const double s01 = 2 * m.mu * e01;
+    out[0] = f * s00;
+    out[1] = f * s01;
+    out[2] = f * s01;
+    out[3] = f * s11;
+    return;
+  }
+  double e[3], S[3];
+  greenStrain(g, e);
+  isotropic(m, e, S);
+  const double F00 = 1 + g[0], F01 = g[1], F10 = g[2], F11 = 1 + g[3];
+  out[0] = f * (F00 * S[0] + F01 * S[1]);
+  out[1] = f * (F00 * S[1] + F01 * S[2]);
+  out[2] = f * (F10 * S[0] + F11 * S[1]);
+  out[3] = f * (F10 * S[1] + F11 * S[2]);
+}
+
+// Forward-mode derivative of weakRes at g along the seed gd (the ADScalar<double,1>
+// pass of element/FEKernels.h:444-472,926-940).  LINEAR: weakRes(gd).
+//   NONLINEAR: scale * t * (gd S + (I + g) S'), S' = S(E'(g; gd)).
+inline void weakResDot(const Material &m, double scale, const double g[4], const double gd[4], double out[4]) {
+  if (m.strain == 0) {
+    weakRes(m, scale, gd, out);
+    return;
+  }
+  const double f = scale * m.t;
+  double e[3], S[3], ed[3], Sd[3];
+  greenStrain(g, e);
+  isotropic(m, e, S);
+  greenStrainDot(g, gd, ed);
+  isotropic(m, ed, Sd);
+  const double F00 = 1 + g[0], F01 = g[1], F10 = g[2], F11 = 1 + g[3];
+  out[0] = f * (gd[0] * S[0] + gd[1] * S[1] + F00 * Sd[0] + F01 * Sd[1]);
+  out[1] = f * (gd[0] * S[1] + gd[1] * S[2] + F00 * Sd[1] + F01 * Sd[2]);
+  out[2] = f * (gd[2] * S[0] + gd[3] * S[1] + F10 * Sd[0] + F11 * Sd[1]);
+  out[3] = f * (gd[2] * S[1] + gd[3] * S[2] + F10 * Sd[1] + F11 * Sd[2]);
+}
+
+// Strain energy density times scale * t: 1/2 scale t S:E (SymMatMultTrace).
+inline double energy(const Material &m, double scale, const double g[4]) {
+  double e[3], S[3];
+  if (m.strain == 0) {
+    e[0] = g[0];
+    e[1] = 0.5 * (g[1] + g[2]);
+    e[2] = g[3];
+  } else {
+    greenStrain(g, e);
+  }
+  isotropic(m, e, S);
+  return 0.5 * scale * m.t * (S[0] * e[0] + 2 * S[1] * e[1] + S[2] * e[2]);
 }
 
 struct QuadPoint {
@@ -257,7 +335,7 @@ void elementKernel(int p, const double *X, const double *U, const Material &m, d
             seed[k * 2 + 0] = gd0;
             seed[k * 2 + 1] = gd1;
             double Wd[4];
-            weakRes(m, Q.scale, seed, Wd);
+            weakResDot(m, Q.scale, g, seed, Wd);
             std::fill(col.begin(), col.end(), 0.0);
             transformAdd(p, Q, Wd, col.data());
             const int c = b * 2 + k;
@@ -322,9 +400,33 @@ int oracle_lagrange1d(int p, int npts, const double *x, double *N, double *dN) {
 }
 
 // One element: Re[2n] and Ke[2n*2n] (row-major, DOF = node*2 + state).
+// strain: 0 = LINEAR, 1 = NONLINEAR Green strain.
+int oracle_element_ex(int p, const double *X, const double *U, double E, double nu, double t, int strain, double *Re,
+                      double *Ke) {
+  if (p < 1 || p > 4 || strain < 0 || strain > 1) return 1;
+  elementKernel(p, X, U, makeMaterial(E, nu, t, strain), Re, Ke);
+  return 0;
+}
+
 int oracle_element(int p, const double *X, const double *U, double E, double nu, double t, double *Re, double *Ke) {
-  if (p < 1 || p > 4) return 1;
-  elementKernel(p, X, U, makeMaterial(E, nu, t), Re, Ke);
+  return oracle_element_ex(p, X, U, E, nu, t, 0, Re, Ke);
+}
+
+// Element strain energy sum_q 1/2 w detJ t S:E (the quantity the reference's
+// weak residual differentiates), for finite-difference checks of the residual.
+int oracle_element_energy(int p, const double *X, const double *U, double E, double nu, double t, int strain,
+                          double *W) {
+  if (p < 1 || p > 4 || strain < 0 || strain > 1) return 1;
+  const Material m = makeMaterial(E, nu, t, strain);
+  double sum = 0;
+  for (int qx = 0; qx <= p; qx++)
+    for (int qy = 0; qy <= p; qy++) {
+      const QuadPoint Q = quadPoint(p, qx, qy, X);
+      double g[4];
+      realGradient(p, Q, U, g);
+      sum += energy(m, Q.scale, g);
+    }
+  *W = sum;
   return 0;
 }
 
@@ -332,12 +434,12 @@ int oracle_element(int p, const double *X, const double *U, double E, double nu,
 // with the runJacobianKernel contract (FEKernels.h:1125-1136): accumulate into
 // residual (nullable) and matEntries (nullable); map[e*n*n + a*n + b] is the
 // offset (in doubles) of the 2x2 block coupling local nodes a and b.
-int oracle_assemble(int p, const int *connPtr, const int *conn, int64_t numElements, const double *states,
-                    const double *coords, double E, double nu, double t, const int *map, double *residual,
-                    double *matEntries) {
-  if (p < 1 || p > 4) return 1;
+int oracle_assemble_ex(int p, const int *connPtr, const int *conn, int64_t numElements, const double *states,
+                       const double *coords, double E, double nu, double t, int strain, const int *map,
+                       double *residual, double *matEntries) {
+  if (p < 1 || p > 4 || strain < 0 || strain > 1) return 1;
   const int n = (p + 1) * (p + 1), nd = 2 * n;
-  const Material m = makeMaterial(E, nu, t);
+  const Material m = makeMaterial(E, nu, t, strain);
   const bool jac = (matEntries != nullptr && map != nullptr);
   const int64_t chunk = 4096;
   std::vector<double> reBuf((size_t)chunk * nd);
@@ -372,6 +474,12 @@ int oracle_assemble(int p, const int *connPtr, const int *conn, int64_t numEleme
     }
   }
   return 0;
+}
+
+int oracle_assemble(int p, const int *connPtr, const int *conn, int64_t numElements, const double *states,
+                    const double *coords, double E, double nu, double t, const int *map, double *residual,
+                    double *matEntries) {
+  return oracle_assemble_ex(p, connPtr, conn, numElements, states, coords, E, nu, t, 0, map, residual, matEntries);
 }
 
 // Throughput variant used as the timed CPU baseline: OpenMP over elements with

@@ -32,7 +32,10 @@ def _load():
     lib.oracle_tables.argtypes = [i, p, p, p]
     lib.oracle_lagrange1d.argtypes = [i, i, p, p, p]
     lib.oracle_element.argtypes = [i, p, p, d, d, d, p, p]
+    lib.oracle_element_ex.argtypes = [i, p, p, d, d, d, i, p, p]
+    lib.oracle_element_energy.argtypes = [i, p, p, d, d, d, i, p]
     lib.oracle_assemble.argtypes = [i, p, p, i64, p, p, d, d, d, p, p, p]
+    lib.oracle_assemble_ex.argtypes = [i, p, p, i64, p, p, d, d, d, i, p, p, p]
     lib.oracle_assemble_parallel.argtypes = [i, p, p, i64, p, p, d, d, d, p, p, p]
     lib.oracle_bsr_pattern.argtypes = [i, p, p, i64, p, p]
     lib.oracle_bsr_pattern.restype = i64
@@ -87,13 +90,24 @@ def lagrange1d(p: int, x):
     return N, dN
 
 
-def element(p: int, X, U, E: float, nu: float, t: float):
+STRAIN = {"linear": 0, "nonlinear": 1}
+
+
+def element(p: int, X, U, E: float, nu: float, t: float, strain: str = "linear"):
     """Element residual [2n] and stiffness [2n, 2n] for node coords X [n,2], states U [n,2]."""
     n = (p + 1) ** 2
     X, U = _c(X, np.float64), _c(U, np.float64)
     Re, Ke = np.zeros(2 * n), np.zeros((2 * n, 2 * n))
-    assert lib().oracle_element(p, _ptr(X), _ptr(U), E, nu, t, _ptr(Re), _ptr(Ke)) == 0
+    assert lib().oracle_element_ex(p, _ptr(X), _ptr(U), E, nu, t, STRAIN[strain], _ptr(Re), _ptr(Ke)) == 0
     return Re, Ke
+
+
+def element_energy(p: int, X, U, E: float, nu: float, t: float, strain: str = "linear") -> float:
+    """Element strain energy sum_q 1/2 w detJ t S:E."""
+    X, U = _c(X, np.float64), _c(U, np.float64)
+    W = np.zeros(1)
+    assert lib().oracle_element_energy(p, _ptr(X), _ptr(U), E, nu, t, STRAIN[strain], _ptr(W)) == 0
+    return float(W[0])
 
 
 def bsr_pattern(num_nodes: int, conn_ptr, conn):
@@ -124,10 +138,11 @@ def check_colouring(num_nodes: int, conn_ptr, conn, colour, num_colours: int) ->
 
 
 def assemble(mesh, bsr_map=None, nnzb: int | None = None, residual: bool = True, jacobian: bool = True,
-             parallel: bool = False, num_elements: int | None = None):
+             parallel: bool = False, num_elements: int | None = None, strain: str = "linear"):
     """Residual [numNodes*2] and BSR values [nnzb*4] (zero-initialised, then
     accumulated as runJacobianKernel does).  parallel=True uses the OpenMP
-    atomic-scatter variant (timed CPU baseline; summation order not fixed)."""
+    atomic-scatter variant (timed CPU baseline; summation order not fixed;
+    linear strain only)."""
     ne = mesh.num_elements if num_elements is None else num_elements
     cp, cn = _c(mesh.conn_ptr, np.int32), _c(mesh.conn, np.int32)
     st, xy = _c(mesh.states, np.float64), _c(mesh.coords, np.float64)
@@ -137,9 +152,13 @@ def assemble(mesh, bsr_map=None, nnzb: int | None = None, residual: bool = True,
     if jacobian:
         mp = _c(bsr_map, np.int32)
         mat = np.zeros(int(nnzb) * 4)
-    fn = lib().oracle_assemble_parallel if parallel else lib().oracle_assemble
-    rc = fn(mesh.order, _ptr(cp), _ptr(cn), ne, _ptr(st), _ptr(xy), mesh.E, mesh.nu, mesh.t, _ptr(mp), _ptr(res),
-            _ptr(mat))
+    if parallel:
+        assert strain == "linear"
+        rc = lib().oracle_assemble_parallel(mesh.order, _ptr(cp), _ptr(cn), ne, _ptr(st), _ptr(xy), mesh.E, mesh.nu,
+                                            mesh.t, _ptr(mp), _ptr(res), _ptr(mat))
+    else:
+        rc = lib().oracle_assemble_ex(mesh.order, _ptr(cp), _ptr(cn), ne, _ptr(st), _ptr(xy), mesh.E, mesh.nu, mesh.t,
+                                      STRAIN[strain], _ptr(mp), _ptr(res), _ptr(mat))
     assert rc == 0
     return res, mat
 
