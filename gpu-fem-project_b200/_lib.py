@@ -25,6 +25,9 @@ FEM_ERR_BUDGET = 8
 FEM_PRECISION_FP64 = 0
 FEM_PRECISION_MIXED = 1
 
+FEM_STRAIN_LINEAR = 0
+FEM_STRAIN_NONLINEAR = 1
+
 _i = C.c_int
 _i64 = C.c_int64
 _d = C.c_double
@@ -42,6 +45,8 @@ SIGNATURES = {
     "fem_run_jacobian": (_i, [_i, _p, _p, _i, _p, _p, _d, _d, _d, _p, _p, _p, _p, _pd]),
     "fem_run_residual_mixed": (_i, [_i, _p, _p, _i, _p, _p, _d, _d, _d, _p, _p, _pd]),
     "fem_run_jacobian_mixed": (_i, [_i, _p, _p, _i, _p, _p, _d, _d, _d, _p, _p, _p, _p, _pd]),
+    "fem_run_residual_ex": (_i, [_i, _p, _p, _i, _p, _p, _d, _d, _d, _p, _i, _i, _p, _pd]),
+    "fem_run_jacobian_ex": (_i, [_i, _p, _p, _i, _p, _p, _d, _d, _d, _p, _p, _p, _i, _i, _p, _pd]),
     "fem_build_bsr_pattern": (_i, [_i, _p, _p, _i, _p, _p, _pi64]),
     "fem_build_element_bsr_map": (_i, [_p, _p, _i, _i, _p, _p, _p]),
     "fem_colour_elements": (_i, [_i, _p, _p, _i, _p, _pi]),
@@ -52,6 +57,7 @@ SIGNATURES = {
     "fem_plan_get_pattern": (_i, [_p, _p, _p]),
     "fem_plan_device_pattern": (_i, [_p, C.POINTER(_p), C.POINTER(_p)]),
     "fem_plan_assemble": (_i, [_p, _p, _p, _d, _d, _d, _p, _p, _i, _p, _pd]),
+    "fem_plan_assemble_ex": (_i, [_p, _p, _p, _d, _d, _d, _p, _p, _i, _i, _p, _pd]),
     "fem_probe_peak": (_i, [_i, _pd]),
     "fem_server_create": (_i, [_i64, _i, _i, C.POINTER(_p)]),
     "fem_server_destroy": (_i, [_p]),

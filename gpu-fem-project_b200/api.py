@@ -12,15 +12,23 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import FEM_PRECISION_FP64, FEM_PRECISION_MIXED, check, lib
+from ._lib import FEM_PRECISION_FP64, FEM_PRECISION_MIXED, FEM_STRAIN_LINEAR, FEM_STRAIN_NONLINEAR, check, lib
 
 _PRECISION = {"fp64": FEM_PRECISION_FP64, "mixed": FEM_PRECISION_MIXED}
+# A2D::GreenStrainType of the reference kernels' strainType template argument
+_STRAIN = {"linear": FEM_STRAIN_LINEAR, "nonlinear": FEM_STRAIN_NONLINEAR}
 
 
 def _prec(p) -> int:
     if isinstance(p, int):
         return p
     return _PRECISION[p]
+
+
+def _strain(s) -> int:
+    if isinstance(s, int):
+        return s
+    return _STRAIN[s]
 
 
 def _dptr(x, dtype=None, name="array"):
@@ -55,32 +63,41 @@ def _np(a, dt):
 
 
 def run_residual_kernel(element_order, conn_ptr, conn, num_elements, states, node_coords, E, nu, t, residual, *,
-                        precision="fp64", stream=None, timed=True):
-    """runResidualKernel: adds element residuals into `residual`; returns seconds (timed) or None."""
+                        precision="fp64", strain="linear", stream=None, timed=True):
+    """runResidualKernel: adds element residuals into `residual`; returns seconds (timed) or None.
+    strain="nonlinear" selects GreenStrainType::NONLINEAR (FP64 only)."""
     import torch
     el = C.c_double(0.0)
-    fn = lib.fem_run_residual if _prec(precision) == FEM_PRECISION_FP64 else lib.fem_run_residual_mixed
-    st = fn(int(element_order), _dptr(conn_ptr, torch.int32, "connPtr"), _dptr(conn, torch.int32, "conn"),
+    args = (int(element_order), _dptr(conn_ptr, torch.int32, "connPtr"), _dptr(conn, torch.int32, "conn"),
             int(num_elements), _dptr(states, torch.float64, "states"), _dptr(node_coords, torch.float64, "nodeCoords"),
-            float(E), float(nu), float(t), _dptr(residual, torch.float64, "residual"), _stream(stream),
-            C.byref(el) if timed else None)
-    check(st, "fem_run_residual")
+            float(E), float(nu), float(t), _dptr(residual, torch.float64, "residual"))
+    tail = (_stream(stream), C.byref(el) if timed else None)
+    if _strain(strain) != FEM_STRAIN_LINEAR:
+        check(lib.fem_run_residual_ex(*args, _prec(precision), _strain(strain), *tail), "fem_run_residual_ex")
+    else:
+        fn = lib.fem_run_residual if _prec(precision) == FEM_PRECISION_FP64 else lib.fem_run_residual_mixed
+        check(fn(*args, *tail), "fem_run_residual")
     return el.value if timed else None
 
 
 def run_jacobian_kernel(element_order, conn_ptr, conn, num_elements, states, node_coords, E, nu, t,
-                        element_bcsr_map, residual, mat_entries, *, precision="fp64", stream=None, timed=True):
+                        element_bcsr_map, residual, mat_entries, *, precision="fp64", strain="linear", stream=None,
+                        timed=True):
     """runJacobianKernel: adds element matrices (and residuals when `residual` is
-    not None) into the caller-zeroed outputs; returns seconds (timed) or None."""
+    not None) into the caller-zeroed outputs; returns seconds (timed) or None.
+    strain="nonlinear" selects GreenStrainType::NONLINEAR (FP64 only)."""
     import torch
     el = C.c_double(0.0)
-    fn = lib.fem_run_jacobian if _prec(precision) == FEM_PRECISION_FP64 else lib.fem_run_jacobian_mixed
-    st = fn(int(element_order), _dptr(conn_ptr, torch.int32, "connPtr"), _dptr(conn, torch.int32, "conn"),
+    args = (int(element_order), _dptr(conn_ptr, torch.int32, "connPtr"), _dptr(conn, torch.int32, "conn"),
             int(num_elements), _dptr(states, torch.float64, "states"), _dptr(node_coords, torch.float64, "nodeCoords"),
             float(E), float(nu), float(t), _dptr(element_bcsr_map, torch.int32, "elementBCSRMap"),
-            _dptr(residual, torch.float64, "residual"), _dptr(mat_entries, torch.float64, "matEntries"),
-            _stream(stream), C.byref(el) if timed else None)
-    check(st, "fem_run_jacobian")
+            _dptr(residual, torch.float64, "residual"), _dptr(mat_entries, torch.float64, "matEntries"))
+    tail = (_stream(stream), C.byref(el) if timed else None)
+    if _strain(strain) != FEM_STRAIN_LINEAR:
+        check(lib.fem_run_jacobian_ex(*args, _prec(precision), _strain(strain), *tail), "fem_run_jacobian_ex")
+    else:
+        fn = lib.fem_run_jacobian if _prec(precision) == FEM_PRECISION_FP64 else lib.fem_run_jacobian_mixed
+        check(fn(*args, *tail), "fem_run_jacobian")
     return el.value if timed else None
 
 
@@ -162,14 +179,15 @@ class Plan:
         return r.value, c.value
 
     def assemble(self, states, node_coords, E, nu, t, residual=None, mat_entries=None, *, precision="fp64",
-                 stream=None, timed=False):
+                 strain="linear", stream=None, timed=False):
         import torch
         el = C.c_double(0.0)
-        check(lib.fem_plan_assemble(self._h, _dptr(states, torch.float64, "states"),
-                                    _dptr(node_coords, torch.float64, "nodeCoords"), float(E), float(nu), float(t),
-                                    _dptr(residual, torch.float64, "residual"),
-                                    _dptr(mat_entries, torch.float64, "matEntries"), _prec(precision),
-                                    _stream(stream), C.byref(el) if timed else None), "fem_plan_assemble")
+        check(lib.fem_plan_assemble_ex(self._h, _dptr(states, torch.float64, "states"),
+                                       _dptr(node_coords, torch.float64, "nodeCoords"), float(E), float(nu), float(t),
+                                       _dptr(residual, torch.float64, "residual"),
+                                       _dptr(mat_entries, torch.float64, "matEntries"), _prec(precision),
+                                       _strain(strain), _stream(stream), C.byref(el) if timed else None),
+              "fem_plan_assemble_ex")
         return el.value if timed else None
 
     def close(self):

@@ -18,6 +18,54 @@
 #include "fem_device.cuh"
 #include "fem_launch.h"
 
+namespace fem {
+namespace {
+
+// One persistent batched launch of order P over the tile queue `tiles` (plan mode,
+// residual and Jacobian).
+template <int P, typename T>
+int launch_batched_p(const dev::AsmArgs *meshes, const dev::Tile *tiles, int ntiles, int *counter, cudaStream_t s) {
+  using S = dev::Shape<P>;
+  constexpr int NT = S::GT * S::GPC;
+  constexpr int MODE = dev::kPlan | dev::kRes | dev::kJac;
+  auto kernel = dev::assemble_batched_kernel<P, T, MODE>;
+  const size_t smem = dev::Layout<P, T, MODE>::total;
+  LaunchInfo li;
+  int st = launch_info(kernel, NT, smem, li);
+  if (st) return st;
+  const int64_t need = (ntiles + S::GPC - 1) / S::GPC;
+  const int64_t cap = (int64_t)li.grid_per_sm * li.num_sms;
+  const int grid = (int)(need < cap ? need : cap);
+  if (grid <= 0) return FEM_SUCCESS;
+  kernel<<<grid, NT, smem, s>>>(meshes, tiles, ntiles, counter);
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return cuda_fail(err, "assemble_batched_kernel launch");
+  return FEM_SUCCESS;
+}
+
+template <typename T>
+int launch_batched_t(int p, const dev::AsmArgs *meshes, const dev::Tile *tiles, int ntiles, int *counter,
+                     cudaStream_t s) {
+  switch (p) {
+    case 1: return launch_batched_p<1, T>(meshes, tiles, ntiles, counter, s);
+    case 2: return launch_batched_p<2, T>(meshes, tiles, ntiles, counter, s);
+    case 3: return launch_batched_p<3, T>(meshes, tiles, ntiles, counter, s);
+    case 4: return launch_batched_p<4, T>(meshes, tiles, ntiles, counter, s);
+    default: return fail(FEM_ERR_INVALID_ORDER, "order %d", p);
+  }
+}
+
+}  // namespace
+
+int launch_batched(int p, int precision, const dev::AsmArgs *meshes, const dev::Tile *tiles, int ntiles, int *counter,
+                   cudaStream_t s) {
+  if (precision == FEM_PRECISION_FP64) return launch_batched_t<double>(p, meshes, tiles, ntiles, counter, s);
+  if (precision == FEM_PRECISION_MIXED) return launch_batched_t<float>(p, meshes, tiles, ntiles, counter, s);
+  return fail(FEM_ERR_INVALID_ARGUMENT, "precision %d", precision);
+}
+
+}  // namespace fem
+
 namespace {
 
 constexpr int kMaxColours = 64;
@@ -137,9 +185,7 @@ int enqueue_order(fem_batch *b, int p, int precision, cudaStream_t s) {
     const int t0 = b->tileOff[p * (C + 1) + c], t1 = b->tileOff[p * (C + 1) + c + 1];
     if (t1 <= t0) continue;
     int *counter = b->d_counters + p * kMaxColours + c;
-    int st = precision == FEM_PRECISION_FP64
-                 ? fem::launch_batched<double>(p, b->d_args, b->d_tiles + t0, t1 - t0, counter, s)
-                 : fem::launch_batched<float>(p, b->d_args, b->d_tiles + t0, t1 - t0, counter, s);
+    int st = fem::launch_batched(p, precision, b->d_args, b->d_tiles + t0, t1 - t0, counter, s);
     if (st) return st;
   }
   return FEM_SUCCESS;

@@ -30,6 +30,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <type_traits>
 
 namespace fem {
 namespace dev {
@@ -104,7 +105,8 @@ struct Vec2<float> {
   using type = float2;
 };
 
-enum : int { kRes = 1, kJac = 2, kPlan = 4 };
+// kNL: GreenStrainType::NONLINEAR (Green strain, FP64 only); default LINEAR.
+enum : int { kRes = 1, kJac = 2, kPlan = 4, kNL = 8 };
 
 struct AsmArgs {
   const int *connPtr;      // drop-in: CSR offsets
@@ -184,6 +186,46 @@ struct RowSplit<4> {
   static constexpr int WPE = 4;
 };
 
+// Launch shape of the NONLINEAR kernels: four lanes per quadrature point in the
+// quadrature stage (their shared-memory stores then hit 16 distinct banks).
+template <int P>
+struct NLShape;
+template <>
+struct NLShape<1> {
+  static constexpr int GT = 64, EPG = 8, GPC = 2, NPART = 4, MINB = 3;
+};
+template <>
+struct NLShape<2> {
+  static constexpr int GT = 64, EPG = 2, GPC = 2, NPART = 4, MINB = 3;
+};
+template <>
+struct NLShape<3> {
+  static constexpr int GT = 64, EPG = 2, GPC = 2, NPART = 4, MINB = 3;
+};
+template <>
+struct NLShape<4> {
+  static constexpr int GT = 128, EPG = 1, GPC = 1, NPART = 4, MINB = 3;
+};
+template <int P, int MODE>
+using ShapeSel = typename std::conditional<(MODE & kNL) != 0, NLShape<P>, Shape<P>>::type;
+
+// NONLINEAR stiffness geometry.  With Phi the map from nodal DOFs to the state
+// gradient and A the tangent modulus d2W/dg2 (4x4, g = du/dx),
+//   K[(a,i),(b,k)] = sum_q s sum_{l,n} G_al A_{il,kn} G_bn,
+// a product over kappa = (l, q) of the gradient array GA[kappa][a] = G-hat_al
+// and GB[kappa][(2i+k)*NP + b] = sign(s) sum_n A_{il,kn} G-hat_bn (G-hat =
+// sqrt|s| G).  Nodes are padded to NP (multiple of 8, m8n8k4 tiles of NTN node
+// tiles), kappa to KN (multiple of 4).  Row strides RA, RB are 4 (mod 16) doubles:
+// the four kappa rows of a fragment load and the four quadrature points of a
+// quadrature-stage store cover 16 distinct banks.
+template <int P>
+struct NLDims {
+  static constexpr int NN = (P + 1) * (P + 1), NQ = NN;
+  static constexpr int NP = (NN + 7) / 8 * 8, NTN = NP / 8, NPAIR = NTN * (NTN + 1) / 2;
+  static constexpr int KN = (2 * NQ + 3) / 4 * 4, KSN = KN / 4;
+  static constexpr int RA = NP + 4, RB = 4 * NP + 4;
+};
+
 template <int P>
 struct Dims {
   static constexpr int P1 = P + 1, NN = P1 * P1, NQ = NN;
@@ -207,24 +249,32 @@ struct Dims {
 //   lets the quadrature stage store without bank conflicts.
 template <int P, typename T, int MODE>
 struct Layout {
-  using S = Shape<P>;
+  using S = ShapeSel<P, MODE>;
   using D = Dims<P>;
+  using ND = NLDims<P>;
   static constexpr bool TC = sizeof(T) == 8;
+  static constexpr bool NL = (MODE & kNL) != 0;
+  static_assert(!NL || TC, "NONLINEAR strain runs in FP64");
   static constexpr int NN = D::NN, NQ = NN, NNP = NN + 1, EPG = S::EPG;
-  // FP64: one scaled-gradient array per element (G-hat, below); FP32: G and H
-  static constexpr size_t GH_ELEM = TC ? 8 * D::NQP * D::RS : 2 * sizeof(T) * NQ * NNP;  // bytes per element
+  // FP64: one scaled-gradient array per element (G-hat, below); FP32: G and H;
+  // NONLINEAR: GA then GB
+  static constexpr size_t GA_ELEM = 8 * ND::KN * ND::RA;
+  static constexpr size_t GH_ELEM = NL   ? GA_ELEM + 8 * ND::KN * ND::RB
+                                    : TC ? 8 * D::NQP * D::RS
+                                         : 2 * sizeof(T) * NQ * NNP;  // bytes per element
   static constexpr size_t H_ELEM = TC ? 0 : GH_ELEM;
+  static constexpr int NSTRESS = NL ? 4 : 3;  // weak stress components (first Piola: 4)
   static constexpr size_t tabT = 0;                     // double2 [NN][NQ]
   static constexpr size_t wq = tabT + 16 * NQ * NN;     // double  [NQ]
   static constexpr size_t groups = align16(wq + 8 * NQ);
   // group-relative
   static constexpr size_t X = 0;                               // double2 [EPG][NN]
   static constexpr size_t U = X + 16 * EPG * NN;               // double2 [EPG][NN]
-  static constexpr size_t S3 = U + 16 * EPG * NN;              // double  [3][EPG*NQ]  weak stress (SoA)
-  static constexpr size_t G = align16(S3 + 24 * EPG * NQ);     // [EPG] x GH_ELEM
-  static constexpr size_t H = align16(G + EPG * GH_ELEM);      // [EPG] x H_ELEM
-  static constexpr size_t SG = align16(H + EPG * H_ELEM);      // double [EPG][NQP]: sign of w detJ t (FP64)
-  static constexpr size_t nid = align16(SG + (TC ? 8 * EPG * D::NQP : 0));  // int [EPG][NN]
+  static constexpr size_t S3 = U + 16 * EPG * NN;  // double [NSTRESS][EPG*NQ] weak stress (SoA)
+  static constexpr size_t G = align16(S3 + 8 * NSTRESS * EPG * NQ);  // [EPG] x GH_ELEM
+  static constexpr size_t H = align16(G + EPG * GH_ELEM);            // [EPG] x H_ELEM
+  static constexpr size_t SG = align16(H + EPG * H_ELEM);  // double [EPG][NQP]: sign of w detJ t (FP64 linear)
+  static constexpr size_t nid = align16(SG + (TC && !NL ? 8 * EPG * D::NQP : 0));  // int [EPG][NN]
   static constexpr size_t rbase = align16(nid + 4 * EPG * NN);  // int [EPG][NN]
   // staged code records (plan) or element map rows (drop-in Jacobian), double-buffered
   static constexpr size_t STAGE = (MODE & kPlan) ? size_t(EPG) * D::CS
@@ -334,9 +384,52 @@ __device__ __forceinline__ void stiffness_mma(const Out &A, const double *Gm, co
   }
 }
 
-template <int P, typename T>
+// NONLINEAR element stiffness, one warp per node-tile pair (TA <= TB): the four
+// component tiles K[(a,i),(b,k)], a in TA, b in TB, share the GA fragment of TA.
+// Lane l holds (a, b) = (8TA + l/4, 8TB + 2(l%4) + h) of all four, i.e. whole
+// 2x2 blocks; the block (b, a) is written as the transpose (K is symmetric).
+template <int P, int MODE>
+__device__ __forceinline__ void stiffness_nl(const Out &A, const double *GA, const double *GB, int el, int pair,
+                                             int lane) {
+  using N = NLDims<P>;
+  constexpr int NTN = N::NTN, KSN = N::KSN, RA = N::RA, RB = N::RB, NP = N::NP, NN = N::NN;
+  int TA = 0, r = pair;
+#pragma unroll
+  for (int k = 0; k < NTN; k++)
+    if (TA == k && r >= NTN - k) {
+      r -= NTN - k;
+      TA = k + 1;
+    }
+  const int TB = TA + r;
+  const int g = lane >> 2, t = lane & 3;
+  double c[4][2];
+#pragma unroll
+  for (int j = 0; j < 4; j++) c[j][0] = c[j][1] = 0.0;
+  const double *pa = GA + t * RA + 8 * TA + g;
+  const double *pb = GB + t * RB + 8 * TB + g;
+#pragma unroll 4
+  for (int ks = 0; ks < KSN; ks++) {
+    const double av = pa[ks * 4 * RA];
+    double bv[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) bv[j] = pb[ks * 4 * RB + j * NP];
+#pragma unroll
+    for (int j = 0; j < 4; j++) dmma(c[j][0], c[j][1], av, bv[j]);
+  }
+  const int a = 8 * TA + g;
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    const int b = 8 * TB + 2 * t + h;
+    if (a < NN && b < NN && (TA < TB || a <= b)) {
+      write_block<P, MODE>(A, el, a, b, 0, c[0][h], c[1][h], c[2][h], c[3][h]);
+      if (a != b) write_block<P, MODE>(A, el, a, b, 1, c[0][h], c[1][h], c[2][h], c[3][h]);
+    }
+  }
+}
+
+template <int P, typename T, int MODE>
 constexpr int min_blocks() {
-  return Shape<P>::MINB;
+  return ShapeSel<P, MODE>::MINB;
 }
 
 // A group's current batch: EPG (or fewer) consecutive elements k0.. of mesh `mesh`
@@ -417,7 +510,7 @@ struct QueueSource {
 // The per-CTA prologue: derivative table and weights, zeroed MMA padding rows.
 template <int P, typename T, int MODE>
 __device__ __forceinline__ void cta_prologue(unsigned char *smem) {
-  using S = Shape<P>;
+  using S = ShapeSel<P, MODE>;
   using L = Layout<P, T, MODE>;
   using D = Dims<P>;
   constexpr int P1 = P + 1, NN = D::NN, NQ = NN, NQP = D::NQP, RS = D::RS, EPG = S::EPG;
@@ -431,7 +524,16 @@ __device__ __forceinline__ void cta_prologue(unsigned char *smem) {
     tabT[a * NQ + q] = make_double2(__dmul_rn(Ny, dNx), __dmul_rn(Nx, dNy));
   }
   for (int q = threadIdx.x; q < NQ; q += blockDim.x) wq[q] = __dmul_rn(kGW[P][q % P1], kGW[P][q / P1]);
-  if constexpr (L::TC) {
+  if constexpr (L::NL) {
+    // padded kappa rows and node columns of GA/GB feed the MMA: zero once (the
+    // quadrature stage writes only the real entries)
+    constexpr int PER = (int)(L::GH_ELEM / 8);
+    for (int i = threadIdx.x; i < S::GPC * EPG * PER; i += blockDim.x) {
+      const int g = i / (EPG * PER), r = i - g * EPG * PER;
+      unsigned char *gs = smem + L::groups + g * L::group_bytes;
+      reinterpret_cast<double *>(gs + L::G)[r] = 0.0;
+    }
+  } else if constexpr (L::TC) {
     // the padded quadrature rows feed the k dimension of the MMA: zero once
     constexpr int PAD = (NQP - NQ) * RS;
     for (int i = threadIdx.x; i < S::GPC * EPG * PAD; i += blockDim.x) {
@@ -454,10 +556,11 @@ __device__ __forceinline__ void cta_prologue(unsigned char *smem) {
 template <int P, typename T, int MODE, typename Src>
 __device__ __forceinline__ void group_loop(unsigned char *smem, Src &src, const AsmArgs &single,
                                            const AsmArgs *__restrict__ meshes) {
-  using S = Shape<P>;
+  using S = ShapeSel<P, MODE>;
   using L = Layout<P, T, MODE>;
   using D = Dims<P>;
-  constexpr bool TC = L::TC;
+  using ND = NLDims<P>;
+  constexpr bool TC = L::TC, NL = L::NL;
   constexpr int P1 = P + 1, NN = D::NN, NQ = NN, NNP = L::NNP, NTILE = D::NTILE;
   constexpr int NQP = D::NQP, RS = D::RS;
   constexpr int GT = S::GT, EPG = S::EPG, NPART = S::NPART, SQ = EPG * NQ;
@@ -597,6 +700,60 @@ __device__ __forceinline__ void group_loop(unsigned char *smem, Src &src, const 
         const double rs = TC ? sqrt(fabs(st)) : 1.0;
         const double sg = st < 0.0 ? -1.0 : 1.0;
         const double sw = TC ? sg * rs : st;
+        if constexpr (NL) {
+          // F = I + g, Green strain E, S = 2 mu E + lam tr(E) I, first Piola P = F S;
+          // tangent A_{il,kn} = delta_ik S_ln + mu F_in F_kl + mu (F F^T)_ik delta_ln + lam F_il F_kn
+          const double uxx = g00 * i00 + g01 * i10, uxy = g00 * i01 + g01 * i11;
+          const double uyx = g10 * i00 + g11 * i10, uyy = g10 * i01 + g11 * i11;
+          const double F[2][2] = {{1.0 + uxx, uxy}, {uyx, 1.0 + uyy}};
+          const double e00 = 0.5 * (2.0 * uxx + uxx * uxx + uyx * uyx);
+          const double e01 = 0.5 * (uxy + uyx + uxx * uxy + uyx * uyy);
+          const double e11 = 0.5 * (2.0 * uyy + uxy * uxy + uyy * uyy);
+          const double trE = e00 + e11;
+          const double Sm[2][2] = {{2.0 * mu * e00 + lam * trE, 2.0 * mu * e01}, {2.0 * mu * e01, 2.0 * mu * e11 + lam * trE}};
+          if (part == 0) {
+#pragma unroll
+            for (int ii = 0; ii < 2; ii++)
+#pragma unroll
+              for (int jj = 0; jj < 2; jj++)
+                S3[(2 * ii + jj) * SQ + iq] = sw * (F[ii][0] * Sm[0][jj] + F[ii][1] * Sm[1][jj]);
+          }
+          double Cs[2][2][2][2];  // sign(s) * A_{il,kn}, [i][l][k][n]
+#pragma unroll
+          for (int ii = 0; ii < 2; ii++)
+#pragma unroll
+            for (int ll = 0; ll < 2; ll++)
+#pragma unroll
+              for (int kk = 0; kk < 2; kk++)
+#pragma unroll
+                for (int nn = 0; nn < 2; nn++) {
+                  const double bik = F[ii][0] * F[kk][0] + F[ii][1] * F[kk][1];
+                  double v = mu * F[ii][nn] * F[kk][ll] + lam * F[ii][ll] * F[kk][nn];
+                  if (ii == kk) v += Sm[ll][nn];
+                  if (ll == nn) v += mu * bik;
+                  Cs[ii][ll][kk][nn] = sg * v;
+                }
+          double *GA = reinterpret_cast<double *>(gs + L::G) + el * (L::GH_ELEM / 8);
+          double *GB = GA + ND::KN * ND::RA;
+#pragma unroll
+          for (int j = 0; j < MAXJ; j++) {
+            const int a = part + j * NPART;
+            if (a >= NN) continue;
+            const double2 d = dt[j];
+            const double gh[2] = {rs * (d.x * i00 + d.y * i10), rs * (d.x * i01 + d.y * i11)};
+#pragma unroll
+            for (int ll = 0; ll < 2; ll++) {
+              const int kap = ll * NQ + q;
+              GA[kap * ND::RA + a] = gh[ll];
+#pragma unroll
+              for (int ii = 0; ii < 2; ii++)
+#pragma unroll
+                for (int kk = 0; kk < 2; kk++)
+                  GB[kap * ND::RB + (2 * ii + kk) * ND::NP + a] =
+                      Cs[ii][ll][kk][0] * gh[0] + Cs[ii][ll][kk][1] * gh[1];
+            }
+          }
+        } else {
         if (part == 0) {
           const double uxx = g00 * i00 + g01 * i10, uxy = g00 * i01 + g01 * i11;
           const double uyx = g10 * i00 + g11 * i10, uyy = g10 * i01 + g11 * i11;
@@ -629,6 +786,7 @@ __device__ __forceinline__ void group_loop(unsigned char *smem, Src &src, const 
             }
           }
         }
+        }
       }
     }
     group_sync(bar, GT);
@@ -646,7 +804,16 @@ __device__ __forceinline__ void group_loop(unsigned char *smem, Src &src, const 
           for (int q = part; q < NQ; q += NPART) {
             const int iq = el * NQ + q;
             T gx, gy;
-            if constexpr (TC) {
+            if constexpr (NL) {
+              const double *GA = reinterpret_cast<const double *>(gs + L::G) + el * (L::GH_ELEM / 8);
+              gx = GA[q * ND::RA + a];
+              gy = GA[(NQ + q) * ND::RA + a];
+              const double pxx = S3[0 * SQ + iq], pxy = S3[1 * SQ + iq];
+              const double pyx = S3[2 * SQ + iq], pyy = S3[3 * SQ + iq];
+              rx = fma(pxx, gx, fma(pxy, gy, rx));
+              ry = fma(pyx, gx, fma(pyy, gy, ry));
+              continue;
+            } else if constexpr (TC) {
               const double2 gv = *reinterpret_cast<const double2 *>(reinterpret_cast<const double *>(gs + L::G) +
                                                                      (el * NQP + q) * RS + 2 * a);
               gx = gv.x;
@@ -685,7 +852,15 @@ __device__ __forceinline__ void group_loop(unsigned char *smem, Src &src, const 
 
     // 2b. element stiffness
     if constexpr ((MODE & kJac) != 0) {
-      if constexpr (TC) {
+      if constexpr (NL) {
+        // FP64 tensor cores: warps take (element, node-tile pair) work items
+        constexpr int NW = GT / 32;
+        for (int w = warp; w < ne * ND::NPAIR; w += NW) {
+          const int el = w / ND::NPAIR, pair = w - el * ND::NPAIR;
+          const double *GA = reinterpret_cast<const double *>(gs + L::G) + el * (L::GH_ELEM / 8);
+          stiffness_nl<P, MODE>(A, GA, GA + ND::KN * ND::RA, el, pair, lane);
+        }
+      } else if constexpr (TC) {
         // FP64 tensor cores: warps take (element, row range) work items
         constexpr int WPE = RowSplit<P>::WPE;  // warps per element
         constexpr int NW = GT / 32;
@@ -771,9 +946,9 @@ __device__ __forceinline__ void group_loop(unsigned char *smem, Src &src, const 
 
 // Single mesh: A.count elements from A.begin, persistent grid-stride over batches.
 template <int P, typename T, int MODE>
-__global__ void __launch_bounds__(Shape<P>::GT *Shape<P>::GPC, min_blocks<P, T>())
+__global__ void __launch_bounds__(ShapeSel<P, MODE>::GT *ShapeSel<P, MODE>::GPC, min_blocks<P, T, MODE>())
     assemble_kernel(const __grid_constant__ AsmArgs A) {
-  using S = Shape<P>;
+  using S = ShapeSel<P, MODE>;
   extern __shared__ __align__(16) unsigned char smem[];
   cta_prologue<P, T, MODE>(smem);
   const int g = threadIdx.x / S::GT;
@@ -784,10 +959,10 @@ __global__ void __launch_bounds__(Shape<P>::GT *Shape<P>::GPC, min_blocks<P, T>(
 
 // Many meshes of one order: groups pull tiles from the launch's queue.
 template <int P, typename T, int MODE>
-__global__ void __launch_bounds__(Shape<P>::GT *Shape<P>::GPC, min_blocks<P, T>())
+__global__ void __launch_bounds__(ShapeSel<P, MODE>::GT *ShapeSel<P, MODE>::GPC, min_blocks<P, T, MODE>())
     assemble_batched_kernel(const AsmArgs *__restrict__ meshes, const Tile *__restrict__ tiles, int ntiles,
                             int *counter) {
-  using S = Shape<P>;
+  using S = ShapeSel<P, MODE>;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int slots[S::GPC];
   cta_prologue<P, T, MODE>(smem);

@@ -65,9 +65,37 @@ __global__ void __launch_bounds__(256) bsr_spmv_kernel(int numRows, const int *_
 
 namespace fem {
 namespace {
+template <typename T>
+int launch_any(int order, int mode, const dev::AsmArgs &a, cudaStream_t s) {
+  using namespace dev;
+  switch (mode) {
+    case kRes: return launch_mode<T, kRes>(order, a, s);
+    case kJac: return launch_mode<T, kJac>(order, a, s);
+    case kRes | kJac: return launch_mode<T, kRes | kJac>(order, a, s);
+    case kPlan | kRes: return launch_mode<T, kPlan | kRes>(order, a, s);
+    case kPlan | kJac: return launch_mode<T, kPlan | kJac>(order, a, s);
+    case kPlan | kRes | kJac: return launch_mode<T, kPlan | kRes | kJac>(order, a, s);
+    default: return fail(FEM_ERR_INVALID_ARGUMENT, "bad kernel mode %d", mode);
+  }
+}
+}  // namespace
+
+int launch(int order, int precision, int mode, const dev::AsmArgs &a, cudaStream_t s, int strain) {
+  if (strain == FEM_STRAIN_NONLINEAR) {
+    if (precision != FEM_PRECISION_FP64)
+      return fail(FEM_ERR_INVALID_ARGUMENT, "NONLINEAR strain is assembled in FP64 only (precision %d)", precision);
+    return launch_nl(order, mode, a, s);
+  }
+  if (strain != FEM_STRAIN_LINEAR) return fail(FEM_ERR_INVALID_ARGUMENT, "strain type %d", strain);
+  if (precision == FEM_PRECISION_FP64) return launch_any<double>(order, mode, a, s);
+  if (precision == FEM_PRECISION_MIXED) return launch_any<float>(order, mode, a, s);
+  return fail(FEM_ERR_INVALID_ARGUMENT, "precision %d", precision);
+}
+
+namespace {
 int run_dropin(int precision, bool jac, int order, const int *connPtr, const int *conn, int numElements,
                const double *states, const double *coords, double E, double nu, double t, const int *map,
-               double *residual, double *mat, void *stream, double *elapsed) {
+               double *residual, double *mat, void *stream, double *elapsed, int strain = FEM_STRAIN_LINEAR) {
   clear_error();
   if (elapsed) *elapsed = 0.0;
   if (order < 1 || order > 4) return fail(FEM_ERR_INVALID_ORDER, "element order %d (supported: 1..4)", order);
@@ -92,7 +120,7 @@ int run_dropin(int precision, bool jac, int order, const int *connPtr, const int
   set_material(a, E, nu, t);
   const int mode = (jac ? dev::kJac : 0) | (residual ? dev::kRes : 0);
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  return timed(s, elapsed, [&] { return launch(order, precision, mode, a, s); });
+  return timed(s, elapsed, [&] { return launch(order, precision, mode, a, s, strain); });
 }
 
 }  // namespace
@@ -159,6 +187,21 @@ int fem_run_jacobian_mixed(int elementOrder, const int *connPtr, const int *conn
                            double *elapsedSeconds) {
   return fem::run_dropin(FEM_PRECISION_MIXED, true, elementOrder, connPtr, conn, numElements, states, nodeCoords, E,
                          nu, t, elementBCSRMap, residual, matEntries, stream, elapsedSeconds);
+}
+
+int fem_run_residual_ex(int elementOrder, const int *connPtr, const int *conn, int numElements, const double *states,
+                        const double *nodeCoords, double E, double nu, double t, double *residual, int precision,
+                        int strainType, void *stream, double *elapsedSeconds) {
+  return fem::run_dropin(precision, false, elementOrder, connPtr, conn, numElements, states, nodeCoords, E, nu, t,
+                         nullptr, residual, nullptr, stream, elapsedSeconds, strainType);
+}
+
+int fem_run_jacobian_ex(int elementOrder, const int *connPtr, const int *conn, int numElements, const double *states,
+                        const double *nodeCoords, double E, double nu, double t, const int *elementBCSRMap,
+                        double *residual, double *matEntries, int precision, int strainType, void *stream,
+                        double *elapsedSeconds) {
+  return fem::run_dropin(precision, true, elementOrder, connPtr, conn, numElements, states, nodeCoords, E, nu, t,
+                         elementBCSRMap, residual, matEntries, stream, elapsedSeconds, strainType);
 }
 
 int fem_bsr_spmv(int numRows, const int *rowp, const int *cols, const double *A, const double *x, double *y,
@@ -243,6 +286,13 @@ int fem_plan_device_pattern(const fem_plan *plan, const int **rowp, const int **
 int fem_plan_assemble(const fem_plan *plan, const double *states, const double *nodeCoords, double E, double nu,
                       double t, double *residual, double *matEntries, int precision, void *stream,
                       double *elapsedSeconds) {
+  return fem_plan_assemble_ex(plan, states, nodeCoords, E, nu, t, residual, matEntries, precision, FEM_STRAIN_LINEAR,
+                              stream, elapsedSeconds);
+}
+
+int fem_plan_assemble_ex(const fem_plan *plan, const double *states, const double *nodeCoords, double E, double nu,
+                         double t, double *residual, double *matEntries, int precision, int strainType, void *stream,
+                         double *elapsedSeconds) {
   fem::clear_error();
   if (elapsedSeconds) *elapsedSeconds = 0.0;
   if (!plan) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "plan is NULL");
@@ -268,7 +318,7 @@ int fem_plan_assemble(const fem_plan *plan, const double *states, const double *
     for (int c = 0; c < plan->numColours; c++) {
       a.begin = plan->colourPtr[c];
       a.count = plan->colourPtr[c + 1] - plan->colourPtr[c];
-      int st = fem::launch(plan->order, precision, mode, a, s);
+      int st = fem::launch(plan->order, precision, mode, a, s, strainType);
       if (st) return st;
     }
     return (int)FEM_SUCCESS;

@@ -54,7 +54,7 @@ int launch_info(K kernel, int nt, size_t smem, LaunchInfo &out) {
 
 template <int P, typename T, int MODE>
 int launch_p(const dev::AsmArgs &a, cudaStream_t s) {
-  using S = dev::Shape<P>;
+  using S = dev::ShapeSel<P, MODE>;
   constexpr int NT = S::GT * S::GPC;
   auto kernel = dev::assemble_kernel<P, T, MODE>;
   const size_t smem = dev::Layout<P, T, MODE>::total;
@@ -83,25 +83,15 @@ int launch_mode(int order, const dev::AsmArgs &a, cudaStream_t s) {
   }
 }
 
-template <typename T>
-int launch_any(int order, int mode, const dev::AsmArgs &a, cudaStream_t s) {
-  using namespace dev;
-  switch (mode) {
-    case kRes: return launch_mode<T, kRes>(order, a, s);
-    case kJac: return launch_mode<T, kJac>(order, a, s);
-    case kRes | kJac: return launch_mode<T, kRes | kJac>(order, a, s);
-    case kPlan | kRes: return launch_mode<T, kPlan | kRes>(order, a, s);
-    case kPlan | kJac: return launch_mode<T, kPlan | kJac>(order, a, s);
-    case kPlan | kRes | kJac: return launch_mode<T, kPlan | kRes | kJac>(order, a, s);
-    default: return fail(FEM_ERR_INVALID_ARGUMENT, "bad kernel mode %d", mode);
-  }
-}
-
-inline int launch(int order, int precision, int mode, const dev::AsmArgs &a, cudaStream_t s) {
-  if (precision == FEM_PRECISION_FP64) return launch_any<double>(order, mode, a, s);
-  if (precision == FEM_PRECISION_MIXED) return launch_any<float>(order, mode, a, s);
-  return fail(FEM_ERR_INVALID_ARGUMENT, "precision %d", precision);
-}
+// The dispatchers below are defined out of line, each in the one translation unit
+// that instantiates its kernels (every kernel is compiled once):
+//   launch          single-mesh kernels, LINEAR (fem_kernels.cu), NONLINEAR via launch_nl
+//   launch_nl       NONLINEAR kernels, FP64 (fem_nonlinear.cu)
+//   launch_batched  tile-queue kernels of batches and the server (fem_batch.cu)
+int launch(int order, int precision, int mode, const dev::AsmArgs &a, cudaStream_t s, int strain = FEM_STRAIN_LINEAR);
+int launch_nl(int order, int mode, const dev::AsmArgs &a, cudaStream_t s);
+int launch_batched(int p, int precision, const dev::AsmArgs *meshes, const dev::Tile *tiles, int ntiles, int *counter,
+                   cudaStream_t s);
 
 inline void set_material(dev::AsmArgs &a, double E, double nu, double t) {
   // element/FEKernels.h:300-301
@@ -142,40 +132,6 @@ inline int epg_of(int p) {
     case 2: return dev::Shape<2>::EPG;
     case 3: return dev::Shape<3>::EPG;
     default: return dev::Shape<4>::EPG;
-  }
-}
-
-// One persistent batched launch of order P over the tile queue `tiles` (plan mode,
-// residual and Jacobian).
-template <int P, typename T>
-int launch_batched_p(const dev::AsmArgs *meshes, const dev::Tile *tiles, int ntiles, int *counter, cudaStream_t s) {
-  using S = dev::Shape<P>;
-  constexpr int NT = S::GT * S::GPC;
-  constexpr int MODE = dev::kPlan | dev::kRes | dev::kJac;
-  auto kernel = dev::assemble_batched_kernel<P, T, MODE>;
-  const size_t smem = dev::Layout<P, T, MODE>::total;
-  LaunchInfo li;
-  int st = launch_info(kernel, NT, smem, li);
-  if (st) return st;
-  const int64_t need = (ntiles + S::GPC - 1) / S::GPC;
-  const int64_t cap = (int64_t)li.grid_per_sm * li.num_sms;
-  const int grid = (int)(need < cap ? need : cap);
-  if (grid <= 0) return FEM_SUCCESS;
-  kernel<<<grid, NT, smem, s>>>(meshes, tiles, ntiles, counter);
-  cudaError_t err = cudaGetLastError();
-  if (err != cudaSuccess) return cuda_fail(err, "assemble_batched_kernel launch");
-  return FEM_SUCCESS;
-}
-
-template <typename T>
-int launch_batched(int p, const dev::AsmArgs *meshes, const dev::Tile *tiles, int ntiles, int *counter,
-                   cudaStream_t s) {
-  switch (p) {
-    case 1: return launch_batched_p<1, T>(meshes, tiles, ntiles, counter, s);
-    case 2: return launch_batched_p<2, T>(meshes, tiles, ntiles, counter, s);
-    case 3: return launch_batched_p<3, T>(meshes, tiles, ntiles, counter, s);
-    case 4: return launch_batched_p<4, T>(meshes, tiles, ntiles, counter, s);
-    default: return fail(FEM_ERR_INVALID_ORDER, "order %d", p);
   }
 }
 

@@ -181,9 +181,7 @@ int issue_wave(fem_server *S, Lane &L, const std::vector<ServerMesh> &wm, const 
   for (size_t j = 0; j < keys.size(); j++) {
     const int p = keys[j].first, c = keys[j].second;
     int *counter = L.d_counters + p * kMaxColoursS + c;
-    st = S->precision == FEM_PRECISION_FP64
-             ? fem::launch_batched<double>(p, L.d_args, L.d_tiles + off[j], off[j + 1] - off[j], counter, L.stream)
-             : fem::launch_batched<float>(p, L.d_args, L.d_tiles + off[j], off[j + 1] - off[j], counter, L.stream);
+    st = fem::launch_batched(p, S->precision, L.d_args, L.d_tiles + off[j], off[j + 1] - off[j], counter, L.stream);
     if (st) return st;
   }
   // outputs: residuals back to the clients (the matrices stay resident)

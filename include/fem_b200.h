@@ -46,6 +46,14 @@ extern "C" {
 #define FEM_PRECISION_FP64 0  /* all element arithmetic in FP64                               */
 #define FEM_PRECISION_MIXED 1 /* FP64 J/detJ/J^-1 and FP64 accumulate, FP32 element products */
 
+/* Strain measure of the weak residual: the reference's A2D::GreenStrainType
+ * template option of planeStressWeakRes and the four assembly kernels
+ * (element/FEKernels.h:286,317,379,589,786).  Its dispatchers always take the
+ * default, LINEAR. */
+#define FEM_STRAIN_LINEAR 0    /* eps = sym(du/dx); weakRes = w detJ t sigma                 */
+#define FEM_STRAIN_NONLINEAR 1 /* Green strain E = 1/2 (g + g^T + g^T g), g = du/dx;        */
+                               /* weakRes = w detJ t (I + g) S, S = 2 mu E + lambda tr(E) I  */
+
 const char *fem_status_string(int status);
 /* Message describing the last failure on the calling host thread ("" if none). */
 const char *fem_last_error(void);
@@ -77,6 +85,21 @@ int fem_run_jacobian_mixed(int elementOrder, const int *connPtr, const int *conn
                            const double *states, const double *nodeCoords, double E, double nu, double t,
                            const int *elementBCSRMap, double *residual, double *matEntries, void *stream,
                            double *elapsedSeconds);
+
+/* The reference kernels with an explicit strainType template argument
+ * (assemblePlaneStressResidualKernel<order,2,2,strainType>, FEKernels.h:585-728;
+ * assemblePlaneStressJacobianKernel<...,strainType>, FEKernels.h:782-1006), which
+ * runResidualKernel/runJacobianKernel never expose.  Same contracts as
+ * fem_run_residual / fem_run_jacobian.  precision: FEM_PRECISION_*; strainType:
+ * FEM_STRAIN_*; FEM_STRAIN_NONLINEAR requires FEM_PRECISION_FP64
+ * (FEM_ERR_INVALID_ARGUMENT otherwise). */
+int fem_run_residual_ex(int elementOrder, const int *connPtr, const int *conn, int numElements, const double *states,
+                        const double *nodeCoords, double E, double nu, double t, double *residual, int precision,
+                        int strainType, void *stream, double *elapsedSeconds);
+int fem_run_jacobian_ex(int elementOrder, const int *connPtr, const int *conn, int numElements, const double *states,
+                        const double *nodeCoords, double E, double nu, double t, const int *elementBCSRMap,
+                        double *residual, double *matEntries, int precision, int strainType, void *stream,
+                        double *elapsedSeconds);
 
 /* ---- host-side setup helpers (HOST pointers) ------------------------------------------- */
 
@@ -130,6 +153,10 @@ int fem_plan_device_pattern(const fem_plan *plan, const int **rowp, const int **
 int fem_plan_assemble(const fem_plan *plan, const double *states, const double *nodeCoords, double E, double nu,
                       double t, double *residual, double *matEntries, int precision, void *stream,
                       double *elapsedSeconds);
+/* fem_plan_assemble with a strain measure (FEM_STRAIN_*; NONLINEAR in FP64 only). */
+int fem_plan_assemble_ex(const fem_plan *plan, const double *states, const double *nodeCoords, double E, double nu,
+                         double t, double *residual, double *matEntries, int precision, int strainType, void *stream,
+                         double *elapsedSeconds);
 
 /* ---- batched assembly of many meshes (config: 256 meshes, mixed orders) --------------- */
 /* A batch references existing plans (they must outlive it) and assembles all of
