@@ -17,8 +17,8 @@ CSRC = PKG / "csrc"
 INCLUDE = ROOT / "include"
 LIB = PKG / "libfemb200.so"
 
-SOURCES = ["fem_kernels.cu", "fem_nonlinear.cu", "fem_batch.cu", "fem_server.cu", "fem_static.cu", "fem_host.cpp",
-           "fem_probe.cu"]
+SOURCES = ["fem_kernels.cu", "fem_nonlinear.cu", "fem_rows.cu", "fem_batch.cu", "fem_server.cu", "fem_static.cu",
+           "fem_host.cpp", "fem_probe.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

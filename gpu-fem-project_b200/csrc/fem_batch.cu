@@ -84,6 +84,7 @@ struct fem_batch {
   int tileBatches[kOrders] = {0, 16, 16, 16, 16};  // tile length in element batches, per order
   std::vector<fem::dev::Tile> tiles;
   std::vector<int> tileOff;  // [kOrders][maxColours + 1]
+  int rowTile0 = 0, rowTile1 = 0;  // order-1 row-assembly tiles (chunks), after the colour tiles
   fem::dev::Tile *d_tiles = nullptr;
   size_t d_tiles_cap = 0;
   bool tiles_dirty = true;
@@ -137,7 +138,7 @@ void build_tiles(fem_batch *b) {
       b->tileOff[p * (C + 1) + c] = (int)b->tiles.size();
       for (size_t m = 0; m < b->plans.size(); m++) {
         const fem_plan *pl = b->plans[m];
-        if (pl->order != p || c >= pl->numColours) continue;
+        if (pl->order != p || c >= pl->numColours || fem::plan_rows(pl)) continue;
         for (int64_t k = pl->colourPtr[c]; k < pl->colourPtr[c + 1]; k += len) {
           fem::dev::Tile t;
           t.mesh = (int)m;
@@ -149,6 +150,19 @@ void build_tiles(fem_batch *b) {
     }
     b->tileOff[p * (C + 1) + C] = (int)b->tiles.size();
   }
+  b->rowTile0 = (int)b->tiles.size();
+  for (size_t m = 0; m < b->plans.size(); m++) {
+    const fem_plan *pl = b->plans[m];
+    if (!fem::plan_rows(pl)) continue;
+    for (int k = 0; k < pl->numChunks; k += fem::kRowTileChunks) {
+      fem::dev::Tile t;
+      t.mesh = (int)m;
+      t.begin = k;
+      t.count = std::min(fem::kRowTileChunks, pl->numChunks - k);
+      b->tiles.push_back(t);
+    }
+  }
+  b->rowTile1 = (int)b->tiles.size();
   b->tiles_dirty = true;
 }
 
@@ -178,9 +192,15 @@ int sync_device_state(fem_batch *b) {
   return FEM_SUCCESS;
 }
 
-// The colour chain of one order on stream s (counters reset by the caller).
+// The colour chain of one order on stream s (counters reset by the caller); order 1
+// meshes with row tables run one row-assembly launch (queue counter [0][0]).
 int enqueue_order(fem_batch *b, int p, int precision, cudaStream_t s) {
   const int C = b->maxColours;
+  if (p == 1 && b->rowTile1 > b->rowTile0) {
+    int st = fem::launch_rows_batched(b->d_args, b->d_tiles + b->rowTile0, b->rowTile1 - b->rowTile0,
+                                      b->d_counters, s);
+    if (st) return st;
+  }
   for (int c = 0; c < C; c++) {
     const int t0 = b->tileOff[p * (C + 1) + c], t1 = b->tileOff[p * (C + 1) + c + 1];
     if (t1 <= t0) continue;
@@ -193,7 +213,7 @@ int enqueue_order(fem_batch *b, int p, int precision, cudaStream_t s) {
 
 bool order_has_work(const fem_batch *b, int p) {
   const int C = b->maxColours;
-  return b->tileOff[p * (C + 1) + C] > b->tileOff[p * (C + 1)];
+  return b->tileOff[p * (C + 1) + C] > b->tileOff[p * (C + 1)] || (p == 1 && b->rowTile1 > b->rowTile0);
 }
 
 // Whole batch: reset queues, fork one stream per order, join back into s.
@@ -247,9 +267,7 @@ int fem_batch_create(int numMeshes, fem_plan *const *plans, fem_batch **batch) {
     b->maxColours = std::max(b->maxColours, plans[m]->numColours);
     b->totalElements += plans[m]->numElements;
     fem::dev::AsmArgs a{};
-    a.connList = plans[m]->d_connList;
-    a.blockCode = plans[m]->d_blockCode;
-    a.rowp = plans[m]->d_rowp;
+    fem::plan_args(a, plans[m]);
     b->args.push_back(a);
   }
   b->bound.assign(numMeshes, 0);

@@ -36,7 +36,14 @@ struct HostPlan {
   // to a multiple of 16 bytes (records are copied to shared memory in 16-byte chunks).
   int codeStride = 0;
   std::vector<uint8_t> blockCode;
+  // Order 1, row assembly (each block row written once by the warp that owns it):
+  // rowElemPtr[numNodes+1] indexes rowElem, two ints per (node r, element k listing
+  // r): {k << 2 | a (local index of r), ranks of the element's four nodes in row r,
+  // one byte each}; rowChunk[numChunks+1] cuts the rows into chunks of at most
+  // kRowChunkRows rows and kRowChunkBlocks blocks.  Empty when not applicable.
+  std::vector<int> rowElemPtr, rowElem, rowChunk;
 };
+constexpr int kRowChunkRows = 32, kRowChunkBlocks = 320;
 int build_host_plan(int order, int numNodes, const int *connPtr, const int *conn, int numElements, HostPlan &hp);
 
 }  // namespace fem

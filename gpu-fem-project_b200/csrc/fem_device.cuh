@@ -109,10 +109,20 @@ struct Vec2<float> {
 enum : int { kRes = 1, kJac = 2, kPlan = 4, kNL = 8 };
 
 struct AsmArgs {
-  const int *connPtr;      // drop-in: CSR offsets
-  const int *conn;         // drop-in: node ids
-  const int *map;          // drop-in: element block offsets (doubles)
-  const int *connList;     // plan: node ids of the listed elements, nn each
+  // drop-in fields | order-1 plan row tables (a plan never reads the drop-in ones)
+  union {
+    const int *connPtr;     // drop-in: CSR offsets
+    const int *rowElemPtr;  // plan, order 1: per row, range of rowElem entries
+  };
+  union {
+    const int *conn;     // drop-in: node ids
+    const int *rowElem;  // plan, order 1: {k << 2 | a, four ranks} per (row, element)
+  };
+  union {
+    const int *map;       // drop-in: element block offsets (doubles)
+    const int *rowChunk;  // plan, order 1: row ranges of the warp chunks
+  };
+  const int *connList;       // plan: node ids of the listed elements, nn each
   const uint8_t *blockCode;  // plan: per listed element a Dims<P>::CS-byte code record
   const int *rowp;           // plan: BSR row pointers
   const double *states;
@@ -120,7 +130,7 @@ struct AsmArgs {
   double *residual;
   double *mat;
   double mu, lam, t;
-  int64_t begin, count;  // element (or list position) range of this launch
+  int64_t begin, count;  // element (or list position, or row chunk) range of this launch
 };
 
 // The output side of one batch: global outputs (registers) and the batch's

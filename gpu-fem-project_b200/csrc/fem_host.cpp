@@ -132,6 +132,49 @@ int colour_greedy(int numNodes, const int *connPtr, const int *conn, int numElem
   return FEM_SUCCESS;
 }
 
+// Row assembly tables of an order-1 plan (see HostPlan).  Left empty (the plan then
+// assembles by colours) when a row is longer than one chunk or the element count
+// does not fit the k << 2 packing.
+static void build_row_plan(HostPlan &hp) {
+  const int N = hp.numNodes, nE = hp.numElements;
+  if (nE >= (1 << 29)) return;
+  for (int r = 0; r < N; r++)
+    if (hp.rowp[r + 1] - hp.rowp[r] > kRowChunkBlocks) return;
+  std::vector<int> ptr((size_t)N + 1, 0);
+  for (int64_t i = 0; i < (int64_t)nE * 4; i++) ptr[hp.connList[i] + 1]++;
+  for (int r = 0; r < N; r++) ptr[r + 1] += ptr[r];
+  std::vector<int> ent((size_t)ptr[N] * 2);
+  std::vector<int> fill(ptr.begin(), ptr.end() - 1);
+  for (int k = 0; k < nE; k++) {  // ascending k: each row lists its elements in colour order
+    const uint8_t *rec = &hp.blockCode[(size_t)k * hp.codeStride];
+    for (int a = 0; a < 4; a++) {
+      const int r = hp.connList[(size_t)k * 4 + a];
+      int ranks = 0;
+      for (int b = 0; b < 4; b++) ranks |= (rec[a * 4 + b] & 0x7f) << (8 * b);
+      const int j = fill[r]++;
+      ent[2 * (size_t)j] = (k << 2) | a;
+      ent[2 * (size_t)j + 1] = ranks;
+    }
+  }
+  std::vector<int> chunk(1, 0);
+  int rows = 0;
+  int64_t blocks = 0;
+  for (int r = 0; r < N; r++) {
+    const int64_t len = hp.rowp[r + 1] - hp.rowp[r];
+    if (rows == kRowChunkRows || blocks + len > kRowChunkBlocks) {
+      chunk.push_back(r);
+      rows = 0;
+      blocks = 0;
+    }
+    rows++;
+    blocks += len;
+  }
+  chunk.push_back(N);
+  hp.rowElemPtr.swap(ptr);
+  hp.rowElem.swap(ent);
+  hp.rowChunk.swap(chunk);
+}
+
 int build_host_plan(int order, int numNodes, const int *connPtr, const int *conn, int numElements, HostPlan &hp) {
   const int nn = (order + 1) * (order + 1);
   int st = validate_mesh(numNodes, connPtr, conn, numElements);
@@ -198,6 +241,7 @@ int build_host_plan(int order, int numNodes, const int *connPtr, const int *conn
     }
   }
   if (bad) return fail(FEM_ERR_UNSUPPORTED, "a BSR row holds more than 128 blocks; use the map-based entry points");
+  if (order == 1) build_row_plan(hp);
   return FEM_SUCCESS;
 }
 

@@ -140,6 +140,9 @@ void plan_free(fem_plan *p) {
   cudaFree(p->d_cols);
   cudaFree(p->d_connList);
   cudaFree(p->d_blockCode);
+  cudaFree(p->d_rowElemPtr);
+  cudaFree(p->d_rowElem);
+  cudaFree(p->d_rowChunk);
   cudaSetDevice(cur);
   delete p;
 }
@@ -244,6 +247,15 @@ int fem_plan_create(int elementOrder, int numNodes, const int *connPtr, const in
     plan_free(p);
     return st;
   }
+  if (!hp.rowChunk.empty()) {
+    if ((st = upload(hp.rowElemPtr, &p->d_rowElemPtr, p->deviceBytes)) ||
+        (st = upload(hp.rowElem, &p->d_rowElem, p->deviceBytes)) ||
+        (st = upload(hp.rowChunk, &p->d_rowChunk, p->deviceBytes))) {
+      plan_free(p);
+      return st;
+    }
+    p->numChunks = (int)hp.rowChunk.size() - 1;
+  }
   *plan = p;
   return FEM_SUCCESS;
 }
@@ -304,9 +316,7 @@ int fem_plan_assemble_ex(const fem_plan *plan, const double *states, const doubl
     return fem::fail(FEM_ERR_MISALIGNED, "matEntries must be 32-byte aligned (one 2x2 block per 256-bit store)");
   if (plan->numElements == 0) return FEM_SUCCESS;
   fem::dev::AsmArgs a{};
-  a.connList = plan->d_connList;
-  a.blockCode = plan->d_blockCode;
-  a.rowp = plan->d_rowp;
+  fem::plan_args(a, plan);
   a.states = states;
   a.coords = nodeCoords;
   a.residual = residual;
@@ -314,6 +324,14 @@ int fem_plan_assemble_ex(const fem_plan *plan, const double *states, const doubl
   fem::set_material(a, E, nu, t);
   const int mode = fem::dev::kPlan | (residual ? fem::dev::kRes : 0) | (matEntries ? fem::dev::kJac : 0);
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (fem::plan_rows(plan) && strainType == FEM_STRAIN_LINEAR) {
+    // order 1: row assembly (FP64 arithmetic for both precisions)
+    if (precision != FEM_PRECISION_FP64 && precision != FEM_PRECISION_MIXED)
+      return fem::fail(FEM_ERR_INVALID_ARGUMENT, "precision %d", precision);
+    a.begin = 0;
+    a.count = plan->numChunks;
+    return fem::timed(s, elapsedSeconds, [&] { return fem::launch_rows(mode, a, s); });
+  }
   return fem::timed(s, elapsedSeconds, [&] {
     for (int c = 0; c < plan->numColours; c++) {
       a.begin = plan->colourPtr[c];

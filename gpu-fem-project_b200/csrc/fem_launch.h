@@ -92,6 +92,13 @@ int launch(int order, int precision, int mode, const dev::AsmArgs &a, cudaStream
 int launch_nl(int order, int mode, const dev::AsmArgs &a, cudaStream_t s);
 int launch_batched(int p, int precision, const dev::AsmArgs *meshes, const dev::Tile *tiles, int ntiles, int *counter,
                    cudaStream_t s);
+// Order-1 row assembly (fem_rows.cu): chunks [a.begin, a.begin + a.count) of one
+// mesh; or tiles of chunks of many meshes (residual and Jacobian).
+int launch_rows(int mode, const dev::AsmArgs &a, cudaStream_t s);
+int launch_rows_batched(const dev::AsmArgs *meshes, const dev::Tile *tiles, int ntiles, int *counter,
+                        cudaStream_t s);
+// Chunks per row tile of the batched row kernel.
+constexpr int kRowTileChunks = 16;
 
 inline void set_material(dev::AsmArgs &a, double E, double nu, double t) {
   // element/FEKernels.h:300-301
@@ -145,5 +152,22 @@ struct fem_plan {
   std::vector<int> colourPtr;
   int *d_rowp = nullptr, *d_cols = nullptr, *d_connList = nullptr;
   uint8_t *d_blockCode = nullptr;  // per-element code records (Dims<P>::CS bytes each)
+  // order 1: row assembly tables (HostPlan::rowElemPtr/rowElem/rowChunk); numChunks == 0: none
+  int *d_rowElemPtr = nullptr, *d_rowElem = nullptr, *d_rowChunk = nullptr;
+  int numChunks = 0;
   int64_t deviceBytes = 0;
 };
+
+namespace fem {
+// The plan's device tables in an argument block (inputs/outputs/material are the caller's).
+inline void plan_args(dev::AsmArgs &a, const fem_plan *p) {
+  a.connList = p->d_connList;
+  a.blockCode = p->d_blockCode;
+  a.rowp = p->d_rowp;
+  a.rowElemPtr = p->d_rowElemPtr;
+  a.rowElem = p->d_rowElem;
+  a.rowChunk = p->d_rowChunk;
+}
+// Whether the LINEAR assembly of this plan runs as row assembly.
+inline bool plan_rows(const fem_plan *p) { return p->numChunks > 0; }
+}  // namespace fem

@@ -123,9 +123,7 @@ int issue_wave(fem_server *S, Lane &L, const std::vector<ServerMesh> &wm, const 
   for (int i = 0; i < n; i++) {
     const ServerMesh &m = wm[i];
     fem::dev::AsmArgs a{};
-    a.connList = m.plan->d_connList;
-    a.blockCode = m.plan->d_blockCode;
-    a.rowp = m.plan->d_rowp;
+    fem::plan_args(a, m.plan);
     a.states = m.states;
     a.coords = m.coords;
     a.residual = m.residual;
@@ -146,7 +144,7 @@ int issue_wave(fem_server *S, Lane &L, const std::vector<ServerMesh> &wm, const 
       const int t0 = (int)L.tiles.size();
       for (int i = 0; i < n; i++) {
         const fem_plan *pl = wm[i].plan;
-        if (pl->order != p || c >= pl->numColours) continue;
+        if (pl->order != p || c >= pl->numColours || fem::plan_rows(pl)) continue;
         for (int64_t k = pl->colourPtr[c]; k < pl->colourPtr[c + 1]; k += len) {
           fem::dev::Tile t;
           t.mesh = i;
@@ -159,6 +157,25 @@ int issue_wave(fem_server *S, Lane &L, const std::vector<ServerMesh> &wm, const 
         keys.push_back({p, c});
         off.push_back(t0);
       }
+    }
+  }
+  // order-1 meshes with row tables: one row-assembly launch (key colour -1)
+  {
+    const int t0 = (int)L.tiles.size();
+    for (int i = 0; i < n; i++) {
+      const fem_plan *pl = wm[i].plan;
+      if (!fem::plan_rows(pl)) continue;
+      for (int k = 0; k < pl->numChunks; k += fem::kRowTileChunks) {
+        fem::dev::Tile t;
+        t.mesh = i;
+        t.begin = k;
+        t.count = std::min(fem::kRowTileChunks, pl->numChunks - k);
+        L.tiles.push_back(t);
+      }
+    }
+    if ((int)L.tiles.size() > t0) {
+      keys.push_back({1, -1});
+      off.push_back(t0);
     }
   }
   off.push_back((int)L.tiles.size());
@@ -180,6 +197,11 @@ int issue_wave(fem_server *S, Lane &L, const std::vector<ServerMesh> &wm, const 
   if (err != cudaSuccess) return fem::cuda_fail(err, "wave staging");
   for (size_t j = 0; j < keys.size(); j++) {
     const int p = keys[j].first, c = keys[j].second;
+    if (c < 0) {  // row assembly, queue counter [0][0]
+      st = fem::launch_rows_batched(L.d_args, L.d_tiles + off[j], off[j + 1] - off[j], L.d_counters, L.stream);
+      if (st) return st;
+      continue;
+    }
     int *counter = L.d_counters + p * kMaxColoursS + c;
     st = fem::launch_batched(p, S->precision, L.d_args, L.d_tiles + off[j], off[j + 1] - off[j], counter, L.stream);
     if (st) return st;
