@@ -31,63 +31,102 @@ namespace dev {
 
 constexpr int kRowWarps = 4;
 
-// One chunk c of mesh M, by the calling warp; acc is the warp's kRowChunkBlocks
-// blocks of shared memory (two double2 per block).  NP, NM: the 1D basis values
-// N(x) at the Gauss point on the node's own side / the opposite side,
-// fma(0.5, g, 0.5) and fma(-0.5, g, 0.5) as in lagrangePoly1dDeriv<double,1>.
+// Shared-memory position (in double2 units) of chunk block i: blocks are 32 bytes
+// apart with 16 more bytes after every 9 (the row length of a structured p = 1
+// mesh), so the 32 lanes' rows start in different banks; a function of i alone,
+// so the streaming store needs no row lookup.
+__device__ __forceinline__ int acc_pos(int i) { return 2 * i + i / 9; }
+constexpr int kAccUnits = 2 * kRowChunkBlocks + kRowChunkBlocks / 9 + 1;  // double2 per warp
+
+// One chunk c of mesh M, by the calling warp; acc is the warp's kAccUnits double2
+// of shared memory.  NP, NM: the 1D basis values at the Gauss point on the node's
+// own side / the opposite side, fma(0.5, g, 0.5) and fma(-0.5, g, 0.5) as in
+// lagrangePoly1dDeriv<double,1>.  For the bilinear element the xi-column of
+// J = sum_b x_b (x) dN_b depends on the point's eta only and the eta-column on its
+// xi only: with the edge vectors e0 = x1 - x0, e1 = x3 - x2, f0 = x2 - x0,
+// f1 = x3 - x1, dx/dxi(qy) = (NP e_qy + NM e_(1-qy)) / 2 and
+// dx/deta(qx) = (NP f_qx + NM f_(1-qx)) / 2 (likewise for the states).
 template <int MODE>
 __device__ __forceinline__ void row_chunk(const AsmArgs &M, int64_t c, double2 *acc, int lane, double NP, double NM) {
   const int r0 = __ldg(M.rowChunk + c), r1 = __ldg(M.rowChunk + c + 1);
   const int blk0 = __ldg(M.rowp + r0), nb = __ldg(M.rowp + r1) - blk0;
-  for (int i = lane; i < 2 * nb; i += 32) acc[i] = make_double2(0.0, 0.0);
+  if constexpr ((MODE & kJac) != 0) {
+    for (int i = lane; i < nb; i += 32) {
+      acc[acc_pos(i)] = make_double2(0.0, 0.0);
+      acc[acc_pos(i) + 1] = make_double2(0.0, 0.0);
+    }
+  }
   __syncwarp();
   const double mu = M.mu, lam = M.lam, thick = M.t, c11 = lam + 2.0 * mu;
+  const double hP = 0.5 * NP, hM = 0.5 * NM;
+  const int2 *rowElem = reinterpret_cast<const int2 *>(M.rowElem);
+  const int4 *conn4 = reinterpret_cast<const int4 *>(M.connList);
+  const double2 *X2 = reinterpret_cast<const double2 *>(M.coords);
+  const double2 *U2 = reinterpret_cast<const double2 *>(M.states);
   const int r = r0 + lane;
   double rx = 0.0, ry = 0.0;
   if (r < r1) {
     const int base = __ldg(M.rowp + r) - blk0;
-    const int j1 = __ldg(M.rowElemPtr + r + 1);
-    for (int j = __ldg(M.rowElemPtr + r); j < j1; j++) {
-      const int2 en = __ldg(reinterpret_cast<const int2 *>(M.rowElem) + j);
-      const int k = en.x >> 2, a = en.x & 3;
-      const int4 nd = __ldg(reinterpret_cast<const int4 *>(M.connList) + k);
-      const int node[4] = {nd.x, nd.y, nd.z, nd.w};
-      double2 x[4], u[4];
-#pragma unroll
-      for (int b = 0; b < 4; b++) {
-        x[b] = __ldg(reinterpret_cast<const double2 *>(M.coords) + node[b]);
-        u[b] = __ldg(reinterpret_cast<const double2 *>(M.states) + node[b]);
+    const int j0 = __ldg(M.rowElemPtr + r), j1 = __ldg(M.rowElemPtr + r + 1);
+    // software pipeline: nodal data of entry j in x/u, header of j+1 in enN/ndN
+    int2 enC = make_int2(0, 0), enN = make_int2(0, 0);
+    int4 ndN = make_int4(0, 0, 0, 0);
+    double2 x[4], u[4];
+    if (j0 < j1) {
+      enC = __ldg(rowElem + j0);
+      const int4 nd = __ldg(conn4 + (enC.x >> 2));
+      x[0] = __ldg(X2 + nd.x), x[1] = __ldg(X2 + nd.y), x[2] = __ldg(X2 + nd.z), x[3] = __ldg(X2 + nd.w);
+      u[0] = __ldg(U2 + nd.x), u[1] = __ldg(U2 + nd.y), u[2] = __ldg(U2 + nd.z), u[3] = __ldg(U2 + nd.w);
+    }
+    if (j0 + 1 < j1) {
+      enN = __ldg(rowElem + j0 + 1);
+      ndN = __ldg(conn4 + (enN.x >> 2));
+    }
+    for (int j = j0; j < j1; j++) {
+      // J and grad-u columns at the two eta (xi-derivative) and two xi (eta-derivative) values
+      double2 Jxi[2], Jeta[2], Uxi[2], Ueta[2];
+      {
+        const double2 e0 = make_double2(x[1].x - x[0].x, x[1].y - x[0].y);
+        const double2 e1 = make_double2(x[3].x - x[2].x, x[3].y - x[2].y);
+        const double2 f0 = make_double2(x[2].x - x[0].x, x[2].y - x[0].y);
+        const double2 f1 = make_double2(x[3].x - x[1].x, x[3].y - x[1].y);
+        const double2 a0 = make_double2(u[1].x - u[0].x, u[1].y - u[0].y);
+        const double2 a1 = make_double2(u[3].x - u[2].x, u[3].y - u[2].y);
+        const double2 b0 = make_double2(u[2].x - u[0].x, u[2].y - u[0].y);
+        const double2 b1 = make_double2(u[3].x - u[1].x, u[3].y - u[1].y);
+        Jxi[0] = make_double2(hP * e0.x + hM * e1.x, hP * e0.y + hM * e1.y);
+        Jxi[1] = make_double2(hM * e0.x + hP * e1.x, hM * e0.y + hP * e1.y);
+        Jeta[0] = make_double2(hP * f0.x + hM * f1.x, hP * f0.y + hM * f1.y);
+        Jeta[1] = make_double2(hM * f0.x + hP * f1.x, hM * f0.y + hP * f1.y);
+        Uxi[0] = make_double2(hP * a0.x + hM * a1.x, hP * a0.y + hM * a1.y);
+        Uxi[1] = make_double2(hM * a0.x + hP * a1.x, hM * a0.y + hP * a1.y);
+        Ueta[0] = make_double2(hP * b0.x + hM * b1.x, hP * b0.y + hM * b1.y);
+        Ueta[1] = make_double2(hM * b0.x + hP * b1.x, hM * b0.y + hP * b1.y);
       }
-      double K[4][4];
+      const int2 en = enC;
+      // prefetch: nodal data of entry j+1, header of entry j+2
+      if (j + 1 < j1) {
+        x[0] = __ldg(X2 + ndN.x), x[1] = __ldg(X2 + ndN.y), x[2] = __ldg(X2 + ndN.z), x[3] = __ldg(X2 + ndN.w);
+        u[0] = __ldg(U2 + ndN.x), u[1] = __ldg(U2 + ndN.y), u[2] = __ldg(U2 + ndN.z), u[3] = __ldg(U2 + ndN.w);
+        enC = enN;
+      }
+      if (j + 2 < j1) {
+        enN = __ldg(rowElem + j + 2);
+        ndN = __ldg(conn4 + (enN.x >> 2));
+      }
+      const int a = en.x & 3, ax = a & 1, ay = a >> 1;
+      double Mm[4][4];  // sum_q s G_ai G_bj per column node b: [b][xx, xy, yx, yy]
 #pragma unroll
-      for (int b = 0; b < 4; b++) K[b][0] = K[b][1] = K[b][2] = K[b][3] = 0.0;
+      for (int b = 0; b < 4; b++) Mm[b][0] = Mm[b][1] = Mm[b][2] = Mm[b][3] = 0.0;
 #pragma unroll
       for (int q = 0; q < 4; q++) {
         const int qx = q & 1, qy = q >> 1;
-        // tabulated derivatives of node b = by*2+bx at point q = qy*2+qx (weights are 1)
-        double dxi[4], deta[4];
-#pragma unroll
-        for (int b = 0; b < 4; b++) {
-          const int bx = b & 1, by = b >> 1;
-          dxi[b] = (by == qy ? NP : NM) * (bx ? 0.5 : -0.5);
-          deta[b] = (bx == qx ? NP : NM) * (by ? 0.5 : -0.5);
-        }
-        double j00 = 0, j01 = 0, j10 = 0, j11 = 0, g00 = 0, g01 = 0, g10 = 0, g11 = 0;
-#pragma unroll
-        for (int b = 0; b < 4; b++) {
-          j00 = fma(x[b].x, dxi[b], j00);
-          j01 = fma(x[b].x, deta[b], j01);
-          j10 = fma(x[b].y, dxi[b], j10);
-          j11 = fma(x[b].y, deta[b], j11);
-          g00 = fma(u[b].x, dxi[b], g00);
-          g01 = fma(u[b].x, deta[b], g01);
-          g10 = fma(u[b].y, dxi[b], g10);
-          g11 = fma(u[b].y, deta[b], g11);
-        }
+        const double j00 = Jxi[qy].x, j10 = Jxi[qy].y, j01 = Jeta[qx].x, j11 = Jeta[qx].y;
+        const double g00 = Uxi[qy].x, g10 = Uxi[qy].y, g01 = Ueta[qx].x, g11 = Ueta[qx].y;
         const double det = j00 * j11 - j01 * j10;
         const double inv = 1.0 / det;
         const double i00 = j11 * inv, i01 = -j01 * inv, i10 = -j10 * inv, i11 = j00 * inv;
-        const double st = det * thick;
+        const double st = det * thick;  // the 2x2 Gauss weights are 1
         const double uxx = g00 * i00 + g01 * i10, uxy = g00 * i01 + g01 * i11;
         const double uyx = g10 * i00 + g11 * i10, uyy = g10 * i01 + g11 * i11;
         const double tr = uxx + uyy;
@@ -95,31 +134,37 @@ __device__ __forceinline__ void row_chunk(const AsmArgs &M, int64_t c, double2 *
         double gx[4], gy[4];
 #pragma unroll
         for (int b = 0; b < 4; b++) {
-          gx[b] = dxi[b] * i00 + deta[b] * i10;
-          gy[b] = dxi[b] * i01 + deta[b] * i11;
+          const int bx = b & 1, by = b >> 1;
+          const double dxi = (by == qy ? hP : hM) * (bx ? 1.0 : -1.0);
+          const double deta = (bx == qx ? hP : hM) * (by ? 1.0 : -1.0);
+          gx[b] = dxi * i00 + deta * i10;
+          gy[b] = dxi * i01 + deta * i11;
         }
-        const double gax = a == 0 ? gx[0] : a == 1 ? gx[1] : a == 2 ? gx[2] : gx[3];
-        const double gay = a == 0 ? gy[0] : a == 1 ? gy[1] : a == 2 ? gy[2] : gy[3];
-        const double hx = st * gax, hy = st * gay;
+        // the row node's own gradient, from its tabulated derivatives
+        const double dxa = (ay == qy ? hP : hM) * (ax ? 1.0 : -1.0);
+        const double dea = (ax == qx ? hP : hM) * (ay ? 1.0 : -1.0);
+        const double hx = st * (dxa * i00 + dea * i10), hy = st * (dxa * i01 + dea * i11);
         rx = fma(hx, sxx, fma(hy, sxy, rx));
         ry = fma(hx, sxy, fma(hy, syy, ry));
 #pragma unroll
         for (int b = 0; b < 4; b++) {
-          const double mxx = hx * gx[b], mxy = hx * gy[b], myx = hy * gx[b], myy = hy * gy[b];
-          K[b][0] += c11 * mxx + mu * myy;
-          K[b][1] += lam * mxy + mu * myx;
-          K[b][2] += lam * myx + mu * mxy;
-          K[b][3] += c11 * myy + mu * mxx;
+          Mm[b][0] = fma(hx, gx[b], Mm[b][0]);
+          Mm[b][1] = fma(hx, gy[b], Mm[b][1]);
+          Mm[b][2] = fma(hy, gx[b], Mm[b][2]);
+          Mm[b][3] = fma(hy, gy[b], Mm[b][3]);
         }
       }
       if constexpr ((MODE & kJac) != 0) {
 #pragma unroll
         for (int b = 0; b < 4; b++) {
-          const int slot = base + ((en.y >> (8 * b)) & 0xff);
-          double2 *s = acc + 2 * slot;
-          const double2 p0 = s[0], p1 = s[1];
-          s[0] = make_double2(p0.x + K[b][0], p0.y + K[b][1]);
-          s[1] = make_double2(p1.x + K[b][2], p1.y + K[b][3]);
+          const double kxx = c11 * Mm[b][0] + mu * Mm[b][3];
+          const double kxy = lam * Mm[b][1] + mu * Mm[b][2];
+          const double kyx = lam * Mm[b][2] + mu * Mm[b][1];
+          const double kyy = c11 * Mm[b][3] + mu * Mm[b][0];
+          double2 *sp = acc + acc_pos(base + ((en.y >> (8 * b)) & 0xff));
+          const double2 p0 = sp[0], p1 = sp[1];
+          sp[0] = make_double2(p0.x + kxx, p0.y + kxy);
+          sp[1] = make_double2(p1.x + kyx, p1.y + kyy);
         }
       }
     }
@@ -131,7 +176,7 @@ __device__ __forceinline__ void row_chunk(const AsmArgs &M, int64_t c, double2 *
   if constexpr ((MODE & kJac) != 0) {
     double *dst = M.mat + 4 * (int64_t)blk0;
     for (int i = lane; i < nb; i += 32) {
-      const double2 p0 = acc[2 * i], p1 = acc[2 * i + 1];
+      const double2 p0 = acc[acc_pos(i)], p1 = acc[acc_pos(i) + 1];
       store_block(dst + 4 * i, p0.x, p0.y, p1.x, p1.y);
     }
   }
@@ -145,8 +190,8 @@ __device__ __forceinline__ void p1_basis(double &NP, double &NM) {
 
 // Single mesh: chunks [A.begin, A.begin + A.count), grid-stride over warps.
 template <int MODE>
-__global__ void __launch_bounds__(32 * kRowWarps) rows_p1_kernel(const __grid_constant__ AsmArgs A) {
-  __shared__ double2 acc[kRowWarps][2 * kRowChunkBlocks];
+__global__ void __launch_bounds__(32 * kRowWarps, 3) rows_p1_kernel(const __grid_constant__ AsmArgs A) {
+  __shared__ double2 acc[kRowWarps][kAccUnits];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double NP, NM;
   p1_basis(NP, NM);
@@ -156,10 +201,10 @@ __global__ void __launch_bounds__(32 * kRowWarps) rows_p1_kernel(const __grid_co
 }
 
 // Many meshes: warps pull tiles (mesh, `count` chunks from `begin`) from the queue.
-__global__ void __launch_bounds__(32 * kRowWarps) rows_p1_batched_kernel(const AsmArgs *__restrict__ meshes,
+__global__ void __launch_bounds__(32 * kRowWarps, 3) rows_p1_batched_kernel(const AsmArgs *__restrict__ meshes,
                                                                         const Tile *__restrict__ tiles, int ntiles,
                                                                         int *counter) {
-  __shared__ double2 acc[kRowWarps][2 * kRowChunkBlocks];
+  __shared__ double2 acc[kRowWarps][kAccUnits];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double NP, NM;
   p1_basis(NP, NM);
