@@ -215,13 +215,13 @@ def run_ours(args):
     # plan path (overwrite, no zeroing), FP64 and mixed
     for prec in [x for x in ("fp64", "mixed") if f"plan_{x}" in args.paths]:
         fn = (lambda prec=prec: plan.assemble(d.states, d.coords, E, nu, t, res, mat, precision=prec, stream=sptr))
-        ms, _ = time_steps(fn, max(2, args.steps // 2), args.warmup, plan.num_colours)
+        ms, _ = time_steps(fn, max(2, args.steps // 2), args.warmup, plan.launches())
         paths[f"plan_{prec}"] = {"ms": ms, "elements_per_s": nE / (ms * 1e-3)}
     # GreenStrainType::NONLINEAR (FP64), same mesh and states; not a candidate for the headline
     # (the reference's dispatch always assembles LINEAR)
     if "plan_nonlinear" in args.paths:
         fn = (lambda: plan.assemble(d.states, d.coords, E, nu, t, res, mat, strain="nonlinear", stream=sptr))
-        ms, _ = time_steps(fn, max(2, args.steps // 2), args.warmup, plan.num_colours)
+        ms, _ = time_steps(fn, max(2, args.steps // 2), args.warmup, plan.launches("nonlinear"))
         paths["plan_fp64_nonlinear"] = {"ms": ms, "elements_per_s": nE / (ms * 1e-3)}
     # error of the mixed plan path against the FP64 plan path (FP64 path is oracle-checked in tests)
     err_res = err_mat = float("inf")
@@ -270,7 +270,7 @@ def run_ours(args):
         plan.assemble(d.states, d.coords, E, nu, t, res, mat, precision=prec, stream=sptr)
 
     with ClockSampler(local) as clk:
-        ms, launches = time_steps(step, args.steps, args.warmup, plan.num_colours)
+        ms, launches = time_steps(step, args.steps, args.warmup, plan.launches())
     value = world * nE / (ms * 1e-3)
 
     # end to end through the public API: pinned host state -> device, assemble, residual -> pinned host
@@ -283,12 +283,20 @@ def run_ours(args):
         h_res.copy_(res, non_blocking=True)
 
     with torch.cuda.stream(stream):
-        ms_e2e, _ = time_steps(e2e_step, args.steps, args.warmup, plan.num_colours)
+        ms_e2e, _ = time_steps(e2e_step, args.steps, args.warmup, plan.launches())
     h2d, d2h = h_states.numel() * 8, h_res.numel() * 8
 
     hbm, peak_kind = peaks()
     abytes = algorithmic_bytes(mesh, nnzb)
     achieved = abytes / (ms * 1e-3) / 1e9
+    # FP64 side of the roofline: conventional element flops n_q (24 n^2 + 24 n + 40)
+    # (a 2x2 block of D^T B products per node pair plus the J / grad u / sigma / R
+    # work, no symmetry savings) against this GPU's FP64 tensor-core peak, probed live
+    import ctypes as C
+    nloc = (mesh.order + 1) ** 2
+    aflops = float(nE) * nloc * (24 * nloc * nloc + 24 * nloc + 40)
+    fp64_peak = C.c_double()
+    fem.check(fem.lib.fem_probe_peak(2, C.byref(fp64_peak)), "fem_probe_peak")
     line = {
         "metric": "assembled elements/s (res+Jac)", "value": value, "unit": "elements/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -300,7 +308,14 @@ def run_ours(args):
         "paths": paths,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": None, "peak_kind": peak_kind, "algorithmic_bytes_per_step": abytes,
-                     "kernel": f"assemble_kernel<{mesh.order}> x {plan.num_colours} colour launches per step"},
+                     "kernel": (f"rows_p1_kernel, 1 launch per step" if plan.row_chunks > 0 else
+                                f"assemble_kernel<{mesh.order}> x {plan.num_colours} colour launches per step"),
+                     "fp64": {"algorithmic_flops_per_step": aflops,
+                              "achieved_tflops": aflops / (ms * 1e-3) / 1e12,
+                              "peak_tflops": fp64_peak.value, "peak_kind": "measured (FP64 MMA probe)",
+                              "frac": aflops / (ms * 1e-3) / 1e12 / fp64_peak.value,
+                              "max_bound_frac": max(abytes / (hbm * 1e9), aflops / (fp64_peak.value * 1e12))
+                              / (ms * 1e-3)}},
         "gpu_launches": launches,
         "clocks": clk.summary(),
         "e2e": {"value": world * nE / (ms_e2e * 1e-3), "unit": "elements/s", "h2d_bytes_per_step": h2d,

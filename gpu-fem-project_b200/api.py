@@ -161,6 +161,13 @@ class Plan:
               "fem_plan_info")
         self.num_nodes, self.num_elements, self.nnzb = nn.value, ne.value, nnzb.value
         self.num_colours, self.device_bytes = nc.value, nbytes.value
+        rc = C.c_int()
+        check(lib.fem_plan_row_chunks(self._h, C.byref(rc)), "fem_plan_row_chunks")
+        self.row_chunks = rc.value
+
+    def launches(self, strain="linear") -> int:
+        """Kernel launches of one assemble(): 1 for order-1 row assembly, else one per colour."""
+        return 1 if self.row_chunks > 0 and _strain(strain) == FEM_STRAIN_LINEAR else self.num_colours
 
     @property
     def handle(self) -> int:

@@ -278,6 +278,13 @@ int fem_plan_info(const fem_plan *plan, int *numNodes, int *numElements, int64_t
   return FEM_SUCCESS;
 }
 
+int fem_plan_row_chunks(const fem_plan *plan, int *numChunks) {
+  fem::clear_error();
+  if (!plan || !numChunks) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "NULL argument");
+  *numChunks = plan->numChunks;
+  return FEM_SUCCESS;
+}
+
 int fem_plan_get_pattern(const fem_plan *plan, int *rowp, int *cols) {
   fem::clear_error();
   if (!plan || !rowp || !cols) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "NULL argument");

@@ -145,6 +145,9 @@ int fem_plan_info(const fem_plan *plan, int *numNodes, int *numElements, int64_t
                   int64_t *deviceBytes);
 /* Copy the plan's BSR pattern to host arrays (rowp: numNodes+1, cols: nnzb). */
 int fem_plan_get_pattern(const fem_plan *plan, int *rowp, int *cols);
+/* Row chunks of an order-1 plan: > 0 when its LINEAR assembly runs as row
+ * assembly (one launch, each block row written once), 0 when it runs by colours. */
+int fem_plan_row_chunks(const fem_plan *plan, int *numChunks);
 /* Device pointers of the plan's rowp/cols (owned by the plan). */
 int fem_plan_device_pattern(const fem_plan *plan, const int **rowp, const int **cols);
 /* states/nodeCoords/residual/matEntries are device pointers; residual or
