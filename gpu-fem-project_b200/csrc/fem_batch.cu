@@ -48,8 +48,12 @@ int launch_batched_t(int p, const dev::AsmArgs *meshes, const dev::Tile *tiles, 
                      cudaStream_t s) {
   switch (p) {
     case 1: return launch_batched_p<1, T>(meshes, tiles, ntiles, counter, s);
-    case 2: return launch_batched_p<2, T>(meshes, tiles, ntiles, counter, s);
-    case 3: return launch_batched_p<3, T>(meshes, tiles, ntiles, counter, s);
+    case 2:
+      if constexpr (sizeof(T) == 8) return fail(FEM_ERR_INVALID_ORDER, "order 2 FP64 runs the fragment kernel");
+      else return launch_batched_p<2, T>(meshes, tiles, ntiles, counter, s);
+    case 3:
+      if constexpr (sizeof(T) == 8) return fail(FEM_ERR_INVALID_ORDER, "order 3 FP64 runs the fragment kernel");
+      else return launch_batched_p<3, T>(meshes, tiles, ntiles, counter, s);
     case 4: return launch_batched_p<4, T>(meshes, tiles, ntiles, counter, s);
     default: return fail(FEM_ERR_INVALID_ORDER, "order %d", p);
   }
@@ -59,6 +63,9 @@ int launch_batched_t(int p, const dev::AsmArgs *meshes, const dev::Tile *tiles, 
 
 int launch_batched(int p, int precision, const dev::AsmArgs *meshes, const dev::Tile *tiles, int ntiles, int *counter,
                    cudaStream_t s) {
+  // the same kernel as the single-mesh plan path, so batched results equal lone ones bit for bit
+  if (frag_supported(p, precision, FEM_STRAIN_LINEAR))
+    return launch_frag_batched(p, meshes, tiles, ntiles, counter, s);
   if (precision == FEM_PRECISION_FP64) return launch_batched_t<double>(p, meshes, tiles, ntiles, counter, s);
   if (precision == FEM_PRECISION_MIXED) return launch_batched_t<float>(p, meshes, tiles, ntiles, counter, s);
   return fail(FEM_ERR_INVALID_ARGUMENT, "precision %d", precision);

@@ -276,7 +276,8 @@ struct Layout {
   static constexpr int NSTRESS = NL ? 4 : 3;  // weak stress components (first Piola: 4)
   static constexpr size_t tabT = 0;                     // double2 [NN][NQ]
   static constexpr size_t wq = tabT + 16 * NQ * NN;     // double  [NQ]
-  static constexpr size_t groups = align16(wq + 8 * NQ);
+  static constexpr size_t csum = align16(wq + 8 * NQ);  // double2 [NQ]: sum_a dN(a, q)
+  static constexpr size_t groups = align16(csum + 16 * NQ);
   // group-relative
   static constexpr size_t X = 0;                               // double2 [EPG][NN]
   static constexpr size_t U = X + 16 * EPG * NN;               // double2 [EPG][NN]
@@ -534,6 +535,22 @@ __device__ __forceinline__ void cta_prologue(unsigned char *smem) {
     tabT[a * NQ + q] = make_double2(__dmul_rn(Ny, dNx), __dmul_rn(Nx, dNy));
   }
   for (int q = threadIdx.x; q < NQ; q += blockDim.x) wq[q] = __dmul_rn(kGW[P][q % P1], kGW[P][q / P1]);
+  __syncthreads();
+  // sum_a dN(a, q): zero in exact arithmetic, a few ulp of the table entries in
+  // FP64; Neumaier-compensated sum of the table (error ~1e-30 absolute)
+  double2 *csum = reinterpret_cast<double2 *>(smem + L::csum);
+  for (int q = threadIdx.x; q < NQ; q += blockDim.x) {
+    double s0 = 0.0, c0 = 0.0, s1 = 0.0, c1 = 0.0;
+    for (int a = 0; a < NN; a++) {
+      const double2 d = tabT[a * NQ + q];
+      const double t0 = s0 + d.x, t1 = s1 + d.y;
+      c0 += fabs(s0) >= fabs(d.x) ? (s0 - t0) + d.x : (d.x - t0) + s0;
+      c1 += fabs(s1) >= fabs(d.y) ? (s1 - t1) + d.y : (d.y - t1) + s1;
+      s0 = t0;
+      s1 = t1;
+    }
+    csum[q] = make_double2(s0 + c0, s1 + c1);
+  }
   if constexpr (L::NL) {
     // padded kappa rows and node columns of GA/GB feed the MMA: zero once (the
     // quadrature stage writes only the real entries)
@@ -579,6 +596,7 @@ __device__ __forceinline__ void group_loop(unsigned char *smem, Src &src, const 
   using T2 = typename Vec2<T>::type;
   const double2 *tabT = reinterpret_cast<const double2 *>(smem + L::tabT);
   const double *wq = reinterpret_cast<const double *>(smem + L::wq);
+  const double2 *csum = reinterpret_cast<const double2 *>(smem + L::csum);
 
   const int g = threadIdx.x / GT, tg = threadIdx.x - g * GT;
   const int warp = tg >> 5, lane = tg & 31;
@@ -664,6 +682,9 @@ __device__ __forceinline__ void group_loop(unsigned char *smem, Src &src, const 
     // 1. quadrature points: NPART lanes per (element, q) split the node sums,
     //    every lane of the quad then forms J^-1 and the gradients of its nodes
     //    (their table entries stay in registers between the two loops).
+    //    J = sum_a x_a dN_a cancels by ~h/|x|, so the coordinates enter relative
+    //    to the element's node 0 (exact for nearby values) and x_0 sum_a dN_a is
+    //    added back: the same sum, evaluated without the cancellation.
     constexpr int MAXJ = (NN + NPART - 1) / NPART;
     for (int base = 0; base < EPG * NQ * NPART; base += GT) {
       const int i = base + tg;
@@ -671,6 +692,7 @@ __device__ __forceinline__ void group_loop(unsigned char *smem, Src &src, const 
       const int el = iq / NQ, q = iq - el * NQ;
       const bool act = i < EPG * NQ * NPART && el < ne;
       double j00 = 0, j01 = 0, j10 = 0, j11 = 0, g00 = 0, g01 = 0, g10 = 0, g11 = 0;
+      const double2 x0 = act ? X[el * NN] : make_double2(0.0, 0.0);
       double2 dt[MAXJ];
 #pragma unroll
       for (int j = 0; j < MAXJ; j++) {
@@ -679,7 +701,8 @@ __device__ __forceinline__ void group_loop(unsigned char *smem, Src &src, const 
         if (act && a < NN) {
           const double2 d = tabT[a * NQ + q];
           dt[j] = d;
-          const double2 x = X[el * NN + a], u = U[el * NN + a];
+          const double2 xa = X[el * NN + a], u = U[el * NN + a];
+          const double2 x = make_double2(xa.x - x0.x, xa.y - x0.y);
           j00 = fma(x.x, d.x, j00);
           j01 = fma(x.x, d.y, j01);
           j10 = fma(x.y, d.x, j10);
@@ -702,6 +725,11 @@ __device__ __forceinline__ void group_loop(unsigned char *smem, Src &src, const 
         g11 += __shfl_xor_sync(0xffffffffu, g11, o);
       }
       if (act) {
+        const double2 cs = csum[q];
+        j00 = fma(x0.x, cs.x, j00);
+        j01 = fma(x0.x, cs.y, j01);
+        j10 = fma(x0.y, cs.x, j10);
+        j11 = fma(x0.y, cs.y, j11);
         const double det = j00 * j11 - j01 * j10;
         const double inv = 1.0 / det;
         const double i00 = j11 * inv, i01 = -j01 * inv, i10 = -j10 * inv, i11 = j00 * inv;

@@ -1,0 +1,615 @@
+// Warp-fragment assembly kernel for plan-mode LINEAR FP64 assembly, orders 2 and 3.
+//
+// The element kernel in fem_device.cuh stages every element's coordinates,
+// states and scaled gradients in shared memory and reads them back for each
+// stage; at p = 3 that is ~400 shared-memory wavefronts per element and the
+// L1 data pipe, not HBM, bounds it.  Here a warp assembles two elements per
+// step and keeps their data in registers laid out as FP64 tensor-core
+// (mma.m8n8k4) fragments:
+//
+//   1. gather    lane (g, t) (g = lane/4, t = lane%4) loads component c = g%4
+//                (x, y, u, v) of node 4ks + t of element g/4: that register IS
+//                the A fragment of step 2 (rows = 2 elements x 4 components,
+//                k = element nodes).  Node ids are read two steps ahead, the
+//                coordinates/states one step ahead.
+//   2. J stage   C[(e,c)][(q,d)] = sum_a X[(e,c)][a] dN_d(a, q): the isoparametric
+//                Jacobian and the reference-space state gradient of both
+//                elements at every quadrature point (K4 x K4 MMAs), with the
+//                derivative table as B fragments (shared memory, lane order).
+//   3. transpose three xor-shuffle rounds give each lane all eight values of one
+//                quadrature point q = 4c + t of its element; it forms det J, J^-1,
+//                s = w det J t, the weak stress and sqrt|s| J^-1 (FP64), and
+//                stores the ~10 doubles of q to shared memory.
+//   4. fragments per element, lane (g, t) builds G-hat_i(q, a) = sqrt|s| (dN(a,q) J^-1)_i
+//                for q = 4ks + t and nodes a = 8T + pi(g), pi(g) = 4(g%2) + g/2,
+//                component i: K4 x NTN x 2 doubles, the A and B fragments of the
+//                stiffness product.
+//   5. residual  R_(a,i) = sum_q sum_j G-hat_j S-hat_ij on the FP64 pipe, reduced over
+//                the four lanes of a node by two shuffle rounds; one double2
+//                store (first writer) or two reductions per node.
+//   6. stiffness component-major tiles M_ij[a][b] = sum_q s G_ai G_bj (node tiles
+//                TA <= TB, four (i, j) tiles sharing fragments): lane (g, t) ends
+//                with the WHOLE 2x2 block (a = 8TA + pi(g), b = 8TB + 4h + t),
+//                h = 0, 1, so the plane-stress combination needs no shuffle and
+//                each warp store writes eight runs of four consecutive blocks
+//                (a BSR row holds an element grid row's nodes consecutively).
+//                Blocks of TA < TB tiles are also written transposed (K = K^T).
+//
+// Writes follow the plan codes: a launch is one colour; the first contributor of
+// a block stores it (one 256-bit store); a later colour adds its 2x2 block with
+// one asynchronous bulk reduction (cp.reduce.async.bulk .add.f64, 32 bytes staged
+// in shared memory) instead of four FP64 L2 atomics; residual rows add with
+// atomics (first writer stores).  The arithmetic is the
+// closed form of the reference's per-column forward AD (element/FEKernels.h:
+// 286-315, 884-976) that the element kernel documents.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "fem_common.h"
+#include "fem_device.cuh"
+#include "fem_launch.h"
+
+// Resident CTAs per SM the register budget is sized for: 3 (168 registers) at
+// p = 3, where the 12 live stiffness accumulators need them, 4 (128) at p = 2.
+#ifndef FEM_FRAG_MINB
+#define FEM_FRAG_MINB (P == 3 ? 3 : 4)
+#endif
+
+namespace fem {
+namespace dev {
+
+template <int P>
+struct FragDims {
+  static constexpr int P1 = P + 1, NN = P1 * P1, NQ = NN;
+  static constexpr int K4 = (NN + 3) / 4;   // node k-steps = quadrature k-steps = J column tiles
+  static constexpr int NQP = 4 * K4;        // padded quadrature points
+  static constexpr int NTN = (NN + 7) / 8;  // node tiles of the component-major stiffness product
+  static constexpr int CS = Dims<P>::CS;    // plan code record bytes per element
+  static constexpr int WARPS = 4;           // warps per CTA
+  static_assert(K4 <= 4 && NTN == 2, "fragment kernel: orders 2 and 3");
+};
+
+// Shared memory: CTA tables, then one region per warp.
+template <int P>
+struct FragLayout {
+  using F = FragDims<P>;
+  static constexpr int K4 = F::K4, NTN = F::NTN, NQP = F::NQP, NN = F::NN, CS = F::CS;
+  static constexpr size_t tabJ = 0;                          // double [K4][K4][32]
+  static constexpr size_t tabF = tabJ + 8 * K4 * K4 * 32;    // double2 [K4][NTN][32]
+  static constexpr size_t wq = tabF + 16 * K4 * NTN * 32;    // double [NQP]
+  static constexpr size_t csum = align16(wq + 8 * NQP);       // double2 [NQP]: sum_a dN(a, q)
+  static constexpr size_t warps = align16(csum + 16 * NQP);
+  // warp-relative; [2] = the two elements of the step
+  static constexpr size_t WI0 = 0;                 // double2 [2][NQP]: sqrt|s| (J^-1_0x, J^-1_1x)
+  static constexpr size_t WI1 = WI0 + 16 * 2 * NQP;  // double2 [2][NQP]: sqrt|s| (J^-1_0y, J^-1_1y)
+  static constexpr size_t WS0 = WI1 + 16 * 2 * NQP;  // double2 [2][NQP]: (S-hat_xx, S-hat_xy)
+  static constexpr size_t WS1 = WS0 + 16 * 2 * NQP;  // double2 [2][NQP]: (S-hat_xy, S-hat_yy)
+  static constexpr size_t SG = WS1 + 16 * 2 * NQP;   // double [2][NQP]: sign of s (0 on padding)
+  static constexpr size_t NID = SG + 8 * 2 * NQP;    // int [2][NN]: node ids
+  static constexpr size_t RB = align16(NID + 4 * 2 * NN);  // int [2][NN]: rowp[node]
+  static constexpr size_t STAGE = align16(RB + 4 * 2 * NN);  // [2 buffers][2 elements][CS] code records
+  static constexpr int NSLOT = 8;  // 2x2 blocks one lane writes per element
+  static constexpr size_t REDS = align16(STAGE + 2 * 2 * CS);  // double4 [NSLOT][32]: bulk-reduction sources
+  static constexpr size_t warp_bytes = align16(REDS + 32 * NSLOT * 32);
+  static constexpr size_t total = warps + F::WARPS * warp_bytes;
+};
+
+__device__ __forceinline__ double sel4(double x0, double x1, double x2, double x3, int i) {
+  return i == 0 ? x0 : (i == 1 ? x1 : (i == 2 ? x2 : x3));
+}
+
+template <int P>
+__device__ __forceinline__ void frag_prologue(unsigned char *smem) {
+  using F = FragDims<P>;
+  using L = FragLayout<P>;
+  constexpr int P1 = F::P1, NN = F::NN, NQ = F::NQ, K4 = F::K4, NTN = F::NTN;
+  double *tabJ = reinterpret_cast<double *>(smem + L::tabJ);
+  double2 *tabF = reinterpret_cast<double2 *>(smem + L::tabF);
+  double *wq = reinterpret_cast<double *>(smem + L::wq);
+  // dN(a, q) = (N_y dN_x, N_x dN_y) with the rounding of the element kernel's table
+  auto dN = [&](int a, int q) {
+    double Nx, dNx, Ny, dNy;
+    lag1d(P, kGX[P][q % P1], a % P1, Nx, dNx);
+    lag1d(P, kGX[P][q / P1], a / P1, Ny, dNy);
+    return make_double2(__dmul_rn(Ny, dNx), __dmul_rn(Nx, dNy));
+  };
+  // J-stage B fragments: lane (g, t) of (ks, tn) holds dN_{g%2}(a = 4ks + t, q = 4tn + g/2)
+  for (int i = threadIdx.x; i < K4 * K4 * 32; i += blockDim.x) {
+    const int lane = i & 31, blk = i >> 5, ks = blk / K4, tn = blk - ks * K4;
+    const int g = lane >> 2, t = lane & 3;
+    const int a = 4 * ks + t, q = 4 * tn + (g >> 1);
+    double v = 0.0;
+    if (a < NN && q < NQ) {
+      const double2 d = dN(a, q);
+      v = (g & 1) ? d.y : d.x;
+    }
+    tabJ[i] = v;
+  }
+  // stiffness fragments: lane (g, t) of (ks, T) holds dN(a = 8T + pi(g), q = 4ks + t)
+  for (int i = threadIdx.x; i < K4 * NTN * 32; i += blockDim.x) {
+    const int lane = i & 31, blk = i >> 5, ks = blk / NTN, T = blk - ks * NTN;
+    const int g = lane >> 2, t = lane & 3;
+    const int a = 8 * T + 4 * (g & 1) + (g >> 1), q = 4 * ks + t;
+    tabF[i] = (a < NN && q < NQ) ? dN(a, q) : make_double2(0.0, 0.0);
+  }
+  for (int q = threadIdx.x; q < F::NQP; q += blockDim.x)
+    wq[q] = q < NQ ? __dmul_rn(kGW[P][q % P1], kGW[P][q / P1]) : 0.0;
+  // sum_a dN(a, q): zero in exact arithmetic, a few ulp of the table entries in
+  // FP64; summed with Neumaier compensation (error ~1e-30 absolute)
+  double2 *csum = reinterpret_cast<double2 *>(smem + L::csum);
+  for (int q = threadIdx.x; q < F::NQP; q += blockDim.x) {
+    double s0 = 0.0, c0 = 0.0, s1 = 0.0, c1 = 0.0;
+    if (q < NQ) {
+      for (int a = 0; a < NN; a++) {
+        const double2 d = dN(a, q);
+        const double t0 = s0 + d.x, t1 = s1 + d.y;
+        c0 += fabs(s0) >= fabs(d.x) ? (s0 - t0) + d.x : (d.x - t0) + s0;
+        c1 += fabs(s1) >= fabs(d.y) ? (s1 - t1) + d.y : (d.y - t1) + s1;
+        s0 = t0;
+        s1 = t1;
+      }
+    }
+    csum[q] = make_double2(s0 + c0, s1 + c1);
+  }
+  __syncthreads();
+}
+
+// One 2x2 block of element `el` (staged codes / row bases in O): a 256-bit store
+// when this element is the block's first contributor, else a 32-byte bulk
+// reduction from `slot` (this lane's staging slot; the caller has waited for the
+// slot's previous bulk read).  `which` = 1 writes the transposed block (b, a).
+template <int P>
+__device__ __forceinline__ void frag_write(const Out &O, int el, int a, int b, int which, double kxx, double kxy,
+                                           double kyx, double kyy, double *slot) {
+  constexpr int NN = Dims<P>::NN, CS = Dims<P>::CS;
+  const int r0 = which ? b : a, c0 = which ? a : b;
+  const double v0 = kxx, v1 = which ? kyx : kxy, v2 = which ? kxy : kyx, v3 = kyy;
+  const uint8_t code = O.codes[el * CS + r0 * NN + c0];
+  double *blk = O.mat + 4 * ((int64_t)O.rbase[el * NN + r0] + (code & 0x7f));
+  if (code & 0x80) {
+    store_block(blk, v0, v1, v2, v3);
+  } else {
+    reinterpret_cast<double2 *>(slot)[0] = make_double2(v0, v1);
+    reinterpret_cast<double2 *>(slot)[1] = make_double2(v2, v3);
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(slot);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("cp.reduce.async.bulk.global.shared::cta.bulk_group.add.f64 [%0], [%1], 32;" ::"l"(blk), "r"(sa)
+                 : "memory");
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+  }
+}
+
+// The element pairs a warp assembles, in order.
+struct PairCursor {
+  int mesh;
+  int ne;  // 0 ends the warp's loop
+  int64_t k0;
+};
+
+// Single mesh: pairs p, p + stride, ... of list positions [begin, end).
+struct PairStride {
+  static constexpr bool kBatched = false;
+  int64_t begin, end, p, stride;
+  __device__ PairCursor next(int) {
+    PairCursor c{0, 0, begin + 2 * p};
+    if (c.k0 < end) c.ne = (int)min((int64_t)2, end - c.k0);
+    p += stride;
+    return c;
+  }
+};
+
+// Many meshes: the pairs of the tiles this warp pulls from the launch's queue
+// (one atomic counter per launch; tiles hold even element counts except at the
+// end of a colour range, so pairs never straddle tiles).
+struct PairQueue {
+  static constexpr bool kBatched = true;
+  const Tile *tiles;
+  int ntiles;
+  int *counter;
+  int mesh;
+  int64_t pos, tend;
+  bool done;
+  __device__ PairCursor next(int lane) {
+    PairCursor c{0, 0, 0};
+    while (!done && pos >= tend) {
+      int t = 0;
+      if (lane == 0) t = atomicAdd(counter, 1);
+      t = __shfl_sync(0xffffffffu, t, 0);
+      if (t >= ntiles) {
+        done = true;
+      } else {
+        const Tile tl = tiles[t];
+        mesh = tl.mesh;
+        pos = tl.begin;
+        tend = tl.begin + tl.count;
+      }
+    }
+    if (done) return c;
+    c.mesh = mesh;
+    c.k0 = pos;
+    c.ne = (int)min((int64_t)2, tend - pos);
+    pos += 2;
+    return c;
+  }
+};
+
+// One warp's assembly loop over the pairs its generator yields.  `single` is the
+// single-mesh kernel's argument block; batched generators read meshes[c.mesh].
+template <int P, int MODE, typename Gen>
+__device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const AsmArgs &single,
+                                          const AsmArgs *__restrict__ meshes) {
+  using F = FragDims<P>;
+  using L = FragLayout<P>;
+  constexpr int NN = F::NN, NQ = F::NQ, K4 = F::K4, NTN = F::NTN, NQP = F::NQP, CS = F::CS;
+  constexpr bool RES = (MODE & kRes) != 0, JAC = (MODE & kJac) != 0;
+  static_assert((MODE & kPlan) != 0 && (MODE & kNL) == 0, "plan mode, LINEAR strain");
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const int e_ld = g >> 2, c_ld = g & 3;  // element / component this lane gathers
+  const double *tabJ = reinterpret_cast<const double *>(smem + L::tabJ);
+  const double2 *tabF = reinterpret_cast<const double2 *>(smem + L::tabF);
+  const double *wqs = reinterpret_cast<const double *>(smem + L::wq);
+  const double2 *csum = reinterpret_cast<const double2 *>(smem + L::csum);
+  unsigned char *ws = smem + L::warps + warp * L::warp_bytes;
+  double2 *WI0 = reinterpret_cast<double2 *>(ws + L::WI0);
+  double2 *WI1 = reinterpret_cast<double2 *>(ws + L::WI1);
+  double2 *WS0 = reinterpret_cast<double2 *>(ws + L::WS0);
+  double2 *WS1 = reinterpret_cast<double2 *>(ws + L::WS1);
+  double *SGs = reinterpret_cast<double *>(ws + L::SG);
+  int *nid = reinterpret_cast<int *>(ws + L::NID);
+  int *rb = reinterpret_cast<int *>(ws + L::RB);
+  unsigned char *stage = ws + L::STAGE;
+  double *reds = reinterpret_cast<double *>(ws + L::REDS) + 4 * lane;  // slot j at reds + 128 j
+
+  auto args = [&](const PairCursor &c) -> const AsmArgs & {
+    if constexpr (Gen::kBatched) {
+      return meshes[c.mesh];
+    } else {
+      return single;
+    }
+  };
+  // node ids (two pairs ahead) and coordinate/state values (one pair ahead)
+  int nodeA[K4], nodeB[K4], rbB[K4];
+  double valB[K4];
+  auto load_nodes = [&](const PairCursor &c, int *node) {
+#pragma unroll
+    for (int ks = 0; ks < K4; ks++) {
+      const int a = 4 * ks + t;
+      node[ks] = (e_ld < c.ne && a < NN) ? __ldg(args(c).connList + (c.k0 + e_ld) * NN + a) : -1;
+    }
+  };
+  auto load_values = [&](const PairCursor &c, const int *node, double *val, int *rbv) {
+#pragma unroll
+    for (int ks = 0; ks < K4; ks++) {
+      val[ks] = 0.0;
+      rbv[ks] = 0;
+      if (node[ks] >= 0) {
+        const AsmArgs &M = args(c);
+        const double *src = c_ld < 2 ? M.coords : M.states;
+        val[ks] = __ldg(src + 2 * (int64_t)node[ks] + (c_ld & 1));
+        if (JAC && c_ld == 1) rbv[ks] = __ldg(M.rowp + node[ks]);
+      }
+    }
+  };
+  auto stage_codes = [&](const PairCursor &c, int buf) {
+    if (c.ne > 0) {
+      const unsigned char *src = args(c).blockCode + c.k0 * CS;
+      unsigned char *dst = stage + buf * 2 * CS;
+      for (int i = lane; i < c.ne * CS / 16; i += 32) cp_async16(dst + 16 * i, src + 16 * i);
+    }
+    cp_async_commit();
+  };
+
+  PairCursor cur = gen.next(lane);
+  PairCursor nxt = gen.next(lane);
+  load_nodes(cur, nodeB);
+  load_values(cur, nodeB, valB, rbB);
+  load_nodes(nxt, nodeA);
+  stage_codes(cur, 0);
+  int buf = 0;
+
+  for (; cur.ne > 0; buf ^= 1) {
+    const int ne = cur.ne;
+    const AsmArgs &M = args(cur);
+    const double mu = M.mu, lam = M.lam, thick = M.t, c11 = lam + 2.0 * mu;
+    // 0. commit this pair's gathered data
+    double val[K4];
+#pragma unroll
+    for (int ks = 0; ks < K4; ks++) {
+      val[ks] = valB[ks];
+      const int a = 4 * ks + t;
+      if (nodeB[ks] >= 0) {
+        if (c_ld == 0) nid[e_ld * NN + a] = nodeB[ks];
+        if (JAC && c_ld == 1) rb[e_ld * NN + a] = rbB[ks];
+      }
+    }
+    cp_async_wait_all();
+    __syncwarp();
+    // issue the following pairs' loads
+    const PairCursor nn2 = gen.next(lane);
+    stage_codes(nxt, buf ^ 1);
+#pragma unroll
+    for (int ks = 0; ks < K4; ks++) nodeB[ks] = nodeA[ks];
+    load_values(nxt, nodeB, valB, rbB);
+    load_nodes(nn2, nodeA);
+
+    // 1. J stage: cj[tn] = (d/dxi, d/deta) of component c_ld of element e_ld at q = 4tn + t.
+    //    J = sum_a x_a dN_a cancels by ~h/|x| (1e-4 on a 10x10 square of 1024^2
+    //    elements), so the coordinates enter relative to the element's node 0 (an
+    //    exact subtraction for nearby values) and x_0 sum_a dN_a is added back: the
+    //    same sum, evaluated without the cancellation.
+    const double xn0 = __shfl_sync(0xffffffffu, val[0], lane & ~3);
+    const double x0 = c_ld < 2 ? xn0 : 0.0;
+#pragma unroll
+    for (int ks = 0; ks < K4; ks++) val[ks] -= x0;
+    double cj[4][2];
+#pragma unroll
+    for (int tn = 0; tn < 4; tn++) cj[tn][0] = cj[tn][1] = 0.0;
+#pragma unroll
+    for (int ks = 0; ks < K4; ks++)
+#pragma unroll
+      for (int tn = 0; tn < K4; tn++) dmma(cj[tn][0], cj[tn][1], val[ks], tabJ[(ks * K4 + tn) * 32 + lane]);
+#pragma unroll
+    for (int tn = 0; tn < K4; tn++) {
+      const double2 cs = csum[4 * tn + t];
+      cj[tn][0] = fma(x0, cs.x, cj[tn][0]);
+      cj[tn][1] = fma(x0, cs.y, cj[tn][1]);
+    }
+
+    // 2. transpose: this lane takes quadrature point q = 4 c_ld + t of element e_ld
+    double own0 = sel4(cj[0][0], cj[1][0], cj[2][0], cj[3][0], c_ld);
+    double own1 = sel4(cj[0][1], cj[1][1], cj[2][1], cj[3][1], c_ld);
+    double rv[4][2];
+    rv[0][0] = own0;
+    rv[0][1] = own1;
+#pragma unroll
+    for (int r = 1; r < 4; r++) {
+      const int src = c_ld ^ r;
+      const double s0 = sel4(cj[0][0], cj[1][0], cj[2][0], cj[3][0], src);
+      const double s1 = sel4(cj[0][1], cj[1][1], cj[2][1], cj[3][1], src);
+      rv[r][0] = __shfl_xor_sync(0xffffffffu, s0, r << 2);
+      rv[r][1] = __shfl_xor_sync(0xffffffffu, s1, r << 2);
+    }
+    // component k of this quadrature point came from round k ^ c_ld
+    auto comp = [&](int k, int d) {
+      const int r = k ^ c_ld;
+      return d == 0 ? sel4(rv[0][0], rv[1][0], rv[2][0], rv[3][0], r) : sel4(rv[0][1], rv[1][1], rv[2][1], rv[3][1], r);
+    };
+    {
+      const int q = 4 * c_ld + t;
+      const bool valid = e_ld < ne && c_ld < K4 && q < NQ;
+      double2 wi0 = make_double2(0, 0), wi1 = make_double2(0, 0), ws0 = make_double2(0, 0), ws1 = make_double2(0, 0);
+      double sg = 0.0;
+      if (valid) {
+        const double j00 = comp(0, 0), j01 = comp(0, 1), j10 = comp(1, 0), j11 = comp(1, 1);
+        const double g00 = comp(2, 0), g01 = comp(2, 1), g10 = comp(3, 0), g11 = comp(3, 1);
+        const double det = j00 * j11 - j01 * j10;
+        const double inv = 1.0 / det;
+        const double i00 = j11 * inv, i01 = -j01 * inv, i10 = -j10 * inv, i11 = j00 * inv;
+        const double st = wqs[q] * det * thick;
+        const double rs = sqrt(fabs(st));
+        sg = st < 0.0 ? -1.0 : 1.0;
+        const double sw = sg * rs;
+        const double uxx = g00 * i00 + g01 * i10, uxy = g00 * i01 + g01 * i11;
+        const double uyx = g10 * i00 + g11 * i10, uyy = g10 * i01 + g11 * i11;
+        const double tr = uxx + uyy;
+        const double sxx = sw * (2.0 * mu * uxx + lam * tr);
+        const double sxy = sw * (mu * (uxy + uyx));
+        const double syy = sw * (2.0 * mu * uyy + lam * tr);
+        wi0 = make_double2(rs * i00, rs * i10);
+        wi1 = make_double2(rs * i01, rs * i11);
+        ws0 = make_double2(sxx, sxy);
+        ws1 = make_double2(sxy, syy);
+      }
+      if (c_ld < K4) {
+        const int o = e_ld * NQP + q;
+        WI0[o] = wi0;
+        WI1[o] = wi1;
+        WS0[o] = ws0;
+        WS1[o] = ws1;
+        SGs[o] = sg;
+      }
+    }
+    __syncwarp();
+
+    const Out O{M.mat, M.residual, stage + buf * 2 * CS, rb, nullptr};
+    constexpr int NPAIR = NTN * (NTN + 1) / 2;
+    const int pa = 4 * (g & 1) + (g >> 1);  // pi(g)
+    for (int el = 0; el < ne; el++) {
+      // 3.-5. quadrature k-steps outermost: per step each lane forms its fragments
+      // G-hat_i(q = 4ks + t, a = 8T + pi(g)), adds its residual partials and issues
+      // the 4 NPAIR independent stiffness MMAs of all node-tile pairs
+      double acc[NPAIR][4][2];
+      double rp[NTN][2];
+#pragma unroll
+      for (int k = 0; k < NPAIR; k++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) acc[k][c][0] = acc[k][c][1] = 0.0;
+#pragma unroll
+      for (int T = 0; T < NTN; T++) rp[T][0] = rp[T][1] = 0.0;
+#pragma unroll
+      for (int ks = 0; ks < K4; ks++) {
+        const int o = el * NQP + 4 * ks + t;
+        const double2 w0 = WI0[o], w1 = WI1[o];
+        const double sg = SGs[o];
+        double fr[NTN][2];
+#pragma unroll
+        for (int T = 0; T < NTN; T++) {
+          const double2 d = tabF[(ks * NTN + T) * 32 + lane];
+          fr[T][0] = fma(w0.x, d.x, w0.y * d.y);
+          fr[T][1] = fma(w1.x, d.x, w1.y * d.y);
+        }
+        if constexpr (RES) {
+          const double2 s0 = WS0[o], s1 = WS1[o];
+#pragma unroll
+          for (int T = 0; T < NTN; T++) {
+            rp[T][0] = fma(fr[T][0], s0.x, fma(fr[T][1], s1.x, rp[T][0]));
+            rp[T][1] = fma(fr[T][0], s0.y, fma(fr[T][1], s1.y, rp[T][1]));
+          }
+        }
+        if constexpr (JAC) {
+          int k = 0;
+#pragma unroll
+          for (int TA = 0; TA < NTN; TA++) {
+            const double a0 = sg * fr[TA][0], a1 = sg * fr[TA][1];
+#pragma unroll
+            for (int TB = TA; TB < NTN; TB++, k++) {
+              dmma(acc[k][0][0], acc[k][0][1], a0, fr[TB][0]);
+              dmma(acc[k][1][0], acc[k][1][1], a0, fr[TB][1]);
+              dmma(acc[k][2][0], acc[k][2][1], a1, fr[TB][0]);
+              dmma(acc[k][3][0], acc[k][3][1], a1, fr[TB][1]);
+            }
+          }
+        }
+      }
+      // residual: sum over the four lanes t of a node (reduce-scatter over node tiles)
+      if constexpr (RES) {
+        const int Tm = t >> 1, To = Tm ^ 1;
+        double sx = (Tm ? rp[1][0] : rp[0][0]) + __shfl_xor_sync(0xffffffffu, To ? rp[1][0] : rp[0][0], 2);
+        double sy = (Tm ? rp[1][1] : rp[0][1]) + __shfl_xor_sync(0xffffffffu, To ? rp[1][1] : rp[0][1], 2);
+        sx += __shfl_xor_sync(0xffffffffu, sx, 1);
+        sy += __shfl_xor_sync(0xffffffffu, sy, 1);
+        const int a = 8 * Tm + pa;
+        if ((t & 1) == 0 && a < NN) {
+          double *dst = M.residual + 2 * (int64_t)nid[el * NN + a];
+          if (O.codes[el * CS + NN * NN + a]) {
+            *reinterpret_cast<double2 *>(dst) = make_double2(sx, sy);
+          } else {
+            atomicAdd(dst, sx);
+            atomicAdd(dst + 1, sy);
+          }
+        }
+      }
+      // stiffness blocks: lane (g, t) holds (a = 8TA + pi(g), b = 8TB + 4h + t)
+      if constexpr (JAC) {
+        // the staging slots' previous bulk reads are complete before reuse
+        asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+        int k = 0, slot = 0;
+#pragma unroll
+        for (int TA = 0; TA < NTN; TA++) {
+#pragma unroll
+          for (int TB = TA; TB < NTN; TB++, k++) {
+            const int a = 8 * TA + pa;
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+              const int b = 8 * TB + 4 * h + t;
+              if (a < NN && b < NN) {
+                const double mxx = acc[k][0][h], mxy = acc[k][1][h], myx = acc[k][2][h], myy = acc[k][3][h];
+                const double kxx = c11 * mxx + mu * myy;
+                const double kxy = lam * mxy + mu * myx;
+                const double kyx = lam * myx + mu * mxy;
+                const double kyy = c11 * myy + mu * mxx;
+                frag_write<P>(O, el, a, b, 0, kxx, kxy, kyx, kyy, reds + 128 * slot++);
+                if (TA < TB) frag_write<P>(O, el, a, b, 1, kxx, kxy, kyx, kyy, reds + 128 * slot++);
+              }
+            }
+          }
+        }
+      }
+    }
+    __syncwarp();
+    cur = nxt;
+    nxt = nn2;
+  }
+  cp_async_wait_all();
+  // bulk reductions complete (shared-memory reads and global writes) before exit
+  asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+
+// Plan-mode assembly of one mesh's list positions [A.begin, A.begin + A.count) (one colour).
+template <int P, int MODE>
+__global__ void __launch_bounds__(32 * FragDims<P>::WARPS, FEM_FRAG_MINB) frag_kernel(const __grid_constant__ AsmArgs A) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  frag_prologue<P>(smem);
+  const int warp = threadIdx.x >> 5;
+  PairStride gen{A.begin, A.begin + A.count, (int64_t)blockIdx.x * FragDims<P>::WARPS + warp,
+                 (int64_t)gridDim.x * FragDims<P>::WARPS};
+  frag_loop<P, MODE>(smem, gen, A, nullptr);
+}
+
+// Many meshes of one order (one colour each): warps pull tiles from the launch's queue.
+template <int P>
+__global__ void __launch_bounds__(32 * FragDims<P>::WARPS, FEM_FRAG_MINB)
+    frag_batched_kernel(const AsmArgs *__restrict__ meshes, const Tile *__restrict__ tiles, int ntiles, int *counter) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  frag_prologue<P>(smem);
+  PairQueue gen{tiles, ntiles, counter, 0, 0, 0, false};
+  frag_loop<P, kPlan | kRes | kJac>(smem, gen, meshes[0], meshes);
+}
+
+template <int P, int MODE>
+int launch_frag_p(const AsmArgs &a, cudaStream_t s) {
+  using F = FragDims<P>;
+  constexpr int NT = 32 * F::WARPS;
+  auto kernel = frag_kernel<P, MODE>;
+  const size_t smem = FragLayout<P>::total;
+  LaunchInfo li;
+  int st = launch_info(kernel, NT, smem, li);
+  if (st) return st;
+  const int64_t pairs = (a.count + 1) / 2;
+  const int64_t need = (pairs + F::WARPS - 1) / F::WARPS;
+  const int64_t cap = (int64_t)li.grid_per_sm * li.num_sms;
+  const int grid = (int)(need < cap ? need : cap);
+  if (grid <= 0) return FEM_SUCCESS;
+  kernel<<<grid, NT, smem, s>>>(a);
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return cuda_fail(err, "frag_kernel launch");
+  return FEM_SUCCESS;
+}
+
+template <int P>
+int launch_frag_batched_p(const AsmArgs *meshes, const Tile *tiles, int ntiles, int *counter, cudaStream_t s) {
+  using F = FragDims<P>;
+  constexpr int NT = 32 * F::WARPS;
+  auto kernel = frag_batched_kernel<P>;
+  const size_t smem = FragLayout<P>::total;
+  LaunchInfo li;
+  int st = launch_info(kernel, NT, smem, li);
+  if (st) return st;
+  const int64_t need = (ntiles + F::WARPS - 1) / F::WARPS;
+  const int64_t cap = (int64_t)li.grid_per_sm * li.num_sms;
+  const int grid = (int)(need < cap ? need : cap);
+  if (grid <= 0) return FEM_SUCCESS;
+  kernel<<<grid, NT, smem, s>>>(meshes, tiles, ntiles, counter);
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return cuda_fail(err, "frag_batched_kernel launch");
+  return FEM_SUCCESS;
+}
+
+template <int MODE>
+int launch_frag_mode(int order, const AsmArgs &a, cudaStream_t s) {
+  switch (order) {
+    case 2: return launch_frag_p<2, MODE>(a, s);
+    case 3: return launch_frag_p<3, MODE>(a, s);
+    default: return fail(FEM_ERR_INVALID_ORDER, "fragment kernel: order %d", order);
+  }
+}
+
+}  // namespace dev
+
+bool frag_supported(int order, int precision, int strain) {
+  return (order == 2 || order == 3) && precision == FEM_PRECISION_FP64 && strain == FEM_STRAIN_LINEAR;
+}
+
+int launch_frag(int order, int mode, const dev::AsmArgs &a, cudaStream_t s) {
+  using namespace dev;
+  switch (mode) {
+    case kPlan | kRes: return launch_frag_mode<kPlan | kRes>(order, a, s);
+    case kPlan | kJac: return launch_frag_mode<kPlan | kJac>(order, a, s);
+    case kPlan | kRes | kJac: return launch_frag_mode<kPlan | kRes | kJac>(order, a, s);
+    default: return fail(FEM_ERR_INVALID_ARGUMENT, "fragment kernel: mode %d", mode);
+  }
+}
+
+int launch_frag_batched(int order, const dev::AsmArgs *meshes, const dev::Tile *tiles, int ntiles, int *counter,
+                        cudaStream_t s) {
+  switch (order) {
+    case 2: return dev::launch_frag_batched_p<2>(meshes, tiles, ntiles, counter, s);
+    case 3: return dev::launch_frag_batched_p<3>(meshes, tiles, ntiles, counter, s);
+    default: return fail(FEM_ERR_INVALID_ORDER, "fragment kernel: order %d", order);
+  }
+}
+
+}  // namespace fem

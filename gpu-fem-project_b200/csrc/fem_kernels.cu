@@ -339,11 +339,13 @@ int fem_plan_assemble_ex(const fem_plan *plan, const double *states, const doubl
     a.count = plan->numChunks;
     return fem::timed(s, elapsedSeconds, [&] { return fem::launch_rows(mode, a, s); });
   }
+  const bool frag = fem::frag_supported(plan->order, precision, strainType);
   return fem::timed(s, elapsedSeconds, [&] {
     for (int c = 0; c < plan->numColours; c++) {
       a.begin = plan->colourPtr[c];
       a.count = plan->colourPtr[c + 1] - plan->colourPtr[c];
-      int st = fem::launch(plan->order, precision, mode, a, s, strainType);
+      int st = frag ? fem::launch_frag(plan->order, mode, a, s)
+                    : fem::launch(plan->order, precision, mode, a, s, strainType);
       if (st) return st;
     }
     return (int)FEM_SUCCESS;

@@ -99,6 +99,13 @@ int launch_rows_batched(const dev::AsmArgs *meshes, const dev::Tile *tiles, int 
                         cudaStream_t s);
 // Chunks per row tile of the batched row kernel.
 constexpr int kRowTileChunks = 16;
+// Warp-fragment kernel (fem_frag.cu): plan-mode LINEAR FP64 assembly of one colour,
+// list positions [a.begin, a.begin + a.count), orders 2 and 3.
+bool frag_supported(int order, int precision, int strain);
+int launch_frag(int order, int mode, const dev::AsmArgs &a, cudaStream_t s);
+// Its tile-queue form for batches and the server (residual and Jacobian).
+int launch_frag_batched(int order, const dev::AsmArgs *meshes, const dev::Tile *tiles, int ntiles, int *counter,
+                        cudaStream_t s);
 
 inline void set_material(dev::AsmArgs &a, double E, double nu, double t) {
   // element/FEKernels.h:300-301
