@@ -70,11 +70,14 @@ struct FragDims {
   static_assert(K4 <= 4 && NTN == 2, "fragment kernel: orders 2 and 3");
 };
 
-// Shared memory: CTA tables, then one region per warp.
-template <int P>
+// Shared memory: CTA tables, then one region per warp.  DROP: drop-in mode (the
+// stage holds the reference element map rows, NN*NN ints per element, instead of
+// plan code records).
+template <int P, bool DROP = false>
 struct FragLayout {
   using F = FragDims<P>;
-  static constexpr int K4 = F::K4, NTN = F::NTN, NQP = F::NQP, NN = F::NN, CS = F::CS;
+  static constexpr int K4 = F::K4, NTN = F::NTN, NQP = F::NQP, NN = F::NN;
+  static constexpr int CS = DROP ? 4 * NN * NN : F::CS;  // staged bytes per element
   static constexpr size_t tabJ = 0;                          // double [K4][K4][32]
   static constexpr size_t tabF = tabJ + 8 * K4 * K4 * 32;    // double2 [K4][NTN][32]
   static constexpr size_t wq = tabF + 16 * K4 * NTN * 32;    // double [NQP]
@@ -180,6 +183,32 @@ __device__ __forceinline__ void frag_write(const Out &O, int el, int a, int b, i
   }
 }
 
+// Drop-in mode: element `el`'s 2x2 block added at the reference map's offset
+// (accumulate-into contract; elements of one launch share blocks), one 32-byte bulk
+// reduction when the block address is 16-byte aligned, else four FP64 atomics.
+template <int P>
+__device__ __forceinline__ void frag_add_mapped(const Out &O, int el, int a, int b, int which, double kxx,
+                                                double kxy, double kyx, double kyy, double *slot) {
+  constexpr int NN = Dims<P>::NN;
+  const int r0 = which ? b : a, c0 = which ? a : b;
+  const double v0 = kxx, v1 = which ? kyx : kxy, v2 = which ? kxy : kyx, v3 = kyy;
+  double *blk = O.mat + O.map[(el * NN + r0) * NN + c0];
+  if ((reinterpret_cast<uintptr_t>(blk) & 15u) == 0) {
+    reinterpret_cast<double2 *>(slot)[0] = make_double2(v0, v1);
+    reinterpret_cast<double2 *>(slot)[1] = make_double2(v2, v3);
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(slot);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("cp.reduce.async.bulk.global.shared::cta.bulk_group.add.f64 [%0], [%1], 32;" ::"l"(blk), "r"(sa)
+                 : "memory");
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+  } else {
+    atomicAdd(blk + 0, v0);
+    atomicAdd(blk + 1, v1);
+    atomicAdd(blk + 2, v2);
+    atomicAdd(blk + 3, v3);
+  }
+}
+
 // The element pairs a warp assembles, in order.
 struct PairCursor {
   int mesh;
@@ -239,11 +268,14 @@ struct PairQueue {
 template <int P, int MODE, typename Gen>
 __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const AsmArgs &single,
                                           const AsmArgs *__restrict__ meshes) {
+  constexpr bool PLAN = (MODE & kPlan) != 0;
   using F = FragDims<P>;
-  using L = FragLayout<P>;
+  using L = FragLayout<P, !PLAN>;
   constexpr int NN = F::NN, NQ = F::NQ, K4 = F::K4, NTN = F::NTN, NQP = F::NQP, CS = F::CS;
+  constexpr int STG = L::CS;  // staged bytes per element: plan code record or map rows
   constexpr bool RES = (MODE & kRes) != 0, JAC = (MODE & kJac) != 0;
-  static_assert((MODE & kPlan) != 0 && (MODE & kNL) == 0, "plan mode, LINEAR strain");
+  static_assert((MODE & kNL) == 0, "LINEAR strain");
+  static_assert(PLAN || !Gen::kBatched, "drop-in mode assembles one mesh");
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane >> 2, t = lane & 3;
@@ -277,7 +309,11 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
 #pragma unroll
     for (int ks = 0; ks < K4; ks++) {
       const int a = 4 * ks + t;
-      node[ks] = (e_ld < c.ne && a < NN) ? __ldg(args(c).connList + (c.k0 + e_ld) * NN + a) : -1;
+      if constexpr (PLAN) {
+        node[ks] = (e_ld < c.ne && a < NN) ? __ldg(args(c).connList + (c.k0 + e_ld) * NN + a) : -1;
+      } else {
+        node[ks] = (e_ld < c.ne && a < NN) ? __ldg(args(c).conn + __ldg(args(c).connPtr + c.k0 + e_ld) + a) : -1;
+      }
     }
   };
   auto load_values = [&](const PairCursor &c, const int *node, double *val, int *rbv) {
@@ -289,15 +325,25 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
         const AsmArgs &M = args(c);
         const double *src = c_ld < 2 ? M.coords : M.states;
         val[ks] = __ldg(src + 2 * (int64_t)node[ks] + (c_ld & 1));
-        if (JAC && c_ld == 1) rbv[ks] = __ldg(M.rowp + node[ks]);
+        if (PLAN && JAC && c_ld == 1) rbv[ks] = __ldg(M.rowp + node[ks]);
       }
     }
   };
   auto stage_codes = [&](const PairCursor &c, int buf) {
     if (c.ne > 0) {
-      const unsigned char *src = args(c).blockCode + c.k0 * CS;
-      unsigned char *dst = stage + buf * 2 * CS;
-      for (int i = lane; i < c.ne * CS / 16; i += 32) cp_async16(dst + 16 * i, src + 16 * i);
+      unsigned char *dst = stage + buf * 2 * STG;
+      if constexpr (PLAN) {
+        const unsigned char *src = args(c).blockCode + c.k0 * CS;
+        for (int i = lane; i < c.ne * CS / 16; i += 32) cp_async16(dst + 16 * i, src + 16 * i);
+      } else if constexpr (JAC) {
+        // element map rows: 16-byte copies when a row set is a multiple of 16 bytes
+        const int *src = args(c).map + c.k0 * NN * NN;
+        if ((NN * NN) % 4 == 0 && (reinterpret_cast<uintptr_t>(src) & 15u) == 0) {
+          for (int i = lane; i < c.ne * NN * NN / 4; i += 32) cp_async16(dst + 16 * i, src + 4 * i);
+        } else {
+          for (int i = lane; i < c.ne * NN * NN; i += 32) cp_async4(dst + 4 * i, src + i);
+        }
+      }
     }
     cp_async_commit();
   };
@@ -322,7 +368,7 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
       const int a = 4 * ks + t;
       if (nodeB[ks] >= 0) {
         if (c_ld == 0) nid[e_ld * NN + a] = nodeB[ks];
-        if (JAC && c_ld == 1) rb[e_ld * NN + a] = rbB[ks];
+        if (PLAN && JAC && c_ld == 1) rb[e_ld * NN + a] = rbB[ks];
       }
     }
     cp_async_wait_all();
@@ -414,7 +460,7 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
     }
     __syncwarp();
 
-    const Out O{M.mat, M.residual, stage + buf * 2 * CS, rb, nullptr};
+    const Out O{M.mat, M.residual, stage + buf * 2 * STG, rb, reinterpret_cast<const int *>(stage + buf * 2 * STG)};
     constexpr int NPAIR = NTN * (NTN + 1) / 2;
     const int pa = 4 * (g & 1) + (g >> 1);  // pi(g)
     for (int el = 0; el < ne; el++) {
@@ -474,7 +520,7 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
         const int a = 8 * Tm + pa;
         if ((t & 1) == 0 && a < NN) {
           double *dst = M.residual + 2 * (int64_t)nid[el * NN + a];
-          if (O.codes[el * CS + NN * NN + a]) {
+          if (PLAN && O.codes[el * CS + NN * NN + a]) {
             *reinterpret_cast<double2 *>(dst) = make_double2(sx, sy);
           } else {
             atomicAdd(dst, sx);
@@ -501,8 +547,13 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
                 const double kxy = lam * mxy + mu * myx;
                 const double kyx = lam * myx + mu * mxy;
                 const double kyy = c11 * myy + mu * mxx;
-                frag_write<P>(O, el, a, b, 0, kxx, kxy, kyx, kyy, reds + 128 * slot++);
-                if (TA < TB) frag_write<P>(O, el, a, b, 1, kxx, kxy, kyx, kyy, reds + 128 * slot++);
+                if constexpr (PLAN) {
+                  frag_write<P>(O, el, a, b, 0, kxx, kxy, kyx, kyy, reds + 128 * slot++);
+                  if (TA < TB) frag_write<P>(O, el, a, b, 1, kxx, kxy, kyx, kyy, reds + 128 * slot++);
+                } else {
+                  frag_add_mapped<P>(O, el, a, b, 0, kxx, kxy, kyx, kyy, reds + 128 * slot++);
+                  if (TA < TB) frag_add_mapped<P>(O, el, a, b, 1, kxx, kxy, kyx, kyy, reds + 128 * slot++);
+                }
               }
             }
           }
@@ -518,7 +569,8 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
   asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
 }
 
-// Plan-mode assembly of one mesh's list positions [A.begin, A.begin + A.count) (one colour).
+// One mesh: plan mode, list positions [A.begin, A.begin + A.count) of one colour;
+// drop-in mode, elements [A.begin, A.begin + A.count) through the reference map.
 template <int P, int MODE>
 __global__ void __launch_bounds__(32 * FragDims<P>::WARPS, FEM_FRAG_MINB) frag_kernel(const __grid_constant__ AsmArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -544,7 +596,7 @@ int launch_frag_p(const AsmArgs &a, cudaStream_t s) {
   using F = FragDims<P>;
   constexpr int NT = 32 * F::WARPS;
   auto kernel = frag_kernel<P, MODE>;
-  const size_t smem = FragLayout<P>::total;
+  const size_t smem = FragLayout<P, (MODE & kPlan) == 0>::total;
   LaunchInfo li;
   int st = launch_info(kernel, NT, smem, li);
   if (st) return st;
@@ -599,6 +651,9 @@ int launch_frag(int order, int mode, const dev::AsmArgs &a, cudaStream_t s) {
     case kPlan | kRes: return launch_frag_mode<kPlan | kRes>(order, a, s);
     case kPlan | kJac: return launch_frag_mode<kPlan | kJac>(order, a, s);
     case kPlan | kRes | kJac: return launch_frag_mode<kPlan | kRes | kJac>(order, a, s);
+    case kRes: return launch_frag_mode<kRes>(order, a, s);
+    case kJac: return launch_frag_mode<kJac>(order, a, s);
+    case kRes | kJac: return launch_frag_mode<kRes | kJac>(order, a, s);
     default: return fail(FEM_ERR_INVALID_ARGUMENT, "fragment kernel: mode %d", mode);
   }
 }

@@ -99,8 +99,9 @@ int launch_rows_batched(const dev::AsmArgs *meshes, const dev::Tile *tiles, int 
                         cudaStream_t s);
 // Chunks per row tile of the batched row kernel.
 constexpr int kRowTileChunks = 16;
-// Warp-fragment kernel (fem_frag.cu): plan-mode LINEAR FP64 assembly of one colour,
-// list positions [a.begin, a.begin + a.count), orders 2 and 3.
+// Warp-fragment kernel (fem_frag.cu): LINEAR FP64 assembly at orders 2 and 3, plan
+// mode (one colour, list positions [a.begin, a.begin + a.count)) or drop-in mode
+// (elements through the reference map, accumulate-into).
 bool frag_supported(int order, int precision, int strain);
 int launch_frag(int order, int mode, const dev::AsmArgs &a, cudaStream_t s);
 // Its tile-queue form for batches and the server (residual and Jacobian).
