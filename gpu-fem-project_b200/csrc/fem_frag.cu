@@ -36,10 +36,11 @@
 //                Blocks of TA < TB tiles are also written transposed (K = K^T).
 //
 // Writes follow the plan codes: a launch is one colour; the first contributor of
-// a block stores it (one 256-bit store); a later colour adds its 2x2 block with
-// one asynchronous bulk reduction (cp.reduce.async.bulk .add.f64, 32 bytes staged
-// in shared memory) instead of four FP64 L2 atomics; residual rows add with
-// atomics (first writer stores).  The arithmetic is the
+// a block stores it (one 256-bit store); a later colour adds its 2x2 blocks with
+// asynchronous bulk reductions (cp.reduce.async.bulk .add.f64 from shared memory,
+// one per run of four adjacent blocks) instead of four FP64 L2 atomics per block;
+// residual rows add with atomics (first writer stores).  Drop-in mode adds every
+// block the same way through the reference element map.  The arithmetic is the
 // closed form of the reference's per-column forward AD (element/FEKernels.h:
 // 286-315, 884-976) that the element kernel documents.
 #include <cuda_runtime.h>
@@ -92,7 +93,7 @@ struct FragLayout {
   static constexpr size_t NID = SG + 8 * 2 * NQP;    // int [2][NN]: node ids
   static constexpr size_t RB = align16(NID + 4 * 2 * NN);  // int [2][NN]: rowp[node]
   static constexpr size_t STAGE = align16(RB + 4 * 2 * NN);  // [2 buffers][2 elements][CS] code records
-  static constexpr int NSLOT = 8;  // 2x2 blocks one lane writes per element
+  static constexpr int NSLOT = 8;  // staging slots: 3 node-tile pairs x 2 halves, direct and transposed
   static constexpr size_t REDS = align16(STAGE + 2 * 2 * CS);  // double4 [NSLOT][32]: bulk-reduction sources
   static constexpr size_t warp_bytes = align16(REDS + 32 * NSLOT * 32);
   static constexpr size_t total = warps + F::WARPS * warp_bytes;
@@ -158,7 +159,103 @@ __device__ __forceinline__ void frag_prologue(unsigned char *smem) {
   __syncthreads();
 }
 
-// One 2x2 block of element `el` (staged codes / row bases in O): a 256-bit store
+// Staging slot of node-tile pair k (0: (0,0), 1: (0,1), 2: (1,1)), half h, and
+// direct (0) / transposed (1) blocks.
+__host__ __device__ constexpr int frag_slot(int k, int h, int w) { return k == 0 ? h : (k == 1 ? 2 + 2 * h + w : 6 + h); }
+
+// The block (a, b) of element el (or its transpose (b, a) with w = 1): plan mode
+// stores it when this element is its first contributor; otherwise (and in
+// drop-in mode always) it goes to its staging position for frag_issue_run.
+template <int P, bool PLAN>
+__device__ __forceinline__ void frag_put(const Out &O, int el, int a, int b, int w, double kxx, double kxy,
+                                         double kyx, double kyy, double *stg) {
+  constexpr int NN = Dims<P>::NN, CS = Dims<P>::CS;
+  const int r0 = w ? b : a, c0 = w ? a : b;
+  const double v0 = kxx, v1 = w ? kyx : kxy, v2 = w ? kxy : kyx, v3 = kyy;
+  if constexpr (PLAN) {
+    const uint8_t code = O.codes[el * CS + r0 * NN + c0];
+    if (code & 0x80) {
+      store_block(O.mat + 4 * ((int64_t)O.rbase[el * NN + r0] + (code & 0x7f)), v0, v1, v2, v3);
+      return;
+    }
+  }
+  reinterpret_cast<double2 *>(stg)[0] = make_double2(v0, v1);
+  reinterpret_cast<double2 *>(stg)[1] = make_double2(v2, v3);
+}
+
+__device__ __forceinline__ void bulk_add(double *gdst, const double *src, int bytes) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(src);
+  asm volatile("cp.reduce.async.bulk.global.shared::cta.bulk_group.add.f64 [%0], [%1], %2;" ::"l"(gdst), "r"(sa),
+               "r"(bytes)
+               : "memory");
+}
+
+// Run r of staging slot sl (see frag_slot): four blocks of one matrix row with four
+// consecutive element-local columns.  Blocks to add: drop-in, every valid block;
+// plan, the valid blocks whose code is not a first store.  One 128-byte reduction
+// when all four are added and adjacent in the matrix, else 32 bytes per block
+// (four FP64 atomics for a block whose address is not 16-byte aligned).
+template <int P, bool PLAN>
+__device__ __forceinline__ void frag_issue_run(const Out &O, int el, int sl, int r, const double *redsW) {
+  constexpr int NN = Dims<P>::NN, CS = Dims<P>::CS;
+  const int k = sl < 2 ? 0 : (sl < 6 ? 1 : 2);
+  const int h = sl < 2 ? sl : (sl < 6 ? (sl - 2) >> 1 : sl - 6);
+  const int w = (sl >= 2 && sl < 6) ? ((sl - 2) & 1) : 0;
+  const int TA = k == 2 ? 1 : 0, TB = k == 0 ? 0 : 1;
+  int row, col0, pos0;
+  if (w == 0) {
+    row = 8 * TA + 4 * (r & 1) + (r >> 1);  // pi(r)
+    col0 = 8 * TB + 4 * h;
+    pos0 = 4 * r;
+  } else {
+    const int tt = r >> 1, half = r & 1;
+    row = 8 * TB + 4 * h + tt;
+    col0 = 8 * TA + 4 * half;
+    pos0 = 8 * tt + 4 * half;
+  }
+  if (row >= NN) return;
+  double *dst[4];
+  bool add[4];
+  bool all = true, adj = true;
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const int col = col0 + j;
+    add[j] = col < NN;
+    dst[j] = O.mat;
+    if (add[j]) {
+      if constexpr (PLAN) {
+        const uint8_t code = O.codes[el * CS + row * NN + col];
+        add[j] = !(code & 0x80);
+        dst[j] = O.mat + 4 * ((int64_t)O.rbase[el * NN + row] + (code & 0x7f));
+      } else {
+        dst[j] = O.mat + O.map[(el * NN + row) * NN + col];
+      }
+    }
+    all = all && add[j];
+    if (j > 0) adj = adj && dst[j] == dst[0] + 4 * j;
+  }
+  const double *src = redsW + 128 * sl + 4 * pos0;
+  if (all && adj && (reinterpret_cast<uintptr_t>(dst[0]) & 15u) == 0) {
+    bulk_add(dst[0], src, 128);
+    return;
+  }
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    if (!add[j]) continue;
+    if ((reinterpret_cast<uintptr_t>(dst[j]) & 15u) == 0) {
+      bulk_add(dst[j], src + 4 * j, 32);
+    } else {
+      atomicAdd(dst[j] + 0, src[4 * j + 0]);
+      atomicAdd(dst[j] + 1, src[4 * j + 1]);
+      atomicAdd(dst[j] + 2, src[4 * j + 2]);
+      atomicAdd(dst[j] + 3, src[4 * j + 3]);
+    }
+  }
+}
+
+// Per-block writers (order 2, where four consecutive element-local nodes straddle
+// grid rows and row runs never merge).  One 2x2 block of element `el` (staged codes /
+// row bases in O): a 256-bit store
 // when this element is the block's first contributor, else a 32-byte bulk
 // reduction from `slot` (this lane's staging slot; the caller has waited for the
 // slot's previous bulk read).  `which` = 1 writes the transposed block (b, a).
@@ -274,6 +371,7 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
   constexpr int NN = F::NN, NQ = F::NQ, K4 = F::K4, NTN = F::NTN, NQP = F::NQP, CS = F::CS;
   constexpr int STG = L::CS;  // staged bytes per element: plan code record or map rows
   constexpr bool RES = (MODE & kRes) != 0, JAC = (MODE & kJac) != 0;
+  constexpr bool RUNS = (P == 3);  // order 3: staged row runs, one bulk reduction per adjacent run
   static_assert((MODE & kNL) == 0, "LINEAR strain");
   static_assert(PLAN || !Gen::kBatched, "drop-in mode assembles one mesh");
 
@@ -293,7 +391,7 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
   int *nid = reinterpret_cast<int *>(ws + L::NID);
   int *rb = reinterpret_cast<int *>(ws + L::RB);
   unsigned char *stage = ws + L::STAGE;
-  double *reds = reinterpret_cast<double *>(ws + L::REDS) + 4 * lane;  // slot j at reds + 128 j
+  double *redsW = reinterpret_cast<double *>(ws + L::REDS);  // staging slot s at redsW + 128 s
 
   auto args = [&](const PairCursor &c) -> const AsmArgs & {
     if constexpr (Gen::kBatched) {
@@ -528,11 +626,58 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
           }
         }
       }
-      // stiffness blocks: lane (g, t) holds (a = 8TA + pi(g), b = 8TB + 4h + t)
-      if constexpr (JAC) {
-        // the staging slots' previous bulk reads are complete before reuse
+      // stiffness blocks, order 3: lane (g, t) holds (a = 8TA + pi(g), b = 8TB + 4h + t).  Blocks that
+      // are added (drop-in: all; plan: later colours) are staged so that each row run of
+      // four consecutive columns is contiguous in shared memory -- slot s = (pair, h,
+      // direct/transposed), direct position 4g + t (row a, columns 8TB + 4h + 0..3),
+      // transposed position 8t + pi(g) (row b, columns 8TA + 4*half + 0..3) -- and then
+      // reduced with one 128-byte bulk operation per run whose four blocks are adjacent in
+      // the matrix, else one 32-byte operation per block.
+      if constexpr (JAC && RUNS) {
+        // every lane's previous bulk reads of the staging slots are complete
+        asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+        __syncwarp();
+        int k = 0;
+#pragma unroll
+        for (int TA = 0; TA < NTN; TA++) {
+#pragma unroll
+          for (int TB = TA; TB < NTN; TB++, k++) {
+            const int a = 8 * TA + pa;
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+              const int b = 8 * TB + 4 * h + t;
+              if (a < NN && b < NN) {
+                const double mxx = acc[k][0][h], mxy = acc[k][1][h], myx = acc[k][2][h], myy = acc[k][3][h];
+                const double kxx = c11 * mxx + mu * myy;
+                const double kxy = lam * mxy + mu * myx;
+                const double kyx = lam * myx + mu * mxy;
+                const double kyy = c11 * myy + mu * mxx;
+                const int s0 = frag_slot(k, h, 0);
+                frag_put<P, PLAN>(O, el, a, b, 0, kxx, kxy, kyx, kyy, redsW + 128 * s0 + 4 * (4 * g + t));
+                if (TA < TB) {
+                  const int s1 = frag_slot(k, h, 1);
+                  frag_put<P, PLAN>(O, el, a, b, 1, kxx, kxy, kyx, kyy, redsW + 128 * s1 + 4 * (8 * t + pa));
+                }
+              }
+            }
+          }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncwarp();
+        // 64 runs (8 slots x 8 runs), two per lane
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+          const int run = lane + 32 * u;
+          frag_issue_run<P, PLAN>(O, el, run >> 3, run & 7, redsW);
+        }
+        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+      }
+      // stiffness blocks, order 2: lane (g, t) holds (a = 8TA + pi(g), b = 8TB + 4h + t),
+      // each written (or added) on its own
+      if constexpr (JAC && !RUNS) {
         asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
         int k = 0, slot = 0;
+        double *reds = redsW + 4 * lane;
 #pragma unroll
         for (int TA = 0; TA < NTN; TA++) {
 #pragma unroll
