@@ -64,7 +64,7 @@ int launch_batched_t(int p, const dev::AsmArgs *meshes, const dev::Tile *tiles, 
 int launch_batched(int p, int precision, const dev::AsmArgs *meshes, const dev::Tile *tiles, int ntiles, int *counter,
                    cudaStream_t s) {
   // the same kernel as the single-mesh plan path, so batched results equal lone ones bit for bit
-  if (frag_supported(p, precision, FEM_STRAIN_LINEAR))
+  if (frag_supported(p, precision, FEM_STRAIN_LINEAR, true))
     return launch_frag_batched(p, meshes, tiles, ntiles, counter, s);
   if (precision == FEM_PRECISION_FP64) return launch_batched_t<double>(p, meshes, tiles, ntiles, counter, s);
   if (precision == FEM_PRECISION_MIXED) return launch_batched_t<float>(p, meshes, tiles, ntiles, counter, s);

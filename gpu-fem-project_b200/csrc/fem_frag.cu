@@ -52,9 +52,10 @@
 #include "fem_launch.h"
 
 // Resident CTAs per SM the register budget is sized for: 3 (168 registers) at
-// p = 3, where the 12 live stiffness accumulators need them, 4 (128) at p = 2.
+// p = 3, where the 12 live stiffness accumulators need them, and at p = 4; 4 (128)
+// at p = 2.
 #ifndef FEM_FRAG_MINB
-#define FEM_FRAG_MINB (P == 3 ? 3 : 4)
+#define FEM_FRAG_MINB (P == 2 ? 4 : 3)
 #endif
 
 namespace fem {
@@ -68,7 +69,14 @@ struct FragDims {
   static constexpr int NTN = (NN + 7) / 8;  // node tiles of the component-major stiffness product
   static constexpr int CS = Dims<P>::CS;    // plan code record bytes per element
   static constexpr int WARPS = 4;           // warps per CTA
-  static_assert(K4 <= 4 && NTN == 2, "fragment kernel: orders 2 and 3");
+  static constexpr int TG = (K4 + 3) / 4;   // transpose groups: quadrature points per lane
+  // Stiffness layout: component-major node tiles at p = 2, 3 (two tiles of 8 nodes),
+  // interleaved rows r = 2a + i at p = 4 (50 rows in seven tiles, where node tiles
+  // would pad 25 nodes to 32 and need 280 instead of 196 MMAs per element).
+  static constexpr bool IL = (P == 4);
+  static constexpr int NTAB = IL ? K4 : NTN;  // table tiles per k-step
+  static constexpr int TABW = IL ? 16 : 32;   // table entries per (k-step, tile): lane, or (g/2, t)
+  static_assert(P >= 2 && P <= 4 && (IL || NTN == 2), "fragment kernel: orders 2 to 4");
 };
 
 // Shared memory: CTA tables, then one region per warp.  DROP: drop-in mode (the
@@ -80,8 +88,8 @@ struct FragLayout {
   static constexpr int K4 = F::K4, NTN = F::NTN, NQP = F::NQP, NN = F::NN;
   static constexpr int CS = DROP ? 4 * NN * NN : F::CS;  // staged bytes per element
   static constexpr size_t tabJ = 0;                          // double [K4][K4][32]
-  static constexpr size_t tabF = tabJ + 8 * K4 * K4 * 32;    // double2 [K4][NTN][32]
-  static constexpr size_t wq = tabF + 16 * K4 * NTN * 32;    // double [NQP]
+  static constexpr size_t tabF = tabJ + 8 * K4 * K4 * 32;    // double2 [K4][NTAB][TABW]
+  static constexpr size_t wq = tabF + 16 * K4 * F::NTAB * F::TABW;  // double [NQP]
   static constexpr size_t csum = align16(wq + 8 * NQP);       // double2 [NQP]: sum_a dN(a, q)
   static constexpr size_t warps = align16(csum + 16 * NQP);
   // warp-relative; [2] = the two elements of the step
@@ -93,7 +101,9 @@ struct FragLayout {
   static constexpr size_t NID = SG + 8 * 2 * NQP;    // int [2][NN]: node ids
   static constexpr size_t RB = align16(NID + 4 * 2 * NN);  // int [2][NN]: rowp[node]
   static constexpr size_t STAGE = align16(RB + 4 * 2 * NN);  // [2 buffers][2 elements][CS] code records
-  static constexpr int NSLOT = 8;  // staging slots: 3 node-tile pairs x 2 halves, direct and transposed
+  // staging slots: p = 3, 3 node-tile pairs x 2 halves, direct and transposed; p = 2,
+  // the (at most 8) blocks one lane writes per element; p = 4, a ring of 4 per lane
+  static constexpr int NSLOT = F::IL ? 4 : 8;
   static constexpr size_t REDS = align16(STAGE + 2 * 2 * CS);  // double4 [NSLOT][32]: bulk-reduction sources
   static constexpr size_t warp_bytes = align16(REDS + 32 * NSLOT * 32);
   static constexpr size_t total = warps + F::WARPS * warp_bytes;
@@ -107,7 +117,7 @@ template <int P>
 __device__ __forceinline__ void frag_prologue(unsigned char *smem) {
   using F = FragDims<P>;
   using L = FragLayout<P>;
-  constexpr int P1 = F::P1, NN = F::NN, NQ = F::NQ, K4 = F::K4, NTN = F::NTN;
+  constexpr int P1 = F::P1, NN = F::NN, NQ = F::NQ, K4 = F::K4, NTAB = F::NTAB, TABW = F::TABW;
   double *tabJ = reinterpret_cast<double *>(smem + L::tabJ);
   double2 *tabF = reinterpret_cast<double2 *>(smem + L::tabF);
   double *wq = reinterpret_cast<double *>(smem + L::wq);
@@ -130,11 +140,19 @@ __device__ __forceinline__ void frag_prologue(unsigned char *smem) {
     }
     tabJ[i] = v;
   }
-  // stiffness fragments: lane (g, t) of (ks, T) holds dN(a = 8T + pi(g), q = 4ks + t)
-  for (int i = threadIdx.x; i < K4 * NTN * 32; i += blockDim.x) {
-    const int lane = i & 31, blk = i >> 5, ks = blk / NTN, T = blk - ks * NTN;
-    const int g = lane >> 2, t = lane & 3;
-    const int a = 8 * T + 4 * (g & 1) + (g >> 1), q = 4 * ks + t;
+  // stiffness fragments at (ks, T), q = 4ks + t: component-major, lane (g, t) holds
+  // dN(a = 8T + pi(g), q); interleaved, entry 4(g/2) + t holds dN(a = 4T + g/2, q)
+  for (int i = threadIdx.x; i < K4 * NTAB * TABW; i += blockDim.x) {
+    const int e = i % TABW, blk = i / TABW, ks = blk / NTAB, T = blk - ks * NTAB;
+    int a, q;
+    if constexpr (F::IL) {
+      a = 4 * T + (e >> 2);
+      q = 4 * ks + (e & 3);
+    } else {
+      const int g = e >> 2, t = e & 3;
+      a = 8 * T + 4 * (g & 1) + (g >> 1);
+      q = 4 * ks + t;
+    }
     tabF[i] = (a < NN && q < NQ) ? dN(a, q) : make_double2(0.0, 0.0);
   }
   for (int q = threadIdx.x; q < F::NQP; q += blockDim.x)
@@ -488,9 +506,10 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
     const double x0 = c_ld < 2 ? xn0 : 0.0;
 #pragma unroll
     for (int ks = 0; ks < K4; ks++) val[ks] -= x0;
-    double cj[4][2];
+    constexpr int TG = F::TG;
+    double cj[4 * TG][2];
 #pragma unroll
-    for (int tn = 0; tn < 4; tn++) cj[tn][0] = cj[tn][1] = 0.0;
+    for (int tn = 0; tn < 4 * TG; tn++) cj[tn][0] = cj[tn][1] = 0.0;
 #pragma unroll
     for (int ks = 0; ks < K4; ks++)
 #pragma unroll
@@ -502,28 +521,30 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
       cj[tn][1] = fma(x0, cs.y, cj[tn][1]);
     }
 
-    // 2. transpose: this lane takes quadrature point q = 4 c_ld + t of element e_ld
-    double own0 = sel4(cj[0][0], cj[1][0], cj[2][0], cj[3][0], c_ld);
-    double own1 = sel4(cj[0][1], cj[1][1], cj[2][1], cj[3][1], c_ld);
-    double rv[4][2];
-    rv[0][0] = own0;
-    rv[0][1] = own1;
+    // 2. transpose, per group m of four column tiles: this lane takes quadrature
+    //    point q = 4(4m + c_ld) + t of element e_ld
 #pragma unroll
-    for (int r = 1; r < 4; r++) {
-      const int src = c_ld ^ r;
-      const double s0 = sel4(cj[0][0], cj[1][0], cj[2][0], cj[3][0], src);
-      const double s1 = sel4(cj[0][1], cj[1][1], cj[2][1], cj[3][1], src);
-      rv[r][0] = __shfl_xor_sync(0xffffffffu, s0, r << 2);
-      rv[r][1] = __shfl_xor_sync(0xffffffffu, s1, r << 2);
-    }
-    // component k of this quadrature point came from round k ^ c_ld
-    auto comp = [&](int k, int d) {
-      const int r = k ^ c_ld;
-      return d == 0 ? sel4(rv[0][0], rv[1][0], rv[2][0], rv[3][0], r) : sel4(rv[0][1], rv[1][1], rv[2][1], rv[3][1], r);
-    };
-    {
-      const int q = 4 * c_ld + t;
-      const bool valid = e_ld < ne && c_ld < K4 && q < NQ;
+    for (int m = 0; m < TG; m++) {
+      double rv[4][2];
+      rv[0][0] = sel4(cj[4 * m][0], cj[4 * m + 1][0], cj[4 * m + 2][0], cj[4 * m + 3][0], c_ld);
+      rv[0][1] = sel4(cj[4 * m][1], cj[4 * m + 1][1], cj[4 * m + 2][1], cj[4 * m + 3][1], c_ld);
+#pragma unroll
+      for (int r = 1; r < 4; r++) {
+        const int src = c_ld ^ r;
+        const double s0 = sel4(cj[4 * m][0], cj[4 * m + 1][0], cj[4 * m + 2][0], cj[4 * m + 3][0], src);
+        const double s1 = sel4(cj[4 * m][1], cj[4 * m + 1][1], cj[4 * m + 2][1], cj[4 * m + 3][1], src);
+        rv[r][0] = __shfl_xor_sync(0xffffffffu, s0, r << 2);
+        rv[r][1] = __shfl_xor_sync(0xffffffffu, s1, r << 2);
+      }
+      // component k of this quadrature point came from round k ^ c_ld
+      auto comp = [&](int k, int d) {
+        const int r = k ^ c_ld;
+        return d == 0 ? sel4(rv[0][0], rv[1][0], rv[2][0], rv[3][0], r)
+                      : sel4(rv[0][1], rv[1][1], rv[2][1], rv[3][1], r);
+      };
+      const int tq = 4 * m + c_ld;  // column tile of this lane's quadrature point
+      const int q = 4 * tq + t;
+      const bool valid = e_ld < ne && tq < K4 && q < NQ;
       double2 wi0 = make_double2(0, 0), wi1 = make_double2(0, 0), ws0 = make_double2(0, 0), ws1 = make_double2(0, 0);
       double sg = 0.0;
       if (valid) {
@@ -547,7 +568,7 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
         ws0 = make_double2(sxx, sxy);
         ws1 = make_double2(sxy, syy);
       }
-      if (c_ld < K4) {
+      if (tq < K4) {
         const int o = e_ld * NQP + q;
         WI0[o] = wi0;
         WI1[o] = wi1;
@@ -559,145 +580,260 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
     __syncwarp();
 
     const Out O{M.mat, M.residual, stage + buf * 2 * STG, rb, reinterpret_cast<const int *>(stage + buf * 2 * STG)};
-    constexpr int NPAIR = NTN * (NTN + 1) / 2;
-    const int pa = 4 * (g & 1) + (g >> 1);  // pi(g)
-    for (int el = 0; el < ne; el++) {
-      // 3.-5. quadrature k-steps outermost: per step each lane forms its fragments
-      // G-hat_i(q = 4ks + t, a = 8T + pi(g)), adds its residual partials and issues
-      // the 4 NPAIR independent stiffness MMAs of all node-tile pairs
-      double acc[NPAIR][4][2];
-      double rp[NTN][2];
-#pragma unroll
-      for (int k = 0; k < NPAIR; k++)
-#pragma unroll
-        for (int c = 0; c < 4; c++) acc[k][c][0] = acc[k][c][1] = 0.0;
-#pragma unroll
-      for (int T = 0; T < NTN; T++) rp[T][0] = rp[T][1] = 0.0;
-#pragma unroll
-      for (int ks = 0; ks < K4; ks++) {
-        const int o = el * NQP + 4 * ks + t;
-        const double2 w0 = WI0[o], w1 = WI1[o];
-        const double sg = SGs[o];
-        double fr[NTN][2];
-#pragma unroll
-        for (int T = 0; T < NTN; T++) {
-          const double2 d = tabF[(ks * NTN + T) * 32 + lane];
-          fr[T][0] = fma(w0.x, d.x, w0.y * d.y);
-          fr[T][1] = fma(w1.x, d.x, w1.y * d.y);
-        }
-        if constexpr (RES) {
-          const double2 s0 = WS0[o], s1 = WS1[o];
-#pragma unroll
+    if constexpr (!F::IL) {
+      constexpr int NPAIR = NTN * (NTN + 1) / 2;
+      const int pa = 4 * (g & 1) + (g >> 1);  // pi(g)
+      for (int el = 0; el < ne; el++) {
+        // 3.-5. quadrature k-steps outermost: per step each lane forms its fragments
+        // G-hat_i(q = 4ks + t, a = 8T + pi(g)), adds its residual partials and issues
+        // the 4 NPAIR independent stiffness MMAs of all node-tile pairs
+        double acc[NPAIR][4][2];
+        double rp[NTN][2];
+  #pragma unroll
+        for (int k = 0; k < NPAIR; k++)
+  #pragma unroll
+          for (int c = 0; c < 4; c++) acc[k][c][0] = acc[k][c][1] = 0.0;
+  #pragma unroll
+        for (int T = 0; T < NTN; T++) rp[T][0] = rp[T][1] = 0.0;
+  #pragma unroll
+        for (int ks = 0; ks < K4; ks++) {
+          const int o = el * NQP + 4 * ks + t;
+          const double2 w0 = WI0[o], w1 = WI1[o];
+          const double sg = SGs[o];
+          double fr[NTN][2];
+  #pragma unroll
           for (int T = 0; T < NTN; T++) {
-            rp[T][0] = fma(fr[T][0], s0.x, fma(fr[T][1], s1.x, rp[T][0]));
-            rp[T][1] = fma(fr[T][0], s0.y, fma(fr[T][1], s1.y, rp[T][1]));
+            const double2 d = tabF[(ks * NTN + T) * 32 + lane];
+            fr[T][0] = fma(w0.x, d.x, w0.y * d.y);
+            fr[T][1] = fma(w1.x, d.x, w1.y * d.y);
           }
-        }
-        if constexpr (JAC) {
-          int k = 0;
-#pragma unroll
-          for (int TA = 0; TA < NTN; TA++) {
-            const double a0 = sg * fr[TA][0], a1 = sg * fr[TA][1];
-#pragma unroll
-            for (int TB = TA; TB < NTN; TB++, k++) {
-              dmma(acc[k][0][0], acc[k][0][1], a0, fr[TB][0]);
-              dmma(acc[k][1][0], acc[k][1][1], a0, fr[TB][1]);
-              dmma(acc[k][2][0], acc[k][2][1], a1, fr[TB][0]);
-              dmma(acc[k][3][0], acc[k][3][1], a1, fr[TB][1]);
+          if constexpr (RES) {
+            const double2 s0 = WS0[o], s1 = WS1[o];
+  #pragma unroll
+            for (int T = 0; T < NTN; T++) {
+              rp[T][0] = fma(fr[T][0], s0.x, fma(fr[T][1], s1.x, rp[T][0]));
+              rp[T][1] = fma(fr[T][0], s0.y, fma(fr[T][1], s1.y, rp[T][1]));
+            }
+          }
+          if constexpr (JAC) {
+            int k = 0;
+  #pragma unroll
+            for (int TA = 0; TA < NTN; TA++) {
+              const double a0 = sg * fr[TA][0], a1 = sg * fr[TA][1];
+  #pragma unroll
+              for (int TB = TA; TB < NTN; TB++, k++) {
+                dmma(acc[k][0][0], acc[k][0][1], a0, fr[TB][0]);
+                dmma(acc[k][1][0], acc[k][1][1], a0, fr[TB][1]);
+                dmma(acc[k][2][0], acc[k][2][1], a1, fr[TB][0]);
+                dmma(acc[k][3][0], acc[k][3][1], a1, fr[TB][1]);
+              }
             }
           }
         }
-      }
-      // residual: sum over the four lanes t of a node (reduce-scatter over node tiles)
-      if constexpr (RES) {
-        const int Tm = t >> 1, To = Tm ^ 1;
-        double sx = (Tm ? rp[1][0] : rp[0][0]) + __shfl_xor_sync(0xffffffffu, To ? rp[1][0] : rp[0][0], 2);
-        double sy = (Tm ? rp[1][1] : rp[0][1]) + __shfl_xor_sync(0xffffffffu, To ? rp[1][1] : rp[0][1], 2);
-        sx += __shfl_xor_sync(0xffffffffu, sx, 1);
-        sy += __shfl_xor_sync(0xffffffffu, sy, 1);
-        const int a = 8 * Tm + pa;
-        if ((t & 1) == 0 && a < NN) {
-          double *dst = M.residual + 2 * (int64_t)nid[el * NN + a];
-          if (PLAN && O.codes[el * CS + NN * NN + a]) {
-            *reinterpret_cast<double2 *>(dst) = make_double2(sx, sy);
-          } else {
-            atomicAdd(dst, sx);
-            atomicAdd(dst + 1, sy);
+        // residual: sum over the four lanes t of a node (reduce-scatter over node tiles)
+        if constexpr (RES) {
+          const int Tm = t >> 1, To = Tm ^ 1;
+          double sx = (Tm ? rp[1][0] : rp[0][0]) + __shfl_xor_sync(0xffffffffu, To ? rp[1][0] : rp[0][0], 2);
+          double sy = (Tm ? rp[1][1] : rp[0][1]) + __shfl_xor_sync(0xffffffffu, To ? rp[1][1] : rp[0][1], 2);
+          sx += __shfl_xor_sync(0xffffffffu, sx, 1);
+          sy += __shfl_xor_sync(0xffffffffu, sy, 1);
+          const int a = 8 * Tm + pa;
+          if ((t & 1) == 0 && a < NN) {
+            double *dst = M.residual + 2 * (int64_t)nid[el * NN + a];
+            if (PLAN && O.codes[el * CS + NN * NN + a]) {
+              *reinterpret_cast<double2 *>(dst) = make_double2(sx, sy);
+            } else {
+              atomicAdd(dst, sx);
+              atomicAdd(dst + 1, sy);
+            }
           }
         }
-      }
-      // stiffness blocks, order 3: lane (g, t) holds (a = 8TA + pi(g), b = 8TB + 4h + t).  Blocks that
-      // are added (drop-in: all; plan: later colours) are staged so that each row run of
-      // four consecutive columns is contiguous in shared memory -- slot s = (pair, h,
-      // direct/transposed), direct position 4g + t (row a, columns 8TB + 4h + 0..3),
-      // transposed position 8t + pi(g) (row b, columns 8TA + 4*half + 0..3) -- and then
-      // reduced with one 128-byte bulk operation per run whose four blocks are adjacent in
-      // the matrix, else one 32-byte operation per block.
-      if constexpr (JAC && RUNS) {
-        // every lane's previous bulk reads of the staging slots are complete
-        asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
-        __syncwarp();
-        int k = 0;
-#pragma unroll
-        for (int TA = 0; TA < NTN; TA++) {
-#pragma unroll
-          for (int TB = TA; TB < NTN; TB++, k++) {
-            const int a = 8 * TA + pa;
-#pragma unroll
-            for (int h = 0; h < 2; h++) {
-              const int b = 8 * TB + 4 * h + t;
-              if (a < NN && b < NN) {
-                const double mxx = acc[k][0][h], mxy = acc[k][1][h], myx = acc[k][2][h], myy = acc[k][3][h];
-                const double kxx = c11 * mxx + mu * myy;
-                const double kxy = lam * mxy + mu * myx;
-                const double kyx = lam * myx + mu * mxy;
-                const double kyy = c11 * myy + mu * mxx;
-                const int s0 = frag_slot(k, h, 0);
-                frag_put<P, PLAN>(O, el, a, b, 0, kxx, kxy, kyx, kyy, redsW + 128 * s0 + 4 * (4 * g + t));
-                if (TA < TB) {
-                  const int s1 = frag_slot(k, h, 1);
-                  frag_put<P, PLAN>(O, el, a, b, 1, kxx, kxy, kyx, kyy, redsW + 128 * s1 + 4 * (8 * t + pa));
+        // stiffness blocks, order 3: lane (g, t) holds (a = 8TA + pi(g), b = 8TB + 4h + t).  Blocks that
+        // are added (drop-in: all; plan: later colours) are staged so that each row run of
+        // four consecutive columns is contiguous in shared memory -- slot s = (pair, h,
+        // direct/transposed), direct position 4g + t (row a, columns 8TB + 4h + 0..3),
+        // transposed position 8t + pi(g) (row b, columns 8TA + 4*half + 0..3) -- and then
+        // reduced with one 128-byte bulk operation per run whose four blocks are adjacent in
+        // the matrix, else one 32-byte operation per block.
+        if constexpr (JAC && RUNS) {
+          // every lane's previous bulk reads of the staging slots are complete
+          asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+          __syncwarp();
+          int k = 0;
+  #pragma unroll
+          for (int TA = 0; TA < NTN; TA++) {
+  #pragma unroll
+            for (int TB = TA; TB < NTN; TB++, k++) {
+              const int a = 8 * TA + pa;
+  #pragma unroll
+              for (int h = 0; h < 2; h++) {
+                const int b = 8 * TB + 4 * h + t;
+                if (a < NN && b < NN) {
+                  const double mxx = acc[k][0][h], mxy = acc[k][1][h], myx = acc[k][2][h], myy = acc[k][3][h];
+                  const double kxx = c11 * mxx + mu * myy;
+                  const double kxy = lam * mxy + mu * myx;
+                  const double kyx = lam * myx + mu * mxy;
+                  const double kyy = c11 * myy + mu * mxx;
+                  const int s0 = frag_slot(k, h, 0);
+                  frag_put<P, PLAN>(O, el, a, b, 0, kxx, kxy, kyx, kyy, redsW + 128 * s0 + 4 * (4 * g + t));
+                  if (TA < TB) {
+                    const int s1 = frag_slot(k, h, 1);
+                    frag_put<P, PLAN>(O, el, a, b, 1, kxx, kxy, kyx, kyy, redsW + 128 * s1 + 4 * (8 * t + pa));
+                  }
+                }
+              }
+            }
+          }
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          __syncwarp();
+          // 64 runs (8 slots x 8 runs), two per lane
+  #pragma unroll
+          for (int u = 0; u < 2; u++) {
+            const int run = lane + 32 * u;
+            frag_issue_run<P, PLAN>(O, el, run >> 3, run & 7, redsW);
+          }
+          asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+        }
+        // stiffness blocks, order 2: lane (g, t) holds (a = 8TA + pi(g), b = 8TB + 4h + t),
+        // each written (or added) on its own
+        if constexpr (JAC && !RUNS) {
+          asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+          int k = 0, slot = 0;
+          double *reds = redsW + 4 * lane;
+  #pragma unroll
+          for (int TA = 0; TA < NTN; TA++) {
+  #pragma unroll
+            for (int TB = TA; TB < NTN; TB++, k++) {
+              const int a = 8 * TA + pa;
+  #pragma unroll
+              for (int h = 0; h < 2; h++) {
+                const int b = 8 * TB + 4 * h + t;
+                if (a < NN && b < NN) {
+                  const double mxx = acc[k][0][h], mxy = acc[k][1][h], myx = acc[k][2][h], myy = acc[k][3][h];
+                  const double kxx = c11 * mxx + mu * myy;
+                  const double kxy = lam * mxy + mu * myx;
+                  const double kyx = lam * myx + mu * mxy;
+                  const double kyy = c11 * myy + mu * mxx;
+                  if constexpr (PLAN) {
+                    frag_write<P>(O, el, a, b, 0, kxx, kxy, kyx, kyy, reds + 128 * slot++);
+                    if (TA < TB) frag_write<P>(O, el, a, b, 1, kxx, kxy, kyx, kyy, reds + 128 * slot++);
+                  } else {
+                    frag_add_mapped<P>(O, el, a, b, 0, kxx, kxy, kyx, kyy, reds + 128 * slot++);
+                    if (TA < TB) frag_add_mapped<P>(O, el, a, b, 1, kxx, kxy, kyx, kyy, reds + 128 * slot++);
+                  }
                 }
               }
             }
           }
         }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncwarp();
-        // 64 runs (8 slots x 8 runs), two per lane
-#pragma unroll
-        for (int u = 0; u < 2; u++) {
-          const int run = lane + 32 * u;
-          frag_issue_run<P, PLAN>(O, el, run >> 3, run & 7, redsW);
-        }
-        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
       }
-      // stiffness blocks, order 2: lane (g, t) holds (a = 8TA + pi(g), b = 8TB + 4h + t),
-      // each written (or added) on its own
-      if constexpr (JAC && !RUNS) {
-        asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
-        int k = 0, slot = 0;
-        double *reds = redsW + 4 * lane;
+    } else {
+      // interleaved rows r = 2a + i (p = 4): lane (g, t) builds G-hat_i(q = 4ks + t,
+      // a = 4T + g/2), i = g%2, the A fragment of row tile T and the B fragment of
+      // column tile T; lanes l and l^4 hold the two rows of a 2x2 block.  One pass per
+      // row tile R against the column tiles C >= R, fragments recomputed from the
+      // table in every pass (registers: seven accumulators); the residual has a pass
+      // of its own.
+      const int ii = g & 1, ah = g >> 1;
+      const double2 *WIi = ii ? WI1 : WI0;
+      const double2 *WSi = ii ? WS1 : WS0;
+      double *reds = redsW + 4 * lane;
+      int nw = 0;  // writes so far: ring position of the staging slot
+      for (int el = 0; el < ne; el++) {
+        // residual R_(a,i'): lane partials over its quadrature points, a full sum over the
+        // component pair (xor 4), then a reduce-scatter over the four lanes t (lane t
+        // ends with tiles 2t and 2t + 1)
+        if constexpr (RES) {
+          double rp[8][2];
 #pragma unroll
-        for (int TA = 0; TA < NTN; TA++) {
+          for (int T = 0; T < 8; T++) rp[T][0] = rp[T][1] = 0.0;
 #pragma unroll
-          for (int TB = TA; TB < NTN; TB++, k++) {
-            const int a = 8 * TA + pa;
+          for (int ks = 0; ks < K4; ks++) {
+            const int o = el * NQP + 4 * ks + t;
+            const double2 w = WIi[o];
+            const double2 sj = WSi[o];  // (S-hat_xj, S-hat_yj), j = this lane's component
 #pragma unroll
-            for (int h = 0; h < 2; h++) {
-              const int b = 8 * TB + 4 * h + t;
-              if (a < NN && b < NN) {
-                const double mxx = acc[k][0][h], mxy = acc[k][1][h], myx = acc[k][2][h], myy = acc[k][3][h];
+            for (int C = 0; C < K4; C++) {
+              const double2 d = tabF[(ks * K4 + C) * 16 + 4 * ah + t];
+              const double gv = fma(w.x, d.x, w.y * d.y);
+              rp[C][0] = fma(gv, sj.x, rp[C][0]);
+              rp[C][1] = fma(gv, sj.y, rp[C][1]);
+            }
+          }
+#pragma unroll
+          for (int T = 0; T < K4; T++)
+#pragma unroll
+            for (int c = 0; c < 2; c++) rp[T][c] += __shfl_xor_sync(0xffffffffu, rp[T][c], 4);
+          const int hi = t >> 1, lo = t & 1;
+          double w4[4][2], z[2][2];
+#pragma unroll
+          for (int k = 0; k < 4; k++)
+#pragma unroll
+            for (int c = 0; c < 2; c++)
+              w4[k][c] = (hi ? rp[4 + k][c] : rp[k][c]) + __shfl_xor_sync(0xffffffffu, hi ? rp[k][c] : rp[4 + k][c], 2);
+#pragma unroll
+          for (int mm = 0; mm < 2; mm++)
+#pragma unroll
+            for (int c = 0; c < 2; c++)
+              z[mm][c] = (lo ? w4[2 + mm][c] : w4[mm][c]) + __shfl_xor_sync(0xffffffffu, lo ? w4[mm][c] : w4[2 + mm][c], 1);
+#pragma unroll
+          for (int mm = 0; mm < 2; mm++) {
+            const int a = 4 * (2 * t + mm) + ah;
+            if (ii == 0 && a < NN) {
+              double *dst = M.residual + 2 * (int64_t)nid[el * NN + a];
+              if (PLAN && O.codes[el * CS + NN * NN + a]) {
+                *reinterpret_cast<double2 *>(dst) = make_double2(z[mm][0], z[mm][1]);
+              } else {
+                atomicAdd(dst, z[mm][0]);
+                atomicAdd(dst + 1, z[mm][1]);
+              }
+            }
+          }
+        }
+#pragma unroll 1
+        for (int R = 0; R < (JAC ? K4 : 0); R++) {
+          double acc[K4][2];
+#pragma unroll
+          for (int C = 0; C < K4; C++) acc[C][0] = acc[C][1] = 0.0;
+#pragma unroll
+          for (int ks = 0; ks < K4; ks++) {
+            const int o = el * NQP + 4 * ks + t;
+            const double2 w = WIi[o];
+            const double sg = SGs[o];
+            const double2 dR = tabF[(ks * K4 + R) * 16 + 4 * ah + t];
+            const double af = sg * fma(w.x, dR.x, w.y * dR.y);
+#pragma unroll
+            for (int C = 0; C < K4; C++) {
+              if (C < R) continue;  // warp-uniform
+              const double2 d = tabF[(ks * K4 + C) * 16 + 4 * ah + t];
+              dmma(acc[C][0], acc[C][1], af, fma(w.x, d.x, w.y * d.y));
+            }
+          }
+          // blocks: lane pair (l, l^4) exchanges rows; lane i = 0 writes (a, b), lane
+          // i = 1 writes (b, a) = (a, b)^T
+          if constexpr (JAC) {
+            const int a = 4 * R + ah;
+#pragma unroll
+            for (int C = 0; C < K4; C++) {
+              if (C < R) continue;  // warp-uniform
+              const double o0 = __shfl_xor_sync(0xffffffffu, acc[C][0], 4);
+              const double o1 = __shfl_xor_sync(0xffffffffu, acc[C][1], 4);
+              const double mxx = ii ? o0 : acc[C][0], mxy = ii ? o1 : acc[C][1];
+              const double myx = ii ? acc[C][0] : o0, myy = ii ? acc[C][1] : o1;
+              const int b = 4 * C + t;
+              if (a < NN && b < NN && a <= b && (ii == 0 || a < b)) {
                 const double kxx = c11 * mxx + mu * myy;
                 const double kxy = lam * mxy + mu * myx;
                 const double kyx = lam * myx + mu * mxy;
                 const double kyy = c11 * myy + mu * mxx;
+                // the ring slot's previous bulk read (NSLOT writes ago) is complete
+                asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(L::NSLOT - 1) : "memory");
+                double *slot = reds + 128 * (nw % L::NSLOT);
+                nw++;
                 if constexpr (PLAN) {
-                  frag_write<P>(O, el, a, b, 0, kxx, kxy, kyx, kyy, reds + 128 * slot++);
-                  if (TA < TB) frag_write<P>(O, el, a, b, 1, kxx, kxy, kyx, kyy, reds + 128 * slot++);
+                  frag_write<P>(O, el, a, b, ii, kxx, kxy, kyx, kyy, slot);
                 } else {
-                  frag_add_mapped<P>(O, el, a, b, 0, kxx, kxy, kyx, kyy, reds + 128 * slot++);
-                  if (TA < TB) frag_add_mapped<P>(O, el, a, b, 1, kxx, kxy, kyx, kyy, reds + 128 * slot++);
+                  frag_add_mapped<P>(O, el, a, b, ii, kxx, kxy, kyx, kyy, slot);
                 }
               }
             }
@@ -780,14 +916,22 @@ int launch_frag_mode(int order, const AsmArgs &a, cudaStream_t s) {
   switch (order) {
     case 2: return launch_frag_p<2, MODE>(a, s);
     case 3: return launch_frag_p<3, MODE>(a, s);
+    case 4: return launch_frag_p<4, MODE>(a, s);
     default: return fail(FEM_ERR_INVALID_ORDER, "fragment kernel: order %d", order);
   }
 }
 
 }  // namespace dev
 
-bool frag_supported(int order, int precision, int strain) {
-  return (order == 2 || order == 3) && precision == FEM_PRECISION_FP64 && strain == FEM_STRAIN_LINEAR;
+// Orders 2 and 3 in every mode; order 4 in plan mode only (single meshes, batches,
+// the server): measured on B200, the order-4 fragment kernel is 15 % faster in the
+// 256-mesh batch but 13 % slower on one 512^2 mesh than the element kernel, and
+// plans and batches must run the same kernel (a mesh's batched result equals its
+// single-mesh plan result bit for bit); the order-4 drop-in keeps the element
+// kernel (4.6 ms against 6.9 ms on the 512^2 mesh).
+bool frag_supported(int order, int precision, int strain, bool plan) {
+  if (precision != FEM_PRECISION_FP64 || strain != FEM_STRAIN_LINEAR) return false;
+  return order == 2 || order == 3 || (order == 4 && plan);
 }
 
 int launch_frag(int order, int mode, const dev::AsmArgs &a, cudaStream_t s) {
@@ -808,6 +952,7 @@ int launch_frag_batched(int order, const dev::AsmArgs *meshes, const dev::Tile *
   switch (order) {
     case 2: return dev::launch_frag_batched_p<2>(meshes, tiles, ntiles, counter, s);
     case 3: return dev::launch_frag_batched_p<3>(meshes, tiles, ntiles, counter, s);
+    case 4: return dev::launch_frag_batched_p<4>(meshes, tiles, ntiles, counter, s);
     default: return fail(FEM_ERR_INVALID_ORDER, "fragment kernel: order %d", order);
   }
 }

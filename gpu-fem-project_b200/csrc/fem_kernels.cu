@@ -87,7 +87,7 @@ int launch(int order, int precision, int mode, const dev::AsmArgs &a, cudaStream
     return launch_nl(order, mode, a, s);
   }
   if (strain != FEM_STRAIN_LINEAR) return fail(FEM_ERR_INVALID_ARGUMENT, "strain type %d", strain);
-  if ((mode & dev::kPlan) == 0 && frag_supported(order, precision, strain)) return launch_frag(order, mode, a, s);
+  if ((mode & dev::kPlan) == 0 && frag_supported(order, precision, strain, false)) return launch_frag(order, mode, a, s);
   if (precision == FEM_PRECISION_FP64) return launch_any<double>(order, mode, a, s);
   if (precision == FEM_PRECISION_MIXED) return launch_any<float>(order, mode, a, s);
   return fail(FEM_ERR_INVALID_ARGUMENT, "precision %d", precision);
@@ -340,7 +340,7 @@ int fem_plan_assemble_ex(const fem_plan *plan, const double *states, const doubl
     a.count = plan->numChunks;
     return fem::timed(s, elapsedSeconds, [&] { return fem::launch_rows(mode, a, s); });
   }
-  const bool frag = fem::frag_supported(plan->order, precision, strainType);
+  const bool frag = fem::frag_supported(plan->order, precision, strainType, true);
   return fem::timed(s, elapsedSeconds, [&] {
     for (int c = 0; c < plan->numColours; c++) {
       a.begin = plan->colourPtr[c];

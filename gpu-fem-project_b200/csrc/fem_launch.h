@@ -102,7 +102,7 @@ constexpr int kRowTileChunks = 16;
 // Warp-fragment kernel (fem_frag.cu): LINEAR FP64 assembly at orders 2 and 3, plan
 // mode (one colour, list positions [a.begin, a.begin + a.count)) or drop-in mode
 // (elements through the reference map, accumulate-into).
-bool frag_supported(int order, int precision, int strain);
+bool frag_supported(int order, int precision, int strain, bool plan);
 int launch_frag(int order, int mode, const dev::AsmArgs &a, cudaStream_t s);
 // Its tile-queue form for batches and the server (residual and Jacobian).
 int launch_frag_batched(int order, const dev::AsmArgs *meshes, const dev::Tile *tiles, int ntiles, int *counter,
