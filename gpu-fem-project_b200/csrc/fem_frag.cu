@@ -1,4 +1,5 @@
-// Warp-fragment assembly kernel for plan-mode LINEAR FP64 assembly, orders 2 and 3.
+// Warp-fragment assembly kernel: LINEAR FP64 residual + Jacobian assembly at orders
+// 2 to 4 (which paths use it: frag_supported at the end of this file).
 //
 // The element kernel in fem_device.cuh stages every element's coordinates,
 // states and scaled gradients in shared memory and reads them back for each
@@ -16,33 +17,35 @@
 //                Jacobian and the reference-space state gradient of both
 //                elements at every quadrature point (K4 x K4 MMAs), with the
 //                derivative table as B fragments (shared memory, lane order).
-//   3. transpose three xor-shuffle rounds give each lane all eight values of one
-//                quadrature point q = 4c + t of its element; it forms det J, J^-1,
-//                s = w det J t, the weak stress and sqrt|s| J^-1 (FP64), and
+//   3. transpose three xor-shuffle rounds per group of four column tiles give each
+//                lane all eight values of one quadrature point q = 4(4m + c) + t
+//                (one point per lane at p <= 3, two at p = 4); it forms det J, J^-1,
+//                s = w det J t, the weak stress and sqrt|s| J^-1 (FP64) and
 //                stores the ~10 doubles of q to shared memory.
-//   4. fragments per element, lane (g, t) builds G-hat_i(q, a) = sqrt|s| (dN(a,q) J^-1)_i
-//                for q = 4ks + t and nodes a = 8T + pi(g), pi(g) = 4(g%2) + g/2,
-//                component i: K4 x NTN x 2 doubles, the A and B fragments of the
-//                stiffness product.
-//   5. residual  R_(a,i) = sum_q sum_j G-hat_j S-hat_ij on the FP64 pipe, reduced over
-//                the four lanes of a node by two shuffle rounds; one double2
-//                store (first writer) or two reductions per node.
-//   6. stiffness component-major tiles M_ij[a][b] = sum_q s G_ai G_bj (node tiles
-//                TA <= TB, four (i, j) tiles sharing fragments): lane (g, t) ends
-//                with the WHOLE 2x2 block (a = 8TA + pi(g), b = 8TB + 4h + t),
-//                h = 0, 1, so the plane-stress combination needs no shuffle and
-//                each warp store writes eight runs of four consecutive blocks
-//                (a BSR row holds an element grid row's nodes consecutively).
-//                Blocks of TA < TB tiles are also written transposed (K = K^T).
+//   4. fragments lane (g, t) builds G-hat_i(q, a) = sqrt|s| (dN(a,q) J^-1)_i for
+//                q = 4ks + t from sqrt|s| J^-1 and the table: the A and B fragments
+//                of M_ij[a][b] = sum_q s G_ai G_bj.
+//   5. residual  R_(a,i) = sum_q sum_j G-hat_j S-hat_ij on the FP64 pipe from the
+//                same fragments, reduced over the lanes of a node by shuffles.
+//   6. stiffness p = 2, 3: component-major node tiles (a = 8T + pi(g), pi(g) =
+//                4(g%2) + g/2; pairs TA <= TB, four (i, j) tiles sharing
+//                fragments, k-steps outermost): lane (g, t) ends with WHOLE 2x2
+//                blocks (a, b = 8TB + 4h + t), so the plane-stress combination
+//                needs no shuffle and a warp store covers eight runs of four
+//                consecutive blocks.  p = 4: interleaved rows r = 2a + i in seven
+//                tiles (a = 4T + g/2), one pass per row tile with the fragments
+//                recomputed from the table; lanes l, l^4 exchange the two rows of
+//                a block.  Blocks above the diagonal are also written transposed.
 //
-// Writes follow the plan codes: a launch is one colour; the first contributor of
-// a block stores it (one 256-bit store); a later colour adds its 2x2 blocks with
-// asynchronous bulk reductions (cp.reduce.async.bulk .add.f64 from shared memory,
-// one per run of four adjacent blocks) instead of four FP64 L2 atomics per block;
-// residual rows add with atomics (first writer stores).  Drop-in mode adds every
-// block the same way through the reference element map.  The arithmetic is the
-// closed form of the reference's per-column forward AD (element/FEKernels.h:
-// 286-315, 884-976) that the element kernel documents.
+// Writes.  Plan mode: a launch is one colour; the first contributor of a block
+// stores it (one 256-bit store); a later colour adds its 2x2 blocks with
+// asynchronous bulk reductions (cp.reduce.async.bulk .add.f64 from shared memory)
+// instead of four FP64 L2 atomics per block -- at p = 3 staged by row run, one
+// 128-byte reduction per run of four adjacent blocks.  Drop-in mode (reference
+// element map, accumulate-into) adds every block that way.  Residual rows: first
+// writer stores, others add with atomics.  The arithmetic is the closed form of
+// the reference's per-column forward AD (element/FEKernels.h:286-315, 884-976)
+// that the element kernel documents.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -923,14 +926,20 @@ int launch_frag_mode(int order, const AsmArgs &a, cudaStream_t s) {
 
 }  // namespace dev
 
-// Orders 2 and 3 in every mode; order 4 in plan mode only (single meshes, batches,
-// the server): measured on B200, the order-4 fragment kernel is 15 % faster in the
-// 256-mesh batch but 13 % slower on one 512^2 mesh than the element kernel, and
-// plans and batches must run the same kernel (a mesh's batched result equals its
-// single-mesh plan result bit for bit); the order-4 drop-in keeps the element
-// kernel (4.6 ms against 6.9 ms on the 512^2 mesh).
+// FP64, LINEAR: orders 2 and 3 in every mode; order 4 in plan mode only (single
+// meshes, batches, the server): measured on B200, the order-4 fragment kernel is
+// 15 % faster in the 256-mesh batch but 13 % slower on one 512^2 mesh than the
+// element kernel, and plans and batches must run the same kernel (a mesh's batched
+// result equals its single-mesh plan result bit for bit); the order-4 drop-in keeps
+// the element kernel (4.6 ms against 6.9 ms on the 512^2 mesh).
+// MIXED at orders 2 and 3 also runs this FP64 kernel (faster than the FP32 element
+// products there: 3.1 against 3.8 ms at 1024^2 p = 3), so it returns the FP64
+// result, as order-1 row assembly does; at order 4 the FP32 element kernel is the
+// faster one (2.6 against 3.4 ms) and MIXED keeps it.
 bool frag_supported(int order, int precision, int strain, bool plan) {
-  if (precision != FEM_PRECISION_FP64 || strain != FEM_STRAIN_LINEAR) return false;
+  if (strain != FEM_STRAIN_LINEAR) return false;
+  if (precision == FEM_PRECISION_MIXED) return order == 2 || order == 3;
+  if (precision != FEM_PRECISION_FP64) return false;
   return order == 2 || order == 3 || (order == 4 && plan);
 }
 
