@@ -49,6 +49,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <type_traits>
 
 #include "fem_common.h"
 #include "fem_device.cuh"
@@ -414,11 +415,18 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
   unsigned char *stage = ws + L::STAGE;
   double *redsW = reinterpret_cast<double *>(ws + L::REDS);  // staging slot s at redsW + 128 s
 
+  // Mesh arguments are read through `mtab` (for one mesh, a pointer to the kernel
+  // parameter).  At p = 4 it is laundered once per step: the compiler then reloads
+  // the arguments where they are used instead of hoisting ~20 loop-invariant values
+  // into registers for the whole loop, which pushed the residual + Jacobian kernel
+  // into 400 bytes of spills (3.4 against 3.0 ms on a 512^2 mesh).  At p = 2 the
+  // reloads cost more than they save (1.80 against 1.60 ms on the annulus).
+  const AsmArgs *mtab = meshes;
   auto args = [&](const PairCursor &c) -> const AsmArgs & {
     if constexpr (Gen::kBatched) {
-      return meshes[c.mesh];
+      return mtab[c.mesh];
     } else {
-      return single;
+      return *mtab;
     }
   };
   // node ids (two pairs ahead) and coordinate/state values (one pair ahead)
@@ -476,6 +484,7 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
   int buf = 0;
 
   for (; cur.ne > 0; buf ^= 1) {
+    if constexpr (P == 4) asm volatile("" : "+l"(mtab));
     const int ne = cur.ne;
     const AsmArgs &M = args(cur);
     const double mu = M.mu, lam = M.lam, thick = M.t, c11 = lam + 2.0 * mu;
@@ -733,10 +742,8 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
     } else {
       // interleaved rows r = 2a + i (p = 4): lane (g, t) builds G-hat_i(q = 4ks + t,
       // a = 4T + g/2), i = g%2, the A fragment of row tile T and the B fragment of
-      // column tile T; lanes l and l^4 hold the two rows of a 2x2 block.  One pass per
-      // row tile R against the column tiles C >= R, fragments recomputed from the
-      // table in every pass (registers: seven accumulators); the residual has a pass
-      // of its own.
+      // column tile T; lanes l and l^4 hold the two rows of a 2x2 block.  The residual
+      // has a pass of its own, the stiffness one pass per group of row tiles.
       const int ii = g & 1, ah = g >> 1;
       const double2 *WIi = ii ? WI1 : WI0;
       const double2 *WSi = ii ? WS1 : WS0;
@@ -793,36 +800,45 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
             }
           }
         }
-#pragma unroll 1
-        for (int R = 0; R < (JAC ? K4 : 0); R++) {
-          double acc[K4][2];
+        // stiffness: row tiles in groups {0}, {1}, {2,3}, {4,5,6} (at most nine live
+        // accumulator tiles); within a group the k-steps are outermost, each fragment
+        // of the step is formed once and feeds every tile (R, C >= R) of the group
+        auto group = [&](auto r0c, auto r1c) {
+          constexpr int R0 = decltype(r0c)::value, R1 = decltype(r1c)::value;
+          double acc[R1 - R0][K4][2];
 #pragma unroll
-          for (int C = 0; C < K4; C++) acc[C][0] = acc[C][1] = 0.0;
+          for (int R = R0; R < R1; R++)
+#pragma unroll
+            for (int C = 0; C < K4; C++) acc[R - R0][C][0] = acc[R - R0][C][1] = 0.0;
 #pragma unroll
           for (int ks = 0; ks < K4; ks++) {
             const int o = el * NQP + 4 * ks + t;
             const double2 w = WIi[o];
             const double sg = SGs[o];
-            const double2 dR = tabF[(ks * K4 + R) * 16 + 4 * ah + t];
-            const double af = sg * fma(w.x, dR.x, w.y * dR.y);
+            double fr[K4];
 #pragma unroll
-            for (int C = 0; C < K4; C++) {
-              if (C < R) continue;  // warp-uniform
+            for (int C = R0; C < K4; C++) {
               const double2 d = tabF[(ks * K4 + C) * 16 + 4 * ah + t];
-              dmma(acc[C][0], acc[C][1], af, fma(w.x, d.x, w.y * d.y));
+              fr[C] = fma(w.x, d.x, w.y * d.y);
+            }
+#pragma unroll
+            for (int R = R0; R < R1; R++) {
+              const double af = sg * fr[R];
+#pragma unroll
+              for (int C = R; C < K4; C++) dmma(acc[R - R0][C][0], acc[R - R0][C][1], af, fr[C]);
             }
           }
           // blocks: lane pair (l, l^4) exchanges rows; lane i = 0 writes (a, b), lane
           // i = 1 writes (b, a) = (a, b)^T
-          if constexpr (JAC) {
+#pragma unroll
+          for (int R = R0; R < R1; R++) {
             const int a = 4 * R + ah;
 #pragma unroll
-            for (int C = 0; C < K4; C++) {
-              if (C < R) continue;  // warp-uniform
-              const double o0 = __shfl_xor_sync(0xffffffffu, acc[C][0], 4);
-              const double o1 = __shfl_xor_sync(0xffffffffu, acc[C][1], 4);
-              const double mxx = ii ? o0 : acc[C][0], mxy = ii ? o1 : acc[C][1];
-              const double myx = ii ? acc[C][0] : o0, myy = ii ? acc[C][1] : o1;
+            for (int C = R; C < K4; C++) {
+              const double o0 = __shfl_xor_sync(0xffffffffu, acc[R - R0][C][0], 4);
+              const double o1 = __shfl_xor_sync(0xffffffffu, acc[R - R0][C][1], 4);
+              const double mxx = ii ? o0 : acc[R - R0][C][0], mxy = ii ? o1 : acc[R - R0][C][1];
+              const double myx = ii ? acc[R - R0][C][0] : o0, myy = ii ? acc[R - R0][C][1] : o1;
               const int b = 4 * C + t;
               if (a < NN && b < NN && a <= b && (ii == 0 || a < b)) {
                 const double kxx = c11 * mxx + mu * myy;
@@ -841,6 +857,21 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
               }
             }
           }
+        };
+        if constexpr (JAC) {
+          static_assert(K4 == 7, "row-tile groups of the order-4 layout");
+          // compiler barriers keep each group's table loads inside the group (hoisting
+          // them across groups raises register pressure past the budget)
+          asm volatile("" ::: "memory");
+          group(std::integral_constant<int, 0>{}, std::integral_constant<int, 1>{});
+          asm volatile("" ::: "memory");
+          group(std::integral_constant<int, 1>{}, std::integral_constant<int, 2>{});
+          asm volatile("" ::: "memory");
+          group(std::integral_constant<int, 2>{}, std::integral_constant<int, 3>{});
+          asm volatile("" ::: "memory");
+          group(std::integral_constant<int, 3>{}, std::integral_constant<int, 5>{});
+          asm volatile("" ::: "memory");
+          group(std::integral_constant<int, 5>{}, std::integral_constant<int, 7>{});
         }
       }
     }
@@ -862,7 +893,7 @@ __global__ void __launch_bounds__(32 * FragDims<P>::WARPS, FEM_FRAG_MINB) frag_k
   const int warp = threadIdx.x >> 5;
   PairStride gen{A.begin, A.begin + A.count, (int64_t)blockIdx.x * FragDims<P>::WARPS + warp,
                  (int64_t)gridDim.x * FragDims<P>::WARPS};
-  frag_loop<P, MODE>(smem, gen, A, nullptr);
+  frag_loop<P, MODE>(smem, gen, A, &A);
 }
 
 // Many meshes of one order (one colour each): warps pull tiles from the launch's queue.
@@ -927,11 +958,11 @@ int launch_frag_mode(int order, const AsmArgs &a, cudaStream_t s) {
 }  // namespace dev
 
 // FP64, LINEAR: orders 2 and 3 in every mode; order 4 in plan mode only (single
-// meshes, batches, the server): measured on B200, the order-4 fragment kernel is
-// 15 % faster in the 256-mesh batch but 13 % slower on one 512^2 mesh than the
-// element kernel, and plans and batches must run the same kernel (a mesh's batched
-// result equals its single-mesh plan result bit for bit); the order-4 drop-in keeps
-// the element kernel (4.6 ms against 6.9 ms on the 512^2 mesh).
+// meshes, batches, the server): measured on B200, the order-4 fragment kernel runs
+// the 256-mesh batch in 170 against 217 ms and one 512^2 mesh in 3.03 against
+// 3.00 ms for the element kernel, and plans and batches must run the same kernel
+// (a mesh's batched result equals its single-mesh plan result bit for bit); the
+// order-4 drop-in keeps the element kernel (4.7 ms against 6.9 ms).
 // MIXED at orders 2 and 3 also runs this FP64 kernel (faster than the FP32 element
 // products there: 3.1 against 3.8 ms at 1024^2 p = 3), so it returns the FP64
 // result, as order-1 row assembly does; at order 4 the FP32 element kernel is the
