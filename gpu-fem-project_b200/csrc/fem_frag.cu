@@ -593,7 +593,11 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
 
     const Out O{M.mat, M.residual, stage + buf * 2 * STG, rb, reinterpret_cast<const int *>(stage + buf * 2 * STG)};
     if constexpr (!F::IL) {
-      constexpr int NPAIR = NTN * (NTN + 1) / 2;
+      // node tiles on the tensor cores: both at p = 3; at p = 2 only tile 0 (nodes 0-7),
+      // node 8 (alone in tile 1) has its row and column on the FP64 pipe (12 instead of
+      // 36 MMAs per element)
+      constexpr int NTM = (P == 2) ? 1 : NTN;
+      constexpr int NPAIR = NTM * (NTM + 1) / 2;
       const int pa = 4 * (g & 1) + (g >> 1);  // pi(g)
       for (int el = 0; el < ne; el++) {
         // 3.-5. quadrature k-steps outermost: per step each lane forms its fragments
@@ -601,6 +605,7 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
         // the 4 NPAIR independent stiffness MMAs of all node-tile pairs
         double acc[NPAIR][4][2];
         double rp[NTN][2];
+        double n8[4] = {0.0, 0.0, 0.0, 0.0}, d8[4] = {0.0, 0.0, 0.0, 0.0};  // p = 2: M[8][pi(g)], M[8][8]
   #pragma unroll
         for (int k = 0; k < NPAIR; k++)
   #pragma unroll
@@ -627,13 +632,26 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
               rp[T][1] = fma(fr[T][0], s0.y, fma(fr[T][1], s1.y, rp[T][1]));
             }
           }
+          if constexpr (JAC && P == 2) {
+            // G-hat_i(q, 8) sits in lane (g = 0, t), tile 1
+            const double h0 = __shfl_sync(0xffffffffu, fr[1][0], t), h1 = __shfl_sync(0xffffffffu, fr[1][1], t);
+            const double s0 = sg * h0, s1 = sg * h1;
+            n8[0] = fma(s0, fr[0][0], n8[0]);
+            n8[1] = fma(s0, fr[0][1], n8[1]);
+            n8[2] = fma(s1, fr[0][0], n8[2]);
+            n8[3] = fma(s1, fr[0][1], n8[3]);
+            d8[0] = fma(s0, h0, d8[0]);
+            d8[1] = fma(s0, h1, d8[1]);
+            d8[2] = fma(s1, h0, d8[2]);
+            d8[3] = fma(s1, h1, d8[3]);
+          }
           if constexpr (JAC) {
             int k = 0;
   #pragma unroll
-            for (int TA = 0; TA < NTN; TA++) {
+            for (int TA = 0; TA < NTM; TA++) {
               const double a0 = sg * fr[TA][0], a1 = sg * fr[TA][1];
   #pragma unroll
-              for (int TB = TA; TB < NTN; TB++, k++) {
+              for (int TB = TA; TB < NTM; TB++, k++) {
                 dmma(acc[k][0][0], acc[k][0][1], a0, fr[TB][0]);
                 dmma(acc[k][1][0], acc[k][1][1], a0, fr[TB][1]);
                 dmma(acc[k][2][0], acc[k][2][1], a1, fr[TB][0]);
@@ -713,9 +731,9 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
           int k = 0, slot = 0;
           double *reds = redsW + 4 * lane;
   #pragma unroll
-          for (int TA = 0; TA < NTN; TA++) {
+          for (int TA = 0; TA < NTM; TA++) {
   #pragma unroll
-            for (int TB = TA; TB < NTN; TB++, k++) {
+            for (int TB = TA; TB < NTM; TB++, k++) {
               const int a = 8 * TA + pa;
   #pragma unroll
               for (int h = 0; h < 2; h++) {
@@ -734,6 +752,32 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
                     if (TA < TB) frag_add_mapped<P>(O, el, a, b, 1, kxx, kxy, kyx, kyy, reds + 128 * slot++);
                   }
                 }
+              }
+            }
+          }
+          if constexpr (P == 2) {
+            // node 8: sum the partials over the four lanes t; lane t = 0 writes (8, pi(g)),
+            // t = 1 its transpose (pi(g), 8), lane (g = 0, t = 2) the diagonal block (8, 8)
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+              n8[c] += __shfl_xor_sync(0xffffffffu, n8[c], 1);
+              n8[c] += __shfl_xor_sync(0xffffffffu, n8[c], 2);
+              d8[c] += __shfl_xor_sync(0xffffffffu, d8[c], 1);
+              d8[c] += __shfl_xor_sync(0xffffffffu, d8[c], 2);
+            }
+            const bool diag = (g == 0 && t == 2);
+            if (t < 2 || diag) {
+              const double mxx = diag ? d8[0] : n8[0], mxy = diag ? d8[1] : n8[1];
+              const double myx = diag ? d8[2] : n8[2], myy = diag ? d8[3] : n8[3];
+              const double kxx = c11 * mxx + mu * myy;
+              const double kxy = lam * mxy + mu * myx;
+              const double kyx = lam * myx + mu * mxy;
+              const double kyy = c11 * myy + mu * mxx;
+              const int b = diag ? 8 : pa, w = diag ? 0 : t;
+              if constexpr (PLAN) {
+                frag_write<P>(O, el, 8, b, w, kxx, kxy, kyx, kyy, reds + 128 * slot);
+              } else {
+                frag_add_mapped<P>(O, el, 8, b, w, kxx, kxy, kyx, kyy, reds + 128 * slot);
               }
             }
           }
