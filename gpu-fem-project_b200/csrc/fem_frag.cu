@@ -1,5 +1,6 @@
-// Warp-fragment assembly kernel: LINEAR FP64 residual + Jacobian assembly at orders
-// 2 to 4 (which paths use it: frag_supported at the end of this file).
+// Warp-fragment assembly kernel: FP64 residual + Jacobian assembly, LINEAR strain at
+// orders 2 to 4 and NONLINEAR (Green) strain at orders 2 and 3 (which paths use it:
+// frag_supported at the end of this file).
 //
 // The element kernel in fem_device.cuh stages every element's coordinates,
 // states and scaled gradients in shared memory and reads them back for each
@@ -86,7 +87,7 @@ struct FragDims {
 // Shared memory: CTA tables, then one region per warp.  DROP: drop-in mode (the
 // stage holds the reference element map rows, NN*NN ints per element, instead of
 // plan code records).
-template <int P, bool DROP = false>
+template <int P, bool DROP = false, bool NL = false>
 struct FragLayout {
   using F = FragDims<P>;
   static constexpr int K4 = F::K4, NTN = F::NTN, NQP = F::NQP, NN = F::NN;
@@ -109,7 +110,9 @@ struct FragLayout {
   // the (at most 8) blocks one lane writes per element; p = 4, a ring of 4 per lane
   static constexpr int NSLOT = F::IL ? 4 : 8;
   static constexpr size_t REDS = align16(STAGE + 2 * 2 * CS);  // double4 [NSLOT][32]: bulk-reduction sources
-  static constexpr size_t warp_bytes = align16(REDS + 32 * NSLOT * 32);
+  // NONLINEAR: sign(s) x tangent modulus, double [2][NQP][2 (l)][8 (i, k, n)]
+  static constexpr size_t AT = align16(REDS + 32 * NSLOT * 32);
+  static constexpr size_t warp_bytes = align16(AT + (NL ? 8 * 2 * NQP * 16 : 0));
   static constexpr size_t total = warps + F::WARPS * warp_bytes;
 };
 
@@ -388,13 +391,14 @@ template <int P, int MODE, typename Gen>
 __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const AsmArgs &single,
                                           const AsmArgs *__restrict__ meshes) {
   constexpr bool PLAN = (MODE & kPlan) != 0;
+  constexpr bool NL = (MODE & kNL) != 0;
   using F = FragDims<P>;
-  using L = FragLayout<P, !PLAN>;
+  using L = FragLayout<P, !PLAN, NL>;
   constexpr int NN = F::NN, NQ = F::NQ, K4 = F::K4, NTN = F::NTN, NQP = F::NQP, CS = F::CS;
   constexpr int STG = L::CS;  // staged bytes per element: plan code record or map rows
   constexpr bool RES = (MODE & kRes) != 0, JAC = (MODE & kJac) != 0;
   constexpr bool RUNS = (P == 3);  // order 3: staged row runs, one bulk reduction per adjacent run
-  static_assert((MODE & kNL) == 0, "LINEAR strain");
+  static_assert(!NL || !F::IL, "NONLINEAR strain: orders 2 and 3");
   static_assert(PLAN || !Gen::kBatched, "drop-in mode assembles one mesh");
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -414,6 +418,7 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
   int *rb = reinterpret_cast<int *>(ws + L::RB);
   unsigned char *stage = ws + L::STAGE;
   double *redsW = reinterpret_cast<double *>(ws + L::REDS);  // staging slot s at redsW + 128 s
+  double *ATs = reinterpret_cast<double *>(ws + L::AT);      // NONLINEAR tangent
 
   // Mesh arguments are read through `mtab` (for one mesh, a pointer to the kernel
   // parameter).  At p = 4 it is laundered once per step: the compiler then reloads
@@ -571,14 +576,55 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
         const double sw = sg * rs;
         const double uxx = g00 * i00 + g01 * i10, uxy = g00 * i01 + g01 * i11;
         const double uyx = g10 * i00 + g11 * i10, uyy = g10 * i01 + g11 * i11;
-        const double tr = uxx + uyy;
-        const double sxx = sw * (2.0 * mu * uxx + lam * tr);
-        const double sxy = sw * (mu * (uxy + uyx));
-        const double syy = sw * (2.0 * mu * uyy + lam * tr);
         wi0 = make_double2(rs * i00, rs * i10);
         wi1 = make_double2(rs * i01, rs * i11);
-        ws0 = make_double2(sxx, sxy);
-        ws1 = make_double2(sxy, syy);
+        if constexpr (NL) {
+          // Green strain E = 1/2 (g + g^T + g^T g), S = 2 mu E + lam tr(E) I, first Piola
+          // P = F S (F = I + g); tangent A_{il,kn} = delta_ik S_ln + mu F_in F_kl
+          // + mu (F F^T)_ik delta_ln + lam F_il F_kn (element/FEKernels.h:286-315,
+          // NONLINEAR), stored times sign(s) as [l][i][k][n]
+          const double F[2][2] = {{1.0 + uxx, uxy}, {uyx, 1.0 + uyy}};
+          const double e00 = 0.5 * (2.0 * uxx + uxx * uxx + uyx * uyx);
+          const double e01 = 0.5 * (uxy + uyx + uxx * uxy + uyx * uyy);
+          const double e11 = 0.5 * (2.0 * uyy + uxy * uxy + uyy * uyy);
+          const double trE = e00 + e11;
+          const double Sm[2][2] = {{2.0 * mu * e00 + lam * trE, 2.0 * mu * e01}, {2.0 * mu * e01, 2.0 * mu * e11 + lam * trE}};
+          const double pxx = F[0][0] * Sm[0][0] + F[0][1] * Sm[1][0], pxy = F[0][0] * Sm[0][1] + F[0][1] * Sm[1][1];
+          const double pyx = F[1][0] * Sm[0][0] + F[1][1] * Sm[1][0], pyy = F[1][0] * Sm[0][1] + F[1][1] * Sm[1][1];
+          ws0 = make_double2(sw * pxx, sw * pyx);  // (P-hat_x0, P-hat_y0)
+          ws1 = make_double2(sw * pxy, sw * pyy);  // (P-hat_x1, P-hat_y1)
+          if (JAC && tq < K4) {
+            double *at = ATs + (e_ld * NQP + q) * 16;
+#pragma unroll
+            for (int ll = 0; ll < 2; ll++)
+#pragma unroll
+              for (int ii2 = 0; ii2 < 2; ii2++)
+#pragma unroll
+                for (int kk = 0; kk < 2; kk++) {
+                  double v2[2];
+#pragma unroll
+                  for (int nn = 0; nn < 2; nn++) {
+                    const double bik = F[ii2][0] * F[kk][0] + F[ii2][1] * F[kk][1];
+                    double v = mu * F[ii2][nn] * F[kk][ll] + lam * F[ii2][ll] * F[kk][nn];
+                    if (ii2 == kk) v += Sm[ll][nn];
+                    if (ll == nn) v += mu * bik;
+                    v2[nn] = sg * v;
+                  }
+                  *reinterpret_cast<double2 *>(at + ll * 8 + ii2 * 4 + kk * 2) = make_double2(v2[0], v2[1]);
+                }
+          }
+        } else {
+          const double tr = uxx + uyy;
+          const double sxx = sw * (2.0 * mu * uxx + lam * tr);
+          const double sxy = sw * (mu * (uxy + uyx));
+          const double syy = sw * (2.0 * mu * uyy + lam * tr);
+          ws0 = make_double2(sxx, sxy);
+          ws1 = make_double2(sxy, syy);
+        }
+      } else if (NL && JAC && tq < K4) {
+        double2 *at = reinterpret_cast<double2 *>(ATs + (e_ld * NQP + q) * 16);
+#pragma unroll
+        for (int j = 0; j < 8; j++) at[j] = make_double2(0.0, 0.0);
       }
       if (tq < K4) {
         const int o = e_ld * NQP + q;
@@ -632,7 +678,47 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
               rp[T][1] = fma(fr[T][0], s0.y, fma(fr[T][1], s1.y, rp[T][1]));
             }
           }
-          if constexpr (JAC && P == 2) {
+          if constexpr (JAC && NL) {
+            // K_ik[a][b] = sum over (q, l) of G-hat_l(q, a) B_ikl(q, b),
+            // B_ikl = sign(s) sum_n A_{il,kn} G-hat_n(q, b): 4 (i, k) x 2 (l) MMAs per pair
+            const double *at = ATs + o * 16;
+            double h0 = 0.0, h1 = 0.0;
+            if constexpr (P == 2) {
+              h0 = __shfl_sync(0xffffffffu, fr[1][0], t);
+              h1 = __shfl_sync(0xffffffffu, fr[1][1], t);
+            }
+#pragma unroll
+            for (int ll = 0; ll < 2; ll++) {
+              double C[2][2][2];  // [i][k][n]
+#pragma unroll
+              for (int j = 0; j < 4; j++) {
+                const double2 v = *reinterpret_cast<const double2 *>(at + ll * 8 + 2 * j);
+                C[j >> 1][j & 1][0] = v.x;
+                C[j >> 1][j & 1][1] = v.y;
+              }
+              int k = 0;
+#pragma unroll
+              for (int TA = 0; TA < NTM; TA++) {
+#pragma unroll
+                for (int TB = TA; TB < NTM; TB++, k++) {
+#pragma unroll
+                  for (int ik = 0; ik < 4; ik++) {
+                    const double bv = fma(C[ik >> 1][ik & 1][0], fr[TB][0], C[ik >> 1][ik & 1][1] * fr[TB][1]);
+                    dmma(acc[k][ik][0], acc[k][ik][1], fr[TA][ll], bv);
+                  }
+                }
+              }
+              if constexpr (P == 2) {
+                const double hl = ll ? h1 : h0;
+#pragma unroll
+                for (int ik = 0; ik < 4; ik++) {
+                  n8[ik] = fma(hl, fma(C[ik >> 1][ik & 1][0], fr[0][0], C[ik >> 1][ik & 1][1] * fr[0][1]), n8[ik]);
+                  d8[ik] = fma(hl, fma(C[ik >> 1][ik & 1][0], h0, C[ik >> 1][ik & 1][1] * h1), d8[ik]);
+                }
+              }
+            }
+          }
+          if constexpr (JAC && P == 2 && !NL) {
             // G-hat_i(q, 8) sits in lane (g = 0, t), tile 1
             const double h0 = __shfl_sync(0xffffffffu, fr[1][0], t), h1 = __shfl_sync(0xffffffffu, fr[1][1], t);
             const double s0 = sg * h0, s1 = sg * h1;
@@ -645,7 +731,7 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
             d8[2] = fma(s1, h0, d8[2]);
             d8[3] = fma(s1, h1, d8[3]);
           }
-          if constexpr (JAC) {
+          if constexpr (JAC && !NL) {
             int k = 0;
   #pragma unroll
             for (int TA = 0; TA < NTM; TA++) {
@@ -700,15 +786,28 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
                 const int b = 8 * TB + 4 * h + t;
                 if (a < NN && b < NN) {
                   const double mxx = acc[k][0][h], mxy = acc[k][1][h], myx = acc[k][2][h], myy = acc[k][3][h];
-                  const double kxx = c11 * mxx + mu * myy;
-                  const double kxy = lam * mxy + mu * myx;
-                  const double kyx = lam * myx + mu * mxy;
-                  const double kyy = c11 * myy + mu * mxx;
+                  // LINEAR: plane-stress combination of M; NONLINEAR: the block itself
+                  const double kxx = NL ? mxx : c11 * mxx + mu * myy;
+                  const double kxy = NL ? mxy : lam * mxy + mu * myx;
+                  const double kyx = NL ? myx : lam * myx + mu * mxy;
+                  const double kyy = NL ? myy : c11 * myy + mu * mxx;
                   const int s0 = frag_slot(k, h, 0);
-                  frag_put<P, PLAN>(O, el, a, b, 0, kxx, kxy, kyx, kyy, redsW + 128 * s0 + 4 * (4 * g + t));
                   if (TA < TB) {
                     const int s1 = frag_slot(k, h, 1);
+                    frag_put<P, PLAN>(O, el, a, b, 0, kxx, kxy, kyx, kyy, redsW + 128 * s0 + 4 * (4 * g + t));
                     frag_put<P, PLAN>(O, el, a, b, 1, kxx, kxy, kyx, kyy, redsW + 128 * s1 + 4 * (8 * t + pa));
+                  } else if (!NL) {
+                    frag_put<P, PLAN>(O, el, a, b, 0, kxx, kxy, kyx, kyy, redsW + 128 * s0 + 4 * (4 * g + t));
+                  } else if (a <= b) {
+                    // NONLINEAR diagonal tile: (a, b) for a <= b and, for a < b, its exact
+                    // transpose (b, a) at the staging position the (b, a) lane would use
+                    frag_put<P, PLAN>(O, el, a, b, 0, kxx, kxy, kyx, kyy, redsW + 128 * s0 + 4 * (4 * g + t));
+                    if (a < b) {
+                      const int xb = b - 8 * TA, xa = a - 8 * TA;  // pi(g') = xb; a = 8T + 4h' + t'
+                      const int gb = 2 * (xb & 3) + (xb >> 2);
+                      const int st = frag_slot(k, xa >> 2, 0);
+                      frag_put<P, PLAN>(O, el, a, b, 1, kxx, kxy, kyx, kyy, redsW + 128 * st + 4 * (4 * gb + (xa & 3)));
+                    }
                   }
                 }
               }
@@ -740,16 +839,20 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
                 const int b = 8 * TB + 4 * h + t;
                 if (a < NN && b < NN) {
                   const double mxx = acc[k][0][h], mxy = acc[k][1][h], myx = acc[k][2][h], myy = acc[k][3][h];
-                  const double kxx = c11 * mxx + mu * myy;
-                  const double kxy = lam * mxy + mu * myx;
-                  const double kyx = lam * myx + mu * mxy;
-                  const double kyy = c11 * myy + mu * mxx;
+                  // LINEAR: plane-stress combination of M; NONLINEAR: the block itself
+                  const double kxx = NL ? mxx : c11 * mxx + mu * myy;
+                  const double kxy = NL ? mxy : lam * mxy + mu * myx;
+                  const double kyx = NL ? myx : lam * myx + mu * mxy;
+                  const double kyy = NL ? myy : c11 * myy + mu * mxx;
+                  // NONLINEAR diagonal tiles: (a, b) for a <= b and its exact transpose
+                  const bool dir = TA < TB || !NL || a <= b;
+                  const bool trn = TA < TB || (NL && a < b);
                   if constexpr (PLAN) {
-                    frag_write<P>(O, el, a, b, 0, kxx, kxy, kyx, kyy, reds + 128 * slot++);
-                    if (TA < TB) frag_write<P>(O, el, a, b, 1, kxx, kxy, kyx, kyy, reds + 128 * slot++);
+                    if (dir) frag_write<P>(O, el, a, b, 0, kxx, kxy, kyx, kyy, reds + 128 * slot++);
+                    if (trn) frag_write<P>(O, el, a, b, 1, kxx, kxy, kyx, kyy, reds + 128 * slot++);
                   } else {
-                    frag_add_mapped<P>(O, el, a, b, 0, kxx, kxy, kyx, kyy, reds + 128 * slot++);
-                    if (TA < TB) frag_add_mapped<P>(O, el, a, b, 1, kxx, kxy, kyx, kyy, reds + 128 * slot++);
+                    if (dir) frag_add_mapped<P>(O, el, a, b, 0, kxx, kxy, kyx, kyy, reds + 128 * slot++);
+                    if (trn) frag_add_mapped<P>(O, el, a, b, 1, kxx, kxy, kyx, kyy, reds + 128 * slot++);
                   }
                 }
               }
@@ -769,10 +872,10 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
             if (t < 2 || diag) {
               const double mxx = diag ? d8[0] : n8[0], mxy = diag ? d8[1] : n8[1];
               const double myx = diag ? d8[2] : n8[2], myy = diag ? d8[3] : n8[3];
-              const double kxx = c11 * mxx + mu * myy;
-              const double kxy = lam * mxy + mu * myx;
-              const double kyx = lam * myx + mu * mxy;
-              const double kyy = c11 * myy + mu * mxx;
+              const double kxx = NL ? mxx : c11 * mxx + mu * myy;
+              const double kxy = NL ? mxy : lam * mxy + mu * myx;
+              const double kyx = NL ? myx : lam * myx + mu * mxy;
+              const double kyy = NL ? myy : c11 * myy + mu * mxx;
               const int b = diag ? 8 : pa, w = diag ? 0 : t;
               if constexpr (PLAN) {
                 frag_write<P>(O, el, 8, b, w, kxx, kxy, kyx, kyy, reds + 128 * slot);
@@ -955,7 +1058,7 @@ int launch_frag_p(const AsmArgs &a, cudaStream_t s) {
   using F = FragDims<P>;
   constexpr int NT = 32 * F::WARPS;
   auto kernel = frag_kernel<P, MODE>;
-  const size_t smem = FragLayout<P, (MODE & kPlan) == 0>::total;
+  const size_t smem = FragLayout<P, (MODE & kPlan) == 0, (MODE & kNL) != 0>::total;
   LaunchInfo li;
   int st = launch_info(kernel, NT, smem, li);
   if (st) return st;
@@ -994,7 +1097,9 @@ int launch_frag_mode(int order, const AsmArgs &a, cudaStream_t s) {
   switch (order) {
     case 2: return launch_frag_p<2, MODE>(a, s);
     case 3: return launch_frag_p<3, MODE>(a, s);
-    case 4: return launch_frag_p<4, MODE>(a, s);
+    case 4:
+      if constexpr ((MODE & kNL) != 0) return fail(FEM_ERR_INVALID_ORDER, "fragment kernel, NONLINEAR: order 4");
+      else return launch_frag_p<4, MODE>(a, s);
     default: return fail(FEM_ERR_INVALID_ORDER, "fragment kernel: order %d", order);
   }
 }
@@ -1012,14 +1117,16 @@ int launch_frag_mode(int order, const AsmArgs &a, cudaStream_t s) {
 // result, as order-1 row assembly does; at order 4 the FP32 element kernel is the
 // faster one (2.6 against 3.4 ms) and MIXED keeps it.
 bool frag_supported(int order, int precision, int strain, bool plan) {
+  if (strain == FEM_STRAIN_NONLINEAR) return precision == FEM_PRECISION_FP64 && (order == 2 || order == 3);
   if (strain != FEM_STRAIN_LINEAR) return false;
   if (precision == FEM_PRECISION_MIXED) return order == 2 || order == 3;
   if (precision != FEM_PRECISION_FP64) return false;
   return order == 2 || order == 3 || (order == 4 && plan);
 }
 
-int launch_frag(int order, int mode, const dev::AsmArgs &a, cudaStream_t s) {
+int launch_frag(int order, int mode, const dev::AsmArgs &a, cudaStream_t s, int strain) {
   using namespace dev;
+  if (strain == FEM_STRAIN_NONLINEAR) mode |= kNL;
   switch (mode) {
     case kPlan | kRes: return launch_frag_mode<kPlan | kRes>(order, a, s);
     case kPlan | kJac: return launch_frag_mode<kPlan | kJac>(order, a, s);
@@ -1027,6 +1134,12 @@ int launch_frag(int order, int mode, const dev::AsmArgs &a, cudaStream_t s) {
     case kRes: return launch_frag_mode<kRes>(order, a, s);
     case kJac: return launch_frag_mode<kJac>(order, a, s);
     case kRes | kJac: return launch_frag_mode<kRes | kJac>(order, a, s);
+    case kNL | kPlan | kRes: return launch_frag_mode<kNL | kPlan | kRes>(order, a, s);
+    case kNL | kPlan | kJac: return launch_frag_mode<kNL | kPlan | kJac>(order, a, s);
+    case kNL | kPlan | kRes | kJac: return launch_frag_mode<kNL | kPlan | kRes | kJac>(order, a, s);
+    case kNL | kRes: return launch_frag_mode<kNL | kRes>(order, a, s);
+    case kNL | kJac: return launch_frag_mode<kNL | kJac>(order, a, s);
+    case kNL | kRes | kJac: return launch_frag_mode<kNL | kRes | kJac>(order, a, s);
     default: return fail(FEM_ERR_INVALID_ARGUMENT, "fragment kernel: mode %d", mode);
   }
 }

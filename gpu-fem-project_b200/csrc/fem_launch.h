@@ -103,7 +103,7 @@ constexpr int kRowTileChunks = 16;
 // mode (one colour, list positions [a.begin, a.begin + a.count)) or drop-in mode
 // (elements through the reference map, accumulate-into).
 bool frag_supported(int order, int precision, int strain, bool plan);
-int launch_frag(int order, int mode, const dev::AsmArgs &a, cudaStream_t s);
+int launch_frag(int order, int mode, const dev::AsmArgs &a, cudaStream_t s, int strain = FEM_STRAIN_LINEAR);
 // Its tile-queue form for batches and the server (residual and Jacobian).
 int launch_frag_batched(int order, const dev::AsmArgs *meshes, const dev::Tile *tiles, int ntiles, int *counter,
                         cudaStream_t s);
