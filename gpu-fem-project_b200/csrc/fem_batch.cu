@@ -43,20 +43,17 @@ int launch_batched_p(const dev::AsmArgs *meshes, const dev::Tile *tiles, int nti
   return FEM_SUCCESS;
 }
 
+// The batched element kernel serves what the fragment kernel does not: order 1
+// (meshes whose rows are too long for row assembly) and the FP32 order-4 path
+// (FEM_PRECISION_MIXED); see frag_supported.
 template <typename T>
 int launch_batched_t(int p, const dev::AsmArgs *meshes, const dev::Tile *tiles, int ntiles, int *counter,
                      cudaStream_t s) {
-  switch (p) {
-    case 1: return launch_batched_p<1, T>(meshes, tiles, ntiles, counter, s);
-    case 2:
-      if constexpr (sizeof(T) == 8) return fail(FEM_ERR_INVALID_ORDER, "order 2 FP64 runs the fragment kernel");
-      else return launch_batched_p<2, T>(meshes, tiles, ntiles, counter, s);
-    case 3:
-      if constexpr (sizeof(T) == 8) return fail(FEM_ERR_INVALID_ORDER, "order 3 FP64 runs the fragment kernel");
-      else return launch_batched_p<3, T>(meshes, tiles, ntiles, counter, s);
-    case 4: return launch_batched_p<4, T>(meshes, tiles, ntiles, counter, s);
-    default: return fail(FEM_ERR_INVALID_ORDER, "order %d", p);
+  if (p == 1) return launch_batched_p<1, T>(meshes, tiles, ntiles, counter, s);
+  if constexpr (sizeof(T) == 4) {
+    if (p == 4) return launch_batched_p<4, T>(meshes, tiles, ntiles, counter, s);
   }
+  return fail(FEM_ERR_INVALID_ORDER, "batched element kernel: order %d", p);
 }
 
 }  // namespace
