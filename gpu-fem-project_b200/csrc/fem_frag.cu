@@ -34,9 +34,10 @@
 //                blocks (a, b = 8TB + 4h + t), so the plane-stress combination
 //                needs no shuffle and a warp store covers eight runs of four
 //                consecutive blocks.  p = 4: interleaved rows r = 2a + i in seven
-//                tiles (a = 4T + g/2), one pass per row tile with the fragments
-//                recomputed from the table; lanes l, l^4 exchange the two rows of
-//                a block.  Blocks above the diagonal are also written transposed.
+//                tiles (a = 4T + g/2), one pass per group of tile pairs with the
+//                group's fragments rebuilt from the table (the residual rides on
+//                the first three groups); lanes l, l^4 exchange the two rows of a
+//                block.  Blocks above the diagonal are also written transposed.
 //
 // Writes.  Plan mode: a launch is one colour; the first contributor of a block
 // stores it (one 256-bit store); a later colour adds its 2x2 blocks with
@@ -83,6 +84,9 @@ struct FragDims {
   static constexpr int TABW = IL ? 16 : 32;   // table entries per (k-step, tile): lane, or (g/2, t)
   static_assert(P >= 2 && P <= 4 && (IL || NTN == 2), "fragment kernel: orders 2 to 4");
 };
+
+template <int V>
+using IC = std::integral_constant<int, V>;
 
 // Shared memory: CTA tables, then one region per warp.  DROP: drop-in mode (the
 // stage holds the reference element map rows, NN*NN ints per element, instead of
@@ -889,34 +893,24 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
     } else {
       // interleaved rows r = 2a + i (p = 4): lane (g, t) builds G-hat_i(q = 4ks + t,
       // a = 4T + g/2), i = g%2, the A fragment of row tile T and the B fragment of
-      // column tile T; lanes l and l^4 hold the two rows of a 2x2 block.  The residual
-      // has a pass of its own, the stiffness one pass per group of row tiles.
+      // column tile T; lanes l and l^4 hold the two rows of a 2x2 block.  The stiffness
+      // takes one pass per group of tile pairs; the residual rides on the first three
+      // groups (a pass of its own when the Jacobian is not assembled).
       const int ii = g & 1, ah = g >> 1;
       const double2 *WIi = ii ? WI1 : WI0;
       const double2 *WSi = ii ? WS1 : WS0;
       double *reds = redsW + 4 * lane;
       int nw = 0;  // writes so far: ring position of the staging slot
       for (int el = 0; el < ne; el++) {
-        // residual R_(a,i'): lane partials over its quadrature points, a full sum over the
-        // component pair (xor 4), then a reduce-scatter over the four lanes t (lane t
-        // ends with tiles 2t and 2t + 1)
-        if constexpr (RES) {
-          double rp[8][2];
+        // residual R_(a,i'): lane partials rp over its quadrature points (with the
+        // Jacobian, accumulated by the first three stiffness groups, which between them
+        // form every column tile's fragments; alone, in a pass of its own), then a full
+        // sum over the component pair (xor 4) and a reduce-scatter over the four lanes
+        // t (lane t ends with tiles 2t and 2t + 1)
+        double rp[8][2];
 #pragma unroll
-          for (int T = 0; T < 8; T++) rp[T][0] = rp[T][1] = 0.0;
-#pragma unroll
-          for (int ks = 0; ks < K4; ks++) {
-            const int o = el * NQP + 4 * ks + t;
-            const double2 w = WIi[o];
-            const double2 sj = WSi[o];  // (S-hat_xj, S-hat_yj), j = this lane's component
-#pragma unroll
-            for (int C = 0; C < K4; C++) {
-              const double2 d = tabF[(ks * K4 + C) * 16 + 4 * ah + t];
-              const double gv = fma(w.x, d.x, w.y * d.y);
-              rp[C][0] = fma(gv, sj.x, rp[C][0]);
-              rp[C][1] = fma(gv, sj.y, rp[C][1]);
-            }
-          }
+        for (int T = 0; T < 8; T++) rp[T][0] = rp[T][1] = 0.0;
+        auto res_write = [&]() {
 #pragma unroll
           for (int T = 0; T < K4; T++)
 #pragma unroll
@@ -946,17 +940,37 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
               }
             }
           }
+        };
+        if constexpr (RES && !JAC) {
+#pragma unroll
+          for (int ks = 0; ks < K4; ks++) {
+            const int o = el * NQP + 4 * ks + t;
+            const double2 w = WIi[o];
+            const double2 sj = WSi[o];  // (S-hat_xj, S-hat_yj), j = this lane's component
+#pragma unroll
+            for (int C = 0; C < K4; C++) {
+              const double2 d = tabF[(ks * K4 + C) * 16 + 4 * ah + t];
+              const double gv = fma(w.x, d.x, w.y * d.y);
+              rp[C][0] = fma(gv, sj.x, rp[C][0]);
+              rp[C][1] = fma(gv, sj.y, rp[C][1]);
+            }
+          }
+          res_write();
         }
-        // stiffness: row tiles in groups {0}, {1}, {2,3}, {4,5,6} (at most nine live
-        // accumulator tiles); within a group the k-steps are outermost, each fragment
-        // of the step is formed once and feeds every tile (R, C >= R) of the group
-        auto group = [&](auto r0c, auto r1c) {
+        // stiffness: the 28 tile pairs (R, C >= R) in four groups, each a triangle
+        // {R0..R1-1}^2 or a rectangle {R0..R1-1} x {C0..C1-1} of the upper triangle
+        // (at most ten live accumulator tiles); within a group the k-steps are
+        // outermost and each fragment of the group's rows and columns is formed once
+        // per step: 17 fragment builds per k-step for the 28 tile pairs
+        auto group = [&](auto r0c, auto r1c, auto c0c, auto c1c, auto resc) {
           constexpr int R0 = decltype(r0c)::value, R1 = decltype(r1c)::value;
-          double acc[R1 - R0][K4][2];
+          constexpr int C0 = decltype(c0c)::value, C1 = decltype(c1c)::value;
+          constexpr bool GRES = RES && decltype(resc)::value;  // residual tiles C0..C1-1
+          double acc[R1 - R0][C1 - C0][2];
 #pragma unroll
           for (int R = R0; R < R1; R++)
 #pragma unroll
-            for (int C = 0; C < K4; C++) acc[R - R0][C][0] = acc[R - R0][C][1] = 0.0;
+            for (int C = C0; C < C1; C++) acc[R - R0][C - C0][0] = acc[R - R0][C - C0][1] = 0.0;
 #pragma unroll
           for (int ks = 0; ks < K4; ks++) {
             const int o = el * NQP + 4 * ks + t;
@@ -964,15 +978,26 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
             const double sg = SGs[o];
             double fr[K4];
 #pragma unroll
-            for (int C = R0; C < K4; C++) {
-              const double2 d = tabF[(ks * K4 + C) * 16 + 4 * ah + t];
-              fr[C] = fma(w.x, d.x, w.y * d.y);
+            for (int T = 0; T < K4; T++) {
+              if ((T >= R0 && T < R1) || (T >= C0 && T < C1)) {
+                const double2 d = tabF[(ks * K4 + T) * 16 + 4 * ah + t];
+                fr[T] = fma(w.x, d.x, w.y * d.y);
+              }
+            }
+            if constexpr (GRES) {
+              const double2 sj = WSi[o];
+#pragma unroll
+              for (int C = C0; C < C1; C++) {
+                rp[C][0] = fma(fr[C], sj.x, rp[C][0]);
+                rp[C][1] = fma(fr[C], sj.y, rp[C][1]);
+              }
             }
 #pragma unroll
             for (int R = R0; R < R1; R++) {
               const double af = sg * fr[R];
 #pragma unroll
-              for (int C = R; C < K4; C++) dmma(acc[R - R0][C][0], acc[R - R0][C][1], af, fr[C]);
+              for (int C = (R > C0 ? R : C0); C < C1; C++)
+                dmma(acc[R - R0][C - C0][0], acc[R - R0][C - C0][1], af, fr[C]);
             }
           }
           // blocks: lane pair (l, l^4) exchanges rows; lane i = 0 writes (a, b), lane
@@ -981,11 +1006,11 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
           for (int R = R0; R < R1; R++) {
             const int a = 4 * R + ah;
 #pragma unroll
-            for (int C = R; C < K4; C++) {
-              const double o0 = __shfl_xor_sync(0xffffffffu, acc[R - R0][C][0], 4);
-              const double o1 = __shfl_xor_sync(0xffffffffu, acc[R - R0][C][1], 4);
-              const double mxx = ii ? o0 : acc[R - R0][C][0], mxy = ii ? o1 : acc[R - R0][C][1];
-              const double myx = ii ? acc[R - R0][C][0] : o0, myy = ii ? acc[R - R0][C][1] : o1;
+            for (int C = (R > C0 ? R : C0); C < C1; C++) {
+              const double o0 = __shfl_xor_sync(0xffffffffu, acc[R - R0][C - C0][0], 4);
+              const double o1 = __shfl_xor_sync(0xffffffffu, acc[R - R0][C - C0][1], 4);
+              const double mxx = ii ? o0 : acc[R - R0][C - C0][0], mxy = ii ? o1 : acc[R - R0][C - C0][1];
+              const double myx = ii ? acc[R - R0][C - C0][0] : o0, myy = ii ? acc[R - R0][C - C0][1] : o1;
               const int b = 4 * C + t;
               if (a < NN && b < NN && a <= b && (ii == 0 || a < b)) {
                 const double kxx = c11 * mxx + mu * myy;
@@ -1006,19 +1031,20 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
           }
         };
         if constexpr (JAC) {
-          static_assert(K4 == 7, "row-tile groups of the order-4 layout");
+          static_assert(K4 == 7, "tile-pair groups of the order-4 layout");
           // compiler barriers keep each group's table loads inside the group (hoisting
           // them across groups raises register pressure past the budget)
           asm volatile("" ::: "memory");
-          group(std::integral_constant<int, 0>{}, std::integral_constant<int, 1>{});
+          group(IC<0>{}, IC<3>{}, IC<0>{}, IC<3>{}, std::true_type{});
           asm volatile("" ::: "memory");
-          group(std::integral_constant<int, 1>{}, std::integral_constant<int, 2>{});
+          group(IC<0>{}, IC<3>{}, IC<3>{}, IC<5>{}, std::true_type{});
           asm volatile("" ::: "memory");
-          group(std::integral_constant<int, 2>{}, std::integral_constant<int, 3>{});
+          group(IC<0>{}, IC<3>{}, IC<5>{}, IC<7>{}, std::true_type{});
+          if constexpr (RES) res_write();
           asm volatile("" ::: "memory");
-          group(std::integral_constant<int, 3>{}, std::integral_constant<int, 5>{});
+          group(IC<3>{}, IC<5>{}, IC<3>{}, IC<7>{}, std::false_type{});
           asm volatile("" ::: "memory");
-          group(std::integral_constant<int, 5>{}, std::integral_constant<int, 7>{});
+          group(IC<5>{}, IC<7>{}, IC<5>{}, IC<7>{}, std::false_type{});
         }
       }
     }
