@@ -187,10 +187,7 @@ def run_ours(args):
     sptr = stream.cuda_stream
     with torch.cuda.stream(stream):
         d = fem.DeviceMesh(mesh, dev)
-        # order 3: the patch layout (CTA-summed element strips, row-segment writes)
-        # unless --paths leaves out plan_patch; the colour path is timed beside it
-        patches = mesh.order == 3 and "plan_patch" in args.paths
-        plan = fem.Plan(mesh.order, mesh.num_nodes, mesh.conn_ptr, mesh.conn, patches=patches)
+        plan = fem.Plan(mesh.order, mesh.num_nodes, mesh.conn_ptr, mesh.conn)
         nnzb = plan.nnzb
         res = torch.empty(mesh.num_nodes * 2, dtype=torch.float64, device=dev)
         mat = torch.empty(nnzb * 4, dtype=torch.float64, device=dev)
@@ -215,24 +212,6 @@ def run_ours(args):
         return ms, launches_per_step * steps
 
     paths = {}
-    if patches:
-        # the colour-ordered plan on the same mesh, for comparison (and as a check:
-        # the two paths sum shared blocks in different orders, nothing else differs)
-        plan_c = fem.Plan(mesh.order, mesh.num_nodes, mesh.conn_ptr, mesh.conn)
-        fn = (lambda: plan_c.assemble(d.states, d.coords, E, nu, t, res, mat, stream=sptr))
-        ms, _ = time_steps(fn, max(2, args.steps // 2), args.warmup, plan_c.launches())
-        paths["plan_fp64_colours"] = {"ms": ms, "elements_per_s": nE / (ms * 1e-3),
-                                      "kernel": kernel_label(plan_c, mesh.order, "fp64")}
-        with torch.cuda.stream(stream):
-            res_c, mat_c = res.clone(), mat.clone()
-            plan.assemble(d.states, d.coords, E, nu, t, res, mat, stream=sptr)
-            paths["plan_fp64_colours"]["max_rel_diff_vs_patches"] = {
-                "residual": float((res - res_c).abs().max() / res_c.abs().max()),
-                "jacobian": float((mat - mat_c).abs().max() / mat_c.abs().max())}
-            del res_c, mat_c
-        stream.synchronize()
-        plan_c.close()
-        del plan_c
     # plan path (overwrite, no zeroing), FP64 and mixed
     for prec in [x for x in ("fp64", "mixed") if f"plan_{x}" in args.paths]:
         fn = (lambda prec=prec: plan.assemble(d.states, d.coords, E, nu, t, res, mat, precision=prec, stream=sptr))
@@ -409,8 +388,6 @@ def kernel_label(plan, order, prec):
     """The kernel that runs one assembly of `plan` (the dispatch of fem_plan_assemble)."""
     if plan.row_chunks > 0:
         return "rows_p1_kernel, 1 launch per step"
-    if plan.num_patches > 0 and order == 3:
-        return f"frag_patch_kernel<3> x {plan.patch_colours} patch-colour launches per step"
     # the fragment kernel serves orders 2-3 in both precisions (MIXED runs it in FP64)
     # and order 4 in FP64; FP32 order 4 runs the element kernel
     if order in (2, 3) or (order == 4 and prec == "fp64"):
@@ -719,9 +696,8 @@ def main():
     ap.add_argument("--batch-precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--ref-elements", type=int, default=131072)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
-    ap.add_argument("--paths", default="plan_fp64,plan_mixed,plan_patch,dropin_fp64,plan_nonlinear",
-                    help="comma list of plan_fp64, plan_mixed, plan_patch (order 3: patch layout), dropin_fp64, "
-                         "dropin_mixed, plan_nonlinear")
+    ap.add_argument("--paths", default="plan_fp64,plan_mixed,dropin_fp64,plan_nonlinear",
+                    help="comma list of plan_fp64, plan_mixed, dropin_fp64, dropin_mixed, plan_nonlinear")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--peaks", action="store_true", help="print measured FP64/FP32/FP64-MMA peaks and exit")
     args = ap.parse_args()

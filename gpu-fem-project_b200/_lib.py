@@ -28,8 +28,6 @@ FEM_PRECISION_MIXED = 1
 FEM_STRAIN_LINEAR = 0
 FEM_STRAIN_NONLINEAR = 1
 
-FEM_PLAN_PATCHES = 1
-
 _i = C.c_int
 _i64 = C.c_int64
 _d = C.c_double
@@ -54,9 +52,6 @@ SIGNATURES = {
     "fem_colour_elements": (_i, [_i, _p, _p, _i, _p, _pi]),
     "fem_bsr_spmv": (_i, [_i, _p, _p, _p, _p, _p, _p]),
     "fem_plan_create": (_i, [_i, _i, _p, _p, _i, C.POINTER(_p)]),
-    "fem_plan_create_ex": (_i, [_i, _i, _p, _p, _i, _i, C.POINTER(_p)]),
-    "fem_plan_patches": (_i, [_p, _pi, _pi]),
-    "fem_patch_layout": (_i, [_i, _i, _p, _p, _i, _pi, _pi, _pi64, _pi64, _p, _p, _p, _p, _p, _p, _p, _p]),
     "fem_plan_destroy": (_i, [_p]),
     "fem_plan_info": (_i, [_p, _pi, _pi, _pi64, _pi, _pi64]),
     "fem_plan_get_pattern": (_i, [_p, _p, _p]),

@@ -12,8 +12,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import (FEM_PLAN_PATCHES, FEM_PRECISION_FP64, FEM_PRECISION_MIXED, FEM_STRAIN_LINEAR, FEM_STRAIN_NONLINEAR,
-                   check, lib)
+from ._lib import FEM_PRECISION_FP64, FEM_PRECISION_MIXED, FEM_STRAIN_LINEAR, FEM_STRAIN_NONLINEAR, check, lib
 
 _PRECISION = {"fp64": FEM_PRECISION_FP64, "mixed": FEM_PRECISION_MIXED}
 # A2D::GreenStrainType of the reference kernels' strainType template argument
@@ -138,29 +137,6 @@ def colour_elements(num_nodes, conn_ptr, conn):
     return colour, nc.value
 
 
-def patch_layout(element_order, num_nodes, conn_ptr, conn):
-    """The order-3 patch layout on the host (fem_patch_layout): dict of numpy arrays
-    colour_ptr, elem [P, 8], code [P, 8, stride], slot_base [P, 8, nn], seg_ptr,
-    seg [S, 2], node_ptr, node."""
-    cp, cn = _np(conn_ptr, np.int32), _np(conn, np.int32)
-    ne = cp.size - 1
-    npch, ncol = C.c_int(0), C.c_int(0)
-    nseg, nnod = C.c_int64(0), C.c_int64(0)
-    args = (int(element_order), int(num_nodes), cp.ctypes.data, cn.ctypes.data, ne)
-    sizes = (C.byref(npch), C.byref(ncol), C.byref(nseg), C.byref(nnod))
-    check(lib.fem_patch_layout(*args, *sizes, *([None] * 8)), "fem_patch_layout")
-    nn = (int(element_order) + 1) ** 2
-    stride = (nn * nn + nn + 15) // 16 * 16
-    P = npch.value
-    out = dict(colour_ptr=np.zeros(ncol.value + 1, np.int32), elem=np.zeros((P, 8), np.int32),
-               code=np.zeros((P, 8, stride), np.uint8), slot_base=np.zeros((P, 8, nn), np.int32),
-               seg_ptr=np.zeros(P + 1, np.int32), seg=np.zeros((nseg.value, 2), np.int32),
-               node_ptr=np.zeros(P + 1, np.int32), node=np.zeros(nnod.value, np.int32))
-    keys = ("colour_ptr", "elem", "code", "slot_base", "seg_ptr", "seg", "node_ptr", "node")
-    check(lib.fem_patch_layout(*args, *sizes, *(out[k].ctypes.data for k in keys)), "fem_patch_layout")
-    return out
-
-
 def bsr_spmv(rowp, cols, values, x, y, stream=None):
     """y = A x on the device for the 2x2-block BSR matrix (rowp, cols, values)."""
     import torch
@@ -173,12 +149,11 @@ class Plan:
     """Device-resident assembly plan of one mesh (fem_plan_*): BSR pattern,
     colouring and block codes.  `assemble` overwrites the outputs completely."""
 
-    def __init__(self, element_order, num_nodes, conn_ptr, conn, *, patches=False):
+    def __init__(self, element_order, num_nodes, conn_ptr, conn):
         cp, cn = _np(conn_ptr, np.int32), _np(conn, np.int32)
         self._h = C.c_void_p()
-        flags = FEM_PLAN_PATCHES if patches else 0
-        check(lib.fem_plan_create_ex(int(element_order), int(num_nodes), cp.ctypes.data, cn.ctypes.data, cp.size - 1,
-                                     flags, C.byref(self._h)), "fem_plan_create_ex")
+        check(lib.fem_plan_create(int(element_order), int(num_nodes), cp.ctypes.data, cn.ctypes.data, cp.size - 1,
+                                  C.byref(self._h)), "fem_plan_create")
         self.order = int(element_order)
         nn, ne, nc = C.c_int(), C.c_int(), C.c_int()
         nnzb, nbytes = C.c_int64(), C.c_int64()
@@ -189,20 +164,10 @@ class Plan:
         rc = C.c_int()
         check(lib.fem_plan_row_chunks(self._h, C.byref(rc)), "fem_plan_row_chunks")
         self.row_chunks = rc.value
-        pc, pcol = C.c_int(), C.c_int()
-        check(lib.fem_plan_patches(self._h, C.byref(pc), C.byref(pcol)), "fem_plan_patches")
-        self.num_patches, self.patch_colours = pc.value, pcol.value
 
-    def launches(self, strain="linear", jacobian=True) -> int:
-        """Kernel launches of one assemble(): 1 for order-1 row assembly, one per patch
-        colour for a patch-layout Jacobian, else one per element colour."""
-        if _strain(strain) != FEM_STRAIN_LINEAR:
-            return self.num_colours
-        if self.row_chunks > 0:
-            return 1
-        if self.num_patches > 0 and jacobian:
-            return self.patch_colours
-        return self.num_colours
+    def launches(self, strain="linear") -> int:
+        """Kernel launches of one assemble(): 1 for order-1 row assembly, else one per colour."""
+        return 1 if self.row_chunks > 0 and _strain(strain) == FEM_STRAIN_LINEAR else self.num_colours
 
     @property
     def handle(self) -> int:

@@ -18,7 +18,7 @@ INCLUDE = ROOT / "include"
 LIB = PKG / "libfemb200.so"
 
 SOURCES = ["fem_kernels.cu", "fem_nonlinear.cu", "fem_rows.cu", "fem_batch.cu", "fem_server.cu", "fem_static.cu",
-           "fem_frag.cu", "fem_host.cpp", "fem_patch.cpp", "fem_probe.cu"]
+           "fem_frag.cu", "fem_host.cpp", "fem_probe.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -106,25 +106,21 @@ struct Vec2<float> {
 };
 
 // kNL: GreenStrainType::NONLINEAR (Green strain, FP64 only); default LINEAR.
-enum : int { kRes = 1, kJac = 2, kPlan = 4, kNL = 8, kPatch = 16 };
+enum : int { kRes = 1, kJac = 2, kPlan = 4, kNL = 8 };
 
 struct AsmArgs {
-  // drop-in fields | order-1 plan row tables | order-3 patch tables (a plan never
-  // reads the drop-in ones; the patch kernel never reads the row tables)
+  // drop-in fields | order-1 plan row tables (a plan never reads the drop-in ones)
   union {
     const int *connPtr;     // drop-in: CSR offsets
     const int *rowElemPtr;  // plan, order 1: per row, range of rowElem entries
-    const int *patchRb;     // patch layout: slot base * 256 + local node per (position, node)
   };
   union {
-    const int *conn;      // drop-in: node ids
-    const int *rowElem;   // plan, order 1: {k << 2 | a, four ranks} per (row, element)
-    const int *patchTab;  // patch layout: segments (two ints each), then residual rows
+    const int *conn;     // drop-in: node ids
+    const int *rowElem;  // plan, order 1: {k << 2 | a, four ranks} per (row, element)
   };
   union {
     const int *map;       // drop-in: element block offsets (doubles)
     const int *rowChunk;  // plan, order 1: row ranges of the warp chunks
-    const int2 *patchPtr;  // patch layout: per patch (first segment, first residual row in patchTab)
   };
   const int *connList;       // plan: node ids of the listed elements, nn each
   const uint8_t *blockCode;  // plan: per listed element a Dims<P>::CS-byte code record

@@ -90,9 +90,8 @@ using IC = std::integral_constant<int, V>;
 
 // Shared memory: CTA tables, then one region per warp.  DROP: drop-in mode (the
 // stage holds the reference element map rows, NN*NN ints per element, instead of
-// plan code records).  PATCH: no per-warp staging slots; the CTA's patch copy of
-// the matrix blocks and residual rows follows the warp regions.
-template <int P, bool DROP = false, bool NL = false, bool PATCH = false>
+// plan code records).
+template <int P, bool DROP = false, bool NL = false>
 struct FragLayout {
   using F = FragDims<P>;
   static constexpr int K4 = F::K4, NTN = F::NTN, NQP = F::NQP, NN = F::NN;
@@ -113,14 +112,12 @@ struct FragLayout {
   static constexpr size_t STAGE = align16(RB + 4 * 2 * NN);  // [2 buffers][2 elements][CS] code records
   // staging slots: p = 3, 3 node-tile pairs x 2 halves, direct and transposed; p = 2,
   // the (at most 8) blocks one lane writes per element; p = 4, a ring of 4 per lane
-  static constexpr int NSLOT = PATCH ? 0 : (F::IL ? 4 : 8);
+  static constexpr int NSLOT = F::IL ? 4 : 8;
   static constexpr size_t REDS = align16(STAGE + 2 * 2 * CS);  // double4 [NSLOT][32]: bulk-reduction sources
   // NONLINEAR: sign(s) x tangent modulus, double [2][NQP][2 (l)][8 (i, k, n)]
   static constexpr size_t AT = align16(REDS + 32 * NSLOT * 32);
   static constexpr size_t warp_bytes = align16(AT + (NL ? 8 * 2 * NQP * 16 : 0));
-  static constexpr size_t PBUF = (warps + F::WARPS * warp_bytes + 127) / 128 * 128;  // double4 [kPatchSlots]
-  static constexpr size_t PRES = PBUF + 32 * kPatchSlots;                              // double2 [kPatchNodes]
-  static constexpr size_t total = PATCH ? PRES + 16 * kPatchNodes : warps + F::WARPS * warp_bytes;
+  static constexpr size_t total = warps + F::WARPS * warp_bytes;
 };
 
 __device__ __forceinline__ double sel4(double x0, double x1, double x2, double x3, int i) {
@@ -357,44 +354,6 @@ struct PairStride {
   }
 };
 
-// Patch layout: every warp of the CTA takes its pair (positions 2w, 2w + 1) of
-// patches p, p + stride, ... of [begin, end); all warps see the same patches.
-struct PatchStride {
-  static constexpr bool kBatched = false;
-  int64_t begin, end, p, stride;
-  int warp;
-  __device__ PairCursor next(int) {
-    PairCursor c{0, 0, 0};
-    if (begin + p < end) {
-      c.ne = 2;
-      c.k0 = (begin + p) * kPatchElems + 2 * warp;
-    }
-    p += stride;
-    return c;
-  }
-};
-
-// Block (a, b) of element el (or its transpose (b, a) with w = 1) into the CTA's
-// patch copy: slot = slot base of row r0 + rank of the block in that row; stored,
-// or added to the phase-0 value when the code says so.
-template <int P>
-__device__ __forceinline__ void patch_put(const Out &O, double *pbuf, int el, int a, int b, int w, double kxx,
-                                          double kxy, double kyx, double kyy) {
-  constexpr int NN = Dims<P>::NN, CS = Dims<P>::CS;
-  const int r0 = w ? b : a, c0 = w ? a : b;
-  const double v0 = kxx, v1 = w ? kyx : kxy, v2 = w ? kxy : kyx, v3 = kyy;
-  const uint8_t code = O.codes[el * CS + r0 * NN + c0];
-  double2 *d = reinterpret_cast<double2 *>(pbuf + 4 * ((O.rbase[el * NN + r0] >> 8) + (code & 0x7f)));
-  if (code & 0x80) {
-    const double2 x0 = d[0], x1 = d[1];
-    d[0] = make_double2(x0.x + v0, x0.y + v1);
-    d[1] = make_double2(x1.x + v2, x1.y + v3);
-  } else {
-    d[0] = make_double2(v0, v1);
-    d[1] = make_double2(v2, v3);
-  }
-}
-
 // Many meshes: the pairs of the tiles this warp pulls from the launch's queue
 // (one atomic counter per launch; tiles hold even element counts except at the
 // end of a colour range, so pairs never straddle tiles).
@@ -437,16 +396,14 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
                                           const AsmArgs *__restrict__ meshes) {
   constexpr bool PLAN = (MODE & kPlan) != 0;
   constexpr bool NL = (MODE & kNL) != 0;
-  constexpr bool PATCH = (MODE & kPatch) != 0;  // CTA patch copy, phases, segment writes
   using F = FragDims<P>;
-  using L = FragLayout<P, !PLAN, NL, PATCH>;
+  using L = FragLayout<P, !PLAN, NL>;
   constexpr int NN = F::NN, NQ = F::NQ, K4 = F::K4, NTN = F::NTN, NQP = F::NQP, CS = F::CS;
   constexpr int STG = L::CS;  // staged bytes per element: plan code record or map rows
   constexpr bool RES = (MODE & kRes) != 0, JAC = (MODE & kJac) != 0;
   constexpr bool RUNS = (P == 3);  // order 3: staged row runs, one bulk reduction per adjacent run
   static_assert(!NL || !F::IL, "NONLINEAR strain: orders 2 and 3");
   static_assert(PLAN || !Gen::kBatched, "drop-in mode assembles one mesh");
-  static_assert(!PATCH || (P == 3 && PLAN && JAC && !NL && !Gen::kBatched), "patch layout: order 3, LINEAR, one mesh");
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane >> 2, t = lane & 3;
@@ -466,8 +423,6 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
   unsigned char *stage = ws + L::STAGE;
   double *redsW = reinterpret_cast<double *>(ws + L::REDS);  // staging slot s at redsW + 128 s
   double *ATs = reinterpret_cast<double *>(ws + L::AT);      // NONLINEAR tangent
-  double *pbuf = reinterpret_cast<double *>(smem + L::PBUF);   // patch copy: 2x2 blocks (PATCH)
-  double2 *pres = reinterpret_cast<double2 *>(smem + L::PRES);  // patch copy: residual rows (PATCH)
 
   // Mesh arguments are read through `mtab` (for one mesh, a pointer to the kernel
   // parameter).  At p = 4 it is laundered once per step: the compiler then reloads
@@ -506,8 +461,7 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
         const AsmArgs &M = args(c);
         const double *src = c_ld < 2 ? M.coords : M.states;
         val[ks] = __ldg(src + 2 * (int64_t)node[ks] + (c_ld & 1));
-        if (PLAN && JAC && c_ld == 1)
-          rbv[ks] = PATCH ? __ldg(M.patchRb + (c.k0 + e_ld) * NN + 4 * ks + t) : __ldg(M.rowp + node[ks]);
+        if (PLAN && JAC && c_ld == 1) rbv[ks] = __ldg(M.rowp + node[ks]);
       }
     }
   };
@@ -543,13 +497,6 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
     const int ne = cur.ne;
     const AsmArgs &M = args(cur);
     const double mu = M.mu, lam = M.lam, thick = M.t, c11 = lam + 2.0 * mu;
-    // patch positions may be empty (node ids -1): element e is present when its
-    // node 0 (lane 16e, ks = 0) is
-    bool present[2] = {true, true};
-    if constexpr (PATCH) {
-      present[0] = __shfl_sync(0xffffffffu, nodeB[0], 0) >= 0;
-      present[1] = __shfl_sync(0xffffffffu, nodeB[0], 16) >= 0;
-    }
     // 0. commit this pair's gathered data
     double val[K4];
 #pragma unroll
@@ -618,7 +565,7 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
       };
       const int tq = 4 * m + c_ld;  // column tile of this lane's quadrature point
       const int q = 4 * tq + t;
-      const bool valid = e_ld < ne && tq < K4 && q < NQ && (e_ld ? present[1] : present[0]);
+      const bool valid = e_ld < ne && tq < K4 && q < NQ;
       double2 wi0 = make_double2(0, 0), wi1 = make_double2(0, 0), ws0 = make_double2(0, 0), ws1 = make_double2(0, 0);
       double sg = 0.0;
       if (valid) {
@@ -803,13 +750,6 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
             }
           }
         }
-        // patch layout: element el of every pair is phase el.  Before phase 0 the
-        // previous patch's bulk writes have read the patch copy; before phase 1 every
-        // phase-0 value is in it.
-        if constexpr (PATCH) {
-          if (el == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
-          __syncthreads();
-        }
         // residual: sum over the four lanes t of a node (reduce-scatter over node tiles)
         if constexpr (RES) {
           const int Tm = t >> 1, To = Tm ^ 1;
@@ -818,15 +758,7 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
           sx += __shfl_xor_sync(0xffffffffu, sx, 1);
           sy += __shfl_xor_sync(0xffffffffu, sy, 1);
           const int a = 8 * Tm + pa;
-          if (PATCH && (t & 1) == 0 && a < NN && present[el]) {
-            double2 *d = pres + (O.rbase[el * NN + a] & 255);
-            if (O.codes[el * CS + NN * NN + a]) {
-              const double2 x = *d;
-              *d = make_double2(x.x + sx, x.y + sy);
-            } else {
-              *d = make_double2(sx, sy);
-            }
-          } else if (!PATCH && (t & 1) == 0 && a < NN) {
+          if ((t & 1) == 0 && a < NN) {
             double *dst = M.residual + 2 * (int64_t)nid[el * NN + a];
             if (PLAN && O.codes[el * CS + NN * NN + a]) {
               *reinterpret_cast<double2 *>(dst) = make_double2(sx, sy);
@@ -843,31 +775,7 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
         // transposed position 8t + pi(g) (row b, columns 8TA + 4*half + 0..3) -- and then
         // reduced with one 128-byte bulk operation per run whose four blocks are adjacent in
         // the matrix, else one 32-byte operation per block.
-        // stiffness blocks, patch layout: into the patch copy
-        if constexpr (PATCH) {
-          if (present[el]) {
-            int k = 0;
-#pragma unroll
-            for (int TA = 0; TA < NTN; TA++) {
-#pragma unroll
-              for (int TB = TA; TB < NTN; TB++, k++) {
-                const int a = 8 * TA + pa;
-#pragma unroll
-                for (int h = 0; h < 2; h++) {
-                  const int b = 8 * TB + 4 * h + t;
-                  if (a < NN && b < NN) {
-                    const double mxx = acc[k][0][h], mxy = acc[k][1][h], myx = acc[k][2][h], myy = acc[k][3][h];
-                    const double kxx = c11 * mxx + mu * myy, kxy = lam * mxy + mu * myx;
-                    const double kyx = lam * myx + mu * mxy, kyy = c11 * myy + mu * mxx;
-                    patch_put<P>(O, pbuf, el, a, b, 0, kxx, kxy, kyx, kyy);
-                    if (TA < TB) patch_put<P>(O, pbuf, el, a, b, 1, kxx, kxy, kyx, kyy);
-                  }
-                }
-              }
-            }
-          }
-        }
-        if constexpr (JAC && RUNS && !PATCH) {
+        if constexpr (JAC && RUNS) {
           // every lane's previous bulk reads of the staging slots are complete
           asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
           __syncwarp();
@@ -978,44 +886,6 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
               } else {
                 frag_add_mapped<P>(O, el, 8, b, w, kxx, kxy, kyx, kyy, reds + 128 * slot);
               }
-            }
-          }
-        }
-      }
-      // patch layout: the whole patch is in the copy; its segments go out as bulk
-      // copies (stored, or added where an earlier colour stored the blocks), its
-      // residual rows as 16-byte stores or FP64 atomics
-      if constexpr (PATCH) {
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        const int64_t pidx = cur.k0 / kPatchElems;
-        const int2 r0 = __ldg(M.patchPtr + pidx), r1 = __ldg(M.patchPtr + pidx + 1);
-        const unsigned pb = (unsigned)__cvta_generic_to_shared(pbuf);
-        for (int i = r0.x + (int)threadIdx.x; i < r1.x; i += (int)blockDim.x) {
-          const int2 sg = __ldg(reinterpret_cast<const int2 *>(M.patchTab) + i);
-          const unsigned w = (unsigned)sg.y;
-          const unsigned src = pb + 32u * (w & 0xffffu), bytes = 32u * ((w >> 16) & 0x7fffu);
-          double *dst = M.mat + 4 * (int64_t)(unsigned)sg.x;
-          if (w >> 31) {
-            asm volatile("cp.reduce.async.bulk.global.shared::cta.bulk_group.add.f64 [%0], [%1], %2;" ::"l"(dst),
-                         "r"(src), "r"(bytes)
-                         : "memory");
-          } else {
-            asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(src), "r"(bytes)
-                         : "memory");
-          }
-        }
-        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
-        if constexpr (RES) {
-          for (int i = r0.y + (int)threadIdx.x; i < r1.y; i += (int)blockDim.x) {
-            const int v = __ldg(M.patchTab + i);
-            const double2 r = pres[i - r0.y];
-            double *dst = M.residual + 2 * (int64_t)(v & 0x7fffffff);
-            if (v < 0) {
-              atomicAdd(dst, r.x);
-              atomicAdd(dst + 1, r.y);
-            } else {
-              *reinterpret_cast<double2 *>(dst) = r;
             }
           }
         }
@@ -1209,33 +1079,6 @@ __global__ void __launch_bounds__(32 * FragDims<P>::WARPS, FEM_FRAG_MINB)
   frag_loop<P, kPlan | kRes | kJac>(smem, gen, meshes[0], meshes);
 }
 
-// Patch layout (order 3): patches [A.begin, A.begin + A.count) of one patch colour,
-// one per CTA step.  Two resident CTAs per SM (the patch copy takes 82 KB).
-template <int MODE>
-__global__ void __launch_bounds__(32 * FragDims<3>::WARPS, 2) frag_patch_kernel(const __grid_constant__ AsmArgs A) {
-  extern __shared__ __align__(128) unsigned char smem[];
-  frag_prologue<3>(smem);
-  PatchStride gen{A.begin, A.begin + A.count, (int64_t)blockIdx.x, (int64_t)gridDim.x, (int)(threadIdx.x >> 5)};
-  frag_loop<3, MODE>(smem, gen, A, &A);
-}
-
-template <int MODE>
-int launch_frag_patch_m(const AsmArgs &a, cudaStream_t s) {
-  constexpr int NT = 32 * FragDims<3>::WARPS;
-  auto kernel = frag_patch_kernel<MODE>;
-  const size_t smem = FragLayout<3, false, false, true>::total;
-  LaunchInfo li;
-  int st = launch_info(kernel, NT, smem, li);
-  if (st) return st;
-  const int64_t cap = (int64_t)li.grid_per_sm * li.num_sms;
-  const int grid = (int)(a.count < cap ? a.count : cap);
-  if (grid <= 0) return FEM_SUCCESS;
-  kernel<<<grid, NT, smem, s>>>(a);
-  cudaError_t err = cudaGetLastError();
-  if (err != cudaSuccess) return cuda_fail(err, "frag_patch_kernel launch");
-  return FEM_SUCCESS;
-}
-
 template <int P, int MODE>
 int launch_frag_p(const AsmArgs &a, cudaStream_t s) {
   using F = FragDims<P>;
@@ -1324,15 +1167,6 @@ int launch_frag(int order, int mode, const dev::AsmArgs &a, cudaStream_t s, int 
     case kNL | kJac: return launch_frag_mode<kNL | kJac>(order, a, s);
     case kNL | kRes | kJac: return launch_frag_mode<kNL | kRes | kJac>(order, a, s);
     default: return fail(FEM_ERR_INVALID_ARGUMENT, "fragment kernel: mode %d", mode);
-  }
-}
-
-int launch_frag_patch(int mode, const dev::AsmArgs &a, cudaStream_t s) {
-  using namespace dev;
-  switch (mode) {
-    case kPlan | kJac: return launch_frag_patch_m<kPlan | kJac | kPatch>(a, s);
-    case kPlan | kRes | kJac: return launch_frag_patch_m<kPlan | kRes | kJac | kPatch>(a, s);
-    default: return fail(FEM_ERR_INVALID_ARGUMENT, "patch kernel: mode %d", mode);
   }
 }
 

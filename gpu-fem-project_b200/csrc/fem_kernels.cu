@@ -145,11 +145,6 @@ void plan_free(fem_plan *p) {
   cudaFree(p->d_rowElemPtr);
   cudaFree(p->d_rowElem);
   cudaFree(p->d_rowChunk);
-  cudaFree(p->d_patchConn);
-  cudaFree(p->d_patchCode);
-  cudaFree(p->d_patchRb);
-  cudaFree(p->d_patchTab);
-  cudaFree(p->d_patchPtr);
   cudaSetDevice(cur);
   delete p;
 }
@@ -232,23 +227,13 @@ int fem_bsr_spmv(int numRows, const int *rowp, const int *cols, const double *A,
 
 int fem_plan_create(int elementOrder, int numNodes, const int *connPtr, const int *conn, int numElements,
                     fem_plan **plan) {
-  return fem_plan_create_ex(elementOrder, numNodes, connPtr, conn, numElements, 0, plan);
-}
-
-int fem_plan_create_ex(int elementOrder, int numNodes, const int *connPtr, const int *conn, int numElements,
-                       int flags, fem_plan **plan) {
   fem::clear_error();
   if (!plan) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "plan is NULL");
   *plan = nullptr;
   if (elementOrder < 1 || elementOrder > 4) return fem::fail(FEM_ERR_INVALID_ORDER, "element order %d", elementOrder);
-  if (flags & ~FEM_PLAN_PATCHES) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "plan flags %d", flags);
   fem::HostPlan hp;
   int st = fem::build_host_plan(elementOrder, numNodes, connPtr, conn, numElements, hp);
   if (st) return st;
-  fem::PatchPlan pp;
-  if ((flags & FEM_PLAN_PATCHES) && elementOrder == 3 && numElements > 0) {
-    if ((st = fem::build_patch_plan(hp, connPtr, conn, pp))) return st;
-  }
   fem_plan *p = new fem_plan();
   cudaGetDevice(&p->device);
   p->order = hp.order;
@@ -273,31 +258,7 @@ int fem_plan_create_ex(int elementOrder, int numNodes, const int *connPtr, const
     }
     p->numChunks = (int)hp.rowChunk.size() - 1;
   }
-  if (pp.numPatches > 0) {
-    // one int table: the segments (two ints each), then the residual rows; per patch
-    // the first segment and the first residual row (an index into the same table)
-    std::vector<int> tab(pp.seg);
-    tab.insert(tab.end(), pp.node.begin(), pp.node.end());
-    std::vector<int2> ptr((size_t)pp.numPatches + 1);
-    for (int q = 0; q <= pp.numPatches; q++) ptr[q] = make_int2(pp.segPtr[q], (int)pp.seg.size() + pp.nodePtr[q]);
-    if ((st = upload(pp.connList, &p->d_patchConn, p->deviceBytes)) ||
-        (st = upload(pp.code, &p->d_patchCode, p->deviceBytes)) || (st = upload(pp.rb, &p->d_patchRb, p->deviceBytes)) ||
-        (st = upload(tab, &p->d_patchTab, p->deviceBytes)) || (st = upload(ptr, &p->d_patchPtr, p->deviceBytes))) {
-      plan_free(p);
-      return st;
-    }
-    p->numPatches = pp.numPatches;
-    p->patchColourPtr = pp.colourPtr;
-  }
   *plan = p;
-  return FEM_SUCCESS;
-}
-
-int fem_plan_patches(const fem_plan *plan, int *numPatches, int *numColours) {
-  fem::clear_error();
-  if (!plan) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "plan is NULL");
-  if (numPatches) *numPatches = plan->numPatches;
-  if (numColours) *numColours = plan->numPatches > 0 ? (int)plan->patchColourPtr.size() - 1 : 0;
   return FEM_SUCCESS;
 }
 
@@ -381,19 +342,6 @@ int fem_plan_assemble_ex(const fem_plan *plan, const double *states, const doubl
     return fem::timed(s, elapsedSeconds, [&] { return fem::launch_rows(mode, a, s); });
   }
   const bool frag = fem::frag_supported(plan->order, precision, strainType, true);
-  if (plan->numPatches > 0 && frag && strainType == FEM_STRAIN_LINEAR && matEntries) {
-    // patch layout: one launch per patch colour
-    fem::patch_args(a, plan);
-    return fem::timed(s, elapsedSeconds, [&] {
-      for (size_t c = 0; c + 1 < plan->patchColourPtr.size(); c++) {
-        a.begin = plan->patchColourPtr[c];
-        a.count = plan->patchColourPtr[c + 1] - plan->patchColourPtr[c];
-        int st = fem::launch_frag_patch(mode, a, s);
-        if (st) return st;
-      }
-      return (int)FEM_SUCCESS;
-    });
-  }
   return fem::timed(s, elapsedSeconds, [&] {
     for (int c = 0; c < plan->numColours; c++) {
       a.begin = plan->colourPtr[c];

@@ -107,9 +107,6 @@ int launch_frag(int order, int mode, const dev::AsmArgs &a, cudaStream_t s, int 
 // Its tile-queue form for batches and the server (residual and Jacobian).
 int launch_frag_batched(int order, const dev::AsmArgs *meshes, const dev::Tile *tiles, int ntiles, int *counter,
                         cudaStream_t s);
-// Its patch form (order 3, LINEAR, Jacobian with or without the residual): patches
-// [a.begin, a.begin + a.count) of one patch colour, tables from patch_args.
-int launch_frag_patch(int mode, const dev::AsmArgs &a, cudaStream_t s);
 
 inline void set_material(dev::AsmArgs &a, double E, double nu, double t) {
   // element/FEKernels.h:300-301
@@ -166,12 +163,6 @@ struct fem_plan {
   // order 1: row assembly tables (HostPlan::rowElemPtr/rowElem/rowChunk); numChunks == 0: none
   int *d_rowElemPtr = nullptr, *d_rowElem = nullptr, *d_rowChunk = nullptr;
   int numChunks = 0;
-  // order 3 with FEM_PLAN_PATCHES: the patch layout (PatchPlan); numPatches == 0: none
-  int numPatches = 0;
-  std::vector<int> patchColourPtr;
-  int *d_patchConn = nullptr, *d_patchRb = nullptr, *d_patchTab = nullptr;
-  int2 *d_patchPtr = nullptr;
-  uint8_t *d_patchCode = nullptr;
   int64_t deviceBytes = 0;
 };
 
@@ -187,13 +178,4 @@ inline void plan_args(dev::AsmArgs &a, const fem_plan *p) {
 }
 // Whether the LINEAR assembly of this plan runs as row assembly.
 inline bool plan_rows(const fem_plan *p) { return p->numChunks > 0; }
-// The patch tables of a plan in an argument block (element positions in patch order).
-inline void patch_args(dev::AsmArgs &a, const fem_plan *p) {
-  a.connList = p->d_patchConn;
-  a.blockCode = p->d_patchCode;
-  a.rowp = p->d_rowp;
-  a.patchRb = p->d_patchRb;
-  a.patchTab = p->d_patchTab;
-  a.patchPtr = p->d_patchPtr;
-}
 }  // namespace fem

@@ -163,36 +163,6 @@ int fem_plan_assemble_ex(const fem_plan *plan, const double *states, const doubl
                          double t, double *residual, double *matEntries, int precision, int strainType, void *stream,
                          double *elapsedSeconds);
 
-/* Plan creation flags. */
-#define FEM_PLAN_PATCHES 1 /* order 3: also build the patch layout (ignored at other orders) */
-
-/* fem_plan_create with flags.  FEM_PLAN_PATCHES adds the patch layout: neighbouring
- * elements (a strip of up to 8 along a grid row on a structured mesh) are summed
- * by one CTA in shared memory and each matrix row they touch is written as a few
- * contiguous segments by bulk copies, instead of one 32-byte store or reduction
- * per element block.  fem_plan_assemble then uses it for LINEAR Jacobian
- * assembly (FP64, and MIXED, which runs the FP64 kernel at order 3); the other
- * cases keep the colour path.  Results agree with the colour path to rounding
- * (blocks shared by neighbours are summed in another order).  Costs about 0.6 KB
- * of device memory per element.  (No reference counterpart.) */
-int fem_plan_create_ex(int elementOrder, int numNodes, const int *connPtr, const int *conn, int numElements,
-                       int flags, fem_plan **plan);
-/* Patch count and patch colours of a plan (0, 0 without a patch layout). */
-int fem_plan_patches(const fem_plan *plan, int *numPatches, int *numColours);
-
-/* The patch layout of a mesh on the host (no device use), for inspection and
- * tests: the tables fem_plan_create_ex(FEM_PLAN_PATCHES) uploads.  Call with
- * NULL arrays for the sizes.  Arrays: colourPtr[numColours+1]; patchElem[8 P]
- * (element per position, -1 empty; position j: warp j/2, phase j%2);
- * code[8 P codeStride] (codeStride = (nn^2 + nn + 15)/16*16; [a nn + b] = rank of
- * block (a,b) in row conn[a] | 0x80 when added in the patch, [nn^2 + a] = 1 when
- * node a's residual is added); slotBase[8 P nn] (slot base * 256 + patch-local
- * node index); segPtr[P+1], seg[2 S] (first block, slot | count << 16 | add << 31);
- * nodePtr[P+1], node[N] (node id | add << 31).  Order 3 only. */
-int fem_patch_layout(int elementOrder, int numNodes, const int *connPtr, const int *conn, int numElements,
-                     int *numPatches, int *numColours, int64_t *numSegments, int64_t *numPatchNodes, int *colourPtr,
-                     int *patchElem, uint8_t *code, int *slotBase, int *segPtr, int *seg, int *nodePtr, int *node);
-
 /* ---- batched assembly of many meshes (config: 256 meshes, mixed orders) --------------- */
 /* A batch references existing plans (they must outlive it) and assembles all of
  * their meshes with one persistent kernel per (order, colour) whose thread groups

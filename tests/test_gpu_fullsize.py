@@ -71,32 +71,5 @@ def test_square1024_p3_full_size(fem, orc, cuda):
     _full(fem, orc, cuda, fem.square1024_p3())
 
 
-def test_square1024_p3_patch_layout_full_size(fem, cuda):
-    """The patch layout at full size: R = K u through the device SpMV and agreement
-    with the colour-ordered plan to 1e-12 (shared blocks are summed in another order)."""
-    import torch
-    m = fem.square1024_p3()
-    d = fem.DeviceMesh(m, cuda)
-    plan = fem.Plan(3, m.num_nodes, m.conn_ptr, m.conn)
-    res64 = torch.empty(m.num_nodes * 2, dtype=torch.float64, device=cuda)
-    mat64 = torch.empty(plan.nnzb * 4, dtype=torch.float64, device=cuda)
-    plan.assemble(d.states, d.coords, m.E, m.nu, m.t, res64, mat64)
-    plan.close()
-    pp = fem.Plan(3, m.num_nodes, m.conn_ptr, m.conn, patches=True)
-    assert pp.num_patches == m.num_elements // 8 and pp.patch_colours == 4
-    res = torch.empty_like(res64)
-    mat = torch.full_like(mat64, float("nan"))
-    pp.assemble(d.states, d.coords, m.E, m.nu, m.t, res, mat)
-    rowp_d, cols_d = pp.device_pattern()
-    y = torch.empty_like(res)
-    fem.lib.fem_bsr_spmv(m.num_nodes, rowp_d, cols_d, mat.data_ptr(), d.states.data_ptr(), y.data_ptr(),
-                         torch.cuda.current_stream().cuda_stream)
-    torch.cuda.synchronize()
-    assert float((y - res).abs().max() / res.abs().max()) <= 1e-11
-    assert float((res - res64).abs().max() / res64.abs().max()) <= 1e-12
-    assert float((mat - mat64).abs().max() / mat64.abs().max()) <= 1e-12
-    pp.close()
-
-
 def test_annulus512x2048_p2_full_size(fem, orc, cuda):
     _full(fem, orc, cuda, fem.annulus512x2048_p2())
