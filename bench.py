@@ -349,7 +349,7 @@ def run_ours(args):
     line = {
         "metric": "assembled elements/s (res+Jac)", "value": value, "unit": "elements/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64" if prec == "fp64" else "f32/f64", "data": "synthetic",
+        "vs_baseline": None, "dtype": "f64" if prec == "fp64" else ("bf16x6/f64" if mesh.order in (2, 3) else "f32/f64"), "data": "synthetic",
         "config": {"workload": mesh.name, "order": mesh.order, "elements": nE, "dof": mesh.num_dof, "nnzb": nnzb,
                    "path": best, "l2": "inputs and outputs larger than L2 (BSR values %.2f GB)" % (32 * nnzb / 1e9),
                    "parallelism": f"replicas{world}"},
@@ -388,8 +388,11 @@ def kernel_label(plan, order, prec):
     """The kernel that runs one assembly of `plan` (the dispatch of fem_plan_assemble)."""
     if plan.row_chunks > 0:
         return "rows_p1_kernel, 1 launch per step"
-    # the fragment kernel serves orders 2-3 in both precisions (MIXED runs it in FP64)
-    # and order 4 in FP64; FP32 order 4 runs the element kernel
+    # the fragment kernel serves orders 2-3 in both precisions (MIXED with its element
+    # stiffness as BF16x6 tensor-core products) and order 4 in FP64; FP32 order 4 runs
+    # the element kernel
+    if order in (2, 3) and prec == "mixed":
+        return f"frag_kernel<{order}, BF16x6 stiffness> x {plan.num_colours} colour launches per step"
     if order in (2, 3) or (order == 4 and prec == "fp64"):
         return f"frag_kernel<{order}> x {plan.num_colours} colour launches per step"
     return f"assemble_kernel<{order}, float> x {plan.num_colours} colour launches per step"

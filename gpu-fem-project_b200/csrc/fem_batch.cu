@@ -62,7 +62,7 @@ int launch_batched(int p, int precision, const dev::AsmArgs *meshes, const dev::
                    cudaStream_t s) {
   // the same kernel as the single-mesh plan path, so batched results equal lone ones bit for bit
   if (frag_supported(p, precision, FEM_STRAIN_LINEAR, true))
-    return launch_frag_batched(p, meshes, tiles, ntiles, counter, s);
+    return launch_frag_batched(p, precision, meshes, tiles, ntiles, counter, s);
   if (precision == FEM_PRECISION_FP64) return launch_batched_t<double>(p, meshes, tiles, ntiles, counter, s);
   if (precision == FEM_PRECISION_MIXED) return launch_batched_t<float>(p, meshes, tiles, ntiles, counter, s);
   return fail(FEM_ERR_INVALID_ARGUMENT, "precision %d", precision);

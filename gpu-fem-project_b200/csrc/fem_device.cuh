@@ -106,7 +106,9 @@ struct Vec2<float> {
 };
 
 // kNL: GreenStrainType::NONLINEAR (Green strain, FP64 only); default LINEAR.
-enum : int { kRes = 1, kJac = 2, kPlan = 4, kNL = 8 };
+// kB16: fragment kernel, element stiffness on BF16 tensor cores with three-way split
+// operands (FEM_PRECISION_MIXED at orders 2 and 3).
+enum : int { kRes = 1, kJac = 2, kPlan = 4, kNL = 8, kB16 = 32 };
 
 struct AsmArgs {
   // drop-in fields | order-1 plan row tables (a plan never reads the drop-in ones)

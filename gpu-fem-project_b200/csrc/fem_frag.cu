@@ -48,6 +48,7 @@
 // writer stores, others add with atomics.  The arithmetic is the closed form of
 // the reference's per-column forward AD (element/FEKernels.h:286-315, 884-976)
 // that the element kernel documents.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -90,8 +91,8 @@ using IC = std::integral_constant<int, V>;
 
 // Shared memory: CTA tables, then one region per warp.  DROP: drop-in mode (the
 // stage holds the reference element map rows, NN*NN ints per element, instead of
-// plan code records).
-template <int P, bool DROP = false, bool NL = false>
+// plan code records).  B16: the BF16x6 stiffness table follows the CTA tables.
+template <int P, bool DROP = false, bool NL = false, bool B16 = false>
 struct FragLayout {
   using F = FragDims<P>;
   static constexpr int K4 = F::K4, NTN = F::NTN, NQP = F::NQP, NN = F::NN;
@@ -100,7 +101,8 @@ struct FragLayout {
   static constexpr size_t tabF = tabJ + 8 * K4 * K4 * 32;    // double2 [K4][NTAB][TABW]
   static constexpr size_t wq = tabF + 16 * K4 * F::NTAB * F::TABW;  // double [NQP]
   static constexpr size_t csum = align16(wq + 8 * NQP);       // double2 [NQP]: sum_a dN(a, q)
-  static constexpr size_t warps = align16(csum + 16 * NQP);
+  static constexpr size_t tabB = align16(csum + 16 * NQP);    // double2 [8][32]: BF16x6 stiffness operands
+  static constexpr size_t warps = align16(tabB + (B16 ? 16 * 8 * 32 : 0));
   // warp-relative; [2] = the two elements of the step
   static constexpr size_t WI0 = 0;                 // double2 [2][NQP]: sqrt|s| (J^-1_0x, J^-1_1x)
   static constexpr size_t WI1 = WI0 + 16 * 2 * NQP;  // double2 [2][NQP]: sqrt|s| (J^-1_0y, J^-1_1y)
@@ -120,14 +122,34 @@ struct FragLayout {
   static constexpr size_t total = warps + F::WARPS * warp_bytes;
 };
 
+// D += A B, m16n8k16, BF16 operands, FP32 accumulate.
+__device__ __forceinline__ void bmma(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+               : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+               : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// v ~ hi + mid + lo, three BF16 parts (8 significant bits each, 24 together): the
+// FP32 value and its two successive remainders, each rounded to nearest.
+__device__ __forceinline__ void split3(double v, uint32_t &hi, uint32_t &mid, uint32_t &lo) {
+  const float f = __double2float_rn(v);
+  const __nv_bfloat16 h = __float2bfloat16_rn(f);
+  const float r1 = f - __bfloat162float(h);
+  const __nv_bfloat16 m = __float2bfloat16_rn(r1);
+  const __nv_bfloat16 l = __float2bfloat16_rn(r1 - __bfloat162float(m));
+  hi = __bfloat16_as_ushort(h);
+  mid = __bfloat16_as_ushort(m);
+  lo = __bfloat16_as_ushort(l);
+}
+
 __device__ __forceinline__ double sel4(double x0, double x1, double x2, double x3, int i) {
   return i == 0 ? x0 : (i == 1 ? x1 : (i == 2 ? x2 : x3));
 }
 
-template <int P>
+template <int P, bool B16 = false>
 __device__ __forceinline__ void frag_prologue(unsigned char *smem) {
   using F = FragDims<P>;
-  using L = FragLayout<P>;
+  using L = FragLayout<P, false, false, B16>;
   constexpr int P1 = F::P1, NN = F::NN, NQ = F::NQ, K4 = F::K4, NTAB = F::NTAB, TABW = F::TABW;
   double *tabJ = reinterpret_cast<double *>(smem + L::tabJ);
   double2 *tabF = reinterpret_cast<double2 *>(smem + L::tabF);
@@ -168,6 +190,17 @@ __device__ __forceinline__ void frag_prologue(unsigned char *smem) {
   }
   for (int q = threadIdx.x; q < F::NQP; q += blockDim.x)
     wq[q] = q < NQ ? __dmul_rn(kGW[P][q % P1], kGW[P][q / P1]) : 0.0;
+  // BF16x6 stiffness (orders 2, 3): entry (2k + h, lane (g, t)) holds dN(a, q) for the
+  // node a = 8h + pi(g) and quadrature point q = 2t + (k & 1) + 8 (k >> 1) that lane
+  // (g, t) places in its m16n8k16 fragments
+  if constexpr (B16) {
+    double2 *tabB = reinterpret_cast<double2 *>(smem + L::tabB);
+    for (int i = threadIdx.x; i < 8 * 32; i += blockDim.x) {
+      const int lane = i & 31, k = (i >> 5) >> 1, h = (i >> 5) & 1, g = lane >> 2, t = lane & 3;
+      const int a = 8 * h + 4 * (g & 1) + (g >> 1), q = 2 * t + (k & 1) + 8 * (k >> 1);
+      tabB[i] = (a < NN && q < NQ) ? dN(a, q) : make_double2(0.0, 0.0);
+    }
+  }
   // sum_a dN(a, q): zero in exact arithmetic, a few ulp of the table entries in
   // FP64; summed with Neumaier compensation (error ~1e-30 absolute)
   double2 *csum = reinterpret_cast<double2 *>(smem + L::csum);
@@ -396,14 +429,16 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
                                           const AsmArgs *__restrict__ meshes) {
   constexpr bool PLAN = (MODE & kPlan) != 0;
   constexpr bool NL = (MODE & kNL) != 0;
+  constexpr bool B16 = (MODE & kB16) != 0;  // BF16x6 element stiffness
   using F = FragDims<P>;
-  using L = FragLayout<P, !PLAN, NL>;
+  using L = FragLayout<P, !PLAN, NL, B16>;
   constexpr int NN = F::NN, NQ = F::NQ, K4 = F::K4, NTN = F::NTN, NQP = F::NQP, CS = F::CS;
   constexpr int STG = L::CS;  // staged bytes per element: plan code record or map rows
   constexpr bool RES = (MODE & kRes) != 0, JAC = (MODE & kJac) != 0;
   constexpr bool RUNS = (P == 3);  // order 3: staged row runs, one bulk reduction per adjacent run
   static_assert(!NL || !F::IL, "NONLINEAR strain: orders 2 and 3");
   static_assert(PLAN || !Gen::kBatched, "drop-in mode assembles one mesh");
+  static_assert(!B16 || (!NL && P == 3), "BF16x6 stiffness: LINEAR, order 3");
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane >> 2, t = lane & 3;
@@ -412,6 +447,7 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
   const double2 *tabF = reinterpret_cast<const double2 *>(smem + L::tabF);
   const double *wqs = reinterpret_cast<const double *>(smem + L::wq);
   const double2 *csum = reinterpret_cast<const double2 *>(smem + L::csum);
+  const double2 *tabB = reinterpret_cast<const double2 *>(smem + L::tabB);
   unsigned char *ws = smem + L::warps + warp * L::warp_bytes;
   double2 *WI0 = reinterpret_cast<double2 *>(ws + L::WI0);
   double2 *WI1 = reinterpret_cast<double2 *>(ws + L::WI1);
@@ -650,6 +686,138 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
       constexpr int NPAIR = NTM * (NTM + 1) / 2;
       const int pa = 4 * (g & 1) + (g >> 1);  // pi(g)
       for (int el = 0; el < ne; el++) {
+        if constexpr (B16) {
+          // BF16x6 element stiffness: M_ij = sum_q s G_i(q, a) G_j(q, b) as m16n8k16
+          // products (k = quadrature points 0-15; rows a and columns b of the two node
+          // tiles, a = 8h + pi(g) and b = 8h' + pi(n)); each FP64 operand is split into
+          // three BF16 parts and six part products accumulate in FP32 (hi*hi, hi*mid,
+          // mid*hi, hi*lo, lo*hi, mid*mid: ~FP32 accuracy; the two-way BF16x3 split
+          // leaves ~4e-6 relative error in K).  Lane (g, t) holds the values of the
+          // quadrature points q_k = 2t + (k & 1) + 8 (k >> 1) of nodes 8h + pi(g).
+          double gv[2][4][2];  // [i][k][h]: G-hat_i(q_k, 8h + pi(g)) = sqrt|s| (dN J^-1)_i
+          double sgk[4];
+          double rx[2] = {0.0, 0.0}, ry[2] = {0.0, 0.0};
+#pragma unroll
+          for (int k = 0; k < 4; k++) {
+            const int q = 2 * t + (k & 1) + 8 * (k >> 1);
+            const int o = el * NQP + q;
+            const bool qv = q < NQ;
+            const double2 w0 = qv ? WI0[o] : make_double2(0.0, 0.0), w1 = qv ? WI1[o] : make_double2(0.0, 0.0);
+            sgk[k] = qv ? SGs[o] : 0.0;
+            double2 s0 = make_double2(0.0, 0.0), s1 = make_double2(0.0, 0.0);
+            if (RES && qv) {
+              s0 = WS0[o];
+              s1 = WS1[o];
+            }
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+              const double2 d = tabB[(2 * k + h) * 32 + lane];
+              gv[0][k][h] = fma(w0.x, d.x, w0.y * d.y);
+              gv[1][k][h] = fma(w1.x, d.x, w1.y * d.y);
+              if constexpr (RES) {
+                rx[h] = fma(gv[0][k][h], s0.x, fma(gv[1][k][h], s1.x, rx[h]));
+                ry[h] = fma(gv[0][k][h], s0.y, fma(gv[1][k][h], s1.y, ry[h]));
+              }
+            }
+          }
+          if constexpr (RES) {
+            // sum over the four lanes t of node 8h + pi(g); lane t = h writes it
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+              rx[h] += __shfl_xor_sync(0xffffffffu, rx[h], 1);
+              ry[h] += __shfl_xor_sync(0xffffffffu, ry[h], 1);
+              rx[h] += __shfl_xor_sync(0xffffffffu, rx[h], 2);
+              ry[h] += __shfl_xor_sync(0xffffffffu, ry[h], 2);
+            }
+            const int a = 8 * t + pa;
+            if (t < 2 && a < NN) {
+              const double sx = t ? rx[1] : rx[0], sy = t ? ry[1] : ry[0];
+              double *dst = M.residual + 2 * (int64_t)nid[el * NN + a];
+              if (PLAN && O.codes[el * CS + NN * NN + a]) {
+                *reinterpret_cast<double2 *>(dst) = make_double2(sx, sy);
+              } else {
+                atomicAdd(dst, sx);
+                atomicAdd(dst + 1, sy);
+              }
+            }
+          }
+          if constexpr (JAC) {
+            // split operands: B[part][j][h][r] (column node 8h + pi(g)), A = sign(s) B
+            // packed as row fragments: A[part][i][r] (rows pi(g), 8 + pi(g))
+            uint32_t pb[3][2][4][2];  // [part][i][k][h] raw BF16 bits
+#pragma unroll
+            for (int i = 0; i < 2; i++)
+#pragma unroll
+              for (int k = 0; k < 4; k++)
+#pragma unroll
+                for (int h = 0; h < 2; h++) split3(gv[i][k][h], pb[0][i][k][h], pb[1][i][k][h], pb[2][i][k][h]);
+            uint32_t Af[3][2][4], Bf[3][2][2][2];
+#pragma unroll
+            for (int pt = 0; pt < 3; pt++)
+#pragma unroll
+              for (int i = 0; i < 2; i++) {
+                auto sv = [&](int k, int h) { return pb[pt][i][k][h] ^ (sgk[k] < 0.0 ? 0x8000u : 0u); };
+                Af[pt][i][0] = sv(0, 0) | (sv(1, 0) << 16);
+                Af[pt][i][1] = sv(0, 1) | (sv(1, 1) << 16);
+                Af[pt][i][2] = sv(2, 0) | (sv(3, 0) << 16);
+                Af[pt][i][3] = sv(2, 1) | (sv(3, 1) << 16);
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                  Bf[pt][i][h][0] = pb[pt][i][0][h] | (pb[pt][i][1][h] << 16);
+                  Bf[pt][i][h][1] = pb[pt][i][2][h] | (pb[pt][i][3][h] << 16);
+                }
+              }
+            float acc[2][2][2][4];  // [i][j][h (column tile)][c]
+#pragma unroll
+            for (int i = 0; i < 2; i++)
+#pragma unroll
+              for (int j = 0; j < 2; j++)
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+#pragma unroll
+                  for (int c = 0; c < 4; c++) acc[i][j][h][c] = 0.0f;
+                  // smallest terms first
+                  bmma(acc[i][j][h], Af[2][i], Bf[0][j][h][0], Bf[0][j][h][1]);
+                  bmma(acc[i][j][h], Af[0][i], Bf[2][j][h][0], Bf[2][j][h][1]);
+                  bmma(acc[i][j][h], Af[1][i], Bf[1][j][h][0], Bf[1][j][h][1]);
+                  bmma(acc[i][j][h], Af[1][i], Bf[0][j][h][0], Bf[0][j][h][1]);
+                  bmma(acc[i][j][h], Af[0][i], Bf[1][j][h][0], Bf[1][j][h][1]);
+                  bmma(acc[i][j][h], Af[0][i], Bf[0][j][h][0], Bf[0][j][h][1]);
+                }
+            // lane (g, t): c = 2 r + u holds M_ij[a = 8r + pi(g)][b = 8h + 4u + t]: whole
+            // 2x2 blocks, four consecutive columns across the lanes t.  Blocks to add go
+            // to the staging slots of the FP64 layout (node-tile pair (r, h) = (TA, TB);
+            // the pair (1, 0) is the transposed half of (0, 1)) and leave as row runs.
+            asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+            __syncwarp();
+#pragma unroll
+            for (int r = 0; r < 2; r++)
+#pragma unroll
+              for (int h = 0; h < 2; h++)
+#pragma unroll
+                for (int u = 0; u < 2; u++) {
+                  const int a = 8 * r + pa, b = 8 * h + 4 * u + t, c = 2 * r + u;
+                  if (a < NN && b < NN) {
+                    const double mxx = acc[0][0][h][c], mxy = acc[0][1][h][c];
+                    const double myx = acc[1][0][h][c], myy = acc[1][1][h][c];
+                    const double kxx = c11 * mxx + mu * myy, kxy = lam * mxy + mu * myx;
+                    const double kyx = lam * myx + mu * mxy, kyy = c11 * myy + mu * mxx;
+                    const int sl = (r == 1 && h == 0) ? frag_slot(1, g & 1, 1) : frag_slot(r + h, u, 0);
+                    const int pos = (r == 1 && h == 0) ? 8 * (g >> 1) + 4 * u + t : 4 * g + t;
+                    frag_put<P, PLAN>(O, el, a, b, 0, kxx, kxy, kyx, kyy, redsW + 128 * sl + 4 * pos);
+                  }
+                }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncwarp();
+#pragma unroll
+            for (int v = 0; v < 2; v++) {
+              const int run = lane + 32 * v;
+              frag_issue_run<P, PLAN>(O, el, run >> 3, run & 7, redsW);
+            }
+            asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+          }
+          continue;
+        }
         // 3.-5. quadrature k-steps outermost: per step each lane forms its fragments
         // G-hat_i(q = 4ks + t, a = 8T + pi(g)), adds its residual partials and issues
         // the 4 NPAIR independent stiffness MMAs of all node-tile pairs
@@ -1062,7 +1230,7 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
 template <int P, int MODE>
 __global__ void __launch_bounds__(32 * FragDims<P>::WARPS, FEM_FRAG_MINB) frag_kernel(const __grid_constant__ AsmArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
-  frag_prologue<P>(smem);
+  frag_prologue<P, (MODE & kB16) != 0>(smem);
   const int warp = threadIdx.x >> 5;
   PairStride gen{A.begin, A.begin + A.count, (int64_t)blockIdx.x * FragDims<P>::WARPS + warp,
                  (int64_t)gridDim.x * FragDims<P>::WARPS};
@@ -1070,13 +1238,13 @@ __global__ void __launch_bounds__(32 * FragDims<P>::WARPS, FEM_FRAG_MINB) frag_k
 }
 
 // Many meshes of one order (one colour each): warps pull tiles from the launch's queue.
-template <int P>
+template <int P, int MODE>
 __global__ void __launch_bounds__(32 * FragDims<P>::WARPS, FEM_FRAG_MINB)
     frag_batched_kernel(const AsmArgs *__restrict__ meshes, const Tile *__restrict__ tiles, int ntiles, int *counter) {
   extern __shared__ __align__(16) unsigned char smem[];
-  frag_prologue<P>(smem);
+  frag_prologue<P, (MODE & kB16) != 0>(smem);
   PairQueue gen{tiles, ntiles, counter, 0, 0, 0, false};
-  frag_loop<P, kPlan | kRes | kJac>(smem, gen, meshes[0], meshes);
+  frag_loop<P, MODE>(smem, gen, meshes[0], meshes);
 }
 
 template <int P, int MODE>
@@ -1084,7 +1252,7 @@ int launch_frag_p(const AsmArgs &a, cudaStream_t s) {
   using F = FragDims<P>;
   constexpr int NT = 32 * F::WARPS;
   auto kernel = frag_kernel<P, MODE>;
-  const size_t smem = FragLayout<P, (MODE & kPlan) == 0, (MODE & kNL) != 0>::total;
+  const size_t smem = FragLayout<P, (MODE & kPlan) == 0, (MODE & kNL) != 0, (MODE & kB16) != 0>::total;
   LaunchInfo li;
   int st = launch_info(kernel, NT, smem, li);
   if (st) return st;
@@ -1099,12 +1267,12 @@ int launch_frag_p(const AsmArgs &a, cudaStream_t s) {
   return FEM_SUCCESS;
 }
 
-template <int P>
+template <int P, int MODE>
 int launch_frag_batched_p(const AsmArgs *meshes, const Tile *tiles, int ntiles, int *counter, cudaStream_t s) {
   using F = FragDims<P>;
   constexpr int NT = 32 * F::WARPS;
-  auto kernel = frag_batched_kernel<P>;
-  const size_t smem = FragLayout<P>::total;
+  auto kernel = frag_batched_kernel<P, MODE>;
+  const size_t smem = FragLayout<P, false, false, (MODE & kB16) != 0>::total;
   LaunchInfo li;
   int st = launch_info(kernel, NT, smem, li);
   if (st) return st;
@@ -1121,10 +1289,12 @@ int launch_frag_batched_p(const AsmArgs *meshes, const Tile *tiles, int ntiles, 
 template <int MODE>
 int launch_frag_mode(int order, const AsmArgs &a, cudaStream_t s) {
   switch (order) {
-    case 2: return launch_frag_p<2, MODE>(a, s);
+    case 2:
+      if constexpr ((MODE & kB16) != 0) return fail(FEM_ERR_INVALID_ORDER, "fragment kernel, BF16x6: order 2");
+      else return launch_frag_p<2, MODE>(a, s);
     case 3: return launch_frag_p<3, MODE>(a, s);
     case 4:
-      if constexpr ((MODE & kNL) != 0) return fail(FEM_ERR_INVALID_ORDER, "fragment kernel, NONLINEAR: order 4");
+      if constexpr ((MODE & (kNL | kB16)) != 0) return fail(FEM_ERR_INVALID_ORDER, "fragment kernel, mode %d: order 4", MODE);
       else return launch_frag_p<4, MODE>(a, s);
     default: return fail(FEM_ERR_INVALID_ORDER, "fragment kernel: order %d", order);
   }
@@ -1132,16 +1302,25 @@ int launch_frag_mode(int order, const AsmArgs &a, cudaStream_t s) {
 
 }  // namespace dev
 
+// MIXED, LINEAR, order 3: the Jacobian's element stiffness runs as BF16x6 tensor-core
+// products (kB16); everything else of the kernel stays FP64.  Order 2 pads 9 nodes and
+// 9 quadrature points to 16 in both operands and ran slower than FP64 (2.0 against
+// 1.4 ms on the 512x2048 annulus), so MIXED keeps the FP64 kernel there.
+bool b16_stiffness(int order, int precision, int strain) {
+  return precision == FEM_PRECISION_MIXED && strain == FEM_STRAIN_LINEAR && order == 3;
+}
+
 // FP64, LINEAR: orders 2 and 3 in every mode; order 4 in plan mode only (single
 // meshes, batches, the server): measured on B200, the order-4 fragment kernel runs
 // the 256-mesh batch in 170 against 217 ms and one 512^2 mesh in 3.03 against
 // 3.00 ms for the element kernel, and plans and batches must run the same kernel
 // (a mesh's batched result equals its single-mesh plan result bit for bit); the
 // order-4 drop-in keeps the element kernel (4.7 ms against 6.9 ms).
-// MIXED at orders 2 and 3 also runs this FP64 kernel (faster than the FP32 element
-// products there: 3.1 against 3.8 ms at 1024^2 p = 3), so it returns the FP64
-// result, as order-1 row assembly does; at order 4 the FP32 element kernel is the
-// faster one (2.6 against 3.4 ms) and MIXED keeps it.
+// MIXED at orders 2 and 3 also runs this kernel (faster than the FP32 element
+// products there: 3.1 against 3.8 ms at 1024^2 p = 3): at order 3 with the element
+// stiffness as BF16x6 tensor-core products (b16_stiffness), at order 2 in FP64 (the
+// FP64 result, as order-1 row assembly gives); at order 4 the FP32 element kernel is
+// the faster one (2.6 against 3.4 ms) and MIXED keeps it.
 bool frag_supported(int order, int precision, int strain, bool plan) {
   if (strain == FEM_STRAIN_NONLINEAR) return precision == FEM_PRECISION_FP64 && (order == 2 || order == 3);
   if (strain != FEM_STRAIN_LINEAR) return false;
@@ -1150,10 +1329,15 @@ bool frag_supported(int order, int precision, int strain, bool plan) {
   return order == 2 || order == 3 || (order == 4 && plan);
 }
 
-int launch_frag(int order, int mode, const dev::AsmArgs &a, cudaStream_t s, int strain) {
+int launch_frag(int order, int precision, int mode, const dev::AsmArgs &a, cudaStream_t s, int strain) {
   using namespace dev;
   if (strain == FEM_STRAIN_NONLINEAR) mode |= kNL;
+  if (b16_stiffness(order, precision, strain) && (mode & kJac)) mode |= kB16;
   switch (mode) {
+    case kPlan | kJac | kB16: return launch_frag_mode<kPlan | kJac | kB16>(order, a, s);
+    case kPlan | kRes | kJac | kB16: return launch_frag_mode<kPlan | kRes | kJac | kB16>(order, a, s);
+    case kJac | kB16: return launch_frag_mode<kJac | kB16>(order, a, s);
+    case kRes | kJac | kB16: return launch_frag_mode<kRes | kJac | kB16>(order, a, s);
     case kPlan | kRes: return launch_frag_mode<kPlan | kRes>(order, a, s);
     case kPlan | kJac: return launch_frag_mode<kPlan | kJac>(order, a, s);
     case kPlan | kRes | kJac: return launch_frag_mode<kPlan | kRes | kJac>(order, a, s);
@@ -1170,12 +1354,16 @@ int launch_frag(int order, int mode, const dev::AsmArgs &a, cudaStream_t s, int 
   }
 }
 
-int launch_frag_batched(int order, const dev::AsmArgs *meshes, const dev::Tile *tiles, int ntiles, int *counter,
-                        cudaStream_t s) {
+int launch_frag_batched(int order, int precision, const dev::AsmArgs *meshes, const dev::Tile *tiles, int ntiles,
+                        int *counter, cudaStream_t s) {
+  using namespace dev;
+  constexpr int M = kPlan | kRes | kJac;
+  const bool b16 = b16_stiffness(order, precision, FEM_STRAIN_LINEAR);
   switch (order) {
-    case 2: return dev::launch_frag_batched_p<2>(meshes, tiles, ntiles, counter, s);
-    case 3: return dev::launch_frag_batched_p<3>(meshes, tiles, ntiles, counter, s);
-    case 4: return dev::launch_frag_batched_p<4>(meshes, tiles, ntiles, counter, s);
+    case 2: return launch_frag_batched_p<2, M>(meshes, tiles, ntiles, counter, s);
+    case 3: return b16 ? launch_frag_batched_p<3, M | kB16>(meshes, tiles, ntiles, counter, s)
+                       : launch_frag_batched_p<3, M>(meshes, tiles, ntiles, counter, s);
+    case 4: return launch_frag_batched_p<4, M>(meshes, tiles, ntiles, counter, s);
     default: return fail(FEM_ERR_INVALID_ORDER, "fragment kernel: order %d", order);
   }
 }

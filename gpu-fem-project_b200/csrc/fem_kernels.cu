@@ -84,11 +84,13 @@ int launch(int order, int precision, int mode, const dev::AsmArgs &a, cudaStream
   if (strain == FEM_STRAIN_NONLINEAR) {
     if (precision != FEM_PRECISION_FP64)
       return fail(FEM_ERR_INVALID_ARGUMENT, "NONLINEAR strain is assembled in FP64 only (precision %d)", precision);
-    if (frag_supported(order, precision, strain, (mode & dev::kPlan) != 0)) return launch_frag(order, mode, a, s, strain);
+    if (frag_supported(order, precision, strain, (mode & dev::kPlan) != 0))
+      return launch_frag(order, precision, mode, a, s, strain);
     return launch_nl(order, mode, a, s);
   }
   if (strain != FEM_STRAIN_LINEAR) return fail(FEM_ERR_INVALID_ARGUMENT, "strain type %d", strain);
-  if ((mode & dev::kPlan) == 0 && frag_supported(order, precision, strain, false)) return launch_frag(order, mode, a, s);
+  if ((mode & dev::kPlan) == 0 && frag_supported(order, precision, strain, false))
+    return launch_frag(order, precision, mode, a, s);
   if (precision == FEM_PRECISION_FP64) return launch_any<double>(order, mode, a, s);
   if (precision == FEM_PRECISION_MIXED) return launch_any<float>(order, mode, a, s);
   return fail(FEM_ERR_INVALID_ARGUMENT, "precision %d", precision);
@@ -346,7 +348,7 @@ int fem_plan_assemble_ex(const fem_plan *plan, const double *states, const doubl
     for (int c = 0; c < plan->numColours; c++) {
       a.begin = plan->colourPtr[c];
       a.count = plan->colourPtr[c + 1] - plan->colourPtr[c];
-      int st = frag ? fem::launch_frag(plan->order, mode, a, s, strainType)
+      int st = frag ? fem::launch_frag(plan->order, precision, mode, a, s, strainType)
                     : fem::launch(plan->order, precision, mode, a, s, strainType);
       if (st) return st;
     }

@@ -102,11 +102,15 @@ constexpr int kRowTileChunks = 16;
 // Warp-fragment kernel (fem_frag.cu): LINEAR FP64 assembly at orders 2 and 3, plan
 // mode (one colour, list positions [a.begin, a.begin + a.count)) or drop-in mode
 // (elements through the reference map, accumulate-into).
+// FEM_PRECISION_MIXED at order 3 runs its element stiffness as BF16x6 tensor-core
+// products (b16_stiffness); the rest stays FP64.
 bool frag_supported(int order, int precision, int strain, bool plan);
-int launch_frag(int order, int mode, const dev::AsmArgs &a, cudaStream_t s, int strain = FEM_STRAIN_LINEAR);
+bool b16_stiffness(int order, int precision, int strain);
+int launch_frag(int order, int precision, int mode, const dev::AsmArgs &a, cudaStream_t s,
+                int strain = FEM_STRAIN_LINEAR);
 // Its tile-queue form for batches and the server (residual and Jacobian).
-int launch_frag_batched(int order, const dev::AsmArgs *meshes, const dev::Tile *tiles, int ntiles, int *counter,
-                        cudaStream_t s);
+int launch_frag_batched(int order, int precision, const dev::AsmArgs *meshes, const dev::Tile *tiles, int ntiles,
+                        int *counter, cudaStream_t s);
 
 inline void set_material(dev::AsmArgs &a, double E, double nu, double t) {
   // element/FEKernels.h:300-301
