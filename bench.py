@@ -54,6 +54,16 @@ def make_mesh(fem, name):
                            f"square{w['n']}_p{w['p']}")
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per assembly from ncu
+# captures of the headline kernels, keyed by workload and kernel family.  The
+# 1024^2 order-3 figure is the sum over the four colour launches of the 512^2 case
+# (2.835 GB; BF16x6 and FP64 kernels move the same bytes), times 4: traffic grows
+# with the element count.
+MEASURED_TRAFFIC = {
+    ("square1024_p3", "frag_kernel<3"): 4 * 2.835e9,
+}
+
+
 def algorithmic_bytes(mesh, nnzb):
     """Minimal HBM bytes of one residual+Jacobian assembly: read coords and states,
     read conn, write the residual and the BSR values once."""
@@ -337,6 +347,8 @@ def run_ours(args):
 
     hbm, peak_kind = peaks()
     abytes = algorithmic_bytes(mesh, nnzb)
+    label = kernel_label(plan, mesh.order, prec)
+    traffic = next((v for (w, k), v in MEASURED_TRAFFIC.items() if w == mesh.name and label.startswith(k)), None)
     achieved = abytes / (ms * 1e-3) / 1e9
     # FP64 side of the roofline: conventional element flops n_q (24 n^2 + 24 n + 40)
     # (a 2x2 block of D^T B products per node pair plus the J / grad u / sigma / R
@@ -356,10 +368,12 @@ def run_ours(args):
         "dof_per_s": value * mesh.num_dof / nE,
         "paths": paths,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": None, "peak_kind": peak_kind, "algorithmic_bytes_per_step": abytes,
+                     "traffic": traffic, "peak_kind": peak_kind, "algorithmic_bytes_per_step": abytes,
                      "kernel": kernel_label(plan, mesh.order, prec),
-                     "traffic_note": ("ncu DRAM bytes per assembly are in profiles/ (element-scatter writes plus "
-                                      "later colours' reads of blocks an earlier colour stored)"),
+                     "traffic_note": ("DRAM bytes per step (all colour launches of one assembly) from an ncu capture "
+                                      "of a 512^2 order-3 mesh scaled x4 (profiles/); above the algorithmic bytes: "
+                                      "later colours' bulk reductions read the blocks an earlier colour stored"
+                                      if traffic else "no ncu capture for this workload"),
                      "fp64": {"algorithmic_flops_per_step": aflops,
                               "achieved_tflops": aflops / (ms * 1e-3) / 1e12,
                               "peak_tflops": fp64_peak.value, "peak_kind": "measured (FP64 MMA probe)",
@@ -675,7 +689,8 @@ def measure_peaks():
     fem = fem_pkg.load()
     torch.cuda.init()
     out = {}
-    for kind, name in ((0, "fp64_fma_tflops"), (1, "fp32_fma_tflops"), (2, "fp64_mma_tflops")):
+    for kind, name in ((0, "fp64_fma_tflops"), (1, "fp32_fma_tflops"), (2, "fp64_mma_tflops"),
+                       (3, "bf16_mma_sync_tflops")):
         v = C.c_double()
         fem.check(fem.lib.fem_probe_peak(kind, C.byref(v)), "fem_probe_peak")
         out[name] = v.value
@@ -702,7 +717,7 @@ def main():
     ap.add_argument("--paths", default="plan_fp64,plan_mixed,dropin_fp64,plan_nonlinear",
                     help="comma list of plan_fp64, plan_mixed, dropin_fp64, dropin_mixed, plan_nonlinear")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--peaks", action="store_true", help="print measured FP64/FP32/FP64-MMA peaks and exit")
+    ap.add_argument("--peaks", action="store_true", help="print measured FP64/FP32/FP64-MMA/BF16-MMA peaks and exit")
     args = ap.parse_args()
     args.paths = set(args.paths.split(","))
     if args.peaks:
