@@ -44,9 +44,12 @@ extern "C" {
 #define FEM_ERR_BUDGET 8           /* device-memory budget exhausted (serving admission)    */
 
 #define FEM_PRECISION_FP64 0  /* all element arithmetic in FP64                               */
-#define FEM_PRECISION_MIXED 1 /* FP64 J/detJ/J^-1 and FP64 accumulate, FP32 element products
-                               where those are the faster kernel (order 4; order 1 drop-in);
-                               elsewhere the faster FP64 kernel runs and the result is FP64 */
+#define FEM_PRECISION_MIXED 1 /* FP64 J/detJ/J^-1, weak stress and accumulate; element
+                               stiffness in reduced precision where that kernel is the
+                               faster one: order 3 as BF16 tensor-core products of
+                               three-way split operands (FP32 accumulate), order 4 and the
+                               order-1 drop-in as FP32 element products; elsewhere the
+                               faster FP64 kernel runs and the result is FP64 */
 
 /* Strain measure of the weak residual: the reference's A2D::GreenStrainType
  * template option of planeStressWeakRes and the four assembly kernels

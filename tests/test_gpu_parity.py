@@ -123,6 +123,30 @@ def test_mixed_precision_error(fem, orc, cuda, name):
     assert _frob(mat.cpu().numpy(), A0) <= MIXED_TOL
 
 
+@pytest.mark.parametrize("name,reduced", [("sq5x4_p3", True), ("ann5x17_p3", True), ("sq37x23_p2", False)])
+def test_mixed_order3_runs_reduced_precision(fem, orc, cuda, name, reduced):
+    """MIXED at order 3 runs its element stiffness as BF16x6 tensor-core products:
+    the Jacobian differs from the FP64 oracle by FP32-level rounding (well inside
+    1e-6, well above FP64 rounding) while the residual stays FP64; order 2 runs the
+    FP64 kernel and matches at 1e-12."""
+    import torch
+    m = MESHES[name](fem)
+    d = _dev(fem, m, cuda)
+    R0, A0 = orc.assemble(m, d.map_h, d.nnzb)
+    plan = fem.Plan(m.order, m.num_nodes, m.conn_ptr, m.conn)
+    res = torch.empty(m.num_nodes * 2, dtype=torch.float64, device=cuda)
+    mat = torch.empty(d.nnzb * 4, dtype=torch.float64, device=cuda)
+    plan.assemble(d.states, d.coords, m.E, m.nu, m.t, res, mat, precision="mixed")
+    torch.cuda.synchronize()
+    err = _frob(mat.cpu().numpy(), A0)
+    assert _rel(res.cpu().numpy(), R0) <= FP64_TOL
+    if reduced:
+        assert 1e-10 < err <= 1e-6, err
+    else:
+        assert _rel(mat.cpu().numpy(), A0) <= FP64_TOL
+    plan.close()
+
+
 @pytest.mark.parametrize("name", ["sq8_p1", "sq37x23_p2", "sq5x4_p3", "sq41x9_p4", "ann5x17_p3", "one_p4"])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_plan_overwrites_complete_result(fem, orc, cuda, name, precision):
