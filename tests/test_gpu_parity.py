@@ -88,11 +88,13 @@ def test_dropin_accumulates_into_outputs(fem, orc, cuda):
     assert _rel(mat.cpu().numpy() + 1.0, 2 * A0) <= 4 * FP64_TOL
 
 
-@pytest.mark.parametrize("name", ["sq6x5_p2", "sq5x4_p3", "sq3x4_p4"])
-def test_dropin_unaligned_matrix_and_map(fem, orc, cuda, name):
+@pytest.mark.parametrize("name,precision", [("sq6x5_p2", "fp64"), ("sq5x4_p3", "fp64"), ("sq3x4_p4", "fp64"),
+                                            ("sq5x4_p3", "mixed"), ("ann5x17_p3", "mixed")])
+def test_dropin_unaligned_matrix_and_map(fem, orc, cuda, name, precision):
     """The drop-in contract asks only 8-byte alignment of matEntries and 4-byte of
     the element map: a matrix one double and a map one int past a 16-byte boundary
-    take the atomic and 4-byte staging paths and give the same result."""
+    take the atomic and 4-byte staging paths and give the same result (MIXED at
+    order 3: the BF16x6 stiffness through the same write paths)."""
     import torch
     m = MESHES[name](fem)
     d = _dev(fem, m, cuda)
@@ -104,9 +106,12 @@ def test_dropin_unaligned_matrix_and_map(fem, orc, cuda, name):
     mat, dmap = mat_buf[1:], map_buf[1:]
     assert mat.data_ptr() % 16 == 8 and dmap.data_ptr() % 16 == 4
     fem.run_jacobian_kernel(m.order, d.conn_ptr, d.conn, m.num_elements, d.states, d.coords, m.E, m.nu, m.t, dmap,
-                            res, mat)
+                            res, mat, precision=precision)
     assert _rel(res.cpu().numpy(), R0) <= FP64_TOL
-    assert _rel(mat.cpu().numpy(), A0) <= FP64_TOL
+    if precision == "fp64":
+        assert _rel(mat.cpu().numpy(), A0) <= FP64_TOL
+    else:
+        assert _frob(mat.cpu().numpy(), A0) <= MIXED_TOL
 
 
 @pytest.mark.parametrize("name", ["sq8_p1", "sq6x5_p2", "sq5x4_p3", "sq3x4_p4", "ann8x32_p2", "sq41x9_p4"])
