@@ -197,6 +197,25 @@ class Plan:
               "fem_plan_assemble_ex")
         return el.value if timed else None
 
+    def assemble_host(self, host_states, states, node_coords, E, nu, t, host_residual, residual, mat_entries=None, *,
+                      precision="fp64", strain="linear", bands=8, stream=None, timed=False):
+        """fem_plan_assemble_host: upload `host_states` (CPU tensor, pinned for overlap)
+        into the device `states`, assemble, download `residual` into `host_residual`,
+        the copies overlapped with the band-split assembly; results equal assemble()'s."""
+        import torch
+        for name, x in (("host_states", host_states), ("host_residual", host_residual)):
+            if not isinstance(x, torch.Tensor) or x.is_cuda or x.dtype != torch.float64 or not x.is_contiguous():
+                raise ValueError(f"{name}: expected a contiguous float64 CPU tensor")
+        el = C.c_double(0.0)
+        check(lib.fem_plan_assemble_host(self._h, host_states.data_ptr(), _dptr(states, torch.float64, "states"),
+                                         _dptr(node_coords, torch.float64, "nodeCoords"), float(E), float(nu),
+                                         float(t), host_residual.data_ptr(),
+                                         _dptr(residual, torch.float64, "residual"),
+                                         _dptr(mat_entries, torch.float64, "matEntries"), _prec(precision),
+                                         _strain(strain), int(bands), _stream(stream),
+                                         C.byref(el) if timed else None), "fem_plan_assemble_host")
+        return el.value if timed else None
+
     def close(self):
         if self._h and self._h.value:
             lib.fem_plan_destroy(self._h)

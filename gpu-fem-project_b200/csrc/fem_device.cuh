@@ -480,6 +480,13 @@ struct Tile {
   int64_t begin;
 };
 
+// Up to kMaxRanges list-position ranges of one mesh assembled by one launch.
+constexpr int kMaxRanges = 4;
+struct RangeList {
+  int n;
+  int64_t begin[kMaxRanges], count[kMaxRanges];
+};
+
 // Work source of the batched kernel: groups pull tiles from a per-launch queue
 // (one atomic counter per launch) and walk their batches.
 struct QueueSource {

@@ -202,13 +202,17 @@ __device__ __forceinline__ void frag_prologue(unsigned char *smem) {
     }
   }
   // sum_a dN(a, q): zero in exact arithmetic, a few ulp of the table entries in
-  // FP64; summed with Neumaier compensation (error ~1e-30 absolute)
+  // FP64; summed with Neumaier compensation (error ~1e-30 absolute) over the J-stage
+  // table entries written above (lane (g, t) of block (ks, tn) holds component g%2 of
+  // dN(4ks + t, 4tn + g/2)) instead of evaluating the basis again
+  __syncthreads();
   double2 *csum = reinterpret_cast<double2 *>(smem + L::csum);
   for (int q = threadIdx.x; q < F::NQP; q += blockDim.x) {
     double s0 = 0.0, c0 = 0.0, s1 = 0.0, c1 = 0.0;
     if (q < NQ) {
       for (int a = 0; a < NN; a++) {
-        const double2 d = dN(a, q);
+        const int e = (((a >> 2) * K4 + (q >> 2)) * 32) + ((2 * (q & 3)) << 2) + (a & 3);
+        const double2 d = make_double2(tabJ[e], tabJ[e + 4]);
         const double t0 = s0 + d.x, t1 = s1 + d.y;
         c0 += fabs(s0) >= fabs(d.x) ? (s0 - t0) + d.x : (d.x - t0) + s0;
         c1 += fabs(s1) >= fabs(d.y) ? (s1 - t1) + d.y : (d.y - t1) + s1;
@@ -382,6 +386,30 @@ struct PairStride {
   __device__ PairCursor next(int) {
     PairCursor c{0, 0, begin + 2 * p};
     if (c.k0 < end) c.ne = (int)min((int64_t)2, end - c.k0);
+    p += stride;
+    return c;
+  }
+};
+
+// One mesh, up to kMaxRanges list-position ranges of one launch (the band-split
+// launches of fem_plan_assemble_host that share a schedule step): pairs p, p +
+// stride, ... of their concatenation; a pair never straddles two ranges.
+struct PairRanges {
+  static constexpr bool kBatched = false;
+  RangeList r;
+  int64_t p, stride;
+  __device__ PairCursor next(int) {
+    PairCursor c{0, 0, 0};
+    int64_t q = p;
+    for (int i = 0; i < r.n; i++) {
+      const int64_t np = (r.count[i] + 1) / 2;
+      if (q < np) {
+        c.k0 = r.begin[i] + 2 * q;
+        c.ne = (int)min((int64_t)2, r.begin[i] + r.count[i] - c.k0);
+        break;
+      }
+      q -= np;
+    }
     p += stride;
     return c;
   }
@@ -1237,6 +1265,17 @@ __global__ void __launch_bounds__(32 * FragDims<P>::WARPS, FEM_FRAG_MINB) frag_k
   frag_loop<P, MODE>(smem, gen, A, &A);
 }
 
+// One mesh, several list-position ranges (plan mode).
+template <int P, int MODE>
+__global__ void __launch_bounds__(32 * FragDims<P>::WARPS, FEM_FRAG_MINB)
+    frag_ranges_kernel(const __grid_constant__ AsmArgs A, const RangeList R) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  frag_prologue<P, (MODE & kB16) != 0>(smem);
+  const int warp = threadIdx.x >> 5;
+  PairRanges gen{R, (int64_t)blockIdx.x * FragDims<P>::WARPS + warp, (int64_t)gridDim.x * FragDims<P>::WARPS};
+  frag_loop<P, MODE>(smem, gen, A, &A);
+}
+
 // Many meshes of one order (one colour each): warps pull tiles from the launch's queue.
 template <int P, int MODE>
 __global__ void __launch_bounds__(32 * FragDims<P>::WARPS, FEM_FRAG_MINB)
@@ -1264,6 +1303,27 @@ int launch_frag_p(const AsmArgs &a, cudaStream_t s) {
   kernel<<<grid, NT, smem, s>>>(a);
   cudaError_t err = cudaGetLastError();
   if (err != cudaSuccess) return cuda_fail(err, "frag_kernel launch");
+  return FEM_SUCCESS;
+}
+
+template <int P, int MODE>
+int launch_frag_ranges_p(const AsmArgs &a, const RangeList &r, cudaStream_t s) {
+  using F = FragDims<P>;
+  constexpr int NT = 32 * F::WARPS;
+  auto kernel = frag_ranges_kernel<P, MODE>;
+  const size_t smem = FragLayout<P, false, (MODE & kNL) != 0, (MODE & kB16) != 0>::total;
+  LaunchInfo li;
+  int st = launch_info(kernel, NT, smem, li);
+  if (st) return st;
+  int64_t pairs = 0;
+  for (int i = 0; i < r.n; i++) pairs += (r.count[i] + 1) / 2;
+  const int64_t need = (pairs + F::WARPS - 1) / F::WARPS;
+  const int64_t cap = (int64_t)li.grid_per_sm * li.num_sms;
+  const int grid = (int)(need < cap ? need : cap);
+  if (grid <= 0) return FEM_SUCCESS;
+  kernel<<<grid, NT, smem, s>>>(a, r);
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return cuda_fail(err, "frag_ranges_kernel launch");
   return FEM_SUCCESS;
 }
 
@@ -1351,6 +1411,34 @@ int launch_frag(int order, int precision, int mode, const dev::AsmArgs &a, cudaS
     case kNL | kJac: return launch_frag_mode<kNL | kJac>(order, a, s);
     case kNL | kRes | kJac: return launch_frag_mode<kNL | kRes | kJac>(order, a, s);
     default: return fail(FEM_ERR_INVALID_ARGUMENT, "fragment kernel: mode %d", mode);
+  }
+}
+
+int launch_frag_ranges(int order, int precision, int mode, const dev::AsmArgs &a, const dev::RangeList &r,
+                       cudaStream_t s, int strain) {
+  using namespace dev;
+  if (strain == FEM_STRAIN_NONLINEAR) mode |= kNL;
+  if (b16_stiffness(order, precision, strain) && (mode & kJac)) mode |= kB16;
+  auto go = [&](auto mc) -> int {
+    constexpr int M = decltype(mc)::value;
+    switch (order) {
+      case 2:
+        if constexpr ((M & kB16) != 0) return fail(FEM_ERR_INVALID_ORDER, "fragment kernel, BF16x6: order 2");
+        else return launch_frag_ranges_p<2, M>(a, r, s);
+      case 3: return launch_frag_ranges_p<3, M>(a, r, s);
+      case 4:
+        if constexpr ((M & (kNL | kB16)) != 0) return fail(FEM_ERR_INVALID_ORDER, "fragment kernel, mode %d: order 4", M);
+        else return launch_frag_ranges_p<4, M>(a, r, s);
+      default: return fail(FEM_ERR_INVALID_ORDER, "fragment kernel: order %d", order);
+    }
+  };
+  switch (mode) {
+    case kPlan | kRes: return go(IC<kPlan | kRes>{});
+    case kPlan | kRes | kJac: return go(IC<kPlan | kRes | kJac>{});
+    case kPlan | kRes | kJac | kB16: return go(IC<kPlan | kRes | kJac | kB16>{});
+    case kNL | kPlan | kRes: return go(IC<kNL | kPlan | kRes>{});
+    case kNL | kPlan | kRes | kJac: return go(IC<kNL | kPlan | kRes | kJac>{});
+    default: return fail(FEM_ERR_INVALID_ARGUMENT, "fragment kernel, ranges: mode %d", mode);
   }
 }
 

@@ -27,7 +27,9 @@
 // two elements of one colour touch the same block or residual row.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
+#include <vector>
 
 #include "fem_common.h"
 #include "fem_device.cuh"
@@ -147,6 +149,8 @@ void plan_free(fem_plan *p) {
   cudaFree(p->d_rowElemPtr);
   cudaFree(p->d_rowElem);
   cudaFree(p->d_rowChunk);
+  if (p->copyIn) cudaStreamDestroy(p->copyIn);
+  if (p->copyOut) cudaStreamDestroy(p->copyOut);
   cudaSetDevice(cur);
   delete p;
 }
@@ -245,6 +249,14 @@ int fem_plan_create(int elementOrder, int numNodes, const int *connPtr, const in
   p->numColours = hp.numColours;
   p->nnzb = hp.nnzb;
   p->colourPtr = hp.colourPtr;
+  p->elemList = hp.elemList;
+  p->nodeLo.resize((size_t)hp.numElements);
+  p->nodeHi.resize((size_t)hp.numElements);
+  for (int k = 0; k < hp.numElements; k++) {
+    const int *c = &hp.connList[(size_t)k * hp.nn];
+    p->nodeLo[k] = *std::min_element(c, c + hp.nn);
+    p->nodeHi[k] = *std::max_element(c, c + hp.nn);
+  }
   if ((st = upload(hp.rowp, &p->d_rowp, p->deviceBytes)) || (st = upload(hp.cols, &p->d_cols, p->deviceBytes)) ||
       (st = upload(hp.connList, &p->d_connList, p->deviceBytes)) ||
       (st = upload(hp.blockCode, &p->d_blockCode, p->deviceBytes))) {
@@ -354,6 +366,205 @@ int fem_plan_assemble_ex(const fem_plan *plan, const double *states, const doubl
     }
     return (int)FEM_SUCCESS;
   });
+}
+
+// Host-buffer assembly with the copies overlapped: see include/fem_b200.h.  The
+// schedule cuts the elements into bands (element-id ranges) and the nodes into as
+// many chunks; launch (band k, colour c) runs after every launch (k', c - 1) whose
+// band's node span overlaps band k's (t(k, c) = max(k, t(k', c - 1) + 1)), so every
+// block still receives its colours in order and the result equals
+// fem_plan_assemble's bit for bit.
+int fem_plan_assemble_host(const fem_plan *plan, const double *hostStates, double *states, const double *nodeCoords,
+                           double E, double nu, double t, double *hostResidual, double *residual, double *matEntries,
+                           int precision, int strainType, int numBands, void *stream, double *elapsedSeconds) {
+  fem::clear_error();
+  if (elapsedSeconds) *elapsedSeconds = 0.0;
+  if (!plan) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "plan is NULL");
+  if (!hostStates || !states || !nodeCoords || !hostResidual || !residual)
+    return fem::fail(FEM_ERR_INVALID_ARGUMENT, "NULL state, coordinate or residual array");
+  if (numBands < 1 || numBands > 256) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "numBands %d (1..256)", numBands);
+  if (!fem::aligned16(states) || !fem::aligned16(nodeCoords) || !fem::aligned16(residual))
+    return fem::fail(FEM_ERR_MISALIGNED, "states, nodeCoords and residual must be 16-byte aligned");
+  if (matEntries && (reinterpret_cast<uintptr_t>(matEntries) & 31u))
+    return fem::fail(FEM_ERR_MISALIGNED, "matEntries must be 32-byte aligned (one 2x2 block per 256-bit store)");
+  if (strainType != FEM_STRAIN_LINEAR && strainType != FEM_STRAIN_NONLINEAR)
+    return fem::fail(FEM_ERR_INVALID_ARGUMENT, "strain type %d", strainType);
+  if (precision != FEM_PRECISION_FP64 && precision != FEM_PRECISION_MIXED)
+    return fem::fail(FEM_ERR_INVALID_ARGUMENT, "precision %d", precision);
+  if (strainType == FEM_STRAIN_NONLINEAR && precision != FEM_PRECISION_FP64)
+    return fem::fail(FEM_ERR_INVALID_ARGUMENT, "NONLINEAR strain is assembled in FP64 only (precision %d)", precision);
+  if (plan->numElements == 0) return FEM_SUCCESS;
+  fem_plan *mp = const_cast<fem_plan *>(plan);  // the copy streams are created on first use
+  for (cudaStream_t *cs : {&mp->copyIn, &mp->copyOut}) {
+    if (!*cs) {
+      cudaError_t err = cudaStreamCreateWithFlags(cs, cudaStreamNonBlocking);
+      if (err != cudaSuccess) return fem::cuda_fail(err, "cudaStreamCreateWithFlags");
+    }
+  }
+  const int N = plan->numNodes, nE = plan->numElements, nc = plan->numColours;
+  const int B = std::min(numBands, std::max(1, std::min(N, nE)));
+  // node chunk j = [nstart[j], nstart[j + 1]); chunk_of inverts exactly that split
+  std::vector<int64_t> nstart((size_t)B + 1);
+  for (int j = 0; j <= B; j++) nstart[j] = (int64_t)j * N / B;
+  auto chunk_of = [&](int64_t n) {
+    return (int)(std::upper_bound(nstart.begin(), nstart.end(), n) - nstart.begin()) - 1;
+  };
+  auto node0 = [&](int j) { return nstart[j]; };
+  const bool rows = fem::plan_rows(plan) && strainType == FEM_STRAIN_LINEAR;
+
+  struct L {
+    int t, c, k;
+    int64_t p0, p1;
+    int lo, hi;
+  };
+  std::vector<L> ls;
+  if (rows) {
+    ls.push_back({0, 0, 0, 0, plan->numChunks, 0, N - 1});
+  } else {
+    // per (band, colour): list positions and node span; per band: node span
+    std::vector<int> blo(B, INT32_MAX), bhi(B, -1);
+    std::vector<L> cells((size_t)B * nc);
+    for (int c = 0; c < nc; c++) {
+      const int *b0 = plan->elemList.data() + plan->colourPtr[c], *b1 = plan->elemList.data() + plan->colourPtr[c + 1];
+      for (int k = 0; k < B; k++) {
+        L &x = cells[(size_t)k * nc + c];
+        x.c = c;
+        x.k = k;
+        x.p0 = std::lower_bound(b0, b1, (int)((int64_t)k * nE / B)) - plan->elemList.data();
+        x.p1 = std::lower_bound(b0, b1, (int)((int64_t)(k + 1) * nE / B)) - plan->elemList.data();
+        x.lo = INT32_MAX;
+        x.hi = -1;
+        for (int64_t q = x.p0; q < x.p1; q++) {
+          x.lo = std::min(x.lo, plan->nodeLo[q]);
+          x.hi = std::max(x.hi, plan->nodeHi[q]);
+        }
+        blo[k] = std::min(blo[k], x.lo);
+        bhi[k] = std::max(bhi[k], x.hi);
+      }
+    }
+    std::vector<int> tprev(B), tcur(B);
+    for (int k = 0; k < B; k++) tprev[k] = k;
+    for (int c = 0; c < nc; c++) {
+      for (int k = 0; k < B; k++) {
+        int tk = k;
+        if (c > 0)
+          for (int k2 = 0; k2 < B; k2++)
+            if (bhi[k2] >= 0 && bhi[k] >= 0 && blo[k2] <= bhi[k] && blo[k] <= bhi[k2]) tk = std::max(tk, tprev[k2] + 1);
+        tcur[k] = tk;
+        L &x = cells[(size_t)k * nc + c];
+        x.t = tk;
+        if (x.p1 > x.p0) ls.push_back(x);
+      }
+      tprev = tcur;
+    }
+    std::sort(ls.begin(), ls.end(), [](const L &a, const L &b) {
+      return a.t != b.t ? a.t < b.t : (a.c != b.c ? a.c < b.c : a.k < b.k);
+    });
+  }
+  const bool frag = fem::frag_supported(plan->order, precision, strainType, true);
+  // launches: the fragment kernel takes the ranges of one schedule step (independent:
+  // different bands of different colours, or one colour's bands) in one launch
+  struct G {
+    int need, lo, hi;
+    fem::dev::RangeList r;
+  };
+  std::vector<G> gs;
+  for (const L &x : ls) {
+    const bool join = frag && !rows && !gs.empty() && gs.back().r.n < fem::dev::kMaxRanges &&
+                      ls[&x - ls.data() - 1].t == x.t;
+    if (!join) gs.push_back(G{-1, INT32_MAX, -1, fem::dev::RangeList{0, {}, {}}});
+    G &g = gs.back();
+    g.r.begin[g.r.n] = x.p0;
+    g.r.count[g.r.n] = x.p1 - x.p0;
+    g.r.n++;
+    g.lo = std::min(g.lo, x.lo);
+    g.hi = std::max(g.hi, x.hi);
+    g.need = rows ? B - 1 : std::max(g.need, chunk_of(x.hi));
+  }
+  // the last launch touching each node chunk (-1: none)
+  std::vector<int> last(B, -1);
+  for (int i = 0; i < (int)gs.size(); i++)
+    for (int j = chunk_of(gs[i].lo); j <= chunk_of(gs[i].hi); j++) last[j] = i;
+
+  fem::dev::AsmArgs a{};
+  fem::plan_args(a, plan);
+  a.states = states;
+  a.coords = nodeCoords;
+  a.residual = residual;
+  a.mat = matEntries;
+  fem::set_material(a, E, nu, t);
+  const int mode = fem::dev::kPlan | fem::dev::kRes | (matEntries ? fem::dev::kJac : 0);
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  std::vector<cudaEvent_t> evs;
+  auto event = [&](cudaEvent_t *e) {
+    cudaError_t err = cudaEventCreateWithFlags(e, cudaEventDisableTiming);
+    if (err == cudaSuccess) evs.push_back(*e);
+    return err;
+  };
+  const int st = fem::timed(s, elapsedSeconds, [&]() -> int {
+    cudaError_t err;
+    cudaEvent_t start;
+    if ((err = event(&start)) != cudaSuccess || (err = cudaEventRecord(start, s)) != cudaSuccess ||
+        (err = cudaStreamWaitEvent(mp->copyIn, start, 0)) != cudaSuccess ||
+        (err = cudaStreamWaitEvent(mp->copyOut, start, 0)) != cudaSuccess)
+      return fem::cuda_fail(err, "stream ordering");
+    std::vector<cudaEvent_t> in(B), done(gs.size(), nullptr);
+    for (int j = 0; j < B; j++) {
+      const int64_t n0 = node0(j), n1 = node0(j + 1);
+      if (n1 > n0 && (err = cudaMemcpyAsync(states + 2 * n0, hostStates + 2 * n0, 16 * (size_t)(n1 - n0),
+                                            cudaMemcpyHostToDevice, mp->copyIn)) != cudaSuccess)
+        return fem::cuda_fail(err, "state upload");
+      if ((err = event(&in[j])) != cudaSuccess || (err = cudaEventRecord(in[j], mp->copyIn)) != cudaSuccess)
+        return fem::cuda_fail(err, "cudaEventRecord");
+    }
+    int waited = -1;
+    for (int i = 0; i < (int)gs.size(); i++) {
+      const G &g = gs[i];
+      if (g.need > waited) {
+        if ((err = cudaStreamWaitEvent(s, in[g.need], 0)) != cudaSuccess)
+          return fem::cuda_fail(err, "cudaStreamWaitEvent");
+        waited = g.need;
+      }
+      int r;
+      if (rows) {
+        a.begin = 0;
+        a.count = plan->numChunks;
+        r = fem::launch_rows(mode, a, s);
+      } else if (frag) {
+        r = fem::launch_frag_ranges(plan->order, precision, mode, a, g.r, s, strainType);
+      } else {
+        a.begin = g.r.begin[0];
+        a.count = g.r.count[0];
+        r = fem::launch(plan->order, precision, mode, a, s, strainType);
+      }
+      if (r) return r;
+      if (std::find(last.begin(), last.end(), i) != last.end()) {
+        if ((err = event(&done[i])) != cudaSuccess || (err = cudaEventRecord(done[i], s)) != cudaSuccess)
+          return fem::cuda_fail(err, "cudaEventRecord");
+      }
+    }
+    // residual chunks, each once the last launch touching its nodes has run
+    std::vector<int> order(B);
+    for (int j = 0; j < B; j++) order[j] = j;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return last[x] < last[y]; });
+    for (int j : order) {
+      const int64_t n0 = node0(j), n1 = node0(j + 1);
+      if (n1 <= n0) continue;
+      if (last[j] >= 0 && (err = cudaStreamWaitEvent(mp->copyOut, done[last[j]], 0)) != cudaSuccess)
+        return fem::cuda_fail(err, "cudaStreamWaitEvent");
+      if ((err = cudaMemcpyAsync(hostResidual + 2 * n0, residual + 2 * n0, 16 * (size_t)(n1 - n0),
+                                 cudaMemcpyDeviceToHost, mp->copyOut)) != cudaSuccess)
+        return fem::cuda_fail(err, "residual download");
+    }
+    cudaEvent_t end;
+    if ((err = event(&end)) != cudaSuccess || (err = cudaEventRecord(end, mp->copyOut)) != cudaSuccess ||
+        (err = cudaStreamWaitEvent(s, end, 0)) != cudaSuccess ||
+        (err = cudaStreamWaitEvent(s, in[B - 1], 0)) != cudaSuccess)
+      return fem::cuda_fail(err, "stream ordering");
+    return (int)FEM_SUCCESS;
+  });
+  for (cudaEvent_t e : evs) cudaEventDestroy(e);
+  return st;
 }
 
 }  // extern "C"

@@ -108,6 +108,10 @@ bool frag_supported(int order, int precision, int strain, bool plan);
 bool b16_stiffness(int order, int precision, int strain);
 int launch_frag(int order, int precision, int mode, const dev::AsmArgs &a, cudaStream_t s,
                 int strain = FEM_STRAIN_LINEAR);
+// Its multi-range form (plan mode, residual always, Jacobian optional): up to
+// kMaxRanges list-position ranges of one mesh in one launch.
+int launch_frag_ranges(int order, int precision, int mode, const dev::AsmArgs &a, const dev::RangeList &r,
+                       cudaStream_t s, int strain = FEM_STRAIN_LINEAR);
 // Its tile-queue form for batches and the server (residual and Jacobian).
 int launch_frag_batched(int order, int precision, const dev::AsmArgs *meshes, const dev::Tile *tiles, int ntiles,
                         int *counter, cudaStream_t s);
@@ -167,6 +171,10 @@ struct fem_plan {
   // order 1: row assembly tables (HostPlan::rowElemPtr/rowElem/rowChunk); numChunks == 0: none
   int *d_rowElemPtr = nullptr, *d_rowElem = nullptr, *d_rowChunk = nullptr;
   int numChunks = 0;
+  // host side of the overlapped host-buffer assembly (fem_plan_assemble_host): the
+  // colour-ordered element ids and each listed element's smallest and largest node
+  std::vector<int> elemList, nodeLo, nodeHi;
+  cudaStream_t copyIn = nullptr, copyOut = nullptr;  // created on first use
   int64_t deviceBytes = 0;
 };
 

@@ -166,6 +166,25 @@ int fem_plan_assemble_ex(const fem_plan *plan, const double *states, const doubl
                          double t, double *residual, double *matEntries, int precision, int strainType, void *stream,
                          double *elapsedSeconds);
 
+/* fem_plan_assemble_ex from and to HOST buffers, the copies overlapped with the
+ * assembly: the state upload (hostStates -> states) runs in numBands node chunks, the
+ * colour launches are split into numBands element bands (element-id ranges) and each
+ * band launch starts once the state chunks its nodes need have arrived, and each
+ * residual chunk (residual -> hostResidual) is downloaded as soon as the last launch
+ * touching its nodes has run.  Launch (band k, colour c) follows every launch of
+ * colour c - 1 whose band's node range overlaps band k's, so each block still receives
+ * its colours in order: the results equal fem_plan_assemble_ex's bit for bit.  On a
+ * mesh numbered along one axis the bands are strips and the copies overlap the
+ * assembly; on scrambled numbering the bands overlap each other and it runs serially,
+ * with the same result.  hostStates/hostResidual should be pinned (cudaHostAlloc) for
+ * the copies to be asynchronous.  The matrix stays on the device (matEntries may be
+ * NULL).  Uses two internal streams of the plan, created on the first call; calls on
+ * one plan must not overlap.  numBands: 1..256.  (No reference counterpart: the
+ * reference driver copies and assembles in sequence, verification/TestKernels.cpp:228-287.) */
+int fem_plan_assemble_host(const fem_plan *plan, const double *hostStates, double *states, const double *nodeCoords,
+                           double E, double nu, double t, double *hostResidual, double *residual, double *matEntries,
+                           int precision, int strainType, int numBands, void *stream, double *elapsedSeconds);
+
 /* ---- batched assembly of many meshes (config: 256 meshes, mixed orders) --------------- */
 /* A batch references existing plans (they must outlive it) and assembles all of
  * their meshes with one persistent kernel per (order, colour) whose thread groups
