@@ -1,6 +1,9 @@
 // Warp-fragment assembly kernel: FP64 residual + Jacobian assembly, LINEAR strain at
-// orders 2 to 4 and NONLINEAR (Green) strain at orders 2 and 3 (which paths use it:
-// frag_supported at the end of this file).
+// orders 2 to 4 and NONLINEAR (Green) strain at orders 2 and 3; FEM_PRECISION_MIXED at
+// order 3 with the element stiffness as BF16x6 tensor-core products (which paths use
+// it: frag_supported and b16_stiffness at the end of this file).  Launch forms: one
+// list-position range (plans, drop-in), up to four ranges (the band-split launches of
+// fem_plan_assemble_host), tile queues (batches, the server).
 //
 // The element kernel in fem_device.cuh stages every element's coordinates,
 // states and scaled gradients in shared memory and reads them back for each

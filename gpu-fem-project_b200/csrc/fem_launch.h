@@ -99,9 +99,10 @@ int launch_rows_batched(const dev::AsmArgs *meshes, const dev::Tile *tiles, int 
                         cudaStream_t s);
 // Chunks per row tile of the batched row kernel.
 constexpr int kRowTileChunks = 16;
-// Warp-fragment kernel (fem_frag.cu): LINEAR FP64 assembly at orders 2 and 3, plan
-// mode (one colour, list positions [a.begin, a.begin + a.count)) or drop-in mode
-// (elements through the reference map, accumulate-into).
+// Warp-fragment kernel (fem_frag.cu): LINEAR assembly at orders 2 to 4 and NONLINEAR
+// at orders 2 and 3 (frag_supported), plan mode (one colour, list positions
+// [a.begin, a.begin + a.count)) or drop-in mode (elements through the reference map,
+// accumulate-into).
 // FEM_PRECISION_MIXED at order 3 runs its element stiffness as BF16x6 tensor-core
 // products (b16_stiffness); the rest stays FP64.
 bool frag_supported(int order, int precision, int strain, bool plan);
