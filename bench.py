@@ -524,7 +524,7 @@ def run_batch(args):
     line = {
         "metric": "assembled elements/s (res+Jac)", "value": value, "unit": "elements/s", "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_batch * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.batch_precision == "fp64" else "f32/f64",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.batch_precision == "fp64" else "bf16x6 (p3) / f32 (p4) / f64",
         "data": "synthetic",
         "config": {"workload": f"batch{len(specs)}: element counts log-uniform in [1e3, 1e6], orders 1..4",
                    "meshes": len(specs), "elements": tot_el, "waves": len(waves),
