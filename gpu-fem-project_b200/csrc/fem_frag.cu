@@ -193,7 +193,7 @@ __device__ __forceinline__ void frag_prologue(unsigned char *smem) {
   }
   for (int q = threadIdx.x; q < F::NQP; q += blockDim.x)
     wq[q] = q < NQ ? __dmul_rn(kGW[P][q % P1], kGW[P][q / P1]) : 0.0;
-  // BF16x6 stiffness (orders 2, 3): entry (2k + h, lane (g, t)) holds dN(a, q) for the
+  // BF16x6 stiffness (order 3): entry (2k + h, lane (g, t)) holds dN(a, q) for the
   // node a = 8h + pi(g) and quadrature point q = 2t + (k & 1) + 8 (k >> 1) that lane
   // (g, t) places in its m16n8k16 fragments
   if constexpr (B16) {
