@@ -369,7 +369,8 @@ def run_ours(args):
     line = {
         "metric": "assembled elements/s (res+Jac)", "value": value, "unit": "elements/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64" if prec == "fp64" else ("bf16x6/f64" if mesh.order in (2, 3) else "f32/f64"), "data": "synthetic",
+        "vs_baseline": None, "dtype": "f64" if prec == "fp64" else {1: "f64", 2: "f64", 3: "bf16x6/f64"}.get(mesh.order, "f32/f64"),
+        "data": "synthetic",
         "config": {"workload": mesh.name, "order": mesh.order, "elements": nE, "dof": mesh.num_dof, "nnzb": nnzb,
                    "path": best, "l2": "inputs and outputs larger than L2 (BSR values %.2f GB)" % (32 * nnzb / 1e9),
                    "parallelism": f"replicas{world}"},
@@ -413,10 +414,10 @@ def kernel_label(plan, order, prec):
     """The kernel that runs one assembly of `plan` (the dispatch of fem_plan_assemble)."""
     if plan.row_chunks > 0:
         return "rows_p1_kernel, 1 launch per step"
-    # the fragment kernel serves orders 2-3 in both precisions (MIXED with its element
-    # stiffness as BF16x6 tensor-core products) and order 4 in FP64; FP32 order 4 runs
-    # the element kernel
-    if order in (2, 3) and prec == "mixed":
+    # the fragment kernel serves orders 2-3 in both precisions (MIXED at order 3 with
+    # its element stiffness as BF16x6 tensor-core products, at order 2 in FP64) and
+    # order 4 in FP64; FP32 order 4 runs the element kernel
+    if order == 3 and prec == "mixed":
         return f"frag_kernel<{order}, BF16x6 stiffness> x {plan.num_colours} colour launches per step"
     if order in (2, 3) or (order == 4 and prec == "fp64"):
         return f"frag_kernel<{order}> x {plan.num_colours} colour launches per step"
@@ -658,7 +659,7 @@ def run_serve(args):
         "metric": "assembled elements/s (res+Jac); serve p50/p99 ms", "value": best["elements_per_s"],
         "unit": "elements/s", "n_gpus": 1, "steps": sum(x["requests"] for x in sweep), "warmup": len(meshes),
         "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if args.batch_precision == "fp64" else "f32/f64", "data": "synthetic",
+        "dtype": "f64" if args.batch_precision == "fp64" else "bf16x6 (p3) / f32 (p4) / f64", "data": "synthetic",
         "config": {"workload": f"serve{args.clients}: Newton clients, meshes <= 4M DOF, Poisson arrivals",
                    "clients_admitted": len(meshes), "budget_gb": args.budget_gb, "device_bytes_used": used,
                    "max_batch": args.max_batch, "precision": args.batch_precision},
