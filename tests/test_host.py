@@ -24,6 +24,15 @@ def test_library_exports_every_declared_symbol(fem):
     assert fem.lib.fem_version() >= 100
 
 
+def test_python_mirror_binds_every_declared_symbol(fem):
+    """The ctypes table of the host mirror covers the whole C ABI (argument types
+    set for every entry point the header declares)."""
+    from importlib import import_module
+    lib_mod = import_module(fem.__name__ + "._lib")
+    missing = [n for n in _declared() if n not in lib_mod.SIGNATURES]
+    assert not missing, missing
+
+
 def test_status_strings(fem):
     for s in range(0, 9):
         assert fem.lib.fem_status_string(s)
