@@ -13,9 +13,18 @@
 // the process exits.  Host code cannot use the array's name as a device address
 // (in host code it is a stand-in), so the first call on each device looks up the
 // real address with cudaGetSymbolAddress while that device is current and caches
-// it; that first call should be made before any stream capture.  All calls share
-// the array and it keeps the last call's contents: the queue counter is cleared
-// at the start of every call, and calls that overlap on the GPU race on it.
+// it; that first call should be made before any stream capture.  The cached
+// address belongs to the device's current context: after cudaDeviceReset the
+// library must be reloaded.  All calls share the array and it keeps the last
+// call's contents: the queue counter is cleared at the start of every call, and
+// calls that overlap on the GPU race on it.
+//
+// The mesh table and tiles are staged in host arrays and copied with
+// cudaMemcpyAsync from pageable memory, which CUDA may complete only after the
+// work already queued on `stream` (the call can block the host until then).  A
+// captured copy would read those host arrays again at every replay, after later
+// calls had overwritten them, so calls on a stream that is being captured are
+// refused with FEM_ERR_UNSUPPORTED.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -129,6 +138,13 @@ int fem_run_jacobian_batched_static(int numMeshes, const fem_dropin_mesh *meshes
       return fem::fail(FEM_ERR_MISALIGNED, "mesh %d: vectors must be 16-byte aligned", m);
     perOrder[d.elementOrder] += d.numElements;
   }
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaError_t cerr = cudaStreamIsCapturing(s, &cap);
+  if (cerr != cudaSuccess) return fem::cuda_fail(cerr, "cudaStreamIsCapturing");
+  if (cap != cudaStreamCaptureStatusNone)
+    return fem::fail(FEM_ERR_UNSUPPORTED, "the mesh table is staged from host memory at call time: "
+                                          "calls on a capturing stream are refused");
   std::lock_guard<std::mutex> lk(g_static_mu);
   unsigned char *base = nullptr;
   int st = static_scratch(&base);
@@ -174,7 +190,6 @@ int fem_run_jacobian_batched_static(int numMeshes, const fem_dropin_mesh *meshes
     g_host_args[m] = a;
   }
   if (nt == 0) return FEM_SUCCESS;
-  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   auto *d_args = reinterpret_cast<fem::dev::AsmArgs *>(base + StaticLayout::args);
   auto *d_tiles = reinterpret_cast<fem::dev::Tile *>(base + StaticLayout::tiles);
   int *d_counters = reinterpret_cast<int *>(base + StaticLayout::counters);

@@ -273,12 +273,17 @@ typedef struct {
  * What the batched kernel needs besides the caller's arrays lives in a
  * file-scope __device__ array of FEM_STATIC_SCRATCH_BYTES that every GPU using
  * the library holds until the process exits.  The first call on a device looks
- * up that array's device address (make it before any stream capture).  Calls
- * share the array, so calls that overlap on the GPU race; each call clears the
- * queue counters it uses.  Accumulates into caller-zeroed residual and
- * matEntries like fem_run_jacobian; asynchronous on `stream` (the host staging
- * of the mesh table is copied out before the call returns).  More than 256
- * meshes or more work than the tile capacity returns FEM_ERR_UNSUPPORTED.
+ * up that array's device address (make it before any stream capture); the
+ * address is cached for the device's context, so the library must be reloaded
+ * after cudaDeviceReset.  Calls share the array, so calls that overlap on the
+ * GPU race; each call clears the queue counters it uses.  Accumulates into
+ * caller-zeroed residual and matEntries like fem_run_jacobian; asynchronous on
+ * `stream` except that the mesh table is staged in pageable host memory, whose
+ * copy CUDA may start only after the work already queued on `stream` (the call
+ * can block the host until then; the staging is free again when it returns).
+ * A stream that is being captured is refused (FEM_ERR_UNSUPPORTED): a captured
+ * copy would re-read the host staging at every replay.  More than 256 meshes or
+ * more work than the tile capacity returns FEM_ERR_UNSUPPORTED.
  * (No counterpart in the reference: it assembles one mesh per call.) */
 int fem_run_jacobian_batched_static(int numMeshes, const fem_dropin_mesh *meshes, void *stream);
 

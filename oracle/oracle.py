@@ -163,6 +163,56 @@ def assemble(mesh, bsr_map=None, nnzb: int | None = None, residual: bool = True,
     return res, mat
 
 
+REF_LIB_PATH = HERE / "_ref" / "libfemref.so"
+_ref_lib = None
+
+
+def ref_available() -> bool:
+    """Whether oracle/_ref/libfemref.so (the reference's own CPU assembly compiled
+    from its header, oracle/Makefile target `ref`) has been built here."""
+    return REF_LIB_PATH.exists()
+
+
+def ref_lib():
+    global _ref_lib
+    if _ref_lib is None:
+        lib = C.CDLL(str(REF_LIB_PATH))
+        p, i, d = C.c_void_p, C.c_int, C.c_double
+        lib.ref_run_residual.argtypes = [i, p, p, i, p, p, d, d, d, p]
+        lib.ref_run_residual.restype = d
+        lib.ref_run_jacobian.argtypes = [i, p, p, i, p, p, d, d, d, p, p, p]
+        lib.ref_run_jacobian.restype = d
+        lib.ref_assemble_nonlinear.argtypes = [i, p, p, i, p, p, d, d, d, p, p, p]
+        lib.ref_assemble_nonlinear.restype = i
+        _ref_lib = lib
+    return _ref_lib
+
+
+def ref_assemble(mesh, bsr_map=None, nnzb: int | None = None, jacobian: bool = True, strain: str = "linear"):
+    """Residual and BSR values from the reference's own CPU assembly
+    (runResidualKernel / runJacobianKernel, element/FEKernels.h:1030-1225, host
+    build, serial), zero-initialised then accumulated as the reference driver does."""
+    cp, cn = _c(mesh.conn_ptr, np.int32), _c(mesh.conn, np.int32)
+    st, xy = _c(mesh.states, np.float64), _c(mesh.coords, np.float64)
+    res = np.zeros(mesh.num_nodes * 2)
+    mat = mp = None
+    if jacobian:
+        mp = _c(bsr_map, np.int32)
+        mat = np.zeros(int(nnzb) * 4)
+    ne = mesh.num_elements
+    if strain == "nonlinear":
+        rc = ref_lib().ref_assemble_nonlinear(mesh.order, _ptr(cp), _ptr(cn), ne, _ptr(st), _ptr(xy), mesh.E, mesh.nu,
+                                              mesh.t, _ptr(mp), _ptr(res), _ptr(mat))
+        assert rc == 0
+    elif jacobian:
+        ref_lib().ref_run_jacobian(mesh.order, _ptr(cp), _ptr(cn), ne, _ptr(st), _ptr(xy), mesh.E, mesh.nu, mesh.t,
+                                   _ptr(mp), _ptr(res), _ptr(mat))
+    else:
+        ref_lib().ref_run_residual(mesh.order, _ptr(cp), _ptr(cn), ne, _ptr(st), _ptr(xy), mesh.E, mesh.nu, mesh.t,
+                                   _ptr(res))
+    return res, mat
+
+
 def bsr_spmv(rowp, cols, A, x):
     rowp, cols, A, x = _c(rowp, np.int32), _c(cols, np.int32), _c(A, np.float64), _c(x, np.float64)
     y = np.zeros(x.size)
