@@ -7,18 +7,23 @@ perturbation, u in [-1e-3,1e-3], E=70e9, nu=0.3, 4x4 Gauss points; 18,886,658 DO
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
 
-Prints one JSON line (rank 0).  `value` is elements/s of the fastest validated
-path with device-resident inputs; `e2e` is the same metric through the public
-API with a host->device copy of the state and a device->host copy of the
-residual inside every timed step.  Multi-GPU runs are independent replicas (the
-assembly of one mesh is not sharded).  --impl reference times the FP64 CPU
-oracle (restatement of the reference's CPU assembly, element/FEKernels.h:317-508)
-on a bounded sample of the same mesh with all host threads.
+Prints one JSON line (rank 0).  `value` is elements/s of the plain FP64 plan
+assembly (the reference's arithmetic) with device-resident inputs; `e2e` is the
+same metric through the public API with a host->device copy of the state and a
+device->host copy of the residual inside every timed step.  The MIXED-precision
+form, the other paths (each timed for at least one second), a batched leg
+(meshes of the many-mesh configuration in one captured graph) and a served leg
+(Newton clients through the server at a fixed request rate) ride along as
+sub-objects.  Multi-GPU runs are independent replicas (the assembly of one mesh
+is not sharded).  --impl reference times the reference's own CPU assembly
+(element/FEKernels.h compiled as oracle/_ref) on a bounded sample of the same
+mesh with all host threads; it loads nothing from the library.
 """
 from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import pathlib
 import statistics
@@ -42,23 +47,24 @@ WORKLOADS = {
 }
 
 
-def make_mesh(fem, name):
+def make_mesh(mesh_mod, name):
+    """The named workload from the package's mesh generator (pure numpy)."""
     w = WORKLOADS[name]
     if w["kind"] == "square64":
-        return fem.square64_p1()
+        return mesh_mod.square64_p1()
     if w["kind"] == "annulus":
-        return fem.annulus512x2048_p2()
+        return mesh_mod.annulus512x2048_p2()
     if w["p"] == 3:
-        return fem.square1024_p3(w["n"])
-    return fem.square_mesh(w["n"], w["n"], w["p"], 1.0, 1.0, 0.1, 1e-3, 70e9, 0.3, 1.0, 0x5EED0006,
-                           f"square{w['n']}_p{w['p']}")
+        return mesh_mod.square1024_p3(w["n"])
+    return mesh_mod.square_mesh(w["n"], w["n"], w["p"], 1.0, 1.0, 0.1, 1e-3, 70e9, 0.3, 1.0, 0x5EED0006,
+                                f"square{w['n']}_p{w['p']}")
 
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per assembly from ncu
-# captures of the headline kernels, keyed by workload and kernel family.  The
-# 1024^2 order-3 figure is the sum over the four colour launches of the 512^2 case
-# (2.835 GB; BF16x6 and FP64 kernels move the same bytes), times 4: traffic grows
-# with the element count.
+# captures, keyed by workload and kernel label prefix.  The 1024^2 order-3 figure
+# is the sum over the four colour launches of the 512^2 case (2.835 GB; the FP64
+# and BF16x6 kernels move the same bytes) times 4: traffic grows with the element
+# count.
 MEASURED_TRAFFIC = {
     ("square1024_p3", "frag_kernel<3"): 4 * 2.835e9,
 }
@@ -68,12 +74,6 @@ def algorithmic_bytes(mesh, nnzb):
     """Minimal HBM bytes of one residual+Jacobian assembly: read coords and states,
     read conn, write the residual and the BSR values once."""
     return 16 * mesh.num_nodes * 2 + 4 * mesh.num_elements * mesh.nodes_per_element + 16 * mesh.num_nodes + 32 * nnzb
-
-
-def algorithmic_flops(mesh):
-    """Per-element FP64 flop convention n_q*(24n^2 + 24n + 40) with n = n_q = (p+1)^2."""
-    n = mesh.nodes_per_element
-    return mesh.num_elements * n * (24 * n * n + 24 * n + 40)
 
 
 class ClockSampler:
@@ -146,45 +146,138 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def log(msg):
+    print(f"[bench {time.strftime('%H:%M:%S')}] {msg}", file=sys.stderr, flush=True)
+
+
 # ----------------------------------------------------------------------------------------
+def reference_sample(mesh_mod, orc, args):
+    """The bounded CPU sample of the workload: its first elements, with the pattern
+    and element map from the oracle's own builders (nothing from the library)."""
+    mesh = make_mesh(mesh_mod, args.workload)
+    sample = min(mesh.num_elements, args.ref_elements)
+    sub = mesh_mod.submesh(mesh, 0, sample)
+    rowp, cols = orc.bsr_pattern(sub.num_nodes, sub.conn_ptr, sub.conn)
+    mp = orc.element_bsr_map(sub.conn_ptr, sub.conn, sub.nodes_per_element, rowp, cols)
+    return mesh, sub, mp, int(cols.size)
+
+
+def reference_assembler(orc, threads):
+    """(kind, description, fn(sub, map, nnzb)) for the CPU baseline: the reference's
+    own CPU assembly compiled with OpenMP (oracle/_ref/libfemref_omp.so) when it was
+    built from the reference checkout, else the oracle port."""
+    omp = ROOT / "oracle" / "_ref" / "libfemref_omp.so"
+    if omp.exists():
+        import ctypes as C
+        lib = C.CDLL(str(omp))
+        p, i, d = C.c_void_p, C.c_int, C.c_double
+        lib.ref_run_jacobian.argtypes = [i, p, p, i, p, p, d, d, d, p, p, p]
+        lib.ref_run_jacobian.restype = d
+        lib.ref_set_num_threads.argtypes = [i]
+        lib.ref_set_num_threads(threads)
+
+        def run(sub, mp, nnzb):
+            res = np.zeros(sub.num_nodes * 2)
+            mat = np.zeros(nnzb * 4)
+            cp, cn = np.ascontiguousarray(sub.conn_ptr, np.int32), np.ascontiguousarray(sub.conn, np.int32)
+            st, xy = np.ascontiguousarray(sub.states), np.ascontiguousarray(sub.coords)
+            lib.ref_run_jacobian(sub.order, cp.ctypes.data, cn.ctypes.data, sub.num_elements, st.ctypes.data,
+                                 xy.ctypes.data, sub.E, sub.nu, sub.t, mp.ctypes.data, res.ctypes.data,
+                                 mat.ctypes.data)
+
+        return "reference", ("runJacobianKernel host build (element/FEKernels.h compiled from the reference "
+                             "checkout, OpenMP over elements as written; A2D interface restated)"), run
+    orc.set_threads(threads)
+    return "port", "oracle restatement (OpenMP, atomic scatter)", (
+        lambda sub, mp, nnzb: orc.assemble(sub, mp, nnzb, parallel=True))
+
+
 def run_reference(args):
-    """FP64 CPU oracle (restatement of the reference CPU assembly) on a bounded sample."""
+    """The reference's CPU assembly on a bounded sample, all host threads; rank 0 only."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if int(os.environ.get("RANK", "0")) != 0:
         return
     sys.path.insert(0, str(ROOT / "oracle"))
     import fem_pkg
     import oracle as orc
-    fem = fem_pkg.load()
-    mesh = make_mesh(fem, args.workload)
-    sample = min(mesh.num_elements, args.ref_elements)
-    sub = fem.submesh(mesh, 0, sample)
-    rowp, cols = fem.build_bsr_pattern(sub.num_nodes, sub.conn_ptr, sub.conn)
-    mp = fem.build_element_bsr_map(sub.conn_ptr, sub.conn, sub.nodes_per_element, rowp, cols)
+    mesh_mod = fem_pkg.load_module("mesh")
+    mesh, sub, mp, nnzb = reference_sample(mesh_mod, orc, args)
     threads = os.cpu_count() or 1
-    orc.set_threads(threads)
+    kind, what, run = reference_assembler(orc, threads)
     times = []
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        orc.assemble(sub, mp, cols.size, parallel=True)
+        run(sub, mp, nnzb)
         dt = time.perf_counter() - t0
         if i >= args.warmup:
             times.append(dt)
     tot = sum(times)
-    value = sample * len(times) / tot
+    value = sub.num_elements * len(times) / tot
     line = {
         "impl": "reference", "metric": "assembled elements/s (res+Jac)", "value": value, "unit": "elements/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "sample_elements": sample, "order": mesh.order},
-        "cpu_baseline": {"value": value, "unit": "elements/s", "cores": threads, "kind": "port",
-                         "sample": f"first {sample} elements of {mesh.name} (OpenMP over elements, atomic scatter)"},
+        "config": {"workload": args.workload, "order": mesh.order, "sample_elements": sub.num_elements,
+                   "note": "each step assembles a bounded sample of the workload (its first elements); "
+                           "elements/s is a per-element rate"},
+        "cpu_baseline": {"value": value, "unit": "elements/s", "cores": threads, "kind": kind,
+                         "sample": f"first {sub.num_elements} elements of {mesh.name}: {what}"},
         "e2e": {"value": value, "unit": "elements/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
+def cpu_baseline(mesh_mod, args):
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as orc
+    mesh, sub, mp, nnzb = reference_sample(mesh_mod, orc, args)
+    threads = os.cpu_count() or 1
+    kind, what, run = reference_assembler(orc, threads)
+    run(sub, mp, nnzb)
+    t0 = time.perf_counter()
+    reps = 0
+    while True:
+        run(sub, mp, nnzb)
+        reps += 1
+        if time.perf_counter() - t0 > args.cpu_seconds:
+            break
+    dt = (time.perf_counter() - t0) / reps
+    return {"value": sub.num_elements / dt, "unit": "elements/s", "cores": threads, "kind": kind,
+            "sample": f"first {sub.num_elements} elements of {mesh.name}, {reps} repeats: {what}"}
+
+
 # ----------------------------------------------------------------------------------------
+class Timer:
+    """CUDA-event timing on one stream; max over ranks."""
+
+    def __init__(self, stream, pg, dev):
+        import fem_pkg
+        self.stream, self.pg, self.dev = stream, pg, dev
+        self.rep = fem_pkg.load_module("replicas")
+
+    def steps(self, fn, steps, warmup):
+        """ms per step over exactly `steps` steps after `warmup` untimed ones."""
+        import torch
+        for _ in range(warmup):
+            fn()
+        self.stream.synchronize()
+        self.rep.barrier(self.pg)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(self.stream)
+        for _ in range(steps):
+            fn()
+        ev1.record(self.stream)
+        ev1.synchronize()
+        return self.rep.max_over_ranks(ev0.elapsed_time(ev1) / steps, self.pg, self.dev)
+
+    def window(self, fn, min_seconds=1.0, warmup=3, max_steps=20000):
+        """(ms per step, steps) over a timed region of at least min_seconds."""
+        est = self.steps(fn, 3, warmup)
+        n = int(min(max_steps, max(5, math.ceil(min_seconds * 1e3 / max(est, 1e-3)))))
+        n = int(self.rep.max_over_ranks(n, self.pg, self.dev))
+        return self.steps(fn, n, 1), n
+
+
 def run_ours(args):
     import torch
     world, rank, local, pg = dist_setup(args)
@@ -192,7 +285,7 @@ def run_ours(args):
     dev = torch.device("cuda", local)
     import fem_pkg
     fem = fem_pkg.load()
-    mesh = make_mesh(fem, args.workload)
+    mesh = make_mesh(fem.mesh, args.workload)
     stream = torch.cuda.Stream(device=dev)
     sptr = stream.cuda_stream
     with torch.cuda.stream(stream):
@@ -204,115 +297,145 @@ def run_ours(args):
     stream.synchronize()
     E, nu, t = mesh.E, mesh.nu, mesh.t
     nE = mesh.num_elements
+    T = Timer(stream, pg, dev)
+    rate = lambda ms: world * nE / (ms * 1e-3)  # noqa: E731
 
-    def time_steps(fn, steps, warmup, launches_per_step):
-        for _ in range(warmup):
-            fn()
-        stream.synchronize()
-        if pg is not None:
-            pg.barrier()
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ev0.record(stream)
-        for _ in range(steps):
-            fn()
-        ev1.record(stream)
-        ev1.synchronize()
-        ms = ev0.elapsed_time(ev1) / steps
-        ms = fem_pkg.load_module("replicas").max_over_ranks(ms, pg, dev)
-        return ms, launches_per_step * steps
+    def assemble(prec="fp64", strain="linear", r=res, m=mat):
+        plan.assemble(d.states, d.coords, E, nu, t, r, m, precision=prec, strain=strain, stream=sptr)
 
-    paths = {}
-    # plan path (overwrite, no zeroing), FP64 and mixed
-    for prec in [x for x in ("fp64", "mixed") if f"plan_{x}" in args.paths]:
-        fn = (lambda prec=prec: plan.assemble(d.states, d.coords, E, nu, t, res, mat, precision=prec, stream=sptr))
-        ms, _ = time_steps(fn, max(2, args.steps // 2), args.warmup, plan.launches())
-        paths[f"plan_{prec}"] = {"ms": ms, "elements_per_s": nE / (ms * 1e-3)}
-    # GreenStrainType::NONLINEAR (FP64), same mesh and states; not a candidate for the headline
-    # (the reference's dispatch always assembles LINEAR)
-    if "plan_nonlinear" in args.paths:
-        fn = (lambda: plan.assemble(d.states, d.coords, E, nu, t, res, mat, strain="nonlinear", stream=sptr))
-        ms, _ = time_steps(fn, max(2, args.steps // 2), args.warmup, plan.launches("nonlinear"))
-        paths["plan_fp64_nonlinear"] = {"ms": ms, "elements_per_s": nE / (ms * 1e-3)}
-    # error of the mixed plan path against the FP64 plan path (FP64 path is oracle-checked in tests)
-    err_res = err_mat = float("inf")
-    if "plan_mixed" in paths:
-        with torch.cuda.stream(stream):
-            plan.assemble(d.states, d.coords, E, nu, t, res, mat, precision="fp64", stream=sptr)
-            res64, mat64 = res.clone(), mat.clone()
-            plan.assemble(d.states, d.coords, E, nu, t, res, mat, precision="mixed", stream=sptr)
-            err_res = float(torch.linalg.vector_norm(res - res64) / torch.linalg.vector_norm(res64))
-            err_mat = float(torch.linalg.vector_norm(mat - mat64) / torch.linalg.vector_norm(mat64))
-            del res64, mat64
-        paths["plan_mixed"]["rel_frobenius_err"] = {"residual": err_res, "jacobian": err_mat}
-    stream.synchronize()
-    # plain drop-in FP64 (reference contract: caller zeroes, kernel accumulates via map, atomics)
-    if any(x.startswith("dropin") for x in args.paths):
-        rowp_h, cols_h = plan.pattern()
-        mp = fem.build_element_bsr_map(mesh.conn_ptr, mesh.conn, mesh.nodes_per_element, rowp_h, cols_h)
-        with torch.cuda.stream(stream):
-            dmap = torch.from_numpy(mp).to(dev)
-        del mp, rowp_h, cols_h
-
-        def dropin(prec="fp64", zero=True):
-            if zero:
-                res.zero_()
-                mat.zero_()
-            fem.run_jacobian_kernel(mesh.order, d.conn_ptr, d.conn, nE, d.states, d.coords, E, nu, t, dmap, res, mat,
-                                    precision=prec, stream=sptr, timed=False)
-
-        with torch.cuda.stream(stream):
-            if "dropin_fp64" in args.paths:
-                ms, _ = time_steps(lambda: dropin("fp64", True), max(2, args.steps // 2), args.warmup, 1)
-                paths["dropin_fp64_with_zeroing"] = {"ms": ms, "elements_per_s": nE / (ms * 1e-3)}
-                ms, _ = time_steps(lambda: dropin("fp64", False), max(2, args.steps // 2), args.warmup, 1)
-                paths["dropin_fp64_kernel_only"] = {"ms": ms, "elements_per_s": nE / (ms * 1e-3)}
-            if "dropin_mixed" in args.paths:
-                ms, _ = time_steps(lambda: dropin("mixed", False), max(2, args.steps // 2), args.warmup, 1)
-                paths["dropin_mixed_kernel_only"] = {"ms": ms, "elements_per_s": nE / (ms * 1e-3)}
-        del dmap
-    best = "plan_fp64"
-    # MIXED is the headline only where it runs a kernel of its own and wins
-    mixed_own = kernel_label(plan, mesh.order, "mixed") != kernel_label(plan, mesh.order, "fp64")
-    if "plan_mixed" in paths and mixed_own and max(err_res, err_mat) <= 1e-6 and (
-            "plan_fp64" not in paths or paths["plan_mixed"]["ms"] < paths["plan_fp64"]["ms"]):
-        best = "plan_mixed"
-    prec = "mixed" if best == "plan_mixed" else "fp64"
-
-    def step():
-        plan.assemble(d.states, d.coords, E, nu, t, res, mat, precision=prec, stream=sptr)
-
+    # headline: FP64 plan assembly, exactly K steps after W warm-up steps
     with ClockSampler(local) as clk:
-        ms, launches = time_steps(step, args.steps, args.warmup, plan.launches())
-    value = world * nE / (ms * 1e-3)
+        ms = T.steps(assemble, args.steps, args.warmup)
+    value = rate(ms)
+    launches = plan.launches() * args.steps
+    log(f"plan fp64 {ms:.3f} ms")
 
     # end to end through the public API: pinned host state -> device, assemble, residual
     # -> pinned host, in one fem_plan_assemble_host call (state upload in node chunks,
     # band-split colour launches, residual download per chunk, all overlapped)
     h_states = torch.from_numpy(np.ascontiguousarray(mesh.states)).pin_memory()
     h_res = torch.empty(mesh.num_nodes * 2, dtype=torch.float64).pin_memory()
+    h2d, d2h = h_states.numel() * 8, h_res.numel() * 8
 
-    def e2e_step():
+    def e2e_step(prec="fp64"):
         plan.assemble_host(h_states, d.states, d.coords, E, nu, t, h_res, res, mat, precision=prec, bands=args.bands,
                            stream=sptr)
 
-    def e2e_serial_step():
+    def e2e_serial_step(prec="fp64"):
         d.states.copy_(h_states, non_blocking=True)
-        plan.assemble(d.states, d.coords, E, nu, t, res, mat, precision=prec, stream=sptr)
+        assemble(prec)
         h_res.copy_(res, non_blocking=True)
 
-    band_launches = plan.launches() if plan.row_chunks > 0 else plan.num_colours * args.bands
     with torch.cuda.stream(stream):
-        ms_e2e, _ = time_steps(e2e_step, args.steps, args.warmup, band_launches)
-        ms_e2e_serial, _ = time_steps(e2e_serial_step, args.steps, args.warmup, plan.launches())
-    h2d, d2h = h_states.numel() * 8, h_res.numel() * 8
+        ms_e2e = T.steps(e2e_step, args.steps, args.warmup)
+        ms_e2e_serial, _ = T.window(e2e_serial_step)
+    ms_piped = pipelined(T, fem, plan, d, mesh, res, h_states, h_res, args, dev, stream)
 
-    # the same per-step work for independent load cases streamed through the GPU:
-    # case k+1's state upload and case k-1's residual download overlap case k's
-    # assembly (copy-in, compute and copy-out streams, two state/residual buffers)
+    # every path timed over at least one second
+    paths = {}
+
+    def path(name, fn, **extra):
+        with torch.cuda.stream(stream):
+            pms, n = T.window(fn, args.min_seconds)
+        paths[name] = {"ms": pms, "elements_per_s": rate(pms), "timed_steps": n, **extra}
+        log(f"{name} {pms:.3f} ms ({n} steps)")
+        return pms
+
+    path("plan_fp64", assemble)
+    ms_mixed = path("plan_mixed", lambda: assemble("mixed"))
+    path("plan_fp64_nonlinear", lambda: assemble("fp64", "nonlinear"))
+    path("plan_fp64_residual_only", lambda: plan.assemble(d.states, d.coords, E, nu, t, res, None, stream=sptr))
+    err = mixed_error(plan, d, mesh, res, mat, stream, sptr)
+    with torch.cuda.stream(stream):
+        ms_e2e_mixed, _ = T.window(lambda: e2e_step("mixed"), args.min_seconds)
+    # plain drop-in FP64 (reference contract: caller zeroes, kernel accumulates via map)
+    rowp_h, cols_h = plan.pattern()
+    mp = fem.build_element_bsr_map(mesh.conn_ptr, mesh.conn, mesh.nodes_per_element, rowp_h, cols_h)
+    with torch.cuda.stream(stream):
+        dmap = torch.from_numpy(mp).to(dev)
+    del mp, rowp_h, cols_h
+
+    def dropin(zero=True):
+        if zero:
+            res.zero_()
+            mat.zero_()
+        fem.run_jacobian_kernel(mesh.order, d.conn_ptr, d.conn, nE, d.states, d.coords, E, nu, t, dmap, res, mat,
+                                stream=sptr, timed=False)
+
+    def dropin_residual():
+        res.zero_()
+        fem.run_residual_kernel(mesh.order, d.conn_ptr, d.conn, nE, d.states, d.coords, E, nu, t, res, stream=sptr,
+                                timed=False)
+
+    path("dropin_fp64_with_zeroing", dropin)
+    path("dropin_fp64_kernel_only", lambda: dropin(False))
+    path("dropin_fp64_residual_with_zeroing", dropin_residual)
+    del dmap
+    torch.cuda.synchronize(dev)
+
+    hbm, peak_kind = peaks()
+    abytes = algorithmic_bytes(mesh, nnzb)
+    label = kernel_label(plan, mesh.order, "fp64")
+    traffic = next((v for (w, k), v in MEASURED_TRAFFIC.items() if w == mesh.name and label.startswith(k)), None)
+    achieved = abytes / (ms * 1e-3) / 1e9
+    line = {
+        "metric": "assembled elements/s (res+Jac)", "value": value, "unit": "elements/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": mesh.name, "order": mesh.order, "elements": nE, "dof": mesh.num_dof, "nnzb": nnzb,
+                   "path": "plan_fp64", "l2": "inputs and outputs larger than L2 (BSR values %.2f GB)" % (32 * nnzb / 1e9),
+                   "parallelism": f"replicas{world}"},
+        "dof_per_s": value * mesh.num_dof / nE,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": traffic, "peak_kind": peak_kind, "algorithmic_bytes_per_step": abytes, "kernel": label,
+                     "traffic_note": ("DRAM bytes per step (all colour launches of one assembly) from an ncu capture "
+                                      "of the 512^2 order-3 mesh scaled x4; above the algorithmic bytes: later "
+                                      "colours' bulk reductions read the blocks an earlier colour stored"
+                                      if traffic else "no ncu capture for this workload")},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+        "e2e": {"value": rate(ms_e2e), "unit": "elements/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": ms_e2e,
+                "api": (f"fem_plan_assemble_host, {args.bands} bands (copies overlapped with the assembly); the "
+                        f"matrix ({32 * nnzb / 1e9:.2f} GB) stays on the device for a device solver -- a host "
+                        f"consumer of the matrix would add that D2H per assembly"),
+                "serial": {"value": rate(ms_e2e_serial), "ms_per_step": ms_e2e_serial,
+                           "note": "state upload, fem_plan_assemble, residual download in sequence"},
+                "pipelined": {"value": rate(ms_piped), "ms_per_step": ms_piped,
+                              "note": "independent load cases: case k+1 uploads and case k-1 downloads "
+                                      "while case k assembles (3 streams, 2 buffers); same copies per step"}},
+        "mixed": {"value": rate(ms_mixed), "ms_per_step": ms_mixed, "dtype": mixed_dtype(mesh.order),
+                  "kernel": kernel_label(plan, mesh.order, "mixed"), "rel_frobenius_err_vs_fp64": err,
+                  "e2e": {"value": rate(ms_e2e_mixed), "ms_per_step": ms_e2e_mixed}},
+        "paths": paths,
+    }
+    plan.close()
+    del res, mat, d
+    torch.cuda.synchronize(dev)
+    torch.cuda.empty_cache()
+    if rank == 0 and world == 1 and not args.no_legs:
+        plain = paths["dropin_fp64_with_zeroing"]["elements_per_s"]
+        line["batched"] = batch_leg(fem, dev, args, plain)
+        line["served"] = serve_leg(fem, dev, args)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(fem.mesh, args)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def pipelined(T, fem, plan, d, mesh, res, h_states, h_res, args, dev, stream):
+    """ms per load case when independent cases stream through the GPU: case k+1's
+    state upload and case k-1's residual download overlap case k's assembly."""
+    import torch
+    sptr = stream.cuda_stream
     s_in, s_out = torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev)
     with torch.cuda.stream(stream):
         st2 = [d.states, torch.empty_like(d.states)]
         rs2 = [res, torch.empty_like(res)]
+        mat = torch.empty(plan.nnzb * 4, dtype=torch.float64, device=dev)
     hs2 = [h_states, h_states.clone().pin_memory()]
     hr2 = [h_res, torch.empty_like(h_res).pin_memory()]
     ev_in = [torch.cuda.Event() for _ in range(2)]
@@ -329,7 +452,7 @@ def run_ours(args):
         ev_in[b].record(s_in)
         stream.wait_event(ev_in[b])
         stream.wait_event(ev_out[b])  # residual buffer b has been downloaded
-        plan.assemble(st2[b], d.coords, E, nu, t, rs2[b], mat, precision=prec, stream=sptr)
+        plan.assemble(st2[b], d.coords, mesh.E, mesh.nu, mesh.t, rs2[b], mat, stream=sptr)
         ev_comp[b].record(stream)
         s_out.wait_event(ev_comp[b])
         with torch.cuda.stream(s_out):
@@ -339,75 +462,36 @@ def run_ours(args):
     for k in range(args.warmup):
         piped_step(k)
     torch.cuda.synchronize(dev)
-    if pg is not None:
-        pg.barrier()
+    T.rep.barrier(T.pg)
+    steps = max(args.steps, 100)
     p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     p0.record(s_in)
-    for k in range(args.steps):
+    for k in range(steps):
         piped_step(k)
     s_in.wait_event(ev_out[0])
     s_in.wait_event(ev_out[1])
     p1.record(s_in)
     p1.synchronize()
-    ms_piped = fem_pkg.load_module("replicas").max_over_ranks(p0.elapsed_time(p1) / args.steps, pg, dev)
+    ms = T.rep.max_over_ranks(p0.elapsed_time(p1) / steps, T.pg, dev)
     torch.cuda.synchronize(dev)
-    del st2, rs2, hs2, hr2
+    return ms
 
-    hbm, peak_kind = peaks()
-    abytes = algorithmic_bytes(mesh, nnzb)
-    label = kernel_label(plan, mesh.order, prec)
-    traffic = next((v for (w, k), v in MEASURED_TRAFFIC.items() if w == mesh.name and label.startswith(k)), None)
-    achieved = abytes / (ms * 1e-3) / 1e9
-    # FP64 side of the roofline: conventional element flops n_q (24 n^2 + 24 n + 40)
-    # (a 2x2 block of D^T B products per node pair plus the J / grad u / sigma / R
-    # work, no symmetry savings) against this GPU's FP64 tensor-core peak, probed live
-    import ctypes as C
-    nloc = (mesh.order + 1) ** 2
-    aflops = float(nE) * nloc * (24 * nloc * nloc + 24 * nloc + 40)
-    fp64_peak = C.c_double()
-    fem.check(fem.lib.fem_probe_peak(2, C.byref(fp64_peak)), "fem_probe_peak")
-    line = {
-        "metric": "assembled elements/s (res+Jac)", "value": value, "unit": "elements/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64" if prec == "fp64" else {1: "f64", 2: "f64", 3: "bf16x6/f64"}.get(mesh.order, "f32/f64"),
-        "data": "synthetic",
-        "config": {"workload": mesh.name, "order": mesh.order, "elements": nE, "dof": mesh.num_dof, "nnzb": nnzb,
-                   "path": best, "l2": "inputs and outputs larger than L2 (BSR values %.2f GB)" % (32 * nnzb / 1e9),
-                   "parallelism": f"replicas{world}"},
-        "dof_per_s": value * mesh.num_dof / nE,
-        "paths": paths,
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": traffic, "peak_kind": peak_kind, "algorithmic_bytes_per_step": abytes,
-                     "kernel": kernel_label(plan, mesh.order, prec),
-                     "traffic_note": ("DRAM bytes per step (all colour launches of one assembly) from an ncu capture "
-                                      "of a 512^2 order-3 mesh scaled x4 (profiles/); above the algorithmic bytes: "
-                                      "later colours' bulk reductions read the blocks an earlier colour stored"
-                                      if traffic else "no ncu capture for this workload"),
-                     "fp64": {"algorithmic_flops_per_step": aflops,
-                              "achieved_tflops": aflops / (ms * 1e-3) / 1e12,
-                              "peak_tflops": fp64_peak.value, "peak_kind": "measured (FP64 MMA probe)",
-                              "frac": aflops / (ms * 1e-3) / 1e12 / fp64_peak.value,
-                              "max_bound_frac": max(abytes / (hbm * 1e9), aflops / (fp64_peak.value * 1e12))
-                              / (ms * 1e-3)}},
-        "gpu_launches": launches,
-        "clocks": clk.summary(),
-        "e2e": {"value": world * nE / (ms_e2e * 1e-3), "unit": "elements/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e,
-                "api": f"fem_plan_assemble_host, {args.bands} bands (copies overlapped with the assembly)",
-                "serial": {"value": world * nE / (ms_e2e_serial * 1e-3), "ms_per_step": ms_e2e_serial,
-                           "note": "state upload, fem_plan_assemble, residual download in sequence"},
-                "pipelined": {"value": world * nE / (ms_piped * 1e-3), "ms_per_step": ms_piped,
-                              "note": "independent load cases: case k+1 uploads and case k-1 downloads "
-                                      "while case k assembles (3 streams, 2 buffers); same copies per step"}},
-    }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(fem, mesh, args)
-    if rank == 0:
-        print(json.dumps(line), flush=True)
-    plan.close()
-    if pg is not None:
-        pg.barrier()
-        pg.destroy_process_group()
+
+def mixed_error(plan, d, mesh, res, mat, stream, sptr):
+    """Relative Frobenius error of the MIXED plan outputs against the FP64 ones."""
+    import torch
+    with torch.cuda.stream(stream):
+        plan.assemble(d.states, d.coords, mesh.E, mesh.nu, mesh.t, res, mat, precision="fp64", stream=sptr)
+        res64, mat64 = res.clone(), mat.clone()
+        plan.assemble(d.states, d.coords, mesh.E, mesh.nu, mesh.t, res, mat, precision="mixed", stream=sptr)
+        out = {"residual": float(torch.linalg.vector_norm(res - res64) / torch.linalg.vector_norm(res64)),
+               "jacobian": float(torch.linalg.vector_norm(mat - mat64) / torch.linalg.vector_norm(mat64))}
+    stream.synchronize()
+    return out
+
+
+def mixed_dtype(order):
+    return {1: "f64", 2: "f64", 3: "bf16x6/f64", 4: "f32/f64"}[order]
 
 
 def kernel_label(plan, order, prec):
@@ -424,6 +508,7 @@ def kernel_label(plan, order, prec):
     return f"assemble_kernel<{order}, float> x {plan.num_colours} colour launches per step"
 
 
+# ----------------------------------------------------------------------------------------
 def mesh_bytes(spec, with_map=True):
     """Device bytes of one batched mesh: plan topology, coordinates/states/residual,
     BSR values and (for the single-mesh comparison) the reference element map."""
@@ -434,29 +519,29 @@ def mesh_bytes(spec, with_map=True):
     return plan + data + (4 * ne * n * n if with_map else 0)
 
 
-def run_batch(args):
-    """Many meshes (log-uniform sizes 1e3..1e6 elements, orders 1..4) per graph launch,
-    in waves that fit the device-memory budget, against the single-mesh FP64 drop-in."""
-    import torch
-    torch.cuda.set_device(0)
-    dev = torch.device("cuda", 0)
-    import fem_pkg
-    fem = fem_pkg.load()
-    specs = fem.batch_specs(count=args.batch_meshes)
-    budget = args.budget_gb * 1e9
+def waves_of(specs, budget_bytes):
     waves, cur, used = [], [], 0
     for sp in specs:
         b = mesh_bytes(sp)
-        if cur and used + b > budget:
+        if cur and used + b > budget_bytes:
             waves.append(cur)
             cur, used = [], 0
         cur.append(sp)
         used += b
     if cur:
         waves.append(cur)
+    return waves
+
+
+def batched_measure(fem, dev, waves, steps, warmup, precisions):
+    """Each wave: plans, one tuned and captured graph per precision, replays timed
+    with CUDA events; the plain FP64 drop-in (zero the outputs, fem_run_jacobian per
+    mesh) on the same meshes; the MIXED error against FP64 on the first meshes."""
+    import torch
     stream = torch.cuda.Stream(device=dev)
     sptr = stream.cuda_stream
-    tot_el, t_batch, t_plain, launches, graph_ms, errs, tiles = 0, 0.0, 0.0, 0, [], [], []
+    out = {"elements": 0, "ms": {p: 0.0 for p in precisions}, "ms_plain": 0.0, "launches": {p: 0 for p in precisions},
+           "tiles": {p: [] for p in precisions}, "errs": [], "wave_ms": {p: [] for p in precisions}}
 
     def ev_time(fn, reps):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -465,7 +550,7 @@ def run_batch(args):
             fn()
         e1.record(stream)
         e1.synchronize()
-        return e0.elapsed_time(e1) / reps * 1e-3
+        return e0.elapsed_time(e1) / reps
 
     for wave in waves:
         meshes = [sp.build() for sp in wave]
@@ -475,108 +560,103 @@ def run_batch(args):
             res = [torch.empty(m.num_nodes * 2, dtype=torch.float64, device=dev) for m in meshes]
             mat = [torch.empty(p.nnzb * 4, dtype=torch.float64, device=dev) for p in plans]
         stream.synchronize()
-        batch = fem.Batch(plans)
-        for i, (m, d) in enumerate(zip(meshes, devs)):
-            batch.bind(i, d.states, d.coords, m.E, m.nu, m.t, res[i], mat[i])
-        prec = args.batch_precision
-        batch.tune(precision=prec, stream=sptr, reps=2)
-        tiles.append(batch.info()["tile_batches"])
-        batch.capture(precision=prec, stream=sptr)
-        for _ in range(args.warmup):
-            batch.replay(stream=sptr)
-        tb = ev_time(lambda: batch.replay(stream=sptr), args.steps)
-        launches += batch.info()["launches"] * args.steps
-        if prec == "mixed":
-            with torch.cuda.stream(stream):
-                keep = [(r.clone(), a.clone()) for r, a in zip(res[:8], mat[:8])]
-                batch.assemble(precision="fp64", stream=sptr)
-                for (r, a), r64, a64 in zip(keep, res[:8], mat[:8]):
-                    errs.append(max(float(torch.linalg.vector_norm(r - r64) / torch.linalg.vector_norm(r64)),
-                                    float(torch.linalg.vector_norm(a - a64) / torch.linalg.vector_norm(a64))))
-            del keep
-        # plain single-mesh FP64 drop-in (reference contract): zero outputs, one call per mesh
+        for prec in precisions:
+            batch = fem.Batch(plans)
+            for i, (m, dm) in enumerate(zip(meshes, devs)):
+                batch.bind(i, dm.states, dm.coords, m.E, m.nu, m.t, res[i], mat[i])
+            batch.tune(precision=prec, stream=sptr, reps=2)
+            out["tiles"][prec].append(batch.info()["tile_batches"])
+            batch.capture(precision=prec, stream=sptr)
+            for _ in range(warmup):
+                batch.replay(stream=sptr)
+            ms = ev_time(lambda: batch.replay(stream=sptr), steps)
+            out["ms"][prec] += ms
+            out["wave_ms"][prec].append(ms)
+            out["launches"][prec] += batch.info()["launches"] * steps
+            if prec == "mixed":
+                with torch.cuda.stream(stream):
+                    keep = [(r.clone(), a.clone()) for r, a in zip(res[:8], mat[:8])]
+                    b64 = fem.Batch(plans)
+                    for i, (m, dm) in enumerate(zip(meshes, devs)):
+                        b64.bind(i, dm.states, dm.coords, m.E, m.nu, m.t, res[i], mat[i])
+                    b64.assemble(precision="fp64", stream=sptr)
+                    for (r, a), r64, a64 in zip(keep, res[:8], mat[:8]):
+                        out["errs"].append(max(
+                            float(torch.linalg.vector_norm(r - r64) / torch.linalg.vector_norm(r64)),
+                            float(torch.linalg.vector_norm(a - a64) / torch.linalg.vector_norm(a64))))
+                    stream.synchronize()
+                    b64.close()
+                del keep
+            batch.close()
         maps = []
         for m, p in zip(meshes, plans):
             rowp, cols = p.pattern()
             mp = fem.build_element_bsr_map(m.conn_ptr, m.conn, m.nodes_per_element, rowp, cols)
-            maps.append(torch.from_numpy(mp).to(dev))
+            with torch.cuda.stream(stream):
+                maps.append(torch.from_numpy(mp).to(dev))
 
         def plain():
-            for m, d, r, a, mp in zip(meshes, devs, res, mat, maps):
+            for m, dm, r, a, mp in zip(meshes, devs, res, mat, maps):
                 r.zero_()
                 a.zero_()
-                fem.run_jacobian_kernel(m.order, d.conn_ptr, d.conn, m.num_elements, d.states, d.coords, m.E, m.nu,
-                                        m.t, mp, r, a, stream=sptr, timed=False)
+                fem.run_jacobian_kernel(m.order, dm.conn_ptr, dm.conn, m.num_elements, dm.states, dm.coords, m.E,
+                                        m.nu, m.t, mp, r, a, stream=sptr, timed=False)
 
         with torch.cuda.stream(stream):
             plain()
-            tp = ev_time(plain, max(1, args.steps // 2))
-        tot_el += sum(m.num_elements for m in meshes)
-        t_batch += tb
-        t_plain += tp
-        graph_ms.append(tb * 1e3)
-        batch.close()
+            out["ms_plain"] += ev_time(plain, max(1, steps // 2))
+        out["elements"] += sum(m.num_elements for m in meshes)
         for p in plans:
             p.close()
-        del meshes, plans, devs, res, mat, maps, batch
-        torch.cuda.synchronize()
+        del meshes, plans, devs, res, mat, maps
+        torch.cuda.synchronize(dev)
         torch.cuda.empty_cache()
-    value = tot_el / t_batch
-    line = {
-        "metric": "assembled elements/s (res+Jac)", "value": value, "unit": "elements/s", "n_gpus": 1,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_batch * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.batch_precision == "fp64" else "bf16x6 (p3) / f32 (p4) / f64",
-        "data": "synthetic",
-        "config": {"workload": f"batch{len(specs)}: element counts log-uniform in [1e3, 1e6], orders 1..4",
-                   "meshes": len(specs), "elements": tot_el, "waves": len(waves),
-                   "budget_gb": args.budget_gb, "precision": args.batch_precision,
-                   "l2": "per-wave inputs and outputs larger than L2"},
-        "plain_fp64_single_mesh": {"elements_per_s": tot_el / t_plain, "ms_per_step": t_plain * 1e3},
-        "batched_over_plain": t_plain / t_batch,
-        "wave_graph_ms": graph_ms, "tuned_tile_batches": tiles,
-        "mixed_rel_frobenius_err_max": max(errs) if errs else None,
-        "gpu_launches": launches,
+    return out
+
+
+def batch_leg(fem, dev, args, plain_single):
+    """The batched configuration in the default run: the first meshes of the
+    256-mesh mix (element counts log-uniform in [1e3, 1e6], orders 1-4) that fit
+    args.leg_batch_gb, one wave, FP64 and MIXED graphs, against the plain FP64
+    drop-in on the same meshes."""
+    t0 = time.perf_counter()
+    specs = fem.batch_specs(count=256)
+    budget = args.leg_batch_gb * 1e9
+    chosen, used = [], 0
+    for sp in specs:
+        b = mesh_bytes(sp)
+        if used + b > budget:
+            continue
+        chosen.append(sp)
+        used += b
+    r = batched_measure(fem, dev, [chosen], args.leg_steps, 3, ("fp64", "mixed"))
+    el = r["elements"]
+    per_order = {p: sum(s.num_elements for s in chosen if s.order == p) for p in (1, 2, 3, 4)}
+    log(f"batched leg {time.perf_counter() - t0:.1f} s")
+    return {
+        "workload": (f"{len(chosen)} of the 256 meshes (element counts log-uniform in [1e3, 1e6], orders 1-4), "
+                     f"first in draw order within {args.leg_batch_gb:g} GB, one captured graph per precision"),
+        "meshes": len(chosen), "elements": el, "elements_per_order": per_order,
+        "fp64": {"elements_per_s": el / (r["ms"]["fp64"] * 1e-3), "ms_per_step": r["ms"]["fp64"],
+                 "tuned_tile_batches": r["tiles"]["fp64"][0]},
+        "mixed": {"elements_per_s": el / (r["ms"]["mixed"] * 1e-3), "ms_per_step": r["ms"]["mixed"],
+                  "tuned_tile_batches": r["tiles"]["mixed"][0],
+                  "rel_frobenius_err_vs_fp64_max": max(r["errs"]) if r["errs"] else None},
+        "plain_fp64_dropin_same_meshes": {"elements_per_s": el / (r["ms_plain"] * 1e-3), "ms_per_step": r["ms_plain"],
+                                          "note": "zero the outputs, fem_run_jacobian per mesh"},
+        "batched_over_plain": {"fp64": r["ms_plain"] / r["ms"]["fp64"], "mixed": r["ms_plain"] / r["ms"]["mixed"]},
+        "mixed_over_plain_single_mesh_headline": (el / (r["ms"]["mixed"] * 1e-3)) / plain_single,
+        "timed_steps": args.leg_steps, "gpu_launches": r["launches"],
     }
-    print(json.dumps(line), flush=True)
 
 
-def run_serve(args):
-    """64 Newton-solve clients with device-resident meshes (drawn like the batched
-    workload, at most 4M DOF each) issue requests as one Poisson stream at each
-    swept aggregate rate; the server admits meshes under the HBM budget and
-    batches concurrent requests.  Latency is measured from each request's arrival
-    (so it includes waiting behind the client's previous request)."""
+def serve_sweep(fem, srv, ids, meshes, states, outs, rates, seconds, rng):
+    """Poisson request streams at each aggregate rate; latency from each request's
+    arrival to its completion (waiting behind the client's previous request included)."""
     import threading
-
-    import torch
-    torch.cuda.set_device(0)
-    dev = torch.device("cuda", 0)
-    import fem_pkg
-    fem = fem_pkg.load()
-    specs = fem.batch_specs(count=args.clients, seed=fem.mesh.SEEDS["serve64"], max_dof=4e6)
-    meshes = [sp.build() for sp in specs]
-    srv = fem.Server(int(args.budget_gb * 1e9), precision=args.batch_precision, max_batch=args.max_batch)
-    ids, admitted = [], []
-    for i, m in enumerate(meshes):
-        try:
-            ids.append(srv.add_mesh(m))
-            admitted.append(i)
-        except fem.FemError as e:
-            if e.status != fem.FEM_ERR_BUDGET:
-                raise
-    meshes = [meshes[i] for i in admitted]
-    rng = np.random.default_rng(12345)
-    states = []
-    for m in meshes:
-        s0 = torch.from_numpy(np.ascontiguousarray(m.states)).pin_memory()
-        s1 = torch.from_numpy(np.ascontiguousarray(m.states * 1.01 + 1e-6)).pin_memory()
-        states.append((s0, s1))
-    outs = [torch.empty(m.num_nodes * 2, dtype=torch.float64).pin_memory() for m in meshes]
-    for i in range(len(meshes)):  # warm-up: one request per client
-        srv.wait(srv.submit(ids[i], states[i][0], outs[i]))
     sweep = []
-    for rate in args.rates:
-        n_req = max(50, int(rate * args.serve_seconds))
+    for rate in rates:
+        n_req = max(50, int(rate * seconds))
         arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n_req))
         who = rng.integers(0, len(meshes), size=n_req)
         per_client = [[] for _ in meshes]
@@ -615,11 +695,39 @@ def run_serve(args):
                       "server_p50_ms": float(np.percentile(np.array(srv_lat) * 1e3, 50)),
                       "server_p99_ms": float(np.percentile(np.array(srv_lat) * 1e3, 99)),
                       "waves": st1["waves"] - st0["waves"], "wall_s": wall})
-    used = srv.stats()["used_bytes"]
-    srv.close()
-    # plain single-mesh FP64 drop-in for a sample of the same requests: H2D state,
-    # zero the outputs, fem_run_jacobian, D2H residual, one request at a time
-    sample = rng.integers(0, len(meshes), size=min(64, len(meshes)))
+    return sweep
+
+
+def serve_setup(fem, clients, budget_gb, precision, max_batch):
+    import torch
+    specs = fem.batch_specs(count=clients, seed=fem.mesh.SEEDS["serve64"], max_dof=4e6)
+    meshes = [sp.build() for sp in specs]
+    srv = fem.Server(int(budget_gb * 1e9), precision=precision, max_batch=max_batch)
+    ids, admitted = [], []
+    for i, m in enumerate(meshes):
+        try:
+            ids.append(srv.add_mesh(m))
+            admitted.append(i)
+        except fem.FemError as e:
+            if e.status != fem.FEM_ERR_BUDGET:
+                raise
+    meshes = [meshes[i] for i in admitted]
+    states = []
+    for m in meshes:
+        s0 = torch.from_numpy(np.ascontiguousarray(m.states)).pin_memory()
+        s1 = torch.from_numpy(np.ascontiguousarray(m.states * 1.01 + 1e-6)).pin_memory()
+        states.append((s0, s1))
+    outs = [torch.empty(m.num_nodes * 2, dtype=torch.float64).pin_memory() for m in meshes]
+    for i in range(len(meshes)):  # warm-up: one request per client
+        srv.wait(srv.submit(ids[i], states[i][0], outs[i]))
+    return srv, ids, meshes, states, outs
+
+
+def serve_plain(fem, dev, meshes, states, outs, rng, count):
+    """Plain single-mesh FP64 drop-in for a sample of requests: H2D state, zero the
+    outputs, fem_run_jacobian, D2H residual, one request at a time."""
+    import torch
+    sample = rng.integers(0, len(meshes), size=min(count, len(meshes)))
     stream = torch.cuda.Stream(device=dev)
     plain_el, plain_t = 0, 0.0
     for c in sorted(set(sample.tolist())):
@@ -627,18 +735,18 @@ def run_serve(args):
         rowp, cols = fem.build_bsr_pattern(m.num_nodes, m.conn_ptr, m.conn)
         mp = fem.build_element_bsr_map(m.conn_ptr, m.conn, m.nodes_per_element, rowp, cols)
         with torch.cuda.stream(stream):
-            d = fem.DeviceMesh(m, dev)
+            dm = fem.DeviceMesh(m, dev)
             dmap = torch.from_numpy(mp).to(dev)
             r = torch.empty(m.num_nodes * 2, dtype=torch.float64, device=dev)
             a = torch.empty(cols.size * 4, dtype=torch.float64, device=dev)
         reps = int((sample == c).sum())
 
         def one():
-            d.states.copy_(states[c][0], non_blocking=True)
+            dm.states.copy_(states[c][0], non_blocking=True)
             r.zero_()
             a.zero_()
-            fem.run_jacobian_kernel(m.order, d.conn_ptr, d.conn, m.num_elements, d.states, d.coords, m.E, m.nu, m.t,
-                                    dmap, r, a, stream=stream.cuda_stream, timed=False)
+            fem.run_jacobian_kernel(m.order, dm.conn_ptr, dm.conn, m.num_elements, dm.states, dm.coords, m.E, m.nu,
+                                    m.t, dmap, r, a, stream=stream.cuda_stream, timed=False)
             outs[c].copy_(r, non_blocking=True)
 
         with torch.cuda.stream(stream):
@@ -652,8 +760,78 @@ def run_serve(args):
             e1.synchronize()
         plain_t += e0.elapsed_time(e1) * 1e-3
         plain_el += reps * m.num_elements
-        del d, dmap, r, a
+        del dm, dmap, r, a
         torch.cuda.empty_cache()
+    return plain_el / plain_t, int(len(sample))
+
+
+def serve_leg(fem, dev, args):
+    """The serving configuration in the default run: the 64 Newton clients at one
+    sub-saturation rate and at a saturating rate, FP64 and MIXED."""
+    t0 = time.perf_counter()
+    rng = np.random.default_rng(12345)
+    out = {"workload": (f"{args.clients} Newton clients (meshes drawn like the batched set, <= 4M DOF each), "
+                        f"Poisson arrivals, state H2D and residual D2H inside every request"),
+           "rates_req_s": args.leg_rates, "seconds_per_rate": args.leg_serve_seconds}
+    for prec in ("fp64", "mixed"):
+        srv, ids, meshes, states, outs = serve_setup(fem, args.clients, args.budget_gb, prec, args.max_batch)
+        sweep = serve_sweep(fem, srv, ids, meshes, states, outs, args.leg_rates, args.leg_serve_seconds, rng)
+        out[prec] = {"clients_admitted": len(meshes), "device_bytes_used": srv.stats()["used_bytes"], "sweep": sweep}
+        srv.close()
+        if prec == "fp64":
+            plain, n = serve_plain(fem, dev, meshes, states, outs, rng, 64)
+            out["plain_fp64_dropin_per_request"] = {"elements_per_s": plain, "requests": n}
+        del srv, meshes, states, outs
+    log(f"served leg {time.perf_counter() - t0:.1f} s")
+    return out
+
+
+def run_batch(args):
+    """Many meshes (log-uniform sizes 1e3..1e6 elements, orders 1..4) per graph launch,
+    in waves that fit the device-memory budget, against the single-mesh FP64 drop-in."""
+    import torch
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    import fem_pkg
+    fem = fem_pkg.load()
+    specs = fem.batch_specs(count=args.batch_meshes)
+    waves = waves_of(specs, args.budget_gb * 1e9)
+    prec = args.batch_precision
+    r = batched_measure(fem, dev, waves, args.steps, args.warmup, (prec,))
+    el = r["elements"]
+    line = {
+        "metric": "assembled elements/s (res+Jac)", "value": el / (r["ms"][prec] * 1e-3), "unit": "elements/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms"][prec],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if prec == "fp64" else "bf16x6 (p3) / f32 (p4) / f64", "data": "synthetic",
+        "config": {"workload": f"batch{len(specs)}: element counts log-uniform in [1e3, 1e6], orders 1..4",
+                   "meshes": len(specs), "elements": el, "waves": len(waves), "budget_gb": args.budget_gb,
+                   "precision": prec, "l2": "per-wave inputs and outputs larger than L2"},
+        "plain_fp64_single_mesh": {"elements_per_s": el / (r["ms_plain"] * 1e-3), "ms_per_step": r["ms_plain"]},
+        "batched_over_plain": r["ms_plain"] / r["ms"][prec],
+        "wave_graph_ms": r["wave_ms"][prec], "tuned_tile_batches": r["tiles"][prec],
+        "mixed_rel_frobenius_err_max": max(r["errs"]) if r["errs"] else None,
+        "gpu_launches": r["launches"][prec],
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_serve(args):
+    """64 Newton-solve clients with device-resident meshes issue requests as one
+    Poisson stream at each swept aggregate rate; the server admits meshes under the
+    HBM budget and batches concurrent requests."""
+    import torch
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    import fem_pkg
+    fem = fem_pkg.load()
+    rng = np.random.default_rng(12345)
+    srv, ids, meshes, states, outs = serve_setup(fem, args.clients, args.budget_gb, args.batch_precision,
+                                                 args.max_batch)
+    sweep = serve_sweep(fem, srv, ids, meshes, states, outs, args.rates, args.serve_seconds, rng)
+    used = srv.stats()["used_bytes"]
+    srv.close()
+    plain, n = serve_plain(fem, dev, meshes, states, outs, rng, 64)
     best = max(sweep, key=lambda x: x["elements_per_s"])
     line = {
         "metric": "assembled elements/s (res+Jac); serve p50/p99 ms", "value": best["elements_per_s"],
@@ -664,47 +842,29 @@ def run_serve(args):
                    "clients_admitted": len(meshes), "budget_gb": args.budget_gb, "device_bytes_used": used,
                    "max_batch": args.max_batch, "precision": args.batch_precision},
         "sweep": sweep,
-        "plain_fp64_single_mesh": {"elements_per_s": plain_el / plain_t, "requests": int(len(sample))},
+        "plain_fp64_single_mesh": {"elements_per_s": plain, "requests": n},
     }
     print(json.dumps(line), flush=True)
 
 
-def cpu_baseline(fem, mesh, args):
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import oracle as orc
-    sample = min(mesh.num_elements, args.ref_elements)
-    sub = fem.submesh(mesh, 0, sample)
-    rowp, cols = fem.build_bsr_pattern(sub.num_nodes, sub.conn_ptr, sub.conn)
-    mp = fem.build_element_bsr_map(sub.conn_ptr, sub.conn, sub.nodes_per_element, rowp, cols)
-    threads = os.cpu_count() or 1
-    orc.set_threads(threads)
-    orc.assemble(sub, mp, cols.size, parallel=True)
-    t0 = time.perf_counter()
-    reps = 0
-    while True:
-        orc.assemble(sub, mp, cols.size, parallel=True)
-        reps += 1
-        if time.perf_counter() - t0 > args.cpu_seconds:
-            break
-    dt = (time.perf_counter() - t0) / reps
-    return {"value": sample / dt, "unit": "elements/s", "cores": threads, "kind": "port",
-            "sample": f"first {sample} elements of {mesh.name}, {reps} repeats (OpenMP, atomic scatter)"}
-
-
 def measure_peaks():
-    """Arithmetic peaks of this GPU from the library's probe kernels (TFLOP/s)."""
+    """Arithmetic peaks of this GPU from the probe library (TFLOP/s)."""
     import ctypes as C
 
     import torch
 
     import fem_pkg
-    fem = fem_pkg.load()
+    fem_pkg.load_builder().build()
+    probe = C.CDLL(str(ROOT / "gpu-fem-project_b200" / "libfemprobe.so"))
+    probe.fem_probe_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
     torch.cuda.init()
     out = {}
     for kind, name in ((0, "fp64_fma_tflops"), (1, "fp32_fma_tflops"), (2, "fp64_mma_tflops"),
                        (3, "bf16_mma_sync_tflops")):
         v = C.c_double()
-        fem.check(fem.lib.fem_probe_peak(kind, C.byref(v)), "fem_probe_peak")
+        rc = probe.fem_probe_peak(kind, C.byref(v))
+        if rc != 0:
+            raise RuntimeError(f"fem_probe_peak({kind}) returned {rc}")
         out[name] = v.value
     out["gpu"] = torch.cuda.get_device_name(0)
     return out
@@ -717,22 +877,25 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="square1024_p3", choices=sorted(WORKLOADS) + ["batch256", "serve64"])
+    ap.add_argument("--min-seconds", type=float, default=1.0, help="timed region of each comparison path")
     ap.add_argument("--clients", type=int, default=64)
     ap.add_argument("--rates", type=lambda v: [float(x) for x in v.split(",")], default=[100, 500, 1000, 2500, 5000])
     ap.add_argument("--serve-seconds", type=float, default=3.0)
     ap.add_argument("--max-batch", type=int, default=64)
     ap.add_argument("--batch-meshes", type=int, default=256)
-    ap.add_argument("--budget-gb", type=float, default=100.0, help="device bytes per batched wave")
+    ap.add_argument("--budget-gb", type=float, default=100.0, help="device bytes per batched wave / server budget")
     ap.add_argument("--batch-precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-legs", action="store_true", help="skip the batched and served legs of the default run")
+    ap.add_argument("--leg-batch-gb", type=float, default=40.0, help="device bytes of the batched leg's meshes")
+    ap.add_argument("--leg-steps", type=int, default=10)
+    ap.add_argument("--leg-rates", type=lambda v: [float(x) for x in v.split(",")], default=[1000, 5000])
+    ap.add_argument("--leg-serve-seconds", type=float, default=2.0)
     ap.add_argument("--ref-elements", type=int, default=131072)
     ap.add_argument("--bands", type=int, default=32, help="element bands / node chunks of the end-to-end call")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
-    ap.add_argument("--paths", default="plan_fp64,plan_mixed,dropin_fp64,plan_nonlinear",
-                    help="comma list of plan_fp64, plan_mixed, dropin_fp64, dropin_mixed, plan_nonlinear")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--peaks", action="store_true", help="print measured FP64/FP32/FP64-MMA/BF16-MMA peaks and exit")
     args = ap.parse_args()
-    args.paths = set(args.paths.split(","))
     if args.peaks:
         print(json.dumps(measure_peaks()))
         return

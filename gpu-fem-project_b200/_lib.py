@@ -60,7 +60,6 @@ SIGNATURES = {
     "fem_plan_row_chunks": (_i, [_p, _pi]),
     "fem_plan_assemble_ex": (_i, [_p, _p, _p, _d, _d, _d, _p, _p, _i, _i, _p, _pd]),
     "fem_plan_assemble_host": (_i, [_p, _p, _p, _p, _d, _d, _d, _p, _p, _p, _i, _i, _i, _p, _pd]),
-    "fem_probe_peak": (_i, [_i, _pd]),
     "fem_server_create": (_i, [_i64, _i, _i, C.POINTER(_p)]),
     "fem_server_destroy": (_i, [_p]),
     "fem_server_add_mesh": (_i, [_p, _i, _i, _p, _p, _i, _p, _d, _d, _d, _pi]),

@@ -18,7 +18,9 @@ INCLUDE = ROOT / "include"
 LIB = PKG / "libfemb200.so"
 
 SOURCES = ["fem_kernels.cu", "fem_nonlinear.cu", "fem_rows.cu", "fem_batch.cu", "fem_server.cu", "fem_static.cu",
-           "fem_frag.cu", "fem_host.cpp", "fem_probe.cu"]
+           "fem_frag.cu", "fem_host.cpp"]
+PROBE_SOURCES = ["fem_probe.cu"]  # libfemprobe.so: arithmetic-peak calibration, not part of the assembly ABI
+PROBE_LIB = PKG / "libfemprobe.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -35,10 +37,16 @@ def _stale(target: pathlib.Path, deps) -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> pathlib.Path:
-    srcs = [CSRC / s for s in SOURCES if (CSRC / s).exists()]
+    _build_lib(LIB, SOURCES, force, verbose)
+    _build_lib(PROBE_LIB, PROBE_SOURCES, force, verbose)
+    return LIB
+
+
+def _build_lib(lib: pathlib.Path, sources, force: bool, verbose: bool) -> None:
+    srcs = [CSRC / s for s in sources if (CSRC / s).exists()]
     deps = srcs + list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
-    if not force and not _stale(LIB, deps):
-        return LIB
+    if not force and not _stale(lib, deps):
+        return
     obj_dir = PKG / "_build"
     obj_dir.mkdir(exist_ok=True)
     common = [f"-I{INCLUDE}", f"-I{CSRC}", "-O3", "-std=c++17"]
@@ -55,8 +63,7 @@ def build(force: bool = False, verbose: bool = False) -> pathlib.Path:
         objs.append(str(obj))
     with concurrent.futures.ThreadPoolExecutor(max_workers=len(cmds)) as ex:
         list(ex.map(_run, cmds))
-    _run([_nvcc(), *ARCH, "-shared", "-Xcompiler", "-fopenmp", "-o", str(LIB), *objs, "-lgomp"])
-    return LIB
+    _run([_nvcc(), *ARCH, "-shared", "-Xcompiler", "-fopenmp", "-o", str(lib), *objs, "-lgomp"])
 
 
 def _run(cmd):

@@ -1,11 +1,13 @@
-// Arithmetic-peak probes used as roofline denominators for the element kernels:
-// dependent-chain-free FMA streams on the FP64 and FP32 pipes, the FP64
-// tensor-core MMA (m8n8k4) of the FP64 stiffness stage and the BF16 MMA
-// (m16n8k16, FP32 accumulate) of the BF16x6 stiffness stage.  Each thread runs
-// 8 independent accumulator chains; the result is written so nothing is elided.
+// Arithmetic-peak probes (libfemprobe.so, include/fem_probe.h): calibration for
+// the benchmark's roofline notes, built as a library of its own so that it is not
+// part of the assembly library's interface.  Dependent-chain-free FMA streams on
+// the FP64 and FP32 pipes, the FP64 tensor-core MMA (m8n8k4) of the FP64 stiffness
+// stage and the BF16 MMA (m16n8k16, FP32 accumulate) of the BF16x6 stiffness
+// stage.  Each thread runs 8 independent accumulator chains; the result is written
+// so nothing is elided.
 #include <cuda_runtime.h>
 
-#include "fem_common.h"
+#include "fem_probe.h"
 
 namespace fem {
 namespace dev {
@@ -70,15 +72,14 @@ extern "C" {
 // kind 0: FP64 FMA, 1: FP32 FMA, 2: FP64 MMA m8n8k4, 3: BF16 MMA m16n8k16 (FP32
 // accumulate).  Returns TFLOP/s (2 flops per FMA).
 int fem_probe_peak(int kind, double *tflops) {
-  fem::clear_error();
-  if (!tflops || kind < 0 || kind > 3) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "bad probe arguments");
+  if (!tflops || kind < 0 || kind > 3) return -1;
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int grid = sms * 8, block = 256, iters = 4096;
   void *buf = nullptr;
   cudaError_t err = cudaMalloc(&buf, sizeof(double) * grid * block);
-  if (err != cudaSuccess) return fem::fail(FEM_ERR_CUDA, "cudaMalloc: %s", cudaGetErrorString(err));
+  if (err != cudaSuccess) return (int)err;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -103,7 +104,7 @@ int fem_probe_peak(int kind, double *tflops) {
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   cudaFree(buf);
-  if (err != cudaSuccess) return fem::fail(FEM_ERR_CUDA, "probe: %s", cudaGetErrorString(err));
+  if (err != cudaSuccess) return (int)err;
   const double threads = double(grid) * block;
   double flops;
   if (kind == 2)
@@ -113,7 +114,7 @@ int fem_probe_peak(int kind, double *tflops) {
   else
     flops = threads * iters * 8 * 2.0;
   *tflops = flops / (best * 1e-3) / 1e12;
-  return FEM_SUCCESS;
+  return 0;
 }
 
 }  // extern "C"

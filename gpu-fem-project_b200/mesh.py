@@ -232,3 +232,34 @@ def submesh(mesh: Mesh, e0: int, e1: int) -> Mesh:
     return Mesh(mesh.order, np.ascontiguousarray(mesh.coords[nodes]), new_ptr, inv.astype(np.int32),
                 np.ascontiguousarray(mesh.states[nodes]), mesh.E, mesh.nu, mesh.t, f"{mesh.name}[{e0}:{e1}]",
                 mesh.seed)
+
+
+def submesh_elements(mesh: Mesh, elements) -> Mesh:
+    """The listed elements of `mesh` (ascending ids) with their nodes renumbered
+    compactly in ascending original id, so that sorted node lists keep their order."""
+    el = np.unique(np.asarray(elements, dtype=np.int64))
+    n = mesh.nodes_per_element
+    cp = mesh.conn_ptr.astype(np.int64)
+    conn = np.concatenate([mesh.conn[cp[e]:cp[e] + n] for e in el]) if el.size else np.zeros(0, np.int32)
+    nodes, inv = np.unique(conn, return_inverse=True)
+    ptr = (np.arange(el.size + 1, dtype=np.int64) * n).astype(np.int32)
+    sub = Mesh(mesh.order, np.ascontiguousarray(mesh.coords[nodes]), ptr, inv.astype(np.int32),
+               np.ascontiguousarray(mesh.states[nodes]), mesh.E, mesh.nu, mesh.t, f"{mesh.name}[patch]", mesh.seed)
+    sub.global_nodes = nodes
+    return sub
+
+
+def row_complete_patch(mesh: Mesh, core_elements):
+    """Node rows that a small submesh assembles completely: S = every node of the
+    core elements, and the patch = every element that touches a node of S.  Each
+    node of S has all its elements in the patch, so the patch's assembled residual
+    and matrix rows of S equal the full mesh's.  Returns (patch, S as global ids,
+    S as patch-local ids); the mesh must list each element's nodes contiguously
+    with a fixed count (structured meshes)."""
+    n = mesh.nodes_per_element
+    conn = mesh.conn.reshape(-1, n)
+    S = np.unique(conn[np.asarray(core_elements, dtype=np.int64)])
+    touching = np.nonzero(np.isin(conn, S).any(axis=1))[0]
+    patch = submesh_elements(mesh, touching)
+    local = np.searchsorted(patch.global_nodes, S)
+    return patch, S, local

@@ -287,14 +287,6 @@ typedef struct {
  * (No counterpart in the reference: it assembles one mesh per call.) */
 int fem_run_jacobian_batched_static(int numMeshes, const fem_dropin_mesh *meshes, void *stream);
 
-/* ---- calibration ---------------------------------------------------------------------- */
-/* Measured arithmetic peak of the current device in TFLOP/s, used as the
- * roofline denominator of the element arithmetic: kind 0 = FP64 FMA pipe,
- * 1 = FP32 FMA pipe, 2 = FP64 tensor-core MMA (m8n8k4), 3 = BF16 tensor-core
- * MMA (m16n8k16, FP32 accumulate).  Allocates a scratch buffer and synchronises
- * the device.  (No reference counterpart.) */
-int fem_probe_peak(int kind, double *tflops);
-
 #ifdef __cplusplus
 }
 #endif

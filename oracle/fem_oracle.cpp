@@ -235,6 +235,13 @@ struct QuadPoint {
   double xi[2];
 };
 
+// Extended-precision mode (oracle_set_extended_j): J = sum_a x_a (x) dN_a is
+// accumulated in long double (64-bit significand) and rounded to double once.  On
+// large, finely divided meshes the FP64 sum cancels by ~h/|x| (the terms are ~|x|,
+// J ~ h), so the plain sum carries an error of ~ulp(|x|)/|J| relative; the
+// extended sum is the same formula on the same FP64 inputs, evaluated to ~1e-16.
+bool g_extended_j = false;
+
 // One quadrature point: J (interpParamGradient), MatInv/MatDet (FEKernels.h:352-359).
 inline QuadPoint quadPoint(int p, int qx, int qy, const double *X) {
   QuadPoint Q;
@@ -242,15 +249,23 @@ inline QuadPoint quadPoint(int p, int qx, int qy, const double *X) {
   Q.xi[1] = kGaussX[p][qy];
   const double w = kGaussW[p][qx] * kGaussW[p][qy];
   double J[4] = {0, 0, 0, 0};
+  long double JL[4] = {0, 0, 0, 0};
   for (int ay = 0; ay <= p; ay++) {
     for (int ax = 0; ax <= p; ax++) {
       const int a = ay * (p + 1) + ax;
       double d[2];
       lagrange2dDeriv(p, Q.xi, ax, ay, d);
       for (int i = 0; i < 2; i++)
-        for (int j = 0; j < 2; j++) J[i * 2 + j] += X[a * 2 + i] * d[j];
+        for (int j = 0; j < 2; j++) {
+          if (g_extended_j)
+            JL[i * 2 + j] += (long double)X[a * 2 + i] * (long double)d[j];
+          else
+            J[i * 2 + j] += X[a * 2 + i] * d[j];
+        }
     }
   }
+  if (g_extended_j)
+    for (int i = 0; i < 4; i++) J[i] = (double)JL[i];
   Q.detJ = J[0] * J[3] - J[1] * J[2];
   const double inv = 1.0 / Q.detJ;
   Q.Jinv[0] = J[3] * inv;
@@ -352,6 +367,10 @@ void elementKernel(int p, const double *X, const double *U, const Material &m, d
 extern "C" {
 
 int oracle_version() { return 1; }
+
+// 1: accumulate the isoparametric Jacobian in long double (see g_extended_j);
+// 0: the reference's plain FP64 sum (default).
+void oracle_set_extended_j(int on) { g_extended_j = on != 0; }
 
 int oracle_num_threads() {
 #ifdef _OPENMP

@@ -45,6 +45,7 @@ def _load():
     lib.oracle_check_colouring.restype = i64
     lib.oracle_bsr_spmv.argtypes = [i, p, p, p, p, p]
     lib.oracle_set_num_threads.argtypes = [i]
+    lib.oracle_set_extended_j.argtypes = [i]
     return lib
 
 
@@ -68,6 +69,12 @@ def _c(a, dt):
 
 def set_threads(n: int) -> None:
     lib().oracle_set_num_threads(int(n))
+
+
+def set_extended_j(on: bool) -> None:
+    """Accumulate the isoparametric Jacobian in long double (True) or with the
+    reference's plain FP64 sum (False, the default)."""
+    lib().oracle_set_extended_j(1 if on else 0)
 
 
 def num_threads() -> int:

@@ -2,13 +2,21 @@
 // dispatchers runResidualKernel / runJacobianKernel, :1030-1225), compiled from
 // the header where it lies in the reference checkout with the A2D interface
 // restated in oracle/a2d_shim/ (A2D is not part of the checkout).  Built by
-// oracle/Makefile (target `ref`) into oracle/_ref/libfemref.so, without OpenMP:
-// the reference's CPU matrix scatter has no atomic (FEKernels.h:95-99), so it is
-// run serially, which makes it deterministic.
+// oracle/Makefile (target `ref`) twice:
+//   * oracle/_ref/libfemref.so without OpenMP: the reference's CPU matrix scatter
+//     has no atomic (FEKernels.h:95-99), so serial execution is what makes it
+//     deterministic; the tests and the golden vectors use this one;
+//   * oracle/_ref/libfemref_omp.so with OpenMP, the reference's parallel loops as
+//     written (their unsynchronised matrix scatter included), timed as the CPU
+//     baseline of bench.py and never used as a checker.
 //
 // TEST INFRASTRUCTURE ONLY: tests/ compare the oracle restatement (and, through
 // the committed fixtures of tests/golden/, the CUDA library) with it.
 #include "FEKernels.h"
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 namespace {
 template <int order>
@@ -26,6 +34,15 @@ void res_nl(const int *connPtr, const int *conn, int nE, const double *states, c
 }  // namespace
 
 extern "C" {
+
+// Threads of the OpenMP build's parallel loops (no effect in the serial build).
+void ref_set_num_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+#else
+  (void)n;
+#endif
+}
 
 // runResidualKernel (FEKernels.h:1030-1102), host build.  Accumulates into residual.
 double ref_run_residual(int order, const int *connPtr, const int *conn, int nE, const double *states,

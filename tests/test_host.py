@@ -24,6 +24,18 @@ def test_library_exports_every_declared_symbol(fem):
     assert fem.lib.fem_version() >= 100
 
 
+def test_probe_library_exports_its_symbols(fem):
+    """The arithmetic-peak probes live in libfemprobe.so (include/fem_probe.h),
+    outside the assembly library's interface."""
+    import ctypes as C
+    txt = re.sub(r"/\*.*?\*/", "", (HEADER.parent / "fem_probe.h").read_text(), flags=re.S)
+    names = sorted(set(re.findall(r"\b(fem_[a-z0-9_]+)\s*\(", txt)))
+    assert names == ["fem_probe_peak"]
+    probe = C.CDLL(str(pathlib.Path(fem.lib._name).parent / "libfemprobe.so"))
+    assert all(getattr(probe, n, None) is not None for n in names)
+    assert getattr(fem.lib, "fem_probe_peak", None) is None
+
+
 def test_python_mirror_binds_every_declared_symbol(fem):
     """The ctypes table of the host mirror covers the whole C ABI (argument types
     set for every entry point the header declares)."""
