@@ -21,6 +21,7 @@ FEM_ERR_OVERFLOW = 5
 FEM_ERR_NOT_FOUND = 6
 FEM_ERR_UNSUPPORTED = 7
 FEM_ERR_BUDGET = 8
+FEM_ERR_TIMEOUT = 9
 
 FEM_PRECISION_FP64 = 0
 FEM_PRECISION_MIXED = 1
@@ -60,6 +61,11 @@ SIGNATURES = {
     "fem_plan_row_chunks": (_i, [_p, _pi]),
     "fem_plan_assemble_ex": (_i, [_p, _p, _p, _d, _d, _d, _p, _p, _i, _i, _p, _pd]),
     "fem_plan_assemble_host": (_i, [_p, _p, _p, _p, _d, _d, _d, _p, _p, _p, _i, _i, _i, _p, _pd]),
+    "fem_plan_set_schedule": (_i, [_p, _i, _i]),
+    "fem_plan_get_schedule": (_i, [_p, _pi, _pi, _pi, _pi]),
+    "fem_plan_schedule_status": (_i, [_p, _p, _pi64]),
+    "fem_plan_get_schedule_tables": (_i, [_p, _p, _p, _p, _p, _p, _p]),
+    "fem_plan_set_schedule_waits": (_i, [_p, _i64, _i]),
     "fem_server_create": (_i, [_i64, _i, _i, C.POINTER(_p)]),
     "fem_server_destroy": (_i, [_p]),
     "fem_server_add_mesh": (_i, [_p, _i, _i, _p, _p, _i, _p, _d, _d, _d, _pi]),

@@ -165,9 +165,60 @@ class Plan:
         check(lib.fem_plan_row_chunks(self._h, C.byref(rc)), "fem_plan_row_chunks")
         self.row_chunks = rc.value
 
-    def launches(self, strain="linear") -> int:
-        """Kernel launches of one assemble(): 1 for order-1 row assembly, else one per colour."""
-        return 1 if self.row_chunks > 0 and _strain(strain) == FEM_STRAIN_LINEAR else self.num_colours
+    def launches(self, strain="linear", precision="fp64") -> int:
+        """Kernel launches of one assemble(): 1 for order-1 row assembly and for a
+        dependency-ordered plan, else one per colour."""
+        if self.row_chunks > 0 and _strain(strain) == FEM_STRAIN_LINEAR:
+            return 1
+        return 1 if self.scheduled(strain, precision) else self.num_colours
+
+    def scheduled(self, strain="linear", precision="fp64") -> bool:
+        """Whether assemble() runs all colours in one dependency-ordered launch: the
+        plan has a schedule and the assembly runs the fragment kernel (orders 2-3,
+        and order 4 in FP64 LINEAR)."""
+        if self.schedule()["groups"] == 0:
+            return False
+        nl, fp64 = _strain(strain) != FEM_STRAIN_LINEAR, _prec(precision) == FEM_PRECISION_FP64
+        if nl:
+            return fp64 and self.order in (2, 3)
+        return self.order in (2, 3) or (self.order == 4 and fp64)
+
+    def schedule(self):
+        """The dependency-ordered schedule: band and tile lengths (elements), groups, tiles."""
+        b, t, g, n = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        check(lib.fem_plan_get_schedule(self._h, C.byref(b), C.byref(t), C.byref(g), C.byref(n)),
+              "fem_plan_get_schedule")
+        return {"band": b.value, "tile": t.value, "groups": g.value, "tiles": n.value}
+
+    def schedule_tables(self):
+        """Host copies of the schedule: tile (begin, count, group) arrays, tiles per
+        group and the dependency CSR (dep_ptr, deps)."""
+        info = self.schedule()
+        T, G = info["tiles"], info["groups"]
+        begin, count, group = np.zeros(T, np.int64), np.zeros(T, np.int32), np.zeros(T, np.int32)
+        gt, ptr = np.zeros(G, np.int32), np.zeros(G + 1, np.int32)
+        check(lib.fem_plan_get_schedule_tables(self._h, begin.ctypes.data, count.ctypes.data, group.ctypes.data,
+                                               gt.ctypes.data, ptr.ctypes.data, None), "fem_plan_get_schedule_tables")
+        deps = np.zeros(max(int(ptr[-1]), 1), np.int32)
+        check(lib.fem_plan_get_schedule_tables(self._h, None, None, None, None, None, deps.ctypes.data),
+              "fem_plan_get_schedule_tables")
+        return {"tile_begin": begin, "tile_count": count, "tile_group": group, "group_tiles": gt, "dep_ptr": ptr,
+                "deps": deps[:int(ptr[-1])]}
+
+    def set_schedule(self, band, tile=0):
+        """band = 0: colour launches; tile = 0: the default tile length."""
+        check(lib.fem_plan_set_schedule(self._h, int(band), int(tile)), "fem_plan_set_schedule")
+
+    def schedule_status(self, stream=None) -> int:
+        """Waits for the stream; in-kernel waits that ran out since the last call."""
+        n = C.c_int64()
+        check(lib.fem_plan_schedule_status(self._h, _stream(stream), C.byref(n)), "fem_plan_schedule_status")
+        return n.value
+
+    def set_schedule_waits(self, wait_limit_ns=0, stall_group=-1):
+        """Failure injection for tests: the wait limit and a group no wait sees finished."""
+        check(lib.fem_plan_set_schedule_waits(self._h, int(wait_limit_ns), int(stall_group)),
+              "fem_plan_set_schedule_waits")
 
     @property
     def handle(self) -> int:

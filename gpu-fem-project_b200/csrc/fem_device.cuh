@@ -487,6 +487,28 @@ struct RangeList {
   int64_t begin[kMaxRanges], count[kMaxRanges];
 };
 
+// Dependency-ordered assembly of one plan in one persistent launch: the list
+// positions are cut into groups (the elements of one colour inside one band of
+// element ids) and the groups into tiles, listed in dispatch order.  A tile's
+// group may write once every group of its dependency list has finished all its
+// tiles; the dependencies keep each block's contributions in colour order, so the
+// result equals the colour-by-colour launches bit for bit.
+struct SchedTile {
+  int64_t begin;  // first list position
+  int count;      // list positions (even except at the end of a group)
+  int group;
+};
+struct SchedArgs {
+  const SchedTile *tiles;
+  const int *groupTiles;  // tiles per group
+  const int *depPtr;      // CSR over groups: the groups each group waits for
+  const int *deps;
+  int *status;            // [0] waits that ran out (sticky), [1] tile dispenser, [2 + g] finished tiles of group g
+  int ntiles;
+  int stallGroup;         // failure injection for tests: no wait ever sees this group finished (-1: none)
+  long long waitLimitNs;  // a wait gives up after this long, counts itself in status[0] and lets the tile proceed
+};
+
 // Work source of the batched kernel: groups pull tiles from a per-launch queue
 // (one atomic counter per launch) and walk their batches.
 struct QueueSource {

@@ -380,11 +380,13 @@ struct PairCursor {
   int mesh;
   int ne;  // 0 ends the warp's loop
   int64_t k0;
+  int tile = -1;      // dependency-ordered launches: the pair's tile
+  bool last = false;  // ... and whether it is the tile's last pair
 };
 
 // Single mesh: pairs p, p + stride, ... of list positions [begin, end).
 struct PairStride {
-  static constexpr bool kBatched = false;
+  static constexpr bool kBatched = false, kSched = false;
   int64_t begin, end, p, stride;
   __device__ PairCursor next(int) {
     PairCursor c{0, 0, begin + 2 * p};
@@ -398,7 +400,7 @@ struct PairStride {
 // launches of fem_plan_assemble_host that share a schedule step): pairs p, p +
 // stride, ... of their concatenation; a pair never straddles two ranges.
 struct PairRanges {
-  static constexpr bool kBatched = false;
+  static constexpr bool kBatched = false, kSched = false;
   RangeList r;
   int64_t p, stride;
   __device__ PairCursor next(int) {
@@ -422,7 +424,7 @@ struct PairRanges {
 // (one atomic counter per launch; tiles hold even element counts except at the
 // end of a colour range, so pairs never straddle tiles).
 struct PairQueue {
-  static constexpr bool kBatched = true;
+  static constexpr bool kBatched = true, kSched = false;
   const Tile *tiles;
   int ntiles;
   int *counter;
@@ -450,6 +452,97 @@ struct PairQueue {
     c.ne = (int)min((int64_t)2, tend - pos);
     pos += 2;
     return c;
+  }
+};
+
+__device__ __forceinline__ int ld_acquire_gpu(const int *p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Waits (one lane) until group g of the schedule has finished all its tiles.  The
+// wait is bounded: after S.waitLimitNs (or 2^22 polls, should the timer stall) it
+// counts itself in status[0] and returns, and once any wait has run out no later
+// wait starts, so a launch whose dependencies can never be met still ends within
+// about one limit.  The tile then writes regardless; the host reports the count.
+__device__ __noinline__ void sched_wait(const SchedArgs *S, int g) {
+  const int target = S->groupTiles[g] + (g == S->stallGroup ? 1 : 0);
+  const int *done = S->status + 2 + g;
+  if (ld_acquire_gpu(done) >= target) return;
+  const unsigned long long t0 = global_ns();
+  for (unsigned it = 0;; it++) {
+    __nanosleep(100);
+    if (ld_acquire_gpu(done) >= target) return;
+    if (ld_acquire_gpu(S->status) != 0) return;
+    if (global_ns() - t0 > (unsigned long long)S->waitLimitNs || it >= (1u << 22)) {
+      atomicAdd(S->status, 1);
+      return;
+    }
+  }
+}
+
+// One mesh, dependency-ordered: warps pull tiles in dispatch order from one counter
+// (status[1]).  Before the first write of a tile's pairs the warp waits for the
+// groups its tile's group depends on (acquire); after the last pair of a tile it
+// completes its writes -- the asynchronous bulk reductions included -- and counts
+// the tile in its group (release).  A warp holds at most the tiles it has pulled,
+// in dispatch order, and every dependency of a tile is an earlier group, so the
+// earliest unfinished tile can always proceed: no wait is circular, whether or not
+// every CTA of the grid is resident.
+struct PairSched {
+  static constexpr bool kBatched = false, kSched = true;
+  const SchedArgs *S;  // the kernel's __grid_constant__ parameter
+  int tile = -1, held = -1;
+  int64_t pos = 0, tend = 0;
+  bool done = false;
+  __device__ PairCursor next(int lane) {
+    PairCursor c{0, 0, 0};
+    while (!done && pos >= tend) {
+      int t = 0;
+      if (lane == 0) t = atomicAdd(S->status + 1, 1);
+      t = __shfl_sync(0xffffffffu, t, 0);
+      if (t >= S->ntiles) {
+        done = true;
+      } else {
+        const SchedTile tl = S->tiles[t];
+        tile = t;
+        pos = tl.begin;
+        tend = tl.begin + tl.count;
+      }
+    }
+    if (done) return c;
+    c.k0 = pos;
+    c.ne = (int)min((int64_t)2, tend - pos);
+    c.tile = tile;
+    pos += 2;
+    c.last = pos >= tend;
+    return c;
+  }
+  __device__ void acquire(const PairCursor &c, int lane) {
+    if (c.tile == held) return;
+    held = c.tile;
+    if (lane == 0) {
+      const int g = S->tiles[c.tile].group;
+      for (int i = S->depPtr[g]; i < S->depPtr[g + 1]; i++) sched_wait(S, S->deps[i]);
+      __threadfence();
+    }
+    __syncwarp();
+    // later bulk reductions (async proxy) are ordered after what the wait observed
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+  }
+  __device__ void release(const PairCursor &c, int lane) {
+    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+    __threadfence();
+    __syncwarp();
+    if (lane == 0) atomicAdd(S->status + 2 + S->tiles[c.tile].group, 1);
   }
 };
 
@@ -708,6 +801,7 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
     }
     __syncwarp();
 
+    if constexpr (Gen::kSched) gen.acquire(cur, lane);
     const Out O{M.mat, M.residual, stage + buf * 2 * STG, rb, reinterpret_cast<const int *>(stage + buf * 2 * STG)};
     if constexpr (!F::IL) {
       // node tiles on the tensor cores: both at p = 3; at p = 2 only tile 0 (nodes 0-7),
@@ -1247,6 +1341,9 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
         }
       }
     }
+    if constexpr (Gen::kSched) {
+      if (cur.last) gen.release(cur, lane);
+    }
     __syncwarp();
     cur = nxt;
     nxt = nn2;
@@ -1276,6 +1373,16 @@ __global__ void __launch_bounds__(32 * FragDims<P>::WARPS, FEM_FRAG_MINB)
   frag_prologue<P, (MODE & kB16) != 0>(smem);
   const int warp = threadIdx.x >> 5;
   PairRanges gen{R, (int64_t)blockIdx.x * FragDims<P>::WARPS + warp, (int64_t)gridDim.x * FragDims<P>::WARPS};
+  frag_loop<P, MODE>(smem, gen, A, &A);
+}
+
+// One mesh, all colours in one dependency-ordered persistent launch (plan mode).
+template <int P, int MODE>
+__global__ void __launch_bounds__(32 * FragDims<P>::WARPS, FEM_FRAG_MINB)
+    frag_sched_kernel(const __grid_constant__ AsmArgs A, const __grid_constant__ SchedArgs S) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  frag_prologue<P, (MODE & kB16) != 0>(smem);
+  PairSched gen{&S};
   frag_loop<P, MODE>(smem, gen, A, &A);
 }
 
@@ -1346,6 +1453,25 @@ int launch_frag_batched_p(const AsmArgs *meshes, const Tile *tiles, int ntiles, 
   kernel<<<grid, NT, smem, s>>>(meshes, tiles, ntiles, counter);
   cudaError_t err = cudaGetLastError();
   if (err != cudaSuccess) return cuda_fail(err, "frag_batched_kernel launch");
+  return FEM_SUCCESS;
+}
+
+template <int P, int MODE>
+int launch_frag_sched_p(const AsmArgs &a, const SchedArgs &sa, cudaStream_t s) {
+  using F = FragDims<P>;
+  constexpr int NT = 32 * F::WARPS;
+  auto kernel = frag_sched_kernel<P, MODE>;
+  const size_t smem = FragLayout<P, false, (MODE & kNL) != 0, (MODE & kB16) != 0>::total;
+  LaunchInfo li;
+  int st = launch_info(kernel, NT, smem, li);
+  if (st) return st;
+  const int64_t need = ((int64_t)sa.ntiles + F::WARPS - 1) / F::WARPS;
+  const int64_t cap = (int64_t)li.grid_per_sm * li.num_sms;
+  const int grid = (int)(need < cap ? need : cap);
+  if (grid <= 0) return FEM_SUCCESS;
+  kernel<<<grid, NT, smem, s>>>(a, sa);
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return cuda_fail(err, "frag_sched_kernel launch");
   return FEM_SUCCESS;
 }
 
@@ -1442,6 +1568,37 @@ int launch_frag_ranges(int order, int precision, int mode, const dev::AsmArgs &a
     case kNL | kPlan | kRes: return go(IC<kNL | kPlan | kRes>{});
     case kNL | kPlan | kRes | kJac: return go(IC<kNL | kPlan | kRes | kJac>{});
     default: return fail(FEM_ERR_INVALID_ARGUMENT, "fragment kernel, ranges: mode %d", mode);
+  }
+}
+
+int launch_frag_sched(int order, int precision, int mode, const dev::AsmArgs &a, const dev::SchedArgs &sa,
+                      cudaStream_t s, int strain) {
+  using namespace dev;
+  if (strain == FEM_STRAIN_NONLINEAR) mode |= kNL;
+  if (b16_stiffness(order, precision, strain) && (mode & kJac)) mode |= kB16;
+  auto go = [&](auto mc) -> int {
+    constexpr int M = decltype(mc)::value;
+    switch (order) {
+      case 2:
+        if constexpr ((M & kB16) != 0) return fail(FEM_ERR_INVALID_ORDER, "fragment kernel, BF16x6: order 2");
+        else return launch_frag_sched_p<2, M>(a, sa, s);
+      case 3: return launch_frag_sched_p<3, M>(a, sa, s);
+      case 4:
+        if constexpr ((M & (kNL | kB16)) != 0) return fail(FEM_ERR_INVALID_ORDER, "fragment kernel, mode %d: order 4", M);
+        else return launch_frag_sched_p<4, M>(a, sa, s);
+      default: return fail(FEM_ERR_INVALID_ORDER, "fragment kernel: order %d", order);
+    }
+  };
+  switch (mode) {
+    case kPlan | kRes: return go(IC<kPlan | kRes>{});
+    case kPlan | kJac: return go(IC<kPlan | kJac>{});
+    case kPlan | kRes | kJac: return go(IC<kPlan | kRes | kJac>{});
+    case kPlan | kJac | kB16: return go(IC<kPlan | kJac | kB16>{});
+    case kPlan | kRes | kJac | kB16: return go(IC<kPlan | kRes | kJac | kB16>{});
+    case kNL | kPlan | kRes: return go(IC<kNL | kPlan | kRes>{});
+    case kNL | kPlan | kJac: return go(IC<kNL | kPlan | kJac>{});
+    case kNL | kPlan | kRes | kJac: return go(IC<kNL | kPlan | kRes | kJac>{});
+    default: return fail(FEM_ERR_INVALID_ARGUMENT, "fragment kernel, schedule: mode %d", mode);
   }
 }
 

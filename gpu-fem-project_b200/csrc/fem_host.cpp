@@ -262,6 +262,7 @@ const char *fem_status_string(int status) {
     case FEM_ERR_NOT_FOUND: return "element block missing from BSR pattern";
     case FEM_ERR_UNSUPPORTED: return "unsupported input";
     case FEM_ERR_BUDGET: return "device memory budget exhausted";
+    case FEM_ERR_TIMEOUT: return "a bounded in-kernel wait ran out";
     default: return "unknown status";
   }
 }

@@ -28,6 +28,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <vector>
 
@@ -149,6 +150,7 @@ void plan_free(fem_plan *p) {
   cudaFree(p->d_rowElemPtr);
   cudaFree(p->d_rowElem);
   cudaFree(p->d_rowChunk);
+  cudaFree(p->d_sched);
   if (p->copyIn) cudaStreamDestroy(p->copyIn);
   if (p->copyOut) cudaStreamDestroy(p->copyOut);
   cudaSetDevice(cur);
@@ -166,6 +168,164 @@ int upload(const std::vector<V> &h, V **d, int64_t &bytes) {
     if (err != cudaSuccess) return fem::fail(FEM_ERR_CUDA, "cudaMemcpy: %s", cudaGetErrorString(err));
   }
   return FEM_SUCCESS;
+}
+// Default band of the dependency-ordered schedule: about 8 MB of matrix blocks per
+// band (one element row of the 1024^2 order-3 mesh), so that the few bands in
+// flight between a band's first and last colour stay well inside the 126 MB L2.
+int default_band(const fem_plan *p) {
+  const double bytesPerElement = 32.0 * (double)p->nnzb / std::max(1, p->numElements);
+  const double band = 8e6 / std::max(bytesPerElement, 1.0);
+  return (int)std::min(65536.0, std::max(256.0, std::round(band / 2.0) * 2.0));
+}
+
+int default_tile(int order) { return order == 4 ? 8 : 16; }
+
+// Builds the dependency-ordered schedule of `p`: bands of `band` consecutive element
+// ids; group (k, c) = band k's elements of colour c, a list-position range (the
+// list holds each colour's elements in ascending id).  Group (k, c) waits for, in
+// every band k' whose node span [lowest, highest node id] meets band k's, the
+// latest non-empty colour c' < c: any earlier-colour element sharing a node with
+// band k's colour-c elements lies in such a band k', and its group is (k', c')
+// or one that (k', c') waits for in turn.  Dispatch step t(k, c) = max(k, t of
+// each dependency + 1); groups run in (t, c, k) order and are cut into tiles of
+// `tile` list positions (even, so element pairs never straddle two tiles).
+int build_schedule(fem_plan *p, int band, int tile) {
+  cudaFree(p->d_sched);
+  p->deviceBytes -= p->schedBytes;
+  p->d_sched = nullptr;
+  p->schedBytes = 0;
+  p->schedBand = p->schedTile = p->schedGroups = p->schedTiles = 0;
+  p->sched = fem::dev::SchedArgs{};
+  if (band <= 0 || p->numElements == 0) return FEM_SUCCESS;
+  const int nE = p->numElements, nc = p->numColours;
+  band = std::max(2, band + (band & 1));
+  tile = std::max(2, tile + (tile & 1));
+  const int B = (int)(((int64_t)nE + band - 1) / band);
+  if ((int64_t)B * nc > 4 * 1024 * 1024)
+    return fem::fail(FEM_ERR_UNSUPPORTED, "schedule of %d bands x %d colours: use longer bands", B, nc);
+  // per (band, colour): list positions; per band: node span
+  std::vector<int64_t> p0((size_t)B * nc), p1((size_t)B * nc);
+  std::vector<int> blo(B, INT32_MAX), bhi(B, -1);
+  for (int c = 0; c < nc; c++) {
+    const int *b0 = p->elemList.data() + p->colourPtr[c], *b1 = p->elemList.data() + p->colourPtr[c + 1];
+    for (int k = 0; k < B; k++) {
+      const size_t x = (size_t)k * nc + c;
+      p0[x] = std::lower_bound(b0, b1, (int)((int64_t)k * band)) - p->elemList.data();
+      p1[x] = std::lower_bound(b0, b1, (int)std::min<int64_t>((int64_t)(k + 1) * band, nE)) - p->elemList.data();
+      for (int64_t q = p0[x]; q < p1[x]; q++) {
+        blo[k] = std::min(blo[k], p->nodeLo[q]);
+        bhi[k] = std::max(bhi[k], p->nodeHi[q]);
+      }
+    }
+  }
+  // bands whose node spans meet: sweep over bands ordered by span start
+  std::vector<int> byLo(B);
+  for (int k = 0; k < B; k++) byLo[k] = k;
+  std::sort(byLo.begin(), byLo.end(), [&](int a, int b) { return blo[a] < blo[b]; });
+  std::vector<std::vector<int>> meets(B);
+  int64_t pairs = 0;
+  for (int i = 0; i < B; i++) {
+    const int k = byLo[i];
+    if (bhi[k] < 0) continue;
+    for (int j = i + 1; j < B && blo[byLo[j]] <= bhi[k]; j++) {
+      const int k2 = byLo[j];
+      if (bhi[k2] < 0) continue;
+      meets[k].push_back(k2);
+      meets[k2].push_back(k);
+      if (++pairs > 64LL * B + 1024)
+        return fem::fail(FEM_ERR_UNSUPPORTED, "band node spans overlap too widely for a schedule (scrambled numbering)");
+    }
+    meets[k].push_back(k);
+  }
+  // groups with their dependencies and steps
+  struct Grp {
+    int t, c, k;
+    std::vector<int> deps;  // cell indices k * nc + c
+  };
+  std::vector<int> step((size_t)B * nc, -1);
+  std::vector<Grp> gs;
+  std::vector<int> cellGroup((size_t)B * nc, -1);
+  for (int c = 0; c < nc; c++) {
+    for (int k = 0; k < B; k++) {
+      const size_t x = (size_t)k * nc + c;
+      if (p1[x] <= p0[x]) continue;
+      Grp g{k, c, k, {}};
+      for (int k2 : meets[k]) {
+        for (int c2 = c - 1; c2 >= 0; c2--) {
+          const size_t y = (size_t)k2 * nc + c2;
+          if (p1[y] > p0[y]) {
+            g.deps.push_back((int)y);
+            g.t = std::max(g.t, step[y] + 1);
+            break;
+          }
+        }
+      }
+      step[x] = g.t;
+      gs.push_back(std::move(g));
+    }
+  }
+  std::vector<int> order(gs.size());
+  for (size_t i = 0; i < gs.size(); i++) order[i] = (int)i;
+  std::sort(order.begin(), order.end(), [&](int a, int b) {
+    const Grp &x = gs[a], &y = gs[b];
+    return x.t != y.t ? x.t < y.t : (x.c != y.c ? x.c < y.c : x.k < y.k);
+  });
+  for (size_t i = 0; i < order.size(); i++) {
+    const Grp &g = gs[order[i]];
+    cellGroup[(size_t)g.k * nc + g.c] = (int)i;
+  }
+  const int G = (int)order.size();
+  std::vector<fem::dev::SchedTile> tiles;
+  std::vector<int> groupTiles(G), depPtr(G + 1, 0), deps;
+  for (int i = 0; i < G; i++) {
+    const Grp &g = gs[order[i]];
+    const size_t x = (size_t)g.k * nc + g.c;
+    int n = 0;
+    for (int64_t q = p0[x]; q < p1[x]; q += tile, n++)
+      tiles.push_back({q, (int)std::min<int64_t>(tile, p1[x] - q), i});
+    groupTiles[i] = n;
+    for (int y : g.deps) deps.push_back(cellGroup[y]);
+    depPtr[i + 1] = (int)deps.size();
+  }
+  // one device allocation: tiles | groupTiles | depPtr | deps | status (2 + G words)
+  auto al = [](size_t b) { return (b + 15) & ~(size_t)15; };
+  const size_t oT = 0, oG = al(oT + tiles.size() * sizeof(fem::dev::SchedTile)), oP = al(oG + 4 * (size_t)G),
+               oD = al(oP + 4 * (size_t)(G + 1)), oS = al(oD + 4 * std::max<size_t>(deps.size(), 1)),
+               total = al(oS + 4 * (size_t)(G + 2));
+  cudaError_t err = cudaMalloc(&p->d_sched, total);
+  if (err != cudaSuccess) return fem::fail(FEM_ERR_CUDA, "cudaMalloc(%zu): %s", total, cudaGetErrorString(err));
+  unsigned char *b = static_cast<unsigned char *>(p->d_sched);
+  if ((err = cudaMemcpy(b + oT, tiles.data(), tiles.size() * sizeof(fem::dev::SchedTile), cudaMemcpyHostToDevice)) ||
+      (err = cudaMemcpy(b + oG, groupTiles.data(), 4 * (size_t)G, cudaMemcpyHostToDevice)) ||
+      (err = cudaMemcpy(b + oP, depPtr.data(), 4 * (size_t)(G + 1), cudaMemcpyHostToDevice)) ||
+      (!deps.empty() && (err = cudaMemcpy(b + oD, deps.data(), 4 * deps.size(), cudaMemcpyHostToDevice))) ||
+      (err = cudaMemset(b + oS, 0, 4 * (size_t)(G + 2)))) {
+    cudaFree(p->d_sched);
+    p->d_sched = nullptr;
+    return fem::fail(FEM_ERR_CUDA, "schedule upload: %s", cudaGetErrorString(err));
+  }
+  p->schedBand = band;
+  p->schedTile = tile;
+  p->schedGroups = G;
+  p->schedTiles = (int)tiles.size();
+  p->schedBytes = (int64_t)total;
+  p->deviceBytes += p->schedBytes;
+  fem::dev::SchedArgs &a = p->sched;
+  a.tiles = reinterpret_cast<const fem::dev::SchedTile *>(b + oT);
+  a.groupTiles = reinterpret_cast<const int *>(b + oG);
+  a.depPtr = reinterpret_cast<const int *>(b + oP);
+  a.deps = reinterpret_cast<const int *>(b + oD);
+  a.status = reinterpret_cast<int *>(b + oS);
+  a.ntiles = p->schedTiles;
+  a.stallGroup = -1;
+  a.waitLimitNs = 500000000LL;
+  return FEM_SUCCESS;
+}
+
+// Whether fem_plan_assemble runs `p` as one dependency-ordered launch.
+bool plan_sched(const fem_plan *p, int precision, int strain) {
+  return p->schedGroups > 0 && fem::frag_supported(p->order, precision, strain, true) &&
+         !(fem::plan_rows(p) && strain == FEM_STRAIN_LINEAR);
 }
 }  // namespace
 
@@ -272,7 +432,93 @@ int fem_plan_create(int elementOrder, int numNodes, const int *connPtr, const in
     }
     p->numChunks = (int)hp.rowChunk.size() - 1;
   }
+  if (p->order >= 2) {
+    // a mesh whose numbering leaves no banded structure keeps the colour launches
+    st = build_schedule(p, default_band(p), default_tile(p->order));
+    if (st == FEM_ERR_UNSUPPORTED) {
+      fem::clear_error();
+      st = FEM_SUCCESS;
+    }
+    if (st) {
+      plan_free(p);
+      return st;
+    }
+  }
   *plan = p;
+  return FEM_SUCCESS;
+}
+
+int fem_plan_set_schedule(fem_plan *plan, int bandElements, int tileElements) {
+  fem::clear_error();
+  if (!plan) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "plan is NULL");
+  if (plan->order < 2) return fem::fail(FEM_ERR_UNSUPPORTED, "order-1 plans assemble by rows (or colours)");
+  if (bandElements < 0 || tileElements < 0) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "negative band or tile");
+  int cur = 0;
+  cudaGetDevice(&cur);
+  cudaSetDevice(plan->device);
+  const int st = build_schedule(plan, bandElements, tileElements ? tileElements : default_tile(plan->order));
+  cudaSetDevice(cur);
+  return st;
+}
+
+int fem_plan_get_schedule(const fem_plan *plan, int *bandElements, int *tileElements, int *numGroups, int *numTiles) {
+  fem::clear_error();
+  if (!plan) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "plan is NULL");
+  if (bandElements) *bandElements = plan->schedBand;
+  if (tileElements) *tileElements = plan->schedTile;
+  if (numGroups) *numGroups = plan->schedGroups;
+  if (numTiles) *numTiles = plan->schedTiles;
+  return FEM_SUCCESS;
+}
+
+int fem_plan_get_schedule_tables(const fem_plan *plan, int64_t *tileBegin, int *tileCount, int *tileGroup,
+                                 int *groupTiles, int *depPtr, int *deps) {
+  fem::clear_error();
+  if (!plan) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "plan is NULL");
+  if (!plan->d_sched) return FEM_SUCCESS;
+  const fem::dev::SchedArgs &a = plan->sched;
+  const int G = plan->schedGroups, T = plan->schedTiles;
+  std::vector<fem::dev::SchedTile> t((size_t)T);
+  std::vector<int> ptr((size_t)G + 1);
+  cudaError_t err = cudaMemcpy(t.data(), a.tiles, sizeof(fem::dev::SchedTile) * (size_t)T, cudaMemcpyDeviceToHost);
+  if (err == cudaSuccess) err = cudaMemcpy(ptr.data(), a.depPtr, sizeof(int) * ((size_t)G + 1), cudaMemcpyDeviceToHost);
+  if (err == cudaSuccess && groupTiles)
+    err = cudaMemcpy(groupTiles, a.groupTiles, sizeof(int) * (size_t)G, cudaMemcpyDeviceToHost);
+  if (err == cudaSuccess && deps && ptr[G] > 0)
+    err = cudaMemcpy(deps, a.deps, sizeof(int) * (size_t)ptr[G], cudaMemcpyDeviceToHost);
+  if (err != cudaSuccess) return fem::cuda_fail(err, "cudaMemcpy(schedule tables)");
+  for (int i = 0; i < T; i++) {
+    if (tileBegin) tileBegin[i] = t[i].begin;
+    if (tileCount) tileCount[i] = t[i].count;
+    if (tileGroup) tileGroup[i] = t[i].group;
+  }
+  if (depPtr) std::copy(ptr.begin(), ptr.end(), depPtr);
+  return FEM_SUCCESS;
+}
+
+int fem_plan_schedule_status(fem_plan *plan, void *stream, int64_t *timedOutWaits) {
+  fem::clear_error();
+  if (!plan || !timedOutWaits) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "NULL argument");
+  *timedOutWaits = 0;
+  if (!plan->d_sched) return FEM_SUCCESS;
+  int v = 0;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  cudaError_t err = cudaMemcpyAsync(&v, plan->sched.status, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+  if (err == cudaSuccess && v) err = cudaMemsetAsync(plan->sched.status, 0, sizeof(int), s);
+  if (err == cudaSuccess && v) err = cudaStreamSynchronize(s);
+  if (err != cudaSuccess) return fem::cuda_fail(err, "reading the schedule status");
+  *timedOutWaits = v;
+  return FEM_SUCCESS;
+}
+
+int fem_plan_set_schedule_waits(fem_plan *plan, int64_t waitLimitNs, int stallGroup) {
+  fem::clear_error();
+  if (!plan) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "plan is NULL");
+  if (stallGroup != -1 && (stallGroup < 0 || stallGroup >= plan->schedGroups))
+    return fem::fail(FEM_ERR_INVALID_ARGUMENT, "stallGroup %d of %d groups", stallGroup, plan->schedGroups);
+  if (waitLimitNs > 0) plan->sched.waitLimitNs = waitLimitNs;
+  plan->sched.stallGroup = stallGroup;
   return FEM_SUCCESS;
 }
 
@@ -356,6 +602,22 @@ int fem_plan_assemble_ex(const fem_plan *plan, const double *states, const doubl
     return fem::timed(s, elapsedSeconds, [&] { return fem::launch_rows(mode, a, s); });
   }
   const bool frag = fem::frag_supported(plan->order, precision, strainType, true);
+  if (plan_sched(plan, precision, strainType)) {
+    // all colours in one dependency-ordered launch; the tile dispenser and the
+    // per-group counters start at zero, the sticky timeout count (word 0) is kept
+    const int st = fem::timed(s, elapsedSeconds, [&]() -> int {
+      cudaError_t err = cudaMemsetAsync(plan->sched.status + 1, 0, sizeof(int) * ((size_t)plan->schedGroups + 1), s);
+      if (err != cudaSuccess) return fem::cuda_fail(err, "cudaMemsetAsync(schedule counters)");
+      return fem::launch_frag_sched(plan->order, precision, mode, a, plan->sched, s, strainType);
+    });
+    if (st || !elapsedSeconds) return st;
+    int64_t waits = 0;
+    const int st2 = fem_plan_schedule_status(const_cast<fem_plan *>(plan), stream, &waits);
+    if (st2) return st2;
+    if (waits) return fem::fail(FEM_ERR_TIMEOUT, "%lld in-kernel waits of the dependency-ordered launch ran out",
+                                (long long)waits);
+    return st;
+  }
   return fem::timed(s, elapsedSeconds, [&] {
     for (int c = 0; c < plan->numColours; c++) {
       a.begin = plan->colourPtr[c];

@@ -113,6 +113,9 @@ int launch_frag(int order, int precision, int mode, const dev::AsmArgs &a, cudaS
 // kMaxRanges list-position ranges of one mesh in one launch.
 int launch_frag_ranges(int order, int precision, int mode, const dev::AsmArgs &a, const dev::RangeList &r,
                        cudaStream_t s, int strain = FEM_STRAIN_LINEAR);
+// All colours of one plan in one dependency-ordered persistent launch (plan mode).
+int launch_frag_sched(int order, int precision, int mode, const dev::AsmArgs &a, const dev::SchedArgs &sa,
+                      cudaStream_t s, int strain = FEM_STRAIN_LINEAR);
 // Its tile-queue form for batches and the server (residual and Jacobian).
 int launch_frag_batched(int order, int precision, const dev::AsmArgs *meshes, const dev::Tile *tiles, int ntiles,
                         int *counter, cudaStream_t s);
@@ -177,6 +180,11 @@ struct fem_plan {
   std::vector<int> elemList, nodeLo, nodeHi;
   cudaStream_t copyIn = nullptr, copyOut = nullptr;  // created on first use
   int64_t deviceBytes = 0;
+  // dependency-ordered assembly (fem_plan_set_schedule): schedBand == 0 runs colour launches
+  int schedBand = 0, schedTile = 0, schedGroups = 0, schedTiles = 0;
+  void *d_sched = nullptr;  // one allocation: tiles, tiles per group, dependency CSR, status words
+  fem::dev::SchedArgs sched{};
+  int64_t schedBytes = 0;
 };
 
 namespace fem {

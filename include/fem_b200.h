@@ -42,6 +42,7 @@ extern "C" {
 #define FEM_ERR_NOT_FOUND 6        /* an element block is missing from the BSR pattern      */
 #define FEM_ERR_UNSUPPORTED 7      /* input outside what this entry point supports          */
 #define FEM_ERR_BUDGET 8           /* device-memory budget exhausted (serving admission)    */
+#define FEM_ERR_TIMEOUT 9          /* a bounded in-kernel wait ran out (results invalid)     */
 
 #define FEM_PRECISION_FP64 0  /* all element arithmetic in FP64                               */
 #define FEM_PRECISION_MIXED 1 /* FP64 J/detJ/J^-1, weak stress and accumulate; element
@@ -161,6 +162,38 @@ int fem_plan_device_pattern(const fem_plan *plan, const int **rowp, const int **
 int fem_plan_assemble(const fem_plan *plan, const double *states, const double *nodeCoords, double E, double nu,
                       double t, double *residual, double *matEntries, int precision, void *stream,
                       double *elapsedSeconds);
+/* Dependency-ordered assembly.  Where an assembly runs the fragment kernel (orders
+ * 2-4, see FEM_PRECISION_*), fem_plan_assemble runs all colours in ONE persistent
+ * launch instead of one launch per colour: the list positions are cut into groups
+ * (the elements of one colour within a band of bandElements consecutive element
+ * ids) and the groups into tiles of tileElements, in an order where each band's
+ * later colours follow its earlier ones and its neighbours' within a few bands, so
+ * that the blocks a later colour adds to are still in L2.  A tile waits (in the
+ * kernel, bounded) until the groups whose elements share nodes with its group's,
+ * in earlier colours, have finished; every block therefore still receives its
+ * contributions in colour order and the result equals the colour launches' bit
+ * for bit.  Set at fem_plan_create (bandElements chosen from the matrix bytes per
+ * element, about 8 MB of blocks per band); bandElements = 0 selects the colour
+ * launches, tileElements = 0 its default.  FEM_ERR_UNSUPPORTED for an order-1 plan
+ * (row assembly). */
+int fem_plan_set_schedule(fem_plan *plan, int bandElements, int tileElements);
+int fem_plan_get_schedule(const fem_plan *plan, int *bandElements, int *tileElements, int *numGroups, int *numTiles);
+/* Copies the schedule to host arrays: per tile (numTiles) its first list position,
+ * length and group; per group (numGroups) its tile count and, as CSR (depPtr has
+ * numGroups + 1 entries), the groups it waits for.  Any pointer may be NULL. */
+int fem_plan_get_schedule_tables(const fem_plan *plan, int64_t *tileBegin, int *tileCount, int *tileGroup,
+                                 int *groupTiles, int *depPtr, int *deps);
+/* Waits for `stream`, then returns (and clears) the number of in-kernel waits of
+ * dependency-ordered launches on this plan that ran out since the last call.  A
+ * wait gives up after waitLimitNs (default 0.5 s; the launch then finishes within
+ * about one limit) and its assembly's results are invalid; with elapsedSeconds
+ * non-NULL fem_plan_assemble checks this itself and returns FEM_ERR_TIMEOUT. */
+int fem_plan_schedule_status(fem_plan *plan, void *stream, int64_t *timedOutWaits);
+/* Failure injection for tests of the bounded waits: waitLimitNs > 0 sets the wait
+ * limit; stallGroup >= 0 makes every wait on that group run out (its completion
+ * can never be observed), -1 restores normal waits. */
+int fem_plan_set_schedule_waits(fem_plan *plan, int64_t waitLimitNs, int stallGroup);
+
 /* fem_plan_assemble with a strain measure (FEM_STRAIN_*; NONLINEAR in FP64 only). */
 int fem_plan_assemble_ex(const fem_plan *plan, const double *states, const double *nodeCoords, double E, double nu,
                          double t, double *residual, double *matEntries, int precision, int strainType, void *stream,
