@@ -5,16 +5,19 @@
 // stay on the device; admission is refused with FEM_ERR_BUDGET when the device
 // bytes would exceed the server's budget) and then submit requests, each with a
 // new host state and a host buffer for the residual.  A dispatcher thread takes
-// everything pending (up to maxBatch requests) whenever one of the server's lanes
-// is free, and issues on that lane's stream: the state copies, one batched
-// persistent launch per (order, colour) over the requested meshes' tiles, and the
-// residual copies.  Requests that arrive while a lane is busy go to the other
-// lane, so two waves overlap on the device; a waiter thread per lane completes its
-// requests when the lane's work has finished.  Results do not depend on which
-// requests share a wave (see the batched kernel: every block receives exactly one
-// contribution per colour).
+// pending requests in arrival order (up to maxBatch requests and, past the first
+// one, up to kWaveElements elements, so that one large mesh does not hold a crowd
+// of small ones) whenever one of the server's kLanes lanes is free, and issues on
+// that lane's stream: the state copies, one batched persistent launch per (order,
+// colour) over the requested meshes' tiles, and the residual copies, smallest
+// first, each followed by an event of its request.  Requests that arrive while
+// lanes are busy go to the next free lane, so waves overlap on the device; a
+// waiter thread per lane completes each request as soon as its own residual has
+// arrived.  Results do not depend on which requests share a wave (see the batched
+// kernel: every block receives exactly one contribution per colour).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <cstdint>
@@ -30,8 +33,9 @@
 
 namespace {
 
-constexpr int kLanes = 2;
+constexpr int kLanes = 4;
 constexpr int kMaxColoursS = 64;
+constexpr int64_t kWaveElements = 1 << 21;  // element cap of a wave past its first request
 
 double now_seconds() {
   using namespace std::chrono;
@@ -58,6 +62,8 @@ struct Request {
 struct Lane {
   cudaStream_t stream = nullptr;
   cudaEvent_t done = nullptr;
+  std::vector<cudaEvent_t> reqDone;  // per request of the wave, after its residual copy (maxBatch events)
+  std::vector<int> doneOrder;        // wave positions in the order their events were recorded
   fem::dev::AsmArgs *d_args = nullptr;
   fem::dev::Tile *d_tiles = nullptr;
   int *d_counters = nullptr;
@@ -206,13 +212,21 @@ int issue_wave(fem_server *S, Lane &L, const std::vector<ServerMesh> &wm, const 
     st = fem::launch_batched(p, S->precision, L.d_args, L.d_tiles + off[j], off[j + 1] - off[j], counter, L.stream);
     if (st) return st;
   }
-  // outputs: residuals back to the clients (the matrices stay resident)
-  for (int i = 0; i < n; i++) {
+  // outputs: residuals back to the clients, smallest first, each request's event
+  // after its own copy (the matrices stay resident)
+  L.doneOrder.resize(n);
+  for (int i = 0; i < n; i++) L.doneOrder[i] = i;
+  auto bytes_of = [&](int i) { return rq[i]->hostResidual ? (int64_t)wm[i].plan->numNodes : (int64_t)-1; };
+  std::stable_sort(L.doneOrder.begin(), L.doneOrder.end(), [&](int a, int b) { return bytes_of(a) < bytes_of(b); });
+  for (int j = 0; j < n; j++) {
+    const int i = L.doneOrder[j];
     const ServerMesh &m = wm[i];
-    if (!rq[i]->hostResidual) continue;
-    err = cudaMemcpyAsync(rq[i]->hostResidual, m.residual, sizeof(double) * 2 * m.plan->numNodes,
-                          cudaMemcpyDeviceToHost, L.stream);
-    if (err != cudaSuccess) return fem::cuda_fail(err, "residual download");
+    if (rq[i]->hostResidual) {
+      err = cudaMemcpyAsync(rq[i]->hostResidual, m.residual, sizeof(double) * 2 * m.plan->numNodes,
+                            cudaMemcpyDeviceToHost, L.stream);
+      if (err != cudaSuccess) return fem::cuda_fail(err, "residual download");
+    }
+    if ((err = cudaEventRecord(L.reqDone[j], L.stream)) != cudaSuccess) return fem::cuda_fail(err, "cudaEventRecord");
   }
   err = cudaEventRecord(L.done, L.stream);
   if (err != cudaSuccess) return fem::cuda_fail(err, "cudaEventRecord");
@@ -242,8 +256,12 @@ void dispatcher_main(fem_server *S) {
     std::vector<ServerMesh> wm;
     std::vector<Request *> rq;
     L.reqs.clear();
+    int64_t waveElements = 0;
     while (!S->pending.empty() && (int)L.reqs.size() < S->maxBatch) {
       const int64_t tk = S->pending.front();
+      const int64_t ne = S->meshes[S->reqs[tk].mesh].plan->numElements;
+      if (!L.reqs.empty() && waveElements + ne > kWaveElements) break;
+      waveElements += ne;
       S->pending.pop_front();
       Request &r = S->reqs[tk];
       L.reqs.push_back(tk);
@@ -280,19 +298,25 @@ void waiter_main(fem_server *S, int l) {
   while (true) {
     L.cv.wait(lk, [&] { return S->stop || L.issued; });
     if (S->stop) return;
-    lk.unlock();
-    cudaError_t err = cudaEventSynchronize(L.done);
-    const double t = now_seconds();
-    lk.lock();
-    for (int64_t tk : L.reqs) {
-      Request &r = S->reqs[tk];
+    // each request completes as soon as its own residual has arrived
+    for (size_t j = 0; j < L.reqs.size(); j++) {
+      lk.unlock();
+      const cudaError_t err = cudaEventSynchronize(L.reqDone[j]);
+      const double t = now_seconds();
+      lk.lock();
+      Request &r = S->reqs[L.reqs[L.doneOrder[j]]];
       r.status = err == cudaSuccess ? FEM_SUCCESS : FEM_ERR_CUDA;
       r.done = true;
       r.tDone = t;
       S->meshes[r.mesh].busy = false;
       S->completed++;
       S->elementsDone += S->meshes[r.mesh].plan->numElements;
+      S->cvDone.notify_all();
     }
+    lk.unlock();
+    const cudaError_t err = cudaEventSynchronize(L.done);
+    lk.lock();
+    (void)err;
     L.reqs.clear();
     L.issued = false;
     L.busy = false;
@@ -321,6 +345,7 @@ void server_free(fem_server *S) {
     cudaFree(L.d_tiles);
     cudaFree(L.d_counters);
     if (L.done) cudaEventDestroy(L.done);
+    for (cudaEvent_t e : L.reqDone) cudaEventDestroy(e);
     if (L.stream) cudaStreamDestroy(L.stream);
   }
   for (auto &m : S->meshes) {
@@ -356,6 +381,9 @@ int fem_server_create(int64_t budgetBytes, int precision, int maxBatch, fem_serv
     if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking);
     if (err == cudaSuccess) err = cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming);
     if (err == cudaSuccess) err = cudaMalloc(&L.d_counters, sizeof(int) * 5 * kMaxColoursS);
+    L.reqDone.assign((size_t)maxBatch, nullptr);
+    for (auto &e : L.reqDone)
+      if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
   }
   if (err != cudaSuccess) {
     int st = fem::cuda_fail(err, "fem_server_create");
