@@ -205,8 +205,9 @@ class Plan:
         return {"tile_begin": begin, "tile_count": count, "tile_group": group, "group_tiles": gt, "dep_ptr": ptr,
                 "deps": deps[:int(ptr[-1])]}
 
-    def set_schedule(self, band, tile=0):
-        """band = 0: colour launches; tile = 0: the default tile length."""
+    def set_schedule(self, band=-1, tile=0):
+        """band = -1: the default band (about 8 MB of blocks), 0: colour launches;
+        tile = 0: the default tile length."""
         check(lib.fem_plan_set_schedule(self._h, int(band), int(tile)), "fem_plan_set_schedule")
 
     def schedule_status(self, stream=None) -> int:

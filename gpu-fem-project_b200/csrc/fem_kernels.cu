@@ -432,18 +432,6 @@ int fem_plan_create(int elementOrder, int numNodes, const int *connPtr, const in
     }
     p->numChunks = (int)hp.rowChunk.size() - 1;
   }
-  if (p->order >= 2) {
-    // a mesh whose numbering leaves no banded structure keeps the colour launches
-    st = build_schedule(p, default_band(p), default_tile(p->order));
-    if (st == FEM_ERR_UNSUPPORTED) {
-      fem::clear_error();
-      st = FEM_SUCCESS;
-    }
-    if (st) {
-      plan_free(p);
-      return st;
-    }
-  }
   *plan = p;
   return FEM_SUCCESS;
 }
@@ -452,11 +440,12 @@ int fem_plan_set_schedule(fem_plan *plan, int bandElements, int tileElements) {
   fem::clear_error();
   if (!plan) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "plan is NULL");
   if (plan->order < 2) return fem::fail(FEM_ERR_UNSUPPORTED, "order-1 plans assemble by rows (or colours)");
-  if (bandElements < 0 || tileElements < 0) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "negative band or tile");
+  if (bandElements < -1 || tileElements < 0) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "bad band or tile length");
   int cur = 0;
   cudaGetDevice(&cur);
   cudaSetDevice(plan->device);
-  const int st = build_schedule(plan, bandElements, tileElements ? tileElements : default_tile(plan->order));
+  const int st = build_schedule(plan, bandElements < 0 ? default_band(plan) : bandElements,
+                                tileElements ? tileElements : default_tile(plan->order));
   cudaSetDevice(cur);
   return st;
 }

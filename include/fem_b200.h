@@ -162,20 +162,21 @@ int fem_plan_device_pattern(const fem_plan *plan, const int **rowp, const int **
 int fem_plan_assemble(const fem_plan *plan, const double *states, const double *nodeCoords, double E, double nu,
                       double t, double *residual, double *matEntries, int precision, void *stream,
                       double *elapsedSeconds);
-/* Dependency-ordered assembly.  Where an assembly runs the fragment kernel (orders
- * 2-4, see FEM_PRECISION_*), fem_plan_assemble runs all colours in ONE persistent
- * launch instead of one launch per colour: the list positions are cut into groups
- * (the elements of one colour within a band of bandElements consecutive element
- * ids) and the groups into tiles of tileElements, in an order where each band's
- * later colours follow its earlier ones and its neighbours' within a few bands, so
- * that the blocks a later colour adds to are still in L2.  A tile waits (in the
- * kernel, bounded) until the groups whose elements share nodes with its group's,
- * in earlier colours, have finished; every block therefore still receives its
- * contributions in colour order and the result equals the colour launches' bit
- * for bit.  Set at fem_plan_create (bandElements chosen from the matrix bytes per
- * element, about 8 MB of blocks per band); bandElements = 0 selects the colour
- * launches, tileElements = 0 its default.  FEM_ERR_UNSUPPORTED for an order-1 plan
- * (row assembly). */
+/* Dependency-ordered assembly (opt-in).  With a schedule set, where an assembly
+ * runs the fragment kernel (orders 2-4, see FEM_PRECISION_*), fem_plan_assemble
+ * runs all colours in ONE persistent launch instead of one launch per colour: the
+ * list positions are cut into groups (the elements of one colour within a band of
+ * bandElements consecutive element ids) and the groups into tiles of tileElements,
+ * dispatched so that each band's later colours follow its earlier ones and its
+ * neighbours' within a few bands.  A tile waits (in the kernel, bounded) until the
+ * groups whose elements share nodes with its group's, in earlier colours, have
+ * finished; every block therefore still receives its contributions in colour
+ * order and the result equals the colour launches' bit for bit.  Plans start
+ * without a schedule (colour launches, the faster form on large meshes);
+ * bandElements = -1 picks a band of about 8 MB of matrix blocks, 0 removes the
+ * schedule; tileElements = 0 picks the default (16, order 4: 8).
+ * FEM_ERR_UNSUPPORTED for an order-1 plan (row assembly), or when the bands' node
+ * ranges overlap too widely (scrambled numbering). */
 int fem_plan_set_schedule(fem_plan *plan, int bandElements, int tileElements);
 int fem_plan_get_schedule(const fem_plan *plan, int *bandElements, int *tileElements, int *numGroups, int *numTiles);
 /* Copies the schedule to host arrays: per tile (numTiles) its first list position,

@@ -61,10 +61,10 @@ def test_row_assembly_selection(fem, cuda):
     assert p1.launches() == 1 and p1.launches("nonlinear") == p1.num_colours
     m2 = fem.square_mesh(5, 5, 2, 1.0, 1.0, 0.1, seed=3)
     p2 = fem.Plan(2, m2.num_nodes, m2.conn_ptr, m2.conn)
-    # order 2: no row tables; one dependency-ordered launch, or one per colour
-    assert p2.row_chunks == 0 and p2.launches() == 1
-    p2.set_schedule(0)
-    assert p2.launches() == p2.num_colours
+    # order 2: no row tables; one launch per colour, or one dependency-ordered launch
+    assert p2.row_chunks == 0 and p2.launches() == p2.num_colours
+    p2.set_schedule(-1)
+    assert p2.launches() == 1
     p1.close()
     p2.close()
 

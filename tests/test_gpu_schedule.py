@@ -103,7 +103,7 @@ def test_schedule_equals_colour_launches(fem, orc, cuda, name, band):
     m = MESHES[name](fem)
     plan = fem.Plan(m.order, m.num_nodes, m.conn_ptr, m.conn)
     try:
-        assert plan.schedule()["groups"] > 0  # a default schedule is built for orders 2-4
+        assert plan.schedule()["groups"] == 0  # plans start with the colour launches
         modes = [("fp64", "linear", True, True), ("fp64", "linear", True, False), ("fp64", "linear", False, True)]
         if m.order in (2, 3):
             modes.append(("fp64", "nonlinear", True, True))
