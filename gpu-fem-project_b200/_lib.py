@@ -29,6 +29,10 @@ FEM_PRECISION_MIXED = 1
 FEM_STRAIN_LINEAR = 0
 FEM_STRAIN_NONLINEAR = 1
 
+# batch kernel variants (fem_batch_get_kernels / fem_batch_set_kernels)
+FEM_KERNELS = {0: "default", 1: "rows", 2: "fragment_fp64", 3: "fragment_bf16x6", 4: "element_fp64",
+               5: "element_fp32"}
+
 _i = C.c_int
 _i64 = C.c_int64
 _d = C.c_double
@@ -83,6 +87,8 @@ SIGNATURES = {
     "fem_batch_set_tiles": (_i, [_p, _p]),
     "fem_batch_assemble": (_i, [_p, _i, _p, _pd]),
     "fem_batch_tune": (_i, [_p, _i, _p, _i, _pd]),
+    "fem_batch_get_kernels": (_i, [_p, _i, _p]),
+    "fem_batch_set_kernels": (_i, [_p, _i, _p]),
     "fem_batch_capture": (_i, [_p, _i, _p]),
     "fem_batch_replay": (_i, [_p, _p, _pd]),
 }

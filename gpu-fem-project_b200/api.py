@@ -12,7 +12,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import FEM_PRECISION_FP64, FEM_PRECISION_MIXED, FEM_STRAIN_LINEAR, FEM_STRAIN_NONLINEAR, check, lib
+from ._lib import FEM_KERNELS, FEM_PRECISION_FP64, FEM_PRECISION_MIXED, FEM_STRAIN_LINEAR, FEM_STRAIN_NONLINEAR, check, lib
 
 _PRECISION = {"fp64": FEM_PRECISION_FP64, "mixed": FEM_PRECISION_MIXED}
 # A2D::GreenStrainType of the reference kernels' strainType template argument
@@ -305,7 +305,19 @@ class Batch:
         tiles = (C.c_int * 4)()
         check(lib.fem_batch_get_tiles(self._h, tiles), "fem_batch_get_tiles")
         return {"elements": ne.value, "tiles": nt.value, "launches": nl.value, "device_bytes": bytes_.value,
-                "tile_batches": list(tiles)}
+                "tile_batches": list(tiles), "kernels_fp64": self.kernels("fp64"), "kernels_mixed": self.kernels("mixed")}
+
+    def kernels(self, precision="fp64"):
+        """Kernel variant per order (1..4) for `precision`, by name (FEM_KERNEL_*)."""
+        arr = (C.c_int * 4)()
+        check(lib.fem_batch_get_kernels(self._h, _prec(precision), arr), "fem_batch_get_kernels")
+        return [FEM_KERNELS[int(v)] for v in arr]
+
+    def set_kernels(self, names, precision="fp64"):
+        """Kernel variants per order (1..4) by name; "default" = the plan path's kernel."""
+        ids = {v: k for k, v in FEM_KERNELS.items()}
+        arr = (C.c_int * 4)(*[ids[n] for n in names])
+        check(lib.fem_batch_set_kernels(self._h, _prec(precision), arr), "fem_batch_set_kernels")
 
     def set_tiles(self, tile_batches):
         arr = (C.c_int * 4)(*[int(x) for x in tile_batches])

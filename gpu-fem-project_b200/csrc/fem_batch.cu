@@ -8,6 +8,16 @@
 // independent chains on their own streams (colours of one order run in sequence:
 // a later colour adds to blocks an earlier one stored); the whole fork/join
 // pattern is captured once into a CUDA graph and replayed with one launch.
+//
+// Per order and precision the batch runs one kernel variant (FEM_KERNEL_*): the
+// single-mesh plan path's kernel by default (batched results then equal the lone
+// ones bit for bit), or one the autotuner picks by timing: the warp-fragment
+// kernel (two elements per warp: 16 threads per element, 8 elements per 4-warp
+// CTA step, FP64 MMA or, at order 3 MIXED, BF16x6 stiffness), the element kernel
+// (one thread group per EPG elements: Shape<P> threads per group, groups per CTA;
+// FP64 or, MIXED, FP32 element products), or order-1 row assembly.  MIXED may run
+// any FP64 variant (FP64 is within its error bound); FP64 runs FP64 variants only.
+// The tuner also picks the tile length of the order's work queues.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -43,20 +53,35 @@ int launch_batched_p(const dev::AsmArgs *meshes, const dev::Tile *tiles, int nti
   return FEM_SUCCESS;
 }
 
-// The batched element kernel serves what the fragment kernel does not: order 1
-// (meshes whose rows are too long for row assembly) and the FP32 order-4 path
-// (FEM_PRECISION_MIXED); see frag_supported.
+// The batched element kernel, every order, FP64 or FP32 element products.
 template <typename T>
 int launch_batched_t(int p, const dev::AsmArgs *meshes, const dev::Tile *tiles, int ntiles, int *counter,
                      cudaStream_t s) {
-  if (p == 1) return launch_batched_p<1, T>(meshes, tiles, ntiles, counter, s);
-  if constexpr (sizeof(T) == 4) {
-    if (p == 4) return launch_batched_p<4, T>(meshes, tiles, ntiles, counter, s);
+  switch (p) {
+    case 1: return launch_batched_p<1, T>(meshes, tiles, ntiles, counter, s);
+    case 2: return launch_batched_p<2, T>(meshes, tiles, ntiles, counter, s);
+    case 3: return launch_batched_p<3, T>(meshes, tiles, ntiles, counter, s);
+    case 4: return launch_batched_p<4, T>(meshes, tiles, ntiles, counter, s);
+    default: return fail(FEM_ERR_INVALID_ORDER, "batched element kernel: order %d", p);
   }
-  return fail(FEM_ERR_INVALID_ORDER, "batched element kernel: order %d", p);
 }
 
 }  // namespace
+
+// The colour launches of order p with kernel variant v (never FEM_KERNEL_DEFAULT
+// or FEM_KERNEL_ROWS here).
+int launch_batched_variant(int p, int v, const dev::AsmArgs *meshes, const dev::Tile *tiles, int ntiles, int *counter,
+                           cudaStream_t s) {
+  switch (v) {
+    case FEM_KERNEL_FRAGMENT_FP64:
+      return launch_frag_batched(p, FEM_PRECISION_FP64, meshes, tiles, ntiles, counter, s);
+    case FEM_KERNEL_FRAGMENT_BF16X6:
+      return launch_frag_batched(p, FEM_PRECISION_MIXED, meshes, tiles, ntiles, counter, s);
+    case FEM_KERNEL_ELEMENT_FP64: return launch_batched_t<double>(p, meshes, tiles, ntiles, counter, s);
+    case FEM_KERNEL_ELEMENT_FP32: return launch_batched_t<float>(p, meshes, tiles, ntiles, counter, s);
+    default: return fail(FEM_ERR_INVALID_ARGUMENT, "kernel variant %d", v);
+  }
+}
 
 int launch_batched(int p, int precision, const dev::AsmArgs *meshes, const dev::Tile *tiles, int ntiles, int *counter,
                    cudaStream_t s) {
@@ -75,6 +100,30 @@ namespace {
 constexpr int kMaxColours = 64;
 constexpr int kOrders = 5;  // index 1..4
 
+// Whether variant v may serve order p at `precision` (FEM_KERNEL_DEFAULT always may).
+bool variant_allowed(int p, int precision, int v) {
+  switch (v) {
+    case FEM_KERNEL_DEFAULT: return true;
+    case FEM_KERNEL_ROWS: return p == 1;
+    case FEM_KERNEL_FRAGMENT_FP64: return p >= 2;
+    case FEM_KERNEL_FRAGMENT_BF16X6: return p == 3 && precision == FEM_PRECISION_MIXED;
+    case FEM_KERNEL_ELEMENT_FP64: return true;
+    case FEM_KERNEL_ELEMENT_FP32: return precision == FEM_PRECISION_MIXED;
+    default: return false;
+  }
+}
+
+// The variant the single-mesh plan path runs for order p (order 1: rows where a
+// mesh has row tables, the element kernel otherwise -- reported as ROWS).
+int default_variant(int p, int precision) {
+  if (p == 1) return FEM_KERNEL_ROWS;
+  if (fem::frag_supported(p, precision, FEM_STRAIN_LINEAR, true))
+    return fem::b16_stiffness(p, precision, FEM_STRAIN_LINEAR) ? FEM_KERNEL_FRAGMENT_BF16X6 : FEM_KERNEL_FRAGMENT_FP64;
+  return precision == FEM_PRECISION_MIXED ? FEM_KERNEL_ELEMENT_FP32 : FEM_KERNEL_ELEMENT_FP64;
+}
+
+int prec_index(int precision) { return precision == FEM_PRECISION_MIXED ? 1 : 0; }
+
 }  // namespace
 
 struct fem_batch {
@@ -86,8 +135,10 @@ struct fem_batch {
   bool args_dirty = true;
   int maxColours = 0;
   int tileBatches[kOrders] = {0, 16, 16, 16, 16};  // tile length in element batches, per order
+  int kernel[2][kOrders] = {};                       // [FP64, MIXED][order]: FEM_KERNEL_*
   std::vector<fem::dev::Tile> tiles;
   std::vector<int> tileOff;  // [kOrders][maxColours + 1]
+  std::vector<int> rowSplit;  // order 1, per colour: tiles of meshes with row tables start here
   int rowTile0 = 0, rowTile1 = 0;  // order-1 row-assembly tiles (chunks), after the colour tiles
   fem::dev::Tile *d_tiles = nullptr;
   size_t d_tiles_cap = 0;
@@ -132,23 +183,30 @@ void batch_free(fem_batch *b) {
 
 int order_of(const fem_batch *b, int m) { return b->plans[m]->order; }
 
+// Colour tiles of every mesh (order-1 meshes with row tables last within each
+// colour, after rowSplit[c], so that row assembly can skip them) and the row
+// tiles of the order-1 meshes that have row tables.
 void build_tiles(fem_batch *b) {
   const int C = b->maxColours;
   b->tiles.clear();
   b->tileOff.assign((size_t)kOrders * (C + 1), 0);
+  b->rowSplit.assign((size_t)C + 1, 0);
   for (int p = 1; p < kOrders; p++) {
     const int64_t len = (int64_t)b->tileBatches[p] * fem::epg_of(p);
     for (int c = 0; c < C; c++) {
       b->tileOff[p * (C + 1) + c] = (int)b->tiles.size();
-      for (size_t m = 0; m < b->plans.size(); m++) {
-        const fem_plan *pl = b->plans[m];
-        if (pl->order != p || c >= pl->numColours || fem::plan_rows(pl)) continue;
-        for (int64_t k = pl->colourPtr[c]; k < pl->colourPtr[c + 1]; k += len) {
-          fem::dev::Tile t;
-          t.mesh = (int)m;
-          t.begin = k;
-          t.count = (int)std::min<int64_t>(len, pl->colourPtr[c + 1] - k);
-          b->tiles.push_back(t);
+      for (int rows = 0; rows < 2; rows++) {
+        if (p == 1 && rows == 1) b->rowSplit[c] = (int)b->tiles.size();
+        for (size_t m = 0; m < b->plans.size(); m++) {
+          const fem_plan *pl = b->plans[m];
+          if (pl->order != p || c >= pl->numColours || (int)fem::plan_rows(pl) != rows) continue;
+          for (int64_t k = pl->colourPtr[c]; k < pl->colourPtr[c + 1]; k += len) {
+            fem::dev::Tile t;
+            t.mesh = (int)m;
+            t.begin = k;
+            t.count = (int)std::min<int64_t>(len, pl->colourPtr[c + 1] - k);
+            b->tiles.push_back(t);
+          }
         }
       }
     }
@@ -196,20 +254,31 @@ int sync_device_state(fem_batch *b) {
   return FEM_SUCCESS;
 }
 
-// The colour chain of one order on stream s (counters reset by the caller); order 1
-// meshes with row tables run one row-assembly launch (queue counter [0][0]).
+// The variant order p runs at `precision`.
+int variant_of(const fem_batch *b, int p, int precision) {
+  const int v = b->kernel[prec_index(precision)][p];
+  return v == FEM_KERNEL_DEFAULT ? default_variant(p, precision) : v;
+}
+
+// The colour chain of one order on stream s (counters reset by the caller).  Order
+// 1 with FEM_KERNEL_ROWS: one row-assembly launch (queue counter [0][0]) for the
+// meshes with row tables, colour launches of the element kernel for the others.
 int enqueue_order(fem_batch *b, int p, int precision, cudaStream_t s) {
   const int C = b->maxColours;
-  if (p == 1 && b->rowTile1 > b->rowTile0) {
+  const int v = variant_of(b, p, precision);
+  const bool rows = p == 1 && v == FEM_KERNEL_ROWS;
+  if (rows && b->rowTile1 > b->rowTile0) {
     int st = fem::launch_rows_batched(b->d_args, b->d_tiles + b->rowTile0, b->rowTile1 - b->rowTile0,
                                       b->d_counters, s);
     if (st) return st;
   }
   for (int c = 0; c < C; c++) {
-    const int t0 = b->tileOff[p * (C + 1) + c], t1 = b->tileOff[p * (C + 1) + c + 1];
+    const int t0 = b->tileOff[p * (C + 1) + c];
+    const int t1 = rows ? b->rowSplit[c] : b->tileOff[p * (C + 1) + c + 1];
     if (t1 <= t0) continue;
     int *counter = b->d_counters + p * kMaxColours + c;
-    int st = fem::launch_batched(p, precision, b->d_args, b->d_tiles + t0, t1 - t0, counter, s);
+    int st = v == FEM_KERNEL_ROWS ? fem::launch_batched(p, precision, b->d_args, b->d_tiles + t0, t1 - t0, counter, s)
+                                  : fem::launch_batched_variant(p, v, b->d_args, b->d_tiles + t0, t1 - t0, counter, s);
     if (st) return st;
   }
   return FEM_SUCCESS;
@@ -217,7 +286,7 @@ int enqueue_order(fem_batch *b, int p, int precision, cudaStream_t s) {
 
 bool order_has_work(const fem_batch *b, int p) {
   const int C = b->maxColours;
-  return b->tileOff[p * (C + 1) + C] > b->tileOff[p * (C + 1)] || (p == 1 && b->rowTile1 > b->rowTile0);
+  return b->tileOff[p * (C + 1) + C] > b->tileOff[p * (C + 1)];
 }
 
 // Whole batch: reset queues, fork one stream per order, join back into s.
@@ -327,11 +396,15 @@ int fem_batch_info(const fem_batch *b, int64_t *totalElements, int64_t *numTiles
   if (!b) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "batch is NULL");
   if (totalElements) *totalElements = b->totalElements;
   if (numTiles) *numTiles = (int64_t)b->tiles.size();
-  if (numLaunches) {
+  if (numLaunches) {  // of an FP64 assembly with the batch's FP64 kernel variants
     int n = 0;
     const int C = b->maxColours;
-    for (int p = 1; p < kOrders; p++)
-      for (int c = 0; c < C; c++) n += b->tileOff[p * (C + 1) + c + 1] > b->tileOff[p * (C + 1) + c];
+    for (int p = 1; p < kOrders; p++) {
+      const bool rows = p == 1 && variant_of(b, p, FEM_PRECISION_FP64) == FEM_KERNEL_ROWS;
+      if (rows) n += b->rowTile1 > b->rowTile0;
+      for (int c = 0; c < C; c++)
+        n += (rows ? b->rowSplit[c] : b->tileOff[p * (C + 1) + c + 1]) > b->tileOff[p * (C + 1) + c];
+    }
     *numLaunches = n;
   }
   if (deviceBytes) *deviceBytes = b->deviceBytes + (int64_t)(sizeof(fem::dev::Tile) * b->d_tiles_cap);
@@ -417,6 +490,29 @@ int fem_batch_replay(fem_batch *b, void *stream, double *elapsedSeconds) {
   });
 }
 
+int fem_batch_get_kernels(const fem_batch *b, int precision, int *kernels) {
+  fem::clear_error();
+  if (!b || !kernels) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (precision != FEM_PRECISION_FP64 && precision != FEM_PRECISION_MIXED)
+    return fem::fail(FEM_ERR_INVALID_ARGUMENT, "precision %d", precision);
+  for (int p = 1; p < kOrders; p++) kernels[p - 1] = variant_of(b, p, precision);
+  return FEM_SUCCESS;
+}
+
+int fem_batch_set_kernels(fem_batch *b, int precision, const int *kernels) {
+  fem::clear_error();
+  if (!b || !kernels) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (precision != FEM_PRECISION_FP64 && precision != FEM_PRECISION_MIXED)
+    return fem::fail(FEM_ERR_INVALID_ARGUMENT, "precision %d", precision);
+  for (int p = 1; p < kOrders; p++)
+    if (!variant_allowed(p, precision, kernels[p - 1]))
+      return fem::fail(FEM_ERR_INVALID_ARGUMENT, "kernel %d cannot serve order %d at precision %d", kernels[p - 1], p,
+                       precision);
+  for (int p = 1; p < kOrders; p++) b->kernel[prec_index(precision)][p] = kernels[p - 1];
+  drop_graph(b);
+  return FEM_SUCCESS;
+}
+
 int fem_batch_tune(fem_batch *b, int precision, void *stream, int reps, double *bestSeconds) {
   fem::clear_error();
   if (!b) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "batch is NULL");
@@ -424,34 +520,43 @@ int fem_batch_tune(fem_batch *b, int precision, void *stream, int reps, double *
   int st = check_ready(b, precision);
   if (st) return st;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  static const int cand[] = {1, 4, 16, 64, 256};
+  static const int lens[] = {1, 4, 16, 64, 256};
+  static const int variants[] = {FEM_KERNEL_ROWS, FEM_KERNEL_FRAGMENT_FP64, FEM_KERNEL_FRAGMENT_BF16X6,
+                                 FEM_KERNEL_ELEMENT_FP64, FEM_KERNEL_ELEMENT_FP32};
+  int *kern = b->kernel[prec_index(precision)];
   double total = 0;
   for (int p = 1; p < kOrders; p++) {
     if (!order_has_work(b, p)) continue;
     double best = 1e30;
-    int bestLen = b->tileBatches[p];
-    for (int len : cand) {
-      b->tileBatches[p] = len;
-      build_tiles(b);
-      if ((st = sync_device_state(b))) return st;
-      double secs = 0;
-      for (int r = 0; r <= reps; r++) {  // first run warms up
-        double one = 0;
-        st = fem::timed(s, &one, [&] {
-          cudaError_t err = cudaMemsetAsync(b->d_counters, 0, sizeof(int) * kOrders * kMaxColours, s);
-          if (err != cudaSuccess) return fem::cuda_fail(err, "cudaMemsetAsync");
-          return enqueue_order(b, p, precision, s);
-        });
-        if (st) return st;
-        if (r > 0) secs += one;
-      }
-      secs /= reps;
-      if (secs < best) {
-        best = secs;
-        bestLen = len;
+    int bestLen = b->tileBatches[p], bestVar = kern[p];
+    for (int v : variants) {
+      if (!variant_allowed(p, precision, v)) continue;
+      kern[p] = v;
+      for (int len : lens) {
+        b->tileBatches[p] = len;
+        build_tiles(b);
+        if ((st = sync_device_state(b))) return st;
+        double secs = 0;
+        for (int r = 0; r <= reps; r++) {  // first run warms up
+          double one = 0;
+          st = fem::timed(s, &one, [&] {
+            cudaError_t err = cudaMemsetAsync(b->d_counters, 0, sizeof(int) * kOrders * kMaxColours, s);
+            if (err != cudaSuccess) return fem::cuda_fail(err, "cudaMemsetAsync");
+            return enqueue_order(b, p, precision, s);
+          });
+          if (st) return st;
+          if (r > 0) secs += one;
+        }
+        secs /= reps;
+        if (secs < best) {
+          best = secs;
+          bestLen = len;
+          bestVar = v;
+        }
       }
     }
     b->tileBatches[p] = bestLen;
+    kern[p] = bestVar;
     total += best;
   }
   build_tiles(b);

@@ -116,6 +116,10 @@ int launch_frag_ranges(int order, int precision, int mode, const dev::AsmArgs &a
 // All colours of one plan in one dependency-ordered persistent launch (plan mode).
 int launch_frag_sched(int order, int precision, int mode, const dev::AsmArgs &a, const dev::SchedArgs &sa,
                       cudaStream_t s, int strain = FEM_STRAIN_LINEAR);
+// The batched colour launches of order p with an explicit kernel variant
+// (FEM_KERNEL_FRAGMENT_* / FEM_KERNEL_ELEMENT_*).
+int launch_batched_variant(int p, int variant, const dev::AsmArgs *meshes, const dev::Tile *tiles, int ntiles,
+                           int *counter, cudaStream_t s);
 // Its tile-queue form for batches and the server (residual and Jacobian).
 int launch_frag_batched(int order, int precision, const dev::AsmArgs *meshes, const dev::Tile *tiles, int ntiles,
                         int *counter, cudaStream_t s);

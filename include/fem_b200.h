@@ -241,10 +241,36 @@ int fem_batch_info(const fem_batch *batch, int64_t *totalElements, int64_t *numT
  * order's kernel shape. */
 int fem_batch_get_tiles(const fem_batch *batch, int *tileBatches);
 int fem_batch_set_tiles(fem_batch *batch, const int *tileBatches);
+/* Kernel variants of a batch, per order and precision.  FEM_KERNEL_DEFAULT is the
+ * single-mesh plan path's kernel (batched results then equal the plan's bit for
+ * bit); the others trade threads per element and elements per CTA:
+ *   ROWS           order 1: row assembly, each block row written once by its warp
+ *                  (meshes without row tables take the element kernel)
+ *   FRAGMENT_FP64  orders 2-4: two elements per warp in FP64 tensor-core fragments
+ *                  (16 threads per element, 8 elements per 4-warp CTA step)
+ *   FRAGMENT_BF16X6  order 3, MIXED: the same with the BF16x6 element stiffness
+ *   ELEMENT_FP64 / ELEMENT_FP32  every order: the shared-memory element kernel
+ *                  (thread groups of 64-128 threads over 1-8 elements, 1-4 groups
+ *                  per CTA), FP64 or (MIXED only) FP32 element products.
+ * A MIXED batch may run any FP64 variant: FP64 results are within its bound. */
+#define FEM_KERNEL_DEFAULT 0
+#define FEM_KERNEL_ROWS 1
+#define FEM_KERNEL_FRAGMENT_FP64 2
+#define FEM_KERNEL_FRAGMENT_BF16X6 3
+#define FEM_KERNEL_ELEMENT_FP64 4
+#define FEM_KERNEL_ELEMENT_FP32 5
+/* kernels[4] (orders 1..4) resolved (never DEFAULT) / set (DEFAULT allowed);
+ * FEM_ERR_INVALID_ARGUMENT for a variant that cannot serve its order at `precision`. */
+int fem_batch_get_kernels(const fem_batch *batch, int precision, int *kernels);
+int fem_batch_set_kernels(fem_batch *batch, int precision, const int *kernels);
 /* One assembly of every mesh, stream-ordered on `stream`. */
 int fem_batch_assemble(fem_batch *batch, int precision, void *stream, double *elapsedSeconds);
-/* Autotuner: per order, times the order's launches for each candidate tile
- * length (reps repetitions after a warm-up) and keeps the fastest. */
+/* Autotuner: per order, times the order's launches for every kernel variant the
+ * precision allows and every candidate tile length (1, 4, 16, 64, 256 element
+ * batches; reps repetitions after a warm-up) and keeps the fastest pair
+ * (fem_batch_get_kernels / fem_batch_get_tiles report it).  Replaces the
+ * (order, precision) reference tables of hand-tuned elements per block
+ * (element/FEKernels.h:1009-1028, 1104-1123). */
 int fem_batch_tune(fem_batch *batch, int precision, void *stream, int reps, double *bestSeconds);
 /* Captures one complete assembly into a CUDA graph (after one uncaptured warm-up
  * run on `stream`); fem_batch_replay launches it.  Rebinding arrays does not
