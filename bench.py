@@ -309,6 +309,12 @@ def run_ours(args):
     value = rate(ms)
     launches = plan.launches() * args.steps
     log(f"plan fp64 {ms:.3f} ms")
+    if args.profile_run:
+        # a short run for ncu captures: the headline launches only
+        plan.close()
+        if pg is not None:
+            pg.destroy_process_group()
+        return
 
     # end to end through the public API: pinned host state -> device, assemble, residual
     # -> pinned host, in one fem_plan_assemble_host call (state upload in node chunks,
@@ -894,6 +900,8 @@ def main():
     ap.add_argument("--bands", type=int, default=32, help="element bands / node chunks of the end-to-end call")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-run", action="store_true",
+                    help="time the headline launches only and print nothing (for ncu captures)")
     ap.add_argument("--peaks", action="store_true", help="print measured FP64/FP32/FP64-MMA/BF16-MMA peaks and exit")
     args = ap.parse_args()
     if args.peaks:
