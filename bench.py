@@ -303,18 +303,22 @@ def run_ours(args):
     def assemble(prec="fp64", strain="linear", r=res, m=mat):
         plan.assemble(d.states, d.coords, E, nu, t, r, m, precision=prec, strain=strain, stream=sptr)
 
+    if args.profile_run:
+        # a short run for ncu captures: only the launches of the chosen path
+        fn = {"jacobian": assemble, "mixed": lambda: assemble("mixed"),
+              "residual": lambda: plan.assemble(d.states, d.coords, E, nu, t, res, None, stream=sptr)}[args.profile_path]
+        log(f"{args.profile_path} {T.steps(fn, args.steps, args.warmup):.3f} ms")
+        plan.close()
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+
     # headline: FP64 plan assembly, exactly K steps after W warm-up steps
     with ClockSampler(local) as clk:
         ms = T.steps(assemble, args.steps, args.warmup)
     value = rate(ms)
     launches = plan.launches() * args.steps
     log(f"plan fp64 {ms:.3f} ms")
-    if args.profile_run:
-        # a short run for ncu captures: the headline launches only
-        plan.close()
-        if pg is not None:
-            pg.destroy_process_group()
-        return
 
     # end to end through the public API: pinned host state -> device, assemble, residual
     # -> pinned host, in one fem_plan_assemble_host call (state upload in node chunks,
@@ -547,7 +551,8 @@ def batched_measure(fem, dev, waves, steps, warmup, precisions):
     stream = torch.cuda.Stream(device=dev)
     sptr = stream.cuda_stream
     out = {"elements": 0, "ms": {p: 0.0 for p in precisions}, "ms_plain": 0.0, "launches": {p: 0 for p in precisions},
-           "tiles": {p: [] for p in precisions}, "errs": [], "wave_ms": {p: [] for p in precisions}}
+           "tiles": {p: [] for p in precisions}, "kernels": {p: [] for p in precisions}, "errs": [],
+           "wave_ms": {p: [] for p in precisions}}
 
     def ev_time(fn, reps):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -572,6 +577,7 @@ def batched_measure(fem, dev, waves, steps, warmup, precisions):
                 batch.bind(i, dm.states, dm.coords, m.E, m.nu, m.t, res[i], mat[i])
             batch.tune(precision=prec, stream=sptr, reps=2)
             out["tiles"][prec].append(batch.info()["tile_batches"])
+            out["kernels"][prec].append(batch.kernels(prec))
             batch.capture(precision=prec, stream=sptr)
             for _ in range(warmup):
                 batch.replay(stream=sptr)
@@ -644,9 +650,9 @@ def batch_leg(fem, dev, args, plain_single):
                      f"first in draw order within {args.leg_batch_gb:g} GB, one captured graph per precision"),
         "meshes": len(chosen), "elements": el, "elements_per_order": per_order,
         "fp64": {"elements_per_s": el / (r["ms"]["fp64"] * 1e-3), "ms_per_step": r["ms"]["fp64"],
-                 "tuned_tile_batches": r["tiles"]["fp64"][0]},
+                 "tuned_tile_batches": r["tiles"]["fp64"][0], "tuned_kernels": r["kernels"]["fp64"][0]},
         "mixed": {"elements_per_s": el / (r["ms"]["mixed"] * 1e-3), "ms_per_step": r["ms"]["mixed"],
-                  "tuned_tile_batches": r["tiles"]["mixed"][0],
+                  "tuned_tile_batches": r["tiles"]["mixed"][0], "tuned_kernels": r["kernels"]["mixed"][0],
                   "rel_frobenius_err_vs_fp64_max": max(r["errs"]) if r["errs"] else None},
         "plain_fp64_dropin_same_meshes": {"elements_per_s": el / (r["ms_plain"] * 1e-3), "ms_per_step": r["ms_plain"],
                                           "note": "zero the outputs, fem_run_jacobian per mesh"},
@@ -668,7 +674,7 @@ def serve_sweep(fem, srv, ids, meshes, states, outs, rates, seconds, rng):
         per_client = [[] for _ in meshes]
         for t, c in zip(arrivals, who):
             per_client[c].append(t)
-        lat, srv_lat, elems = [], [], [0]
+        lat, srv_lat, elems, sizes = [], [], [0], []
         lock = threading.Lock()
         t0 = time.perf_counter() + 0.05
         st0 = srv.stats()
@@ -686,6 +692,7 @@ def serve_sweep(fem, srv, ids, meshes, states, outs, rates, seconds, rng):
                 with lock:
                     lat.append(done - (t0 + t))
                     srv_lat.append(sl)
+                    sizes.append(meshes[c].num_elements)
                     elems[0] += meshes[c].num_elements
 
         threads = [threading.Thread(target=client, args=(c,)) for c in range(len(meshes)) if per_client[c]]
@@ -696,11 +703,18 @@ def serve_sweep(fem, srv, ids, meshes, states, outs, rates, seconds, rng):
         wall = time.perf_counter() - t0
         st1 = srv.stats()
         lat_ms = np.array(lat) * 1e3
+        sz = np.array(sizes)
+        by_size = {}
+        for name, lo, hi in (("small <3e4 el", 0, 3e4), ("medium 3e4-3e5 el", 3e4, 3e5), ("large >=3e5 el", 3e5, 1e12)):
+            sel = lat_ms[(sz >= lo) & (sz < hi)]
+            if sel.size:
+                by_size[name] = {"requests": int(sel.size), "p50_ms": float(np.percentile(sel, 50)),
+                                 "p99_ms": float(np.percentile(sel, 99))}
         sweep.append({"rate_req_s": rate, "requests": len(lat), "elements_per_s": elems[0] / wall,
                       "p50_ms": float(np.percentile(lat_ms, 50)), "p99_ms": float(np.percentile(lat_ms, 99)),
                       "server_p50_ms": float(np.percentile(np.array(srv_lat) * 1e3, 50)),
                       "server_p99_ms": float(np.percentile(np.array(srv_lat) * 1e3, 99)),
-                      "waves": st1["waves"] - st0["waves"], "wall_s": wall})
+                      "by_request_size": by_size, "waves": st1["waves"] - st0["waves"], "wall_s": wall})
     return sweep
 
 
@@ -816,6 +830,7 @@ def run_batch(args):
         "plain_fp64_single_mesh": {"elements_per_s": el / (r["ms_plain"] * 1e-3), "ms_per_step": r["ms_plain"]},
         "batched_over_plain": r["ms_plain"] / r["ms"][prec],
         "wave_graph_ms": r["wave_ms"][prec], "tuned_tile_batches": r["tiles"][prec],
+        "tuned_kernels": r["kernels"][prec],
         "mixed_rel_frobenius_err_max": max(r["errs"]) if r["errs"] else None,
         "gpu_launches": r["launches"][prec],
     }
@@ -901,7 +916,9 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-run", action="store_true",
-                    help="time the headline launches only and print nothing (for ncu captures)")
+                    help="time one path's launches only and print no JSON line (for ncu captures)")
+    ap.add_argument("--profile-path", default="jacobian", choices=["jacobian", "mixed", "residual"],
+                    help="the plan path of --profile-run (FP64 residual+Jacobian, MIXED, FP64 residual only)")
     ap.add_argument("--peaks", action="store_true", help="print measured FP64/FP32/FP64-MMA/BF16-MMA peaks and exit")
     args = ap.parse_args()
     if args.peaks:
