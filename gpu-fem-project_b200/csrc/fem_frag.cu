@@ -63,9 +63,9 @@
 
 // Resident CTAs per SM the register budget is sized for: 3 (168 registers) at
 // p = 3, where the 12 live stiffness accumulators need them, and at p = 4; 4 (128)
-// at p = 2.
+// at p = 2 and for the residual alone (no stiffness accumulators).
 #ifndef FEM_FRAG_MINB
-#define FEM_FRAG_MINB (P == 2 ? 4 : 3)
+#define FEM_FRAG_MINB ((P == 2 || (MODE & kJac) == 0) ? 4 : 3)
 #endif
 
 namespace fem {
@@ -95,7 +95,8 @@ using IC = std::integral_constant<int, V>;
 // Shared memory: CTA tables, then one region per warp.  DROP: drop-in mode (the
 // stage holds the reference element map rows, NN*NN ints per element, instead of
 // plan code records).  B16: the BF16x6 stiffness table follows the CTA tables.
-template <int P, bool DROP = false, bool NL = false, bool B16 = false>
+// JAC = false (residual only): no block staging slots.
+template <int P, bool DROP = false, bool NL = false, bool B16 = false, bool JAC = true>
 struct FragLayout {
   using F = FragDims<P>;
   static constexpr int K4 = F::K4, NTN = F::NTN, NQP = F::NQP, NN = F::NN;
@@ -120,7 +121,7 @@ struct FragLayout {
   static constexpr int NSLOT = F::IL ? 4 : 8;
   static constexpr size_t REDS = align16(STAGE + 2 * 2 * CS);  // double4 [NSLOT][32]: bulk-reduction sources
   // NONLINEAR: sign(s) x tangent modulus, double [2][NQP][2 (l)][8 (i, k, n)]
-  static constexpr size_t AT = align16(REDS + 32 * NSLOT * 32);
+  static constexpr size_t AT = align16(REDS + (JAC ? 32 * NSLOT * 32 : 0));
   static constexpr size_t warp_bytes = align16(AT + (NL ? 8 * 2 * NQP * 16 : 0));
   static constexpr size_t total = warps + F::WARPS * warp_bytes;
 };
@@ -555,7 +556,7 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
   constexpr bool NL = (MODE & kNL) != 0;
   constexpr bool B16 = (MODE & kB16) != 0;  // BF16x6 element stiffness
   using F = FragDims<P>;
-  using L = FragLayout<P, !PLAN, NL, B16>;
+  using L = FragLayout<P, !PLAN, NL, B16, (MODE & kJac) != 0>;
   constexpr int NN = F::NN, NQ = F::NQ, K4 = F::K4, NTN = F::NTN, NQP = F::NQP, CS = F::CS;
   constexpr int STG = L::CS;  // staged bytes per element: plan code record or map rows
   constexpr bool RES = (MODE & kRes) != 0, JAC = (MODE & kJac) != 0;
@@ -1401,7 +1402,7 @@ int launch_frag_p(const AsmArgs &a, cudaStream_t s) {
   using F = FragDims<P>;
   constexpr int NT = 32 * F::WARPS;
   auto kernel = frag_kernel<P, MODE>;
-  const size_t smem = FragLayout<P, (MODE & kPlan) == 0, (MODE & kNL) != 0, (MODE & kB16) != 0>::total;
+  const size_t smem = FragLayout<P, (MODE & kPlan) == 0, (MODE & kNL) != 0, (MODE & kB16) != 0, (MODE & kJac) != 0>::total;
   LaunchInfo li;
   int st = launch_info(kernel, NT, smem, li);
   if (st) return st;
@@ -1421,7 +1422,7 @@ int launch_frag_ranges_p(const AsmArgs &a, const RangeList &r, cudaStream_t s) {
   using F = FragDims<P>;
   constexpr int NT = 32 * F::WARPS;
   auto kernel = frag_ranges_kernel<P, MODE>;
-  const size_t smem = FragLayout<P, false, (MODE & kNL) != 0, (MODE & kB16) != 0>::total;
+  const size_t smem = FragLayout<P, false, (MODE & kNL) != 0, (MODE & kB16) != 0, (MODE & kJac) != 0>::total;
   LaunchInfo li;
   int st = launch_info(kernel, NT, smem, li);
   if (st) return st;
@@ -1461,7 +1462,7 @@ int launch_frag_sched_p(const AsmArgs &a, const SchedArgs &sa, cudaStream_t s) {
   using F = FragDims<P>;
   constexpr int NT = 32 * F::WARPS;
   auto kernel = frag_sched_kernel<P, MODE>;
-  const size_t smem = FragLayout<P, false, (MODE & kNL) != 0, (MODE & kB16) != 0>::total;
+  const size_t smem = FragLayout<P, false, (MODE & kNL) != 0, (MODE & kB16) != 0, (MODE & kJac) != 0>::total;
   LaunchInfo li;
   int st = launch_info(kernel, NT, smem, li);
   if (st) return st;
