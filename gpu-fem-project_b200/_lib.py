@@ -31,7 +31,7 @@ FEM_STRAIN_NONLINEAR = 1
 
 # batch kernel variants (fem_batch_get_kernels / fem_batch_set_kernels)
 FEM_KERNELS = {0: "default", 1: "rows", 2: "fragment_fp64", 3: "fragment_bf16x6", 4: "element_fp64",
-               5: "element_fp32"}
+               5: "element_fp32", 6: "element_tcgen05"}
 
 _i = C.c_int
 _i64 = C.c_int64
@@ -67,7 +67,7 @@ SIGNATURES = {
     "fem_plan_assemble_host": (_i, [_p, _p, _p, _p, _d, _d, _d, _p, _p, _p, _i, _i, _i, _p, _pd]),
     "fem_plan_set_schedule": (_i, [_p, _i, _i]),
     "fem_plan_get_schedule": (_i, [_p, _pi, _pi, _pi, _pi]),
-    "fem_plan_schedule_status": (_i, [_p, _p, _pi64]),
+    "fem_plan_wait_status": (_i, [_p, _p, _pi64]),
     "fem_plan_get_schedule_tables": (_i, [_p, _p, _p, _p, _p, _p, _p]),
     "fem_plan_set_schedule_waits": (_i, [_p, _i64, _i]),
     "fem_server_create": (_i, [_i64, _i, _i, C.POINTER(_p)]),

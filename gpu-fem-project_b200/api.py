@@ -210,10 +210,10 @@ class Plan:
         tile = 0: the default tile length."""
         check(lib.fem_plan_set_schedule(self._h, int(band), int(tile)), "fem_plan_set_schedule")
 
-    def schedule_status(self, stream=None) -> int:
+    def wait_status(self, stream=None) -> int:
         """Waits for the stream; in-kernel waits that ran out since the last call."""
         n = C.c_int64()
-        check(lib.fem_plan_schedule_status(self._h, _stream(stream), C.byref(n)), "fem_plan_schedule_status")
+        check(lib.fem_plan_wait_status(self._h, _stream(stream), C.byref(n)), "fem_plan_wait_status")
         return n.value
 
     def set_schedule_waits(self, wait_limit_ns=0, stall_group=-1):

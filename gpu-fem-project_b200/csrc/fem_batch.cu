@@ -15,7 +15,8 @@
 // kernel (two elements per warp: 16 threads per element, 8 elements per 4-warp
 // CTA step, FP64 MMA or, at order 3 MIXED, BF16x6 stiffness), the element kernel
 // (one thread group per EPG elements: Shape<P> threads per group, groups per CTA;
-// FP64 or, MIXED, FP32 element products), or order-1 row assembly.  MIXED may run
+// FP64 or, MIXED, FP32 element products, at order 4 MIXED also with its stiffness
+// as BF16x6 tcgen05 MMAs), or order-1 row assembly.  MIXED may run
 // any FP64 variant (FP64 is within its error bound); FP64 runs FP64 variants only.
 // The tuner also picks the tile length of the order's work queues.
 #include <cuda_runtime.h>
@@ -66,6 +67,27 @@ int launch_batched_t(int p, const dev::AsmArgs *meshes, const dev::Tile *tiles, 
   }
 }
 
+// The batched order-4 element kernel with its stiffness on the tcgen05 tensor cores.
+int launch_batched_umma(const dev::AsmArgs *meshes, const dev::Tile *tiles, int ntiles, int *counter,
+                        cudaStream_t s) {
+  using S = dev::Shape<4>;
+  constexpr int NT = S::GT * S::GPC;
+  constexpr int MODE = dev::kPlan | dev::kRes | dev::kJac | dev::kU;
+  auto kernel = dev::assemble_batched_kernel<4, float, MODE>;
+  const size_t smem = dev::Layout<4, float, MODE>::total;
+  LaunchInfo li;
+  int st = launch_info(kernel, NT, smem, li);
+  if (st) return st;
+  const int64_t need = (ntiles + S::GPC - 1) / S::GPC;
+  const int64_t cap = (int64_t)li.grid_per_sm * li.num_sms;
+  const int grid = (int)(need < cap ? need : cap);
+  if (grid <= 0) return FEM_SUCCESS;
+  kernel<<<grid, NT, smem, s>>>(meshes, tiles, ntiles, counter);
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return cuda_fail(err, "assemble_batched_kernel (tcgen05) launch");
+  return FEM_SUCCESS;
+}
+
 }  // namespace
 
 // The colour launches of order p with kernel variant v (never FEM_KERNEL_DEFAULT
@@ -79,6 +101,9 @@ int launch_batched_variant(int p, int v, const dev::AsmArgs *meshes, const dev::
       return launch_frag_batched(p, FEM_PRECISION_MIXED, meshes, tiles, ntiles, counter, s);
     case FEM_KERNEL_ELEMENT_FP64: return launch_batched_t<double>(p, meshes, tiles, ntiles, counter, s);
     case FEM_KERNEL_ELEMENT_FP32: return launch_batched_t<float>(p, meshes, tiles, ntiles, counter, s);
+    case FEM_KERNEL_ELEMENT_TCGEN05:
+      if (p != 4) return fail(FEM_ERR_INVALID_ARGUMENT, "tcgen05 element kernel: order 4 only");
+      return launch_batched_umma(meshes, tiles, ntiles, counter, s);
     default: return fail(FEM_ERR_INVALID_ARGUMENT, "kernel variant %d", v);
   }
 }
@@ -89,6 +114,8 @@ int launch_batched(int p, int precision, const dev::AsmArgs *meshes, const dev::
   if (frag_supported(p, precision, FEM_STRAIN_LINEAR, true))
     return launch_frag_batched(p, precision, meshes, tiles, ntiles, counter, s);
   if (precision == FEM_PRECISION_FP64) return launch_batched_t<double>(p, meshes, tiles, ntiles, counter, s);
+  if (precision == FEM_PRECISION_MIXED && p == 4 && umma_order4())
+    return launch_batched_umma(meshes, tiles, ntiles, counter, s);
   if (precision == FEM_PRECISION_MIXED) return launch_batched_t<float>(p, meshes, tiles, ntiles, counter, s);
   return fail(FEM_ERR_INVALID_ARGUMENT, "precision %d", precision);
 }
@@ -109,6 +136,7 @@ bool variant_allowed(int p, int precision, int v) {
     case FEM_KERNEL_FRAGMENT_BF16X6: return p == 3 && precision == FEM_PRECISION_MIXED;
     case FEM_KERNEL_ELEMENT_FP64: return true;
     case FEM_KERNEL_ELEMENT_FP32: return precision == FEM_PRECISION_MIXED;
+    case FEM_KERNEL_ELEMENT_TCGEN05: return p == 4 && precision == FEM_PRECISION_MIXED;
     default: return false;
   }
 }
@@ -119,7 +147,9 @@ int default_variant(int p, int precision) {
   if (p == 1) return FEM_KERNEL_ROWS;
   if (fem::frag_supported(p, precision, FEM_STRAIN_LINEAR, true))
     return fem::b16_stiffness(p, precision, FEM_STRAIN_LINEAR) ? FEM_KERNEL_FRAGMENT_BF16X6 : FEM_KERNEL_FRAGMENT_FP64;
-  return precision == FEM_PRECISION_MIXED ? FEM_KERNEL_ELEMENT_FP32 : FEM_KERNEL_ELEMENT_FP64;
+  if (precision == FEM_PRECISION_MIXED)
+    return p == 4 && fem::umma_order4() ? FEM_KERNEL_ELEMENT_TCGEN05 : FEM_KERNEL_ELEMENT_FP32;
+  return FEM_KERNEL_ELEMENT_FP64;
 }
 
 int prec_index(int precision) { return precision == FEM_PRECISION_MIXED ? 1 : 0; }
@@ -522,7 +552,7 @@ int fem_batch_tune(fem_batch *b, int precision, void *stream, int reps, double *
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   static const int lens[] = {1, 4, 16, 64, 256};
   static const int variants[] = {FEM_KERNEL_ROWS, FEM_KERNEL_FRAGMENT_FP64, FEM_KERNEL_FRAGMENT_BF16X6,
-                                 FEM_KERNEL_ELEMENT_FP64, FEM_KERNEL_ELEMENT_FP32};
+                                 FEM_KERNEL_ELEMENT_FP64, FEM_KERNEL_ELEMENT_FP32, FEM_KERNEL_ELEMENT_TCGEN05};
   int *kern = b->kernel[prec_index(precision)];
   double total = 0;
   for (int p = 1; p < kOrders; p++) {

@@ -32,6 +32,8 @@
 #include <cstdint>
 #include <type_traits>
 
+#include "fem_umma.cuh"
+
 namespace fem {
 namespace dev {
 
@@ -108,7 +110,9 @@ struct Vec2<float> {
 // kNL: GreenStrainType::NONLINEAR (Green strain, FP64 only); default LINEAR.
 // kB16: fragment kernel, element stiffness on BF16 tensor cores with three-way split
 // operands (FEM_PRECISION_MIXED at orders 2 and 3).
-enum : int { kRes = 1, kJac = 2, kPlan = 4, kNL = 8, kB16 = 32 };
+// kU: element kernel (order 4, FP32 element arithmetic), element stiffness as BF16x6
+// products on the fifth-generation tensor cores (tcgen05, accumulator in TMEM).
+enum : int { kRes = 1, kJac = 2, kPlan = 4, kNL = 8, kB16 = 32, kU = 64 };
 
 struct AsmArgs {
   // drop-in fields | order-1 plan row tables (a plan never reads the drop-in ones)
@@ -133,6 +137,7 @@ struct AsmArgs {
   double *mat;
   double mu, lam, t;
   int64_t begin, count;  // element (or list position, or row chunk) range of this launch
+  int *waits;            // plan: count of bounded in-kernel waits that ran out (nullptr: not counted)
 };
 
 // The output side of one batch: global outputs (registers) and the batch's
@@ -295,7 +300,15 @@ struct Layout {
                                                   : 16;
   static constexpr size_t stage = align16(rbase + 4 * EPG * NN);  // [2][STAGE] bytes
   static constexpr size_t group_bytes = align16(stage + 2 * align16(STAGE));
-  static constexpr size_t total = groups + S::GPC * group_bytes;
+  // kU: BF16 operand tiles [A, B][part hi, mid, lo][K-step 0, 1] (umma::kTileBytes
+  // each), the MMA-completion mbarrier and the TMEM base address
+  static constexpr bool UM = (MODE & kU) != 0;
+  static_assert(!UM || (P == 4 && !TC && !NL && S::GPC == 1 && S::EPG == 1 && S::GT == 128),
+                "tcgen05 stiffness: order 4, FP32 element arithmetic, one 128-thread group per CTA");
+  static constexpr size_t uop = (groups + S::GPC * group_bytes + 127) & ~size_t(127);
+  static constexpr size_t umbar = uop + (UM ? 12 * umma::kTileBytes : 0);
+  static constexpr size_t utmem = umbar + 8;
+  static constexpr size_t total = UM ? utmem + 8 : groups + S::GPC * group_bytes;
 };
 
 __device__ __forceinline__ void group_sync(int id, int nthreads) {
@@ -684,6 +697,21 @@ __device__ __forceinline__ void group_loop(unsigned char *smem, Src &src, const 
     cp_async_commit();
   };
 
+  // kU: zero the operand tiles once (their padding -- rows 2 NN..63 and K columns
+  // NQ..31 -- stays zero), set up the MMA-completion mbarrier, allocate 64 TMEM
+  // columns (the 64 x 64 FP32 accumulator)
+  uint32_t u_tmem = 0, u_phase = 0;
+  if constexpr (L::UM) {
+    uint4 *z = reinterpret_cast<uint4 *>(smem + L::uop);
+    for (int i = tg; i < 12 * umma::kTileBytes / 16; i += GT) z[i] = make_uint4(0u, 0u, 0u, 0u);
+    if (tg == 0) umma::mbar_init(reinterpret_cast<uint64_t *>(smem + L::umbar), 1);
+    if (warp == 0) umma::tmem_alloc(reinterpret_cast<uint32_t *>(smem + L::utmem), 64);
+    umma::fence_before_sync();
+    group_sync(bar, GT);
+    umma::fence_after_sync();
+    u_tmem = *reinterpret_cast<const uint32_t *>(smem + L::utmem);
+  }
+
   Cursor cur = src.first(tg, bar);
   prefetch(cur);
   stage_codes(cur, 0);
@@ -959,6 +987,97 @@ __device__ __forceinline__ void group_loop(unsigned char *smem, Src &src, const 
             }
           }
         }
+      } else if constexpr (L::UM) {
+        // tcgen05: M[(a,i),(b,j)] = sum_q H_i(q,a) G_j(q,b) as one 64 x 64 x 32 product per
+        // element (rows r = 2a + i and columns n = 2b + j padded from 50 to 64, K = the 25
+        // quadrature points padded to 32), each FP32 operand split into three BF16 parts
+        // and the six part products (lo.hi, hi.lo, mid.mid, mid.hi, hi.mid, hi.hi;
+        // ~FP32 accuracy, as the fragment kernel's order-3 form) accumulated in FP32 in
+        // TMEM: 12 MMAs of 64 x 64 x 16 issued by one thread.
+        unsigned char *uop = smem + L::uop;
+        uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + L::umbar);
+        const T2 *G = reinterpret_cast<const T2 *>(gs + L::G);
+        const T2 *H = reinterpret_cast<const T2 *>(gs + L::H);
+        // operands: (A = H | B = G, row r < 2 NN, chunk of 8 quadrature points)
+        constexpr int NR = 2 * NN, NCH = 4;
+        for (int it = tg; it < 2 * NR * NCH; it += GT) {
+          const int op = it / (NR * NCH), rem = it - op * NR * NCH;
+          const int r = rem / NCH, c = rem - (rem / NCH) * NCH;
+          const int a = r >> 1, i = r & 1;
+          const T2 *src_ = op ? G : H;
+          uint32_t w[3][4];
+#pragma unroll
+          for (int j = 0; j < 8; j += 2) {
+            float v2[2];
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+              const int q = 8 * c + j + h;
+              const T2 gv = q < NQ ? src_[q * NNP + a] : T2{0.0f, 0.0f};
+              v2[h] = i ? gv.y : gv.x;
+            }
+            uint32_t pk[3] = {0u, 0u, 0u};
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+              const __nv_bfloat16 hi = __float2bfloat16_rn(v2[h]);
+              const float r1 = v2[h] - __bfloat162float(hi);
+              const __nv_bfloat16 mid = __float2bfloat16_rn(r1);
+              const __nv_bfloat16 lo = __float2bfloat16_rn(r1 - __bfloat162float(mid));
+              pk[0] |= (uint32_t)__bfloat16_as_ushort(hi) << (16 * h);
+              pk[1] |= (uint32_t)__bfloat16_as_ushort(mid) << (16 * h);
+              pk[2] |= (uint32_t)__bfloat16_as_ushort(lo) << (16 * h);
+            }
+#pragma unroll
+            for (int pt = 0; pt < 3; pt++) w[pt][j >> 1] = pk[pt];
+          }
+#pragma unroll
+          for (int pt = 0; pt < 3; pt++) {
+            unsigned char *tile = uop + ((op * 3 + pt) * 2 + (c >> 1)) * umma::kTileBytes;
+            *reinterpret_cast<uint4 *>(tile + umma::tile_offset(r, 8 * (c & 1))) =
+                make_uint4(w[pt][0], w[pt][1], w[pt][2], w[pt][3]);
+          }
+        }
+        umma::fence_smem_to_async();
+        umma::fence_before_sync();
+        group_sync(bar, GT);
+        umma::fence_after_sync();
+        if (tg == 0) {
+          // smallest part products first: (A part, B part) = (lo, hi), (hi, lo), (mid, mid), (mid, hi), (hi, mid), (hi, hi)
+          constexpr int pa[6] = {2, 0, 1, 1, 0, 0}, pb[6] = {0, 2, 1, 0, 1, 0};
+          const uint32_t base = umma::smem_u32(uop);
+#pragma unroll
+          for (int k = 0; k < 6; k++)
+#pragma unroll
+            for (int ks = 0; ks < 2; ks++)
+              umma::mma_bf16(u_tmem, umma::smem_desc(base + ((0 * 3 + pa[k]) * 2 + ks) * umma::kTileBytes),
+                             umma::smem_desc(base + ((1 * 3 + pb[k]) * 2 + ks) * umma::kTileBytes),
+                             umma::kIdescBF16_M64N64, (k | ks) != 0);
+          umma::commit(mbar);
+        }
+        if (!umma::mbar_wait(mbar, u_phase, 1u << 20) && tg == 0 && M.waits) atomicAdd(M.waits, 1);
+        u_phase ^= 1u;
+        umma::fence_after_sync();
+        // epilogue: lanes 0-15 of warp w hold rows r = 16 w + lane; lane pairs (2a, 2a + 1)
+        // exchange their rows, lane 2a writes K(a, b), lane 2a + 1 writes K(b, a) (b > a)
+        const int r = 16 * warp + (lane & 15), a = r >> 1, iw = r & 1;
+        const bool rowv = lane < 16 && r < NR;
+#pragma unroll 1
+        for (int cc = 0; cc < 4; cc++) {
+          float v[16];
+          umma::tmem_ld16(u_tmem + ((uint32_t)(32 * warp) << 16) + 16 * cc, v);
+#pragma unroll
+          for (int jb = 0; jb < 8; jb++) {
+            const int b = 8 * cc + jb;
+            const float o0 = __shfl_xor_sync(0xffffffffu, v[2 * jb], 1);
+            const float o1 = __shfl_xor_sync(0xffffffffu, v[2 * jb + 1], 1);
+            if (!rowv || b >= NN || a > b || (iw == 1 && a == b)) continue;
+            const double mxx = iw ? o0 : v[2 * jb], mxy = iw ? o1 : v[2 * jb + 1];
+            const double myx = iw ? v[2 * jb] : o0, myy = iw ? v[2 * jb + 1] : o1;
+            const double kxx = (lam + 2.0 * mu) * mxx + mu * myy, kxy = lam * mxy + mu * myx;
+            const double kyx = lam * myx + mu * mxy, kyy = (lam + 2.0 * mu) * myy + mu * mxx;
+            write_block<P, MODE>(A, 0, a, b, iw, kxx, kxy, kyx, kyy);
+          }
+        }
+        umma::fence_before_sync();
       } else {
         // FP32 CUDA cores: one (p+1)-row tile x one column per thread, upper triangle
         const T2 *G = reinterpret_cast<const T2 *>(gs + L::G);
@@ -1011,6 +1130,11 @@ __device__ __forceinline__ void group_loop(unsigned char *smem, Src &src, const 
     buf ^= 1;
   }
   cp_async_wait_all();
+  if constexpr (L::UM) {
+    umma::fence_before_sync();
+    group_sync(bar, GT);
+    if (warp == 0) umma::tmem_dealloc(u_tmem, 64);
+  }
 }
 
 // Single mesh: A.count elements from A.begin, persistent grid-stride over batches.

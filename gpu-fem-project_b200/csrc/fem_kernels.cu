@@ -30,6 +30,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
+#include <string>
 #include <vector>
 
 #include "fem_common.h"
@@ -83,6 +85,16 @@ int launch_any(int order, int mode, const dev::AsmArgs &a, cudaStream_t s) {
 }
 }  // namespace
 
+// Order-4 MIXED element stiffness on the fifth-generation tensor cores (kU) unless
+// FEM_ORDER4_MIXED_STIFFNESS=fp32 selects the FP32 CUDA-core products.
+bool umma_order4() {
+  static const bool on = [] {
+    const char *v = std::getenv("FEM_ORDER4_MIXED_STIFFNESS");
+    return !(v && std::string(v) == "fp32");
+  }();
+  return on;
+}
+
 int launch(int order, int precision, int mode, const dev::AsmArgs &a, cudaStream_t s, int strain) {
   if (strain == FEM_STRAIN_NONLINEAR) {
     if (precision != FEM_PRECISION_FP64)
@@ -95,6 +107,16 @@ int launch(int order, int precision, int mode, const dev::AsmArgs &a, cudaStream
   if ((mode & dev::kPlan) == 0 && frag_supported(order, precision, strain, false))
     return launch_frag(order, precision, mode, a, s);
   if (precision == FEM_PRECISION_FP64) return launch_any<double>(order, mode, a, s);
+  if (precision == FEM_PRECISION_MIXED && order == 4 && (mode & dev::kJac) && umma_order4()) {
+    using namespace dev;
+    switch (mode) {
+      case kJac: return launch_p<4, float, kJac | kU>(a, s);
+      case kRes | kJac: return launch_p<4, float, kRes | kJac | kU>(a, s);
+      case kPlan | kJac: return launch_p<4, float, kPlan | kJac | kU>(a, s);
+      case kPlan | kRes | kJac: return launch_p<4, float, kPlan | kRes | kJac | kU>(a, s);
+      default: return fail(FEM_ERR_INVALID_ARGUMENT, "bad kernel mode %d", mode);
+    }
+  }
   if (precision == FEM_PRECISION_MIXED) return launch_any<float>(order, mode, a, s);
   return fail(FEM_ERR_INVALID_ARGUMENT, "precision %d", precision);
 }
@@ -151,6 +173,7 @@ void plan_free(fem_plan *p) {
   cudaFree(p->d_rowElem);
   cudaFree(p->d_rowChunk);
   cudaFree(p->d_sched);
+  cudaFree(p->d_waits);
   if (p->copyIn) cudaStreamDestroy(p->copyIn);
   if (p->copyOut) cudaStreamDestroy(p->copyOut);
   cudaSetDevice(cur);
@@ -417,7 +440,8 @@ int fem_plan_create(int elementOrder, int numNodes, const int *connPtr, const in
     p->nodeLo[k] = *std::min_element(c, c + hp.nn);
     p->nodeHi[k] = *std::max_element(c, c + hp.nn);
   }
-  if ((st = upload(hp.rowp, &p->d_rowp, p->deviceBytes)) || (st = upload(hp.cols, &p->d_cols, p->deviceBytes)) ||
+  if ((st = upload(std::vector<int>(1, 0), &p->d_waits, p->deviceBytes)) ||
+      (st = upload(hp.rowp, &p->d_rowp, p->deviceBytes)) || (st = upload(hp.cols, &p->d_cols, p->deviceBytes)) ||
       (st = upload(hp.connList, &p->d_connList, p->deviceBytes)) ||
       (st = upload(hp.blockCode, &p->d_blockCode, p->deviceBytes))) {
     plan_free(p);
@@ -485,19 +509,21 @@ int fem_plan_get_schedule_tables(const fem_plan *plan, int64_t *tileBegin, int *
   return FEM_SUCCESS;
 }
 
-int fem_plan_schedule_status(fem_plan *plan, void *stream, int64_t *timedOutWaits) {
+int fem_plan_wait_status(fem_plan *plan, void *stream, int64_t *timedOutWaits) {
   fem::clear_error();
   if (!plan || !timedOutWaits) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "NULL argument");
   *timedOutWaits = 0;
-  if (!plan->d_sched) return FEM_SUCCESS;
-  int v = 0;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  cudaError_t err = cudaMemcpyAsync(&v, plan->sched.status, sizeof(int), cudaMemcpyDeviceToHost, s);
+  int v[2] = {0, 0};
+  cudaError_t err = cudaMemcpyAsync(&v[0], plan->d_waits, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (err == cudaSuccess && plan->d_sched)
+    err = cudaMemcpyAsync(&v[1], plan->sched.status, sizeof(int), cudaMemcpyDeviceToHost, s);
   if (err == cudaSuccess) err = cudaStreamSynchronize(s);
-  if (err == cudaSuccess && v) err = cudaMemsetAsync(plan->sched.status, 0, sizeof(int), s);
-  if (err == cudaSuccess && v) err = cudaStreamSynchronize(s);
-  if (err != cudaSuccess) return fem::cuda_fail(err, "reading the schedule status");
-  *timedOutWaits = v;
+  if (err == cudaSuccess && v[0]) err = cudaMemsetAsync(plan->d_waits, 0, sizeof(int), s);
+  if (err == cudaSuccess && v[1]) err = cudaMemsetAsync(plan->sched.status, 0, sizeof(int), s);
+  if (err == cudaSuccess && (v[0] || v[1])) err = cudaStreamSynchronize(s);
+  if (err != cudaSuccess) return fem::cuda_fail(err, "reading the wait status");
+  *timedOutWaits = (int64_t)v[0] + v[1];
   return FEM_SUCCESS;
 }
 
@@ -601,7 +627,7 @@ int fem_plan_assemble_ex(const fem_plan *plan, const double *states, const doubl
     });
     if (st || !elapsedSeconds) return st;
     int64_t waits = 0;
-    const int st2 = fem_plan_schedule_status(const_cast<fem_plan *>(plan), stream, &waits);
+    const int st2 = fem_plan_wait_status(const_cast<fem_plan *>(plan), stream, &waits);
     if (st2) return st2;
     if (waits) return fem::fail(FEM_ERR_TIMEOUT, "%lld in-kernel waits of the dependency-ordered launch ran out",
                                 (long long)waits);

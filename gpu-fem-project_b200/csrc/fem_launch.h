@@ -89,6 +89,8 @@ int launch_mode(int order, const dev::AsmArgs &a, cudaStream_t s) {
 //   launch_nl       NONLINEAR kernels, FP64 (fem_nonlinear.cu)
 //   launch_batched  tile-queue kernels of batches and the server (fem_batch.cu)
 int launch(int order, int precision, int mode, const dev::AsmArgs &a, cudaStream_t s, int strain = FEM_STRAIN_LINEAR);
+// Whether the order-4 MIXED element stiffness runs on the tcgen05 tensor cores (kU).
+bool umma_order4();
 int launch_nl(int order, int mode, const dev::AsmArgs &a, cudaStream_t s);
 int launch_batched(int p, int precision, const dev::AsmArgs *meshes, const dev::Tile *tiles, int ntiles, int *counter,
                    cudaStream_t s);
@@ -184,6 +186,7 @@ struct fem_plan {
   std::vector<int> elemList, nodeLo, nodeHi;
   cudaStream_t copyIn = nullptr, copyOut = nullptr;  // created on first use
   int64_t deviceBytes = 0;
+  int *d_waits = nullptr;  // bounded in-kernel waits of this plan's launches that ran out
   // dependency-ordered assembly (fem_plan_set_schedule): schedBand == 0 runs colour launches
   int schedBand = 0, schedTile = 0, schedGroups = 0, schedTiles = 0;
   void *d_sched = nullptr;  // one allocation: tiles, tiles per group, dependency CSR, status words
@@ -194,6 +197,7 @@ struct fem_plan {
 namespace fem {
 // The plan's device tables in an argument block (inputs/outputs/material are the caller's).
 inline void plan_args(dev::AsmArgs &a, const fem_plan *p) {
+  a.waits = p->d_waits;
   a.connList = p->d_connList;
   a.blockCode = p->d_blockCode;
   a.rowp = p->d_rowp;

@@ -184,12 +184,15 @@ int fem_plan_get_schedule(const fem_plan *plan, int *bandElements, int *tileElem
  * numGroups + 1 entries), the groups it waits for.  Any pointer may be NULL. */
 int fem_plan_get_schedule_tables(const fem_plan *plan, int64_t *tileBegin, int *tileCount, int *tileGroup,
                                  int *groupTiles, int *depPtr, int *deps);
-/* Waits for `stream`, then returns (and clears) the number of in-kernel waits of
- * dependency-ordered launches on this plan that ran out since the last call.  A
- * wait gives up after waitLimitNs (default 0.5 s; the launch then finishes within
- * about one limit) and its assembly's results are invalid; with elapsedSeconds
- * non-NULL fem_plan_assemble checks this itself and returns FEM_ERR_TIMEOUT. */
-int fem_plan_schedule_status(fem_plan *plan, void *stream, int64_t *timedOutWaits);
+/* Waits for `stream`, then returns (and clears) the number of bounded in-kernel
+ * waits of this plan's launches that ran out since the last call: the dependency
+ * waits of dependency-ordered launches (each gives up after waitLimitNs, default
+ * 0.5 s; the launch then finishes within about one limit) and the tensor-core
+ * completion waits of the order-4 MIXED element kernel (2^20 polls).  An assembly
+ * with a wait that ran out has invalid results; with elapsedSeconds non-NULL a
+ * dependency-ordered fem_plan_assemble checks this itself and returns
+ * FEM_ERR_TIMEOUT. */
+int fem_plan_wait_status(fem_plan *plan, void *stream, int64_t *timedOutWaits);
 /* Failure injection for tests of the bounded waits: waitLimitNs > 0 sets the wait
  * limit; stallGroup >= 0 makes every wait on that group run out (its completion
  * can never be observed), -1 restores normal waits. */
@@ -252,6 +255,10 @@ int fem_batch_set_tiles(fem_batch *batch, const int *tileBatches);
  *   ELEMENT_FP64 / ELEMENT_FP32  every order: the shared-memory element kernel
  *                  (thread groups of 64-128 threads over 1-8 elements, 1-4 groups
  *                  per CTA), FP64 or (MIXED only) FP32 element products.
+ *   ELEMENT_TCGEN05  order 4, MIXED: the element kernel with its element stiffness
+ *                  as BF16x6 products on the fifth-generation tensor cores (one
+ *                  64 x 64 x 32 tcgen05 product per element, FP32 accumulator in
+ *                  TMEM); the single-mesh MIXED order-4 path runs it too.
  * A MIXED batch may run any FP64 variant: FP64 results are within its bound. */
 #define FEM_KERNEL_DEFAULT 0
 #define FEM_KERNEL_ROWS 1
@@ -259,6 +266,7 @@ int fem_batch_set_tiles(fem_batch *batch, const int *tileBatches);
 #define FEM_KERNEL_FRAGMENT_BF16X6 3
 #define FEM_KERNEL_ELEMENT_FP64 4
 #define FEM_KERNEL_ELEMENT_FP32 5
+#define FEM_KERNEL_ELEMENT_TCGEN05 6
 /* kernels[4] (orders 1..4) resolved (never DEFAULT) / set (DEFAULT allowed);
  * FEM_ERR_INVALID_ARGUMENT for a variant that cannot serve its order at `precision`. */
 int fem_batch_get_kernels(const fem_batch *batch, int precision, int *kernels);
@@ -326,7 +334,7 @@ typedef struct {
 
 /* Bytes of the library's file-scope device scratch array (the argument table of
  * up to 256 meshes, up to 16384 work-queue tiles and the queue counters). */
-#define FEM_STATIC_SCRATCH_BYTES 294912
+#define FEM_STATIC_SCRATCH_BYTES 299008
 
 /* fem_run_jacobian for up to 256 meshes of mixed orders in one batched pass
  * (one persistent launch per order present), for callers that cannot allocate

@@ -107,7 +107,7 @@ VARIANTS = {  # per order: the variants each precision may run
              ["fragment_fp64", "element_fp64"]],
     "mixed": [["rows", "element_fp64", "element_fp32"], ["fragment_fp64", "element_fp64", "element_fp32"],
               ["fragment_bf16x6", "fragment_fp64", "element_fp64", "element_fp32"],
-              ["element_fp32", "fragment_fp64", "element_fp64"]],
+              ["element_tcgen05", "fragment_fp64", "element_fp64", "element_fp32"]],
 }
 
 
@@ -138,8 +138,8 @@ def test_batch_every_kernel_variant(fem, orc, cuda, precision):
         torch.cuda.synchronize()
         for i, (m, (R0, A0)) in enumerate(zip(meshes, refs)):
             R, A = res[i].cpu().numpy(), mat[i].cpu().numpy()
-            reduced = names[m.order - 1] in ("fragment_bf16x6", "element_fp32")
-            if names[m.order - 1] == "element_fp32":  # FP32 gradients feed the residual too
+            reduced = names[m.order - 1] in ("fragment_bf16x6", "element_fp32", "element_tcgen05")
+            if names[m.order - 1] in ("element_fp32", "element_tcgen05"):  # FP32 gradients feed the residual too
                 assert np.linalg.norm(R - R0) <= 1e-6 * np.linalg.norm(R0), (names, i)
             else:
                 assert np.abs(R - R0).max() <= 1e-12 * np.abs(R0).max(), (names, i)

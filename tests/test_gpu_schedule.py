@@ -121,7 +121,7 @@ def test_schedule_equals_colour_launches(fem, orc, cuda, name, band):
             got = _outputs(fem, cuda, m, plan, *k)
             for x, y in zip(got, ref[k]):
                 assert (x is None and y is None) or np.array_equal(x, y), (k, band)
-        assert plan.schedule_status() == 0
+        assert plan.wait_status() == 0
         rowp, cols = plan.pattern()
         R0, A0 = orc.assemble(m, orc.element_bsr_map(m.conn_ptr, m.conn, m.nodes_per_element, rowp, cols), cols.size)
         R, A = ref[("fp64", "linear", True, True)]
@@ -151,8 +151,8 @@ def test_schedule_bounded_wait_runs_out_and_context_survives(fem, orc, cuda):
         assert ei.value.status == fem.FEM_ERR_TIMEOUT
         # asynchronous form: the count is read (and cleared) by schedule_status
         plan.assemble(d.states, d.coords, m.E, m.nu, m.t, res, mat)
-        assert plan.schedule_status() >= 1
-        assert plan.schedule_status() == 0
+        assert plan.wait_status() >= 1
+        assert plan.wait_status() == 0
         # normal waits again: the same context assembles correctly
         plan.set_schedule_waits(stall_group=-1)
         plan.assemble(d.states, d.coords, m.E, m.nu, m.t, res, mat, timed=True)
