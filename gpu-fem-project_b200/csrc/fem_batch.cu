@@ -78,6 +78,7 @@ int launch_batched_umma(const dev::AsmArgs *meshes, const dev::Tile *tiles, int 
   LaunchInfo li;
   int st = launch_info(kernel, NT, smem, li);
   if (st) return st;
+  umma_residency<4, float, MODE>(li);
   const int64_t need = (ntiles + S::GPC - 1) / S::GPC;
   const int64_t cap = (int64_t)li.grid_per_sm * li.num_sms;
   const int grid = (int)(need < cap ? need : cap);

@@ -888,8 +888,9 @@ __device__ __forceinline__ void group_loop(unsigned char *smem, Src &src, const 
     }
     group_sync(bar, GT);
 
-    // 2a. residual R_a = sum_q S(q) G_a(q), NPART lanes per node split the q sum
-    if constexpr ((MODE & kRes) != 0) {
+    // 2a. residual R_a = sum_q S(q) G_a(q), NPART lanes per node split the q sum (kU: run
+    // while the tensor cores form the element stiffness, below)
+    auto residual_stage = [&]() {
       for (int base = 0; base < EPG * NN * NPART; base += GT) {
         const int i = base + tg;
         const int ia = i / NPART, part = i - ia * NPART;
@@ -945,7 +946,8 @@ __device__ __forceinline__ void group_loop(unsigned char *smem, Src &src, const 
           }
         }
       }
-    }
+    };
+    if constexpr ((MODE & kRes) != 0 && !(L::UM && (MODE & kJac) != 0)) residual_stage();
 
     // 2b. element stiffness
     if constexpr ((MODE & kJac) != 0) {
@@ -998,11 +1000,13 @@ __device__ __forceinline__ void group_loop(unsigned char *smem, Src &src, const 
         uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + L::umbar);
         const T2 *G = reinterpret_cast<const T2 *>(gs + L::G);
         const T2 *H = reinterpret_cast<const T2 *>(gs + L::H);
-        // operands: (A = H | B = G, row r < 2 NN, chunk of 8 quadrature points)
+        // operands: (A = H | B = G, chunk of 8 quadrature points, row r < 2 NN), rows
+        // fastest: a quarter-warp stores eight consecutive rows' 16-byte K runs, eight
+        // distinct bank groups of one tile
         constexpr int NR = 2 * NN, NCH = 4;
         for (int it = tg; it < 2 * NR * NCH; it += GT) {
           const int op = it / (NR * NCH), rem = it - op * NR * NCH;
-          const int r = rem / NCH, c = rem - (rem / NCH) * NCH;
+          const int c = rem / NR, r = rem - c * NR;
           const int a = r >> 1, i = r & 1;
           const T2 *src_ = op ? G : H;
           uint32_t w[3][4];
@@ -1053,31 +1057,58 @@ __device__ __forceinline__ void group_loop(unsigned char *smem, Src &src, const 
                              umma::kIdescBF16_M64N64, (k | ks) != 0);
           umma::commit(mbar);
         }
-        if (!umma::mbar_wait(mbar, u_phase, 1u << 20) && tg == 0 && M.waits) atomicAdd(M.waits, 1);
+        if constexpr ((MODE & kRes) != 0) residual_stage();
+        // one thread waits for the MMAs (bounded), the group follows through its barrier
+        if (tg == 0 && !umma::mbar_wait(mbar, u_phase, 1u << 20) && M.waits) atomicAdd(M.waits, 1);
         u_phase ^= 1u;
+        umma::fence_before_sync();
+        group_sync(bar, GT);
         umma::fence_after_sync();
-        // epilogue: lanes 0-15 of warp w hold rows r = 16 w + lane; lane pairs (2a, 2a + 1)
-        // exchange their rows, lane 2a writes K(a, b), lane 2a + 1 writes K(b, a) (b > a)
-        const int r = 16 * warp + (lane & 15), a = r >> 1, iw = r & 1;
-        const bool rowv = lane < 16 && r < NR;
+        // epilogue: lanes 0-15 of warp w hold accumulator rows 16 w + lane; they stage
+        // the 2 NN valid rows in shared memory (over the operand tiles, free now), then
+        // all threads combine and write the upper-triangle blocks and their transposes
+        // The staging covers only A tiles (the first 6 x 2 KB): the next element rewrites
+        // their rows 0 .. 2 NN - 1 over all 32 K columns (zeros past NQ), and what stays in
+        // rows 2 NN .. 63 reaches only accumulator rows nobody reads; the B tiles keep
+        // their zero padding.
+        // staged row stride in floats: an odd number of float2 pairs, so that the 16 rows a
+        // warp stores land on 16 distinct bank pairs
+        constexpr int AS = (NN % 2) ? 2 * NN : 2 * NN + 2;
+        static_assert(NR * AS * 4 <= 6 * umma::kTileBytes, "staged accumulator fits the A operand tiles");
+        float *acc = reinterpret_cast<float *>(uop);
+        {
+          const int r = 16 * warp + (lane & 15);
 #pragma unroll 1
-        for (int cc = 0; cc < 4; cc++) {
-          float v[16];
-          umma::tmem_ld16(u_tmem + ((uint32_t)(32 * warp) << 16) + 16 * cc, v);
+          for (int cc = 0; cc < (NR + 15) / 16; cc++) {
+            float v[16];
+            umma::tmem_ld16(u_tmem + ((uint32_t)(32 * warp) << 16) + 16 * cc, v);
+            if (lane < 16 && r < NR) {
 #pragma unroll
-          for (int jb = 0; jb < 8; jb++) {
-            const int b = 8 * cc + jb;
-            const float o0 = __shfl_xor_sync(0xffffffffu, v[2 * jb], 1);
-            const float o1 = __shfl_xor_sync(0xffffffffu, v[2 * jb + 1], 1);
-            if (!rowv || b >= NN || a > b || (iw == 1 && a == b)) continue;
-            const double mxx = iw ? o0 : v[2 * jb], mxy = iw ? o1 : v[2 * jb + 1];
-            const double myx = iw ? v[2 * jb] : o0, myy = iw ? v[2 * jb + 1] : o1;
-            const double kxx = (lam + 2.0 * mu) * mxx + mu * myy, kxy = lam * mxy + mu * myx;
-            const double kyx = lam * myx + mu * mxy, kyy = (lam + 2.0 * mu) * myy + mu * mxx;
-            write_block<P, MODE>(A, 0, a, b, iw, kxx, kxy, kyx, kyy);
+              for (int j = 0; j < 16; j += 2)
+                if (16 * cc + j < NR)
+                  *reinterpret_cast<float2 *>(acc + r * AS + 16 * cc + j) = make_float2(v[j], v[j + 1]);
+            }
           }
         }
         umma::fence_before_sync();
+        group_sync(bar, GT);
+        constexpr int NUP = NN * (NN + 1) / 2;
+        for (int u = tg; u < NUP; u += GT) {
+          // u -> (a, b), a <= b, row-major over the upper triangle
+          int a = 0, rem = u;
+          while (rem >= NN - a) {
+            rem -= NN - a;
+            a++;
+          }
+          const int b = a + rem;
+          const float2 m0 = *reinterpret_cast<const float2 *>(acc + (2 * a) * AS + 2 * b);
+          const float2 m1 = *reinterpret_cast<const float2 *>(acc + (2 * a + 1) * AS + 2 * b);
+          const double mxx = m0.x, mxy = m0.y, myx = m1.x, myy = m1.y;
+          const double kxx = (lam + 2.0 * mu) * mxx + mu * myy, kxy = lam * mxy + mu * myx;
+          const double kyx = lam * myx + mu * mxy, kyy = (lam + 2.0 * mu) * myy + mu * mxx;
+          write_block<P, MODE>(A, 0, a, b, 0, kxx, kxy, kyx, kyy);
+          if (a != b) write_block<P, MODE>(A, 0, a, b, 1, kxx, kxy, kyx, kyy);
+        }
       } else {
         // FP32 CUDA cores: one (p+1)-row tile x one column per thread, upper triangle
         const T2 *G = reinterpret_cast<const T2 *>(gs + L::G);

@@ -85,12 +85,16 @@ int launch_any(int order, int mode, const dev::AsmArgs &a, cudaStream_t s) {
 }
 }  // namespace
 
-// Order-4 MIXED element stiffness on the fifth-generation tensor cores (kU) unless
-// FEM_ORDER4_MIXED_STIFFNESS=fp32 selects the FP32 CUDA-core products.
+// Order-4 MIXED element stiffness on the fifth-generation tensor cores (kU) when
+// FEM_ORDER4_MIXED_STIFFNESS=tcgen05; the FP32 CUDA-core products otherwise, the
+// faster form on B200 (2.63 against 3.44 ms for a 512^2 order-4 mesh: both forms
+// are bound by the shared-memory side of the L1 data pipe, and the BF16 operand
+// tiles and the staged accumulator add more of that traffic than the tensor cores
+// take off the FMA pipe).
 bool umma_order4() {
   static const bool on = [] {
     const char *v = std::getenv("FEM_ORDER4_MIXED_STIFFNESS");
-    return !(v && std::string(v) == "fp32");
+    return v && std::string(v) == "tcgen05";
   }();
   return on;
 }

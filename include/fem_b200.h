@@ -258,7 +258,9 @@ int fem_batch_set_tiles(fem_batch *batch, const int *tileBatches);
  *   ELEMENT_TCGEN05  order 4, MIXED: the element kernel with its element stiffness
  *                  as BF16x6 products on the fifth-generation tensor cores (one
  *                  64 x 64 x 32 tcgen05 product per element, FP32 accumulator in
- *                  TMEM); the single-mesh MIXED order-4 path runs it too.
+ *                  TMEM); the single-mesh MIXED order-4 path runs it when the
+ *                  environment sets FEM_ORDER4_MIXED_STIFFNESS=tcgen05 (read once
+ *                  per process), ELEMENT_FP32 otherwise.
  * A MIXED batch may run any FP64 variant: FP64 results are within its bound. */
 #define FEM_KERNEL_DEFAULT 0
 #define FEM_KERNEL_ROWS 1
