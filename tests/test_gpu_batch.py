@@ -109,8 +109,10 @@ VARIANTS = {  # per order: the variants each precision may run
              ["fragment_fp64", "element_fp64"]],
     "mixed": [["rows", "element_fp64", "element_fp32"], ["fragment_fp64", "element_fp64", "element_fp32"],
               ["fragment_bf16x6", "fragment_fp64", "element_fp64", "element_fp32"],
-              ["element_fp32", "element_tcgen05", "fragment_fp64", "element_fp64"]],
+              ["element_fp32", "fragment_fp64", "element_fp64"]],
 }
+if os.environ.get("FEM_ORDER4_MIXED_STIFFNESS") == "tcgen05":  # the opt-in tcgen05 order-4 stiffness
+    VARIANTS["mixed"][3].insert(1, "element_tcgen05")
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
