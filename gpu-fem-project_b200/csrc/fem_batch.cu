@@ -78,6 +78,7 @@ int launch_batched_umma(const dev::AsmArgs *meshes, const dev::Tile *tiles, int 
   LaunchInfo li;
   int st = launch_info(kernel, NT, smem, li);
   if (st) return st;
+  umma_residency<4, float, MODE>(li);
   const int64_t need = (ntiles + S::GPC - 1) / S::GPC;
   const int64_t cap = (int64_t)li.grid_per_sm * li.num_sms;
   const int grid = (int)(need < cap ? need : cap);
@@ -551,8 +552,6 @@ int fem_batch_tune(fem_batch *b, int precision, void *stream, int reps, double *
   if (st) return st;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   static const int lens[] = {1, 4, 16, 64, 256};
-  // the tcgen05 element kernel takes part only where FEM_ORDER4_MIXED_STIFFNESS=tcgen05
-  // opts in to it
   static const int variants[] = {FEM_KERNEL_ROWS, FEM_KERNEL_FRAGMENT_FP64, FEM_KERNEL_FRAGMENT_BF16X6,
                                  FEM_KERNEL_ELEMENT_FP64, FEM_KERNEL_ELEMENT_FP32, FEM_KERNEL_ELEMENT_TCGEN05};
   int *kern = b->kernel[prec_index(precision)];
@@ -563,7 +562,6 @@ int fem_batch_tune(fem_batch *b, int precision, void *stream, int reps, double *
     int bestLen = b->tileBatches[p], bestVar = kern[p];
     for (int v : variants) {
       if (!variant_allowed(p, precision, v)) continue;
-      if (v == FEM_KERNEL_ELEMENT_TCGEN05 && !fem::umma_order4()) continue;
       kern[p] = v;
       for (int len : lens) {
         b->tileBatches[p] = len;

@@ -543,10 +543,16 @@ struct QueueSource {
     }
     return c;
   }
+  // The second barrier keeps thread 0 from rewriting the slot (request(), when the
+  // first batch is also the tile's last) before every thread of the group has read
+  // it: a group whose threads took different tiles would mix two meshes' staged
+  // block codes and row bases.
   __device__ Cursor first(int tg, int) {
     if (tg == 0) *slot = atomicAdd(counter, 1);
     group_sync(bar, gt);
-    return from_tile(*slot);
+    const Cursor c = from_tile(*slot);
+    group_sync(bar, gt);
+    return c;
   }
   // Before the group barrier that precedes next(): grab the following tile when
   // this is the tile's last batch.

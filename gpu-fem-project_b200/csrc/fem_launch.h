@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <map>
 #include <mutex>
@@ -52,6 +53,14 @@ int launch_info(K kernel, int nt, size_t smem, LaunchInfo &out) {
   return FEM_SUCCESS;
 }
 
+// The occupancy query counts one CTA per SM for kernels that allocate tensor memory;
+// the tcgen05 element kernel holds 64 of an SM's 512 TMEM columns per CTA, so its
+// register and shared-memory limit (its minimum-blocks bound) is the real one.
+template <int P, typename T, int MODE>
+void umma_residency(LaunchInfo &li) {
+  if constexpr ((MODE & dev::kU) != 0) li.grid_per_sm = std::max(li.grid_per_sm, dev::min_blocks<P, T, MODE>());
+}
+
 template <int P, typename T, int MODE>
 int launch_p(const dev::AsmArgs &a, cudaStream_t s) {
   using S = dev::ShapeSel<P, MODE>;
@@ -61,6 +70,7 @@ int launch_p(const dev::AsmArgs &a, cudaStream_t s) {
   LaunchInfo li;
   int st = launch_info(kernel, NT, smem, li);
   if (st) return st;
+  umma_residency<P, T, MODE>(li);
   const int64_t groups = (a.count + S::EPG - 1) / S::EPG;
   const int64_t need = (groups + S::GPC - 1) / S::GPC;
   const int64_t cap = (int64_t)li.grid_per_sm * li.num_sms;

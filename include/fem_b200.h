@@ -260,9 +260,7 @@ int fem_batch_set_tiles(fem_batch *batch, const int *tileBatches);
  *                  64 x 64 x 32 tcgen05 product per element, FP32 accumulator in
  *                  TMEM); the single-mesh MIXED order-4 path runs it when the
  *                  environment sets FEM_ORDER4_MIXED_STIFFNESS=tcgen05 (read once
- *                  per process), ELEMENT_FP32 otherwise; the autotuner
- *                  considers it only then.  It runs at the residency the CUDA
- *                  occupancy query grants (one CTA per SM).
+ *                  per process), ELEMENT_FP32 otherwise.
  * A MIXED batch may run any FP64 variant: FP64 results are within its bound. */
 #define FEM_KERNEL_DEFAULT 0
 #define FEM_KERNEL_ROWS 1

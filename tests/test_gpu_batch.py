@@ -109,10 +109,8 @@ VARIANTS = {  # per order: the variants each precision may run
              ["fragment_fp64", "element_fp64"]],
     "mixed": [["rows", "element_fp64", "element_fp32"], ["fragment_fp64", "element_fp64", "element_fp32"],
               ["fragment_bf16x6", "fragment_fp64", "element_fp64", "element_fp32"],
-              ["element_fp32", "fragment_fp64", "element_fp64"]],
+              ["element_fp32", "element_tcgen05", "fragment_fp64", "element_fp64"]],
 }
-if os.environ.get("FEM_ORDER4_MIXED_STIFFNESS") == "tcgen05":  # the opt-in tcgen05 order-4 stiffness
-    VARIANTS["mixed"][3].insert(1, "element_tcgen05")
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
@@ -134,9 +132,13 @@ def test_batch_every_kernel_variant(fem, orc, cuda, precision):
     if precision == "mixed" and os.environ.get("FEM_ORDER4_MIXED_STIFFNESS") == "tcgen05":
         default[3] = "element_tcgen05"  # the library's order-4 MIXED default follows that switch
     assert batch.kernels(precision) == default
-    for k in range(4):
+    tiles0 = batch.info()["tile_batches"]
+    # each variant with the default tiles and with tiles of one element batch (a
+    # group's first batch is then its tile's last: the queue slot is rewritten at once)
+    for k, tiles in [(k, t) for k in range(4) for t in (tiles0, [1, 1, 1, 1])]:
         names = [v[min(k, len(v) - 1)] for v in VARIANTS[precision]]
         batch.set_kernels(names, precision)
+        batch.set_tiles(tiles)
         assert batch.kernels(precision) == names
         for r, a in zip(res, mat):
             r.fill_(float("nan"))
