@@ -261,6 +261,7 @@ void build_tiles(fem_batch *b) {
 
 int sync_device_state(fem_batch *b) {
   cudaError_t err;
+  const bool any = b->args_dirty || b->tiles_dirty;
   if (b->args_dirty) {
     err = cudaMemcpy(b->d_args, b->args.data(), sizeof(fem::dev::AsmArgs) * b->args.size(), cudaMemcpyHostToDevice);
     if (err != cudaSuccess) return fem::cuda_fail(err, "cudaMemcpy(mesh table)");
@@ -282,7 +283,8 @@ int sync_device_state(fem_batch *b) {
     }
     b->tiles_dirty = false;
   }
-  return FEM_SUCCESS;
+  // the batch's launches run on non-blocking streams: the tables must have landed
+  return any ? fem::uploads_visible("batch table upload") : (int)FEM_SUCCESS;
 }
 
 // The variant order p runs at `precision`.

@@ -331,6 +331,11 @@ int build_schedule(fem_plan *p, int band, int tile) {
     p->d_sched = nullptr;
     return fem::fail(FEM_ERR_CUDA, "schedule upload: %s", cudaGetErrorString(err));
   }
+  if (int st = fem::uploads_visible("schedule upload")) {
+    cudaFree(p->d_sched);
+    p->d_sched = nullptr;
+    return st;
+  }
   p->schedBand = band;
   p->schedTile = tile;
   p->schedGroups = G;
@@ -459,6 +464,10 @@ int fem_plan_create(int elementOrder, int numNodes, const int *connPtr, const in
       return st;
     }
     p->numChunks = (int)hp.rowChunk.size() - 1;
+  }
+  if ((st = fem::uploads_visible("fem_plan_create: table upload"))) {
+    plan_free(p);
+    return st;
   }
   *plan = p;
   return FEM_SUCCESS;

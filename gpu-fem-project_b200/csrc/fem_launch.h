@@ -136,6 +136,16 @@ int launch_batched_variant(int p, int variant, const dev::AsmArgs *meshes, const
 int launch_frag_batched(int order, int precision, const dev::AsmArgs *meshes, const dev::Tile *tiles, int ntiles,
                         int *counter, cudaStream_t s);
 
+// A synchronous cudaMemcpy from pageable host memory returns once the data is staged,
+// before the DMA has landed, and a synchronous cudaMemset only enqueues; both run on
+// the legacy default stream, which work on non-blocking streams (a caller's, the
+// batch's, the server's) does not wait for.  Tables written that way are fenced with
+// this before any kernel may read them.
+inline int uploads_visible(const char *what) {
+  const cudaError_t err = cudaStreamSynchronize(cudaStreamLegacy);
+  return err == cudaSuccess ? (int)FEM_SUCCESS : cuda_fail(err, what);
+}
+
 inline void set_material(dev::AsmArgs &a, double E, double nu, double t) {
   // element/FEKernels.h:300-301
   a.mu = 0.5 * E / (1.0 + nu);

@@ -432,6 +432,8 @@ int fem_server_add_mesh(fem_server *S, int elementOrder, int numNodes, const int
   if (err == cudaSuccess) err = cudaMalloc(&m.mat, 32 * plan->nnzb + 32);
   if (err == cudaSuccess) err = cudaMemcpy(m.coords, nodeCoords, vec, cudaMemcpyHostToDevice);
   if (err == cudaSuccess) err = cudaMemset(m.states, 0, vec);
+  // the lanes' streams do not wait for the legacy stream's copy and clear
+  if (err == cudaSuccess) err = cudaStreamSynchronize(cudaStreamLegacy);
   if (err != cudaSuccess) {
     cudaFree(m.coords);
     cudaFree(m.states);

@@ -104,6 +104,41 @@ def test_batch_tune_capture_replay(fem, cuda):
     batch.close()
 
 
+def test_batch_tables_reach_nonblocking_streams(fem, cuda):
+    """Tile and mesh tables rebuilt between runs (new tile lengths, the tuner) are in
+    place before launches on a non-blocking stream read them: results unchanged."""
+    import torch
+    specs = _specs(fem)
+    meshes, plans, devs, res, mat = _setup(fem, cuda, specs)
+    batch = fem.Batch(plans)
+    for i, (m, d) in enumerate(zip(meshes, devs)):
+        batch.bind(i, d.states, d.coords, m.E, m.nu, m.t, res[i], mat[i])
+    batch.assemble()
+    torch.cuda.synchronize()
+    ref = [(r.clone(), a.clone()) for r, a in zip(res, mat)]
+    stream = torch.cuda.Stream(device=cuda)  # created non-blocking
+    for tiles in ([1, 1, 1, 1], [256, 64, 16, 4], [4, 1, 64, 16], [16, 16, 16, 16]) * 3:
+        batch.set_tiles(tiles)
+        for r, a in zip(res, mat):
+            r.fill_(float("nan"))
+            a.fill_(float("nan"))
+        torch.cuda.synchronize()
+        batch.assemble(stream=stream.cuda_stream)
+        stream.synchronize()
+        for (r, a), (r0, a0) in zip(zip(res, mat), ref):
+            assert torch.equal(r, r0) and torch.equal(a, a0), tiles
+    batch.tune(stream=stream.cuda_stream, reps=1)
+    exact = batch.kernels("fp64") == ["rows", "fragment_fp64", "fragment_fp64", "fragment_fp64"]
+    batch.assemble(stream=stream.cuda_stream)
+    stream.synchronize()
+    for (r, a), (r0, a0) in zip(zip(res, mat), ref):
+        if exact:
+            assert torch.equal(r, r0) and torch.equal(a, a0)
+        else:
+            assert float((a - a0).abs().max()) <= 1e-12 * float(a0.abs().max())
+    batch.close()
+
+
 VARIANTS = {  # per order: the variants each precision may run
     "fp64": [["rows", "element_fp64"], ["fragment_fp64", "element_fp64"], ["fragment_fp64", "element_fp64"],
              ["fragment_fp64", "element_fp64"]],
