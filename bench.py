@@ -66,7 +66,7 @@ def make_mesh(mesh_mod, name):
 # and BF16x6 kernels move the same bytes) times 4: traffic grows with the element
 # count.
 MEASURED_TRAFFIC = {
-    ("square1024_p3", "frag_kernel<3"): 4 * 2.835e9,
+    ("square1024_p3", "frag_kernel<3", "colours"): 4 * 2.835e9,
 }
 
 
@@ -352,6 +352,12 @@ def run_ours(args):
         return pms
 
     path("plan_fp64", assemble)
+    layout = plan.layout()
+    if layout[0] == "pairs":
+        # the same launches with the element colouring (what batches and the server run)
+        plan.set_layout("colours")
+        path("plan_fp64_colour_layout", assemble)
+        plan.set_layout("pairs")
     ms_mixed = path("plan_mixed", lambda: assemble("mixed"))
     path("plan_fp64_nonlinear", lambda: assemble("fp64", "nonlinear"))
     path("plan_fp64_residual_only", lambda: plan.assemble(d.states, d.coords, E, nu, t, res, None, stream=sptr))
@@ -386,14 +392,16 @@ def run_ours(args):
     hbm, peak_kind = peaks()
     abytes = algorithmic_bytes(mesh, nnzb)
     label = kernel_label(plan, mesh.order, "fp64")
-    traffic = next((v for (w, k), v in MEASURED_TRAFFIC.items() if w == mesh.name and label.startswith(k)), None)
+    traffic = next((v for (w, k, lay), v in MEASURED_TRAFFIC.items()
+                    if w == mesh.name and label.startswith(k) and label.endswith(f"({lay} layout)")), None)
     achieved = abytes / (ms * 1e-3) / 1e9
     line = {
         "metric": "assembled elements/s (res+Jac)", "value": value, "unit": "elements/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": mesh.name, "order": mesh.order, "elements": nE, "dof": mesh.num_dof, "nnzb": nnzb,
-                   "path": "plan_fp64", "l2": "inputs and outputs larger than L2 (BSR values %.2f GB)" % (32 * nnzb / 1e9),
+                   "path": "plan_fp64", "layout": {"order": layout[0], "pairs": layout[1], "colours": layout[2]},
+                   "l2": "inputs and outputs larger than L2 (BSR values %.2f GB)" % (32 * nnzb / 1e9),
                    "parallelism": f"replicas{world}"},
         "dof_per_s": value * mesh.num_dof / nE,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
@@ -511,10 +519,12 @@ def kernel_label(plan, order, prec):
     # the fragment kernel serves orders 2-3 in both precisions (MIXED at order 3 with
     # its element stiffness as BF16x6 tensor-core products, at order 2 in FP64) and
     # order 4 in FP64; FP32 order 4 runs the element kernel
+    n = plan.launches(precision=prec)
+    lay = plan.layout()[0]
     if order == 3 and prec == "mixed":
-        return f"frag_kernel<{order}, BF16x6 stiffness> x {plan.num_colours} colour launches per step"
+        return f"frag_kernel<{order}, BF16x6 stiffness> x {n} colour launches per step ({lay} layout)"
     if order in (2, 3) or (order == 4 and prec == "fp64"):
-        return f"frag_kernel<{order}> x {plan.num_colours} colour launches per step"
+        return f"frag_kernel<{order}> x {n} colour launches per step ({lay} layout)"
     return f"assemble_kernel<{order}, float> x {plan.num_colours} colour launches per step"
 
 

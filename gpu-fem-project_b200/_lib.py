@@ -29,6 +29,10 @@ FEM_PRECISION_MIXED = 1
 FEM_STRAIN_LINEAR = 0
 FEM_STRAIN_NONLINEAR = 1
 
+# element order of the fragment kernel's single-mesh colour launches (fem_plan_set_layout)
+FEM_LAYOUT_COLOURS = 0
+FEM_LAYOUT_PAIRS = 1
+
 # batch kernel variants (fem_batch_get_kernels / fem_batch_set_kernels)
 FEM_KERNELS = {0: "default", 1: "rows", 2: "fragment_fp64", 3: "fragment_bf16x6", 4: "element_fp64",
                5: "element_fp32", 6: "element_tcgen05"}
@@ -55,6 +59,7 @@ SIGNATURES = {
     "fem_build_bsr_pattern": (_i, [_i, _p, _p, _i, _p, _p, _pi64]),
     "fem_build_element_bsr_map": (_i, [_p, _p, _i, _i, _p, _p, _p]),
     "fem_colour_elements": (_i, [_i, _p, _p, _i, _p, _pi]),
+    "fem_pair_layout": (_i, [_i, _i, _p, _p, _i, _p, _p, _pi, _pi64, _p, _pi]),
     "fem_bsr_spmv": (_i, [_i, _p, _p, _p, _p, _p, _p]),
     "fem_plan_create": (_i, [_i, _i, _p, _p, _i, C.POINTER(_p)]),
     "fem_plan_destroy": (_i, [_p]),
@@ -63,6 +68,8 @@ SIGNATURES = {
     "fem_plan_device_pattern": (_i, [_p, C.POINTER(_p), C.POINTER(_p)]),
     "fem_plan_assemble": (_i, [_p, _p, _p, _d, _d, _d, _p, _p, _i, _p, _pd]),
     "fem_plan_row_chunks": (_i, [_p, _pi]),
+    "fem_plan_set_layout": (_i, [_p, _i]),
+    "fem_plan_get_layout": (_i, [_p, _pi, _pi64, _pi]),
     "fem_plan_assemble_ex": (_i, [_p, _p, _p, _d, _d, _d, _p, _p, _i, _i, _p, _pd]),
     "fem_plan_assemble_host": (_i, [_p, _p, _p, _p, _d, _d, _d, _p, _p, _p, _i, _i, _i, _p, _pd]),
     "fem_plan_set_schedule": (_i, [_p, _i, _i]),

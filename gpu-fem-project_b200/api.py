@@ -12,6 +12,7 @@ import ctypes as C
 
 import numpy as np
 
+from . import _lib
 from ._lib import FEM_KERNELS, FEM_PRECISION_FP64, FEM_PRECISION_MIXED, FEM_STRAIN_LINEAR, FEM_STRAIN_NONLINEAR, check, lib
 
 _PRECISION = {"fp64": FEM_PRECISION_FP64, "mixed": FEM_PRECISION_MIXED}
@@ -137,6 +138,25 @@ def colour_elements(num_nodes, conn_ptr, conn):
     return colour, nc.value
 
 
+def pair_layout(order, num_nodes, conn_ptr, conn, codes=False):
+    """The pair layout of an order-2..4 plan (host): (elemList, colourPtr, numPairs,
+    codes uint8[numElements, codeStride] or None).  colourPtr is empty when the plan
+    has no pair layout."""
+    cp, cn = _np(conn_ptr, np.int32), _np(conn, np.int32)
+    ne = cp.size - 1
+    nn = (order + 1) ** 2
+    stride = (nn * nn + nn + 15) // 16 * 16
+    elist = np.zeros(max(ne, 1), np.int32)
+    cptr = np.zeros(65, np.int32)
+    nc, npairs, cs = C.c_int(0), C.c_int64(0), C.c_int(0)
+    rec = np.zeros((max(ne, 1), stride), np.uint8) if codes else None
+    check(lib.fem_pair_layout(int(order), int(num_nodes), cp.ctypes.data, cn.ctypes.data, ne, elist.ctypes.data,
+                              cptr.ctypes.data, C.byref(nc), C.byref(npairs),
+                              rec.ctypes.data if codes else None, C.byref(cs)), "fem_pair_layout")
+    assert not codes or cs.value == stride
+    return elist[:ne], cptr[:nc.value + 1] if nc.value else cptr[:0], npairs.value, (rec[:ne] if codes else None)
+
+
 def bsr_spmv(rowp, cols, values, x, y, stream=None):
     """y = A x on the device for the 2x2-block BSR matrix (rowp, cols, values)."""
     import torch
@@ -170,7 +190,18 @@ class Plan:
         dependency-ordered plan, else one per colour."""
         if self.row_chunks > 0 and _strain(strain) == FEM_STRAIN_LINEAR:
             return 1
-        return 1 if self.scheduled(strain, precision) else self.num_colours
+        if self.scheduled(strain, precision):
+            return 1
+        lay, _, pair_colours = self.layout()
+        return pair_colours if lay == "pairs" and self.fragment(strain, precision) else self.num_colours
+
+    def fragment(self, strain="linear", precision="fp64") -> bool:
+        """Whether assemble() runs the warp-fragment kernel (orders 2-3, order 4 in
+        FP64 LINEAR)."""
+        nl, fp64 = _strain(strain) != FEM_STRAIN_LINEAR, _prec(precision) == FEM_PRECISION_FP64
+        if nl:
+            return fp64 and self.order in (2, 3)
+        return self.order in (2, 3) or (self.order == 4 and fp64)
 
     def scheduled(self, strain="linear", precision="fp64") -> bool:
         """Whether assemble() runs all colours in one dependency-ordered launch: the
@@ -178,10 +209,7 @@ class Plan:
         and order 4 in FP64 LINEAR)."""
         if self.schedule()["groups"] == 0:
             return False
-        nl, fp64 = _strain(strain) != FEM_STRAIN_LINEAR, _prec(precision) == FEM_PRECISION_FP64
-        if nl:
-            return fp64 and self.order in (2, 3)
-        return self.order in (2, 3) or (self.order == 4 and fp64)
+        return self.fragment(strain, precision)
 
     def schedule(self):
         """The dependency-ordered schedule: band and tile lengths (elements), groups, tiles."""
@@ -204,6 +232,18 @@ class Plan:
               "fem_plan_get_schedule_tables")
         return {"tile_begin": begin, "tile_count": count, "tile_group": group, "group_tiles": gt, "dep_ptr": ptr,
                 "deps": deps[:int(ptr[-1])]}
+
+    def set_layout(self, layout):
+        """'pairs' (default where built) or 'colours': the element order of the
+        fragment kernel's single-mesh colour launches."""
+        code = {"colours": _lib.FEM_LAYOUT_COLOURS, "pairs": _lib.FEM_LAYOUT_PAIRS}[layout]
+        check(lib.fem_plan_set_layout(self._h, code), "fem_plan_set_layout")
+
+    def layout(self):
+        """(layout name, pairs formed, pair colours)."""
+        lay, npairs, ncol = C.c_int(), C.c_int64(), C.c_int()
+        check(lib.fem_plan_get_layout(self._h, C.byref(lay), C.byref(npairs), C.byref(ncol)), "fem_plan_get_layout")
+        return ("pairs" if lay.value == _lib.FEM_LAYOUT_PAIRS else "colours"), npairs.value, ncol.value
 
     def set_schedule(self, band=-1, tile=0):
         """band = -1: the default band (about 8 MB of blocks), 0: colour launches;

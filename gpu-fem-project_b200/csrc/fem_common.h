@@ -42,6 +42,17 @@ struct HostPlan {
   // one byte each}; rowChunk[numChunks+1] cuts the rows into chunks of at most
   // kRowChunkRows rows and kRowChunkBlocks blocks.  Empty when not applicable.
   std::vector<int> rowElemPtr, rowElem, rowChunk;
+  // Orders 2-4, pair layout of the fragment kernel's single-mesh assembly: elements
+  // paired with the neighbour across their right edge (its left edge, node for
+  // node), pairs coloured so that the pairs of one colour share no node, each
+  // colour listing its pairs (two consecutive positions, the pair's first element
+  // first) and then its unpaired elements.  Codes as above, in list order, so the
+  // second element of a pair adds to the blocks and residual rows of the shared
+  // edge that the first one stored.
+  int numPairColours = 0;
+  int64_t numPairs = 0;
+  std::vector<int> pairColourPtr, pairList, pairConnList;
+  std::vector<uint8_t> pairCode;
 };
 constexpr int kRowChunkRows = 32, kRowChunkBlocks = 320;
 int build_host_plan(int order, int numNodes, const int *connPtr, const int *conn, int numElements, HostPlan &hp);

@@ -253,6 +253,19 @@ __device__ __forceinline__ void frag_put(const Out &O, int el, int a, int b, int
   reinterpret_cast<double2 *>(stg)[1] = make_double2(v2, v3);
 }
 
+// Before the second element of a step writes.  In a plan's pair layout it shares an
+// edge with the first: where the first stored a shared block (a generic-proxy
+// 256-bit store) the second adds to it with a bulk reduction (async proxy, maybe
+// another lane), and where both add (an earlier colour stored it) the first one's
+// reduction must land first, or the two would round in either order.  So: wait
+// for this lane's reductions to complete, order the lanes, order the proxies.
+// Residual rows go generic store or atomic, then atomics: the barrier orders them.
+__device__ __forceinline__ void pair_order_fence() {
+  asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+  __syncwarp();
+  asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+
 __device__ __forceinline__ void bulk_add(double *gdst, const double *src, int bytes) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(src);
   asm volatile("cp.reduce.async.bulk.global.shared::cta.bulk_group.add.f64 [%0], [%1], %2;" ::"l"(gdst), "r"(sa),
@@ -812,6 +825,8 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
       constexpr int NPAIR = NTM * (NTM + 1) / 2;
       const int pa = 4 * (g & 1) + (g >> 1);  // pi(g)
       for (int el = 0; el < ne; el++) {
+        // pair layout: the first element's residual writes before the second's
+        if (PLAN && el > 0) __syncwarp();
         if constexpr (B16) {
           // BF16x6 element stiffness: M_ij = sum_q s G_i(q, a) G_j(q, b) as m16n8k16
           // products (k = quadrature points 0-15; rows a and columns b of the two node
@@ -914,6 +929,7 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
             // 2x2 blocks, four consecutive columns across the lanes t.  Blocks to add go
             // to the staging slots of the FP64 layout (node-tile pair (r, h) = (TA, TB);
             // the pair (1, 0) is the transposed half of (0, 1)) and leave as row runs.
+            if (PLAN && el > 0) pair_order_fence();
             asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
             __syncwarp();
 #pragma unroll
@@ -1070,6 +1086,7 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
         // reduced with one 128-byte bulk operation per run whose four blocks are adjacent in
         // the matrix, else one 32-byte operation per block.
         if constexpr (JAC && RUNS) {
+          if (PLAN && el > 0) pair_order_fence();
           // every lane's previous bulk reads of the staging slots are complete
           asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
           __syncwarp();
@@ -1124,6 +1141,7 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
         // stiffness blocks, order 2: lane (g, t) holds (a = 8TA + pi(g), b = 8TB + 4h + t),
         // each written (or added) on its own
         if constexpr (JAC && !RUNS) {
+          if (PLAN && el > 0) pair_order_fence();
           asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
           int k = 0, slot = 0;
           double *reds = redsW + 4 * lane;
@@ -1196,6 +1214,7 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
       double *reds = redsW + 4 * lane;
       int nw = 0;  // writes so far: ring position of the staging slot
       for (int el = 0; el < ne; el++) {
+        if (PLAN && el > 0) pair_order_fence();
         // residual R_(a,i'): lane partials rp over its quadrature points (with the
         // Jacobian, accumulated by the first three stiffness groups, which between them
         // form every column tile's fragments; alone, in a pass of its own), then a full

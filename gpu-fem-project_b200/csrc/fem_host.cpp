@@ -175,6 +175,125 @@ static void build_row_plan(HostPlan &hp) {
   hp.rowChunk.swap(chunk);
 }
 
+// Pair layout (HostPlan::pairColourPtr ...).  Element f is e's right neighbour when
+// f's nodes (0, ly) are e's nodes (P, ly) for every ly (tensor order: local node
+// a = ly (P + 1) + lx); elements are paired greedily in id order.  Units (pairs
+// and unpaired elements) are coloured greedily like the elements of the colour
+// layout; codes are computed per colour with the units in parallel (they share no
+// node) and the two elements of a pair in order.  Leaves the layout empty when
+// the units need more than 64 colours.
+static void build_pair_plan(const int *connPtr, const int *conn, HostPlan &hp) {
+  const int P = hp.order, P1 = P + 1, nn = hp.nn, nE = hp.numElements;
+  auto node = [&](int e, int lx, int ly) { return conn[connPtr[e] + ly * P1 + lx]; };
+  auto key = [](int a, int b) { return ((uint64_t)(uint32_t)a << 32) | (uint32_t)b; };
+  // left edge (corner nodes (0, 0), (0, P)) -> element, sorted for lookup
+  std::vector<std::pair<uint64_t, int>> left((size_t)nE);
+  for (int e = 0; e < nE; e++) left[e] = {key(node(e, 0, 0), node(e, 0, P)), e};
+  std::sort(left.begin(), left.end());
+  std::vector<int> partner((size_t)nE, -1);
+  std::vector<char> lead((size_t)nE, 0);
+  for (int e = 0; e < nE; e++) {
+    if (partner[e] >= 0) continue;
+    const uint64_t k = key(node(e, P, 0), node(e, P, P));
+    auto it = std::lower_bound(left.begin(), left.end(), std::make_pair(k, INT_MIN));
+    if (it == left.end() || it->first != k) continue;
+    if (it + 1 != left.end() && (it + 1)->first == k) continue;  // two elements share that left edge
+    const int f = it->second;
+    if (f == e || partner[f] >= 0) continue;
+    bool same = true;
+    for (int ly = 0; ly <= P && same; ly++) same = node(e, P, ly) == node(f, 0, ly);
+    if (!same) continue;
+    partner[e] = f;
+    partner[f] = e;
+    lead[e] = 1;
+  }
+  // units in order of their lead element, coloured greedily over node bit masks
+  std::vector<int> unitLead, unitColour;
+  std::vector<uint64_t> used((size_t)hp.numNodes, 0);
+  int nc = 0;
+  for (int e = 0; e < nE; e++) {
+    if (partner[e] >= 0 && !lead[e]) continue;
+    uint64_t m = 0;
+    for (int w = 0; w < (partner[e] >= 0 ? 2 : 1); w++) {
+      const int x = w ? partner[e] : e;
+      for (int i = connPtr[x]; i < connPtr[x + 1]; i++) m |= used[conn[i]];
+    }
+    if (~m == 0) return;  // more than 64 colours: no pair layout
+    const int c = __builtin_ctzll(~m);
+    nc = std::max(nc, c + 1);
+    for (int w = 0; w < (partner[e] >= 0 ? 2 : 1); w++) {
+      const int x = w ? partner[e] : e;
+      for (int i = connPtr[x]; i < connPtr[x + 1]; i++) used[conn[i]] |= (1ull << c);
+    }
+    unitLead.push_back(e);
+    unitColour.push_back(c);
+  }
+  // per colour: pairs, then unpaired elements
+  std::vector<int64_t> pairsOf((size_t)nc, 0), singlesOf((size_t)nc, 0);
+  for (size_t u = 0; u < unitLead.size(); u++)
+    (partner[unitLead[u]] >= 0 ? pairsOf : singlesOf)[unitColour[u]]++;
+  hp.pairColourPtr.assign((size_t)nc + 1, 0);
+  for (int c = 0; c < nc; c++) hp.pairColourPtr[c + 1] = hp.pairColourPtr[c] + (int)(2 * pairsOf[c] + singlesOf[c]);
+  hp.pairList.assign((size_t)nE, -1);
+  std::vector<int64_t> fillP((size_t)nc), fillS((size_t)nc);
+  for (int c = 0; c < nc; c++) {
+    fillP[c] = hp.pairColourPtr[c];
+    fillS[c] = hp.pairColourPtr[c] + 2 * pairsOf[c];
+  }
+  // unit start positions (a pair's two elements are consecutive)
+  std::vector<int64_t> unitPos(unitLead.size());
+  for (size_t u = 0; u < unitLead.size(); u++) {
+    const int e = unitLead[u], c = unitColour[u];
+    if (partner[e] >= 0) {
+      unitPos[u] = fillP[c];
+      hp.pairList[fillP[c]++] = e;
+      hp.pairList[fillP[c]++] = partner[e];
+    } else {
+      unitPos[u] = fillS[c];
+      hp.pairList[fillS[c]++] = e;
+    }
+  }
+  hp.pairConnList.resize((size_t)nE * nn);
+  hp.pairCode.assign((size_t)nE * hp.codeStride, 0);
+  std::vector<uint8_t> blockWritten((size_t)hp.nnzb, 0), nodeWritten((size_t)hp.numNodes, 0);
+  // units grouped by colour, in list order
+  std::vector<std::vector<int>> byColour((size_t)nc);
+  for (size_t u = 0; u < unitLead.size(); u++) byColour[unitColour[u]].push_back((int)u);
+  for (int c = 0; c < nc; c++) {
+    const std::vector<int> &units = byColour[c];
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)units.size(); i++) {
+      const int u = units[i];
+      const int e0 = unitLead[u];
+      const int n = partner[e0] >= 0 ? 2 : 1;
+      for (int w = 0; w < n; w++) {
+        const int64_t k = unitPos[u] + w;
+        const int e = hp.pairList[k];
+        const int *en = conn + connPtr[e];
+        int *cl = &hp.pairConnList[(size_t)k * nn];
+        uint8_t *rec = &hp.pairCode[(size_t)k * hp.codeStride];
+        for (int a = 0; a < nn; a++) cl[a] = en[a];
+        for (int a = 0; a < nn; a++) {
+          const int r = en[a];
+          rec[nn * nn + a] = nodeWritten[r] ? 0 : 1;
+          nodeWritten[r] = 1;
+          const int *c0 = hp.cols.data() + hp.rowp[r], *c1 = hp.cols.data() + hp.rowp[r + 1];
+          for (int b = 0; b < nn; b++) {
+            const int *pos = std::lower_bound(c0, c1, en[b]);  // present: the colour layout found it
+            uint8_t &bf = blockWritten[(size_t)(pos - hp.cols.data())];
+            rec[a * nn + b] = (uint8_t)((pos - c0) | (bf ? 0 : 0x80));
+            bf = 1;
+          }
+        }
+      }
+    }
+  }
+  hp.numPairColours = nc;
+  int64_t np = 0;
+  for (int c = 0; c < nc; c++) np += pairsOf[c];
+  hp.numPairs = np;
+}
+
 int build_host_plan(int order, int numNodes, const int *connPtr, const int *conn, int numElements, HostPlan &hp) {
   const int nn = (order + 1) * (order + 1);
   int st = validate_mesh(numNodes, connPtr, conn, numElements);
@@ -242,6 +361,7 @@ int build_host_plan(int order, int numNodes, const int *connPtr, const int *conn
   }
   if (bad) return fail(FEM_ERR_UNSUPPORTED, "a BSR row holds more than 128 blocks; use the map-based entry points");
   if (order == 1) build_row_plan(hp);
+  if (order >= 2) build_pair_plan(connPtr, conn, hp);
   return FEM_SUCCESS;
 }
 
@@ -312,6 +432,27 @@ int fem_colour_elements(int numNodes, const int *connPtr, const int *conn, int n
                         int *numColours) {
   fem::clear_error();
   return fem::colour_greedy(numNodes, connPtr, conn, numElements, colour, numColours);
+}
+
+int fem_pair_layout(int elementOrder, int numNodes, const int *connPtr, const int *conn, int numElements,
+                    int *elemList, int *colourPtr, int *numColours, int64_t *numPairs, uint8_t *codes,
+                    int *codeStride) {
+  fem::clear_error();
+  if (!elemList || !colourPtr || !numColours || !numPairs)
+    return fem::fail(FEM_ERR_INVALID_ARGUMENT, "NULL output");
+  if (elementOrder < 2 || elementOrder > 4)
+    return fem::fail(FEM_ERR_INVALID_ORDER, "pair layout: orders 2..4 (order %d)", elementOrder);
+  fem::HostPlan hp;
+  int st = fem::build_host_plan(elementOrder, numNodes, connPtr, conn, numElements, hp);
+  if (st) return st;
+  *numColours = hp.numPairColours;
+  *numPairs = hp.numPairs;
+  if (codeStride) *codeStride = hp.codeStride;
+  if (hp.numPairColours == 0) return FEM_SUCCESS;
+  std::copy(hp.pairList.begin(), hp.pairList.end(), elemList);
+  std::copy(hp.pairColourPtr.begin(), hp.pairColourPtr.end(), colourPtr);
+  if (codes) std::copy(hp.pairCode.begin(), hp.pairCode.end(), codes);
+  return FEM_SUCCESS;
 }
 
 }  // extern "C"

@@ -173,6 +173,8 @@ void plan_free(fem_plan *p) {
   cudaFree(p->d_cols);
   cudaFree(p->d_connList);
   cudaFree(p->d_blockCode);
+  cudaFree(p->d_pairConnList);
+  cudaFree(p->d_pairCode);
   cudaFree(p->d_rowElemPtr);
   cudaFree(p->d_rowElem);
   cudaFree(p->d_rowChunk);
@@ -465,6 +467,17 @@ int fem_plan_create(int elementOrder, int numNodes, const int *connPtr, const in
     }
     p->numChunks = (int)hp.rowChunk.size() - 1;
   }
+  if (hp.numPairColours > 0) {
+    if ((st = upload(hp.pairConnList, &p->d_pairConnList, p->deviceBytes)) ||
+        (st = upload(hp.pairCode, &p->d_pairCode, p->deviceBytes))) {
+      plan_free(p);
+      return st;
+    }
+    p->pairColourPtr = hp.pairColourPtr;
+    p->numPairColours = hp.numPairColours;
+    p->numPairs = hp.numPairs;
+    p->usePairs = true;
+  }
   if ((st = fem::uploads_visible("fem_plan_create: table upload"))) {
     plan_free(p);
     return st;
@@ -646,16 +659,45 @@ int fem_plan_assemble_ex(const fem_plan *plan, const double *states, const doubl
                                 (long long)waits);
     return st;
   }
+  // the fragment kernel runs the pair layout (a step's two elements share an edge,
+  // so the lines of the rows they share are written while they are still in L2)
+  const bool pairs = frag && plan->usePairs && plan->numPairColours > 0;
+  if (pairs) {
+    a.connList = plan->d_pairConnList;
+    a.blockCode = plan->d_pairCode;
+  }
+  const std::vector<int> &cptr = pairs ? plan->pairColourPtr : plan->colourPtr;
+  const int ncol = pairs ? plan->numPairColours : plan->numColours;
   return fem::timed(s, elapsedSeconds, [&] {
-    for (int c = 0; c < plan->numColours; c++) {
-      a.begin = plan->colourPtr[c];
-      a.count = plan->colourPtr[c + 1] - plan->colourPtr[c];
+    for (int c = 0; c < ncol; c++) {
+      a.begin = cptr[c];
+      a.count = cptr[c + 1] - cptr[c];
       int st = frag ? fem::launch_frag(plan->order, precision, mode, a, s, strainType)
                     : fem::launch(plan->order, precision, mode, a, s, strainType);
       if (st) return st;
     }
     return (int)FEM_SUCCESS;
   });
+}
+
+int fem_plan_set_layout(fem_plan *plan, int layout) {
+  fem::clear_error();
+  if (!plan) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "plan is NULL");
+  if (layout != FEM_LAYOUT_COLOURS && layout != FEM_LAYOUT_PAIRS)
+    return fem::fail(FEM_ERR_INVALID_ARGUMENT, "layout %d", layout);
+  if (layout == FEM_LAYOUT_PAIRS && plan->numPairColours == 0)
+    return fem::fail(FEM_ERR_UNSUPPORTED, "this plan has no pair layout (order 1, or its pairs need > 64 colours)");
+  plan->usePairs = layout == FEM_LAYOUT_PAIRS;
+  return FEM_SUCCESS;
+}
+
+int fem_plan_get_layout(const fem_plan *plan, int *layout, int64_t *numPairs, int *numPairColours) {
+  fem::clear_error();
+  if (!plan) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "plan is NULL");
+  if (layout) *layout = plan->usePairs ? FEM_LAYOUT_PAIRS : FEM_LAYOUT_COLOURS;
+  if (numPairs) *numPairs = plan->numPairs;
+  if (numPairColours) *numPairColours = plan->numPairColours;
+  return FEM_SUCCESS;
 }
 
 // Host-buffer assembly with the copies overlapped: see include/fem_b200.h.  The

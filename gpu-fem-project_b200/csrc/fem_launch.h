@@ -198,6 +198,14 @@ struct fem_plan {
   std::vector<int> colourPtr;
   int *d_rowp = nullptr, *d_cols = nullptr, *d_connList = nullptr;
   uint8_t *d_blockCode = nullptr;  // per-element code records (Dims<P>::CS bytes each)
+  // orders 2-4: pair layout of the fragment kernel's single-mesh colour launches
+  // (HostPlan::pairColourPtr ...); usePairs selects it (fem_plan_set_layout)
+  int *d_pairConnList = nullptr;
+  uint8_t *d_pairCode = nullptr;
+  std::vector<int> pairColourPtr;
+  int numPairColours = 0;
+  int64_t numPairs = 0;
+  bool usePairs = false;
   // order 1: row assembly tables (HostPlan::rowElemPtr/rowElem/rowChunk); numChunks == 0: none
   int *d_rowElemPtr = nullptr, *d_rowElem = nullptr, *d_rowChunk = nullptr;
   int numChunks = 0;

@@ -128,6 +128,17 @@ int fem_build_element_bsr_map(const int *connPtr, const int *conn, int numElemen
  * counterpart: the reference scatters with atomics only.) */
 int fem_colour_elements(int numNodes, const int *connPtr, const int *conn, int numElements, int *colour,
                         int *numColours);
+/* The pair layout a plan of order 2-4 builds for its single-mesh fragment-kernel
+ * launches (fem_plan_set_layout), computed on the host: elemList[numElements]
+ * (pairs first within each colour, a pair's elements consecutive),
+ * colourPtr[numColours + 1] (at most 65 entries), the pairs formed and, when
+ * codes != NULL, the code records (numElements * codeStride bytes: per listed
+ * element, [a*nn + b] = rank of block (a, b) in row conn[a] | 0x80 for its first
+ * contributor, [nn*nn + a] = 1 for the first writer of node a's residual).
+ * numColours = 0: no pair layout (more than 64 colours).  (No reference counterpart.) */
+int fem_pair_layout(int elementOrder, int numNodes, const int *connPtr, const int *conn, int numElements,
+                    int *elemList, int *colourPtr, int *numColours, int64_t *numPairs, uint8_t *codes,
+                    int *codeStride);
 
 /* y = A x for a 2x2-block BSR matrix on the device (rowp/cols/A/x/y device
  * pointers).  Consumer of the assembled Jacobian (the reference exports the
@@ -154,6 +165,24 @@ int fem_plan_get_pattern(const fem_plan *plan, int *rowp, int *cols);
 /* Row chunks of an order-1 plan: > 0 when its LINEAR assembly runs as row
  * assembly (one launch, each block row written once), 0 when it runs by colours. */
 int fem_plan_row_chunks(const fem_plan *plan, int *numChunks);
+/* Element order of the single-mesh colour launches that the warp-fragment kernel
+ * runs (orders 2-4; fem_plan_assemble without a schedule):
+ *   FEM_LAYOUT_PAIRS    (default where built) each element is paired with the
+ *                       neighbour across its right edge (that element's left edge,
+ *                       node for node); pairs are coloured so that one colour's
+ *                       pairs share no node, and a warp assembles a pair in one
+ *                       step, the second element adding to the shared edge's
+ *                       blocks the first one stored, so that the rows the two
+ *                       share are written while their lines are in L2;
+ *   FEM_LAYOUT_COLOURS  the element colouring above (what every other path runs).
+ * The results agree to rounding: a block's contributions are added in another
+ * order where more than two elements share it.  fem_plan_get_layout also reports
+ * the pairs formed and their colours (0, 0 when the plan has no pair layout).
+ * (No reference counterpart.) */
+#define FEM_LAYOUT_COLOURS 0
+#define FEM_LAYOUT_PAIRS 1
+int fem_plan_set_layout(fem_plan *plan, int layout);
+int fem_plan_get_layout(const fem_plan *plan, int *layout, int64_t *numPairs, int *numPairColours);
 /* Device pointers of the plan's rowp/cols (owned by the plan). */
 int fem_plan_device_pattern(const fem_plan *plan, const int **rowp, const int **cols);
 /* states/nodeCoords/residual/matEntries are device pointers; residual or

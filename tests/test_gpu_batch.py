@@ -43,6 +43,8 @@ def test_batch_equals_alone_bitwise(fem, orc, cuda, precision):
     for i, (m, p, d) in enumerate(zip(meshes, plans, devs)):
         r1 = torch.full_like(res[i], 5.0)
         a1 = torch.full_like(mat[i], 5.0)
+        if m.order > 1:
+            p.set_layout("colours")  # batches run the colour layout
         p.assemble(d.states, d.coords, m.E, m.nu, m.t, r1, a1, precision=precision)
         torch.cuda.synchronize()
         assert np.array_equal(r1.cpu().numpy(), batched[i][0]), i

@@ -110,6 +110,7 @@ def test_schedule_equals_colour_launches(fem, orc, cuda, name, band):
         if m.order == 3:
             modes.append(("mixed", "linear", True, True))
         plan.set_schedule(0)
+        plan.set_layout("colours")  # the schedule orders the colour layout's groups
         ref = {k: _outputs(fem, cuda, m, plan, *k) for k in modes}
         if band:
             plan.set_schedule(band, 2 if band <= 6 else 0)

@@ -19,6 +19,8 @@ def _alone(fem, cuda, m, x, precision):
     """Residual and A*x of m assembled by its own plan (single-mesh path)."""
     import torch
     p = fem.Plan(m.order, m.num_nodes, m.conn_ptr, m.conn)
+    if m.order > 1:
+        p.set_layout("colours")  # the server runs the colour layout
     d = fem.DeviceMesh(m, cuda)
     r = torch.empty(m.num_nodes * 2, dtype=torch.float64, device=cuda)
     a = torch.empty(p.nnzb * 4, dtype=torch.float64, device=cuda)
