@@ -46,11 +46,9 @@ struct HostPlan {
   // paired with the neighbour across their right edge (its left edge, node for
   // node), pairs coloured so that the pairs of one colour share no node, each
   // colour listing its pairs (two consecutive positions, the pair's first element
-  // first) and then its unpaired elements.  Codes as above, in list order, except
-  // that a pair's first element hands the blocks between its right-edge nodes and
-  // its right-edge residual rows to the second (residual byte bit 1 on the first's
-  // right-edge nodes, bit 2 on the second's left-edge nodes; the handed-over
-  // blocks carry no first-store bit), which adds them to its own.
+  // first) and then its unpaired elements.  Codes as above, in list order, so the
+  // second element of a pair adds to the blocks and residual rows of the shared
+  // edge that the first one stored.
   int numPairColours = 0;
   int64_t numPairs = 0;
   std::vector<int> pairColourPtr, pairList, pairConnList;

@@ -122,11 +122,7 @@ struct FragLayout {
   static constexpr size_t REDS = align16(STAGE + 2 * 2 * CS);  // double4 [NSLOT][32]: bulk-reduction sources
   // NONLINEAR: sign(s) x tangent modulus, double [2][NQP][2 (l)][8 (i, k, n)]
   static constexpr size_t AT = align16(REDS + (JAC ? 32 * NSLOT * 32 : 0));
-  // plan mode, pair layout: the first element's shared-edge blocks (double4 [P1][P1],
-  // by (ly of row, ly of column)) and residual rows (double2 [P1], by ly) for the second
-  static constexpr size_t CARRY = align16(AT + (NL ? 8 * 2 * NQP * 16 : 0));
-  static constexpr size_t CARRY_RES = CARRY + (DROP ? 0 : 32 * F::P1 * F::P1);
-  static constexpr size_t warp_bytes = align16(CARRY_RES + (DROP ? 0 : 16 * F::P1));
+  static constexpr size_t warp_bytes = align16(AT + (NL ? 8 * 2 * NQP * 16 : 0));
   static constexpr size_t total = warps + F::WARPS * warp_bytes;
 };
 
@@ -237,84 +233,16 @@ __device__ __forceinline__ void frag_prologue(unsigned char *smem) {
 // direct (0) / transposed (1) blocks.
 __host__ __device__ constexpr int frag_slot(int k, int h, int w) { return k == 0 ? h : (k == 1 ? 2 + 2 * h + w : 6 + h); }
 
-// A plan's pair layout: a step's two elements share an edge (the first's right edge
-// is the second's left edge).  The first element hands its blocks between shared-edge
-// nodes and its shared-edge residual rows to the second, which adds them to its own
-// before its store or reduction: no block or row gets two contributions in one
-// launch.  `out` / `in`: the element's nodes whose values it hands over / takes
-// (bit a = local node a; from the code record's residual bytes, bits 1 and 2);
-// both are zero in the colour layout.  Carry slots: block (r, c) at
-// (r / P1) P1 + c / P1, residual row a at a / P1 (a node's row along the edge).
-struct PairCarry {
-  uint32_t out = 0, in = 0;
-  double *blk = nullptr;   // double4 [P1 * P1]
-  double2 *res = nullptr;  // double2 [P1]
-};
-
-// The element's carry masks (every lane of the warp calls it).
-template <int P>
-__device__ __forceinline__ PairCarry pair_carry(const Out &O, int el, int lane, double *blk, double2 *res) {
-  constexpr int NN = Dims<P>::NN, CS = Dims<P>::CS;
-  const uint8_t f = lane < NN ? O.codes[el * CS + NN * NN + lane] : 0;
-  PairCarry pc;
-  pc.out = __ballot_sync(0xffffffffu, (f & 2) != 0);
-  pc.in = __ballot_sync(0xffffffffu, (f & 4) != 0);
-  pc.blk = blk;
-  pc.res = res;
-  return pc;
-}
-
-// Applies the pair carry to block (r0, c0): true when the block is handed over (the
-// caller writes nothing); else adds what the first element handed over, if any.
-template <int P>
-__device__ __forceinline__ bool carry_block(const PairCarry &pc, int r0, int c0, double &v0, double &v1, double &v2,
-                                            double &v3) {
-  constexpr int P1 = P + 1;
-  const uint32_t m = (1u << r0) | (1u << c0);
-  if ((pc.out & m) == m) {
-    double *d = pc.blk + 4 * ((r0 / P1) * P1 + c0 / P1);
-    reinterpret_cast<double2 *>(d)[0] = make_double2(v0, v1);
-    reinterpret_cast<double2 *>(d)[1] = make_double2(v2, v3);
-    return true;
-  }
-  if ((pc.in & m) == m) {
-    const double *d = pc.blk + 4 * ((r0 / P1) * P1 + c0 / P1);
-    const double2 a = reinterpret_cast<const double2 *>(d)[0], b = reinterpret_cast<const double2 *>(d)[1];
-    v0 += a.x;
-    v1 += a.y;
-    v2 += b.x;
-    v3 += b.y;
-  }
-  return false;
-}
-
-// Residual row of local node a: false when handed over; else adds the carried row.
-template <int P>
-__device__ __forceinline__ bool carry_residual(const PairCarry &pc, int a, double &sx, double &sy) {
-  constexpr int P1 = P + 1;
-  if ((pc.out >> a) & 1u) {
-    pc.res[a / P1] = make_double2(sx, sy);
-    return false;
-  }
-  if ((pc.in >> a) & 1u) {
-    const double2 r = pc.res[a / P1];
-    sx += r.x;
-    sy += r.y;
-  }
-  return true;
-}
-
 // The block (a, b) of element el (or its transpose (b, a) with w = 1): plan mode
 // stores it when this element is its first contributor; otherwise (and in
 // drop-in mode always) it goes to its staging position for frag_issue_run.
 template <int P, bool PLAN>
 __device__ __forceinline__ void frag_put(const Out &O, int el, int a, int b, int w, double kxx, double kxy,
-                                         double kyx, double kyy, double *stg, const PairCarry &pc) {
+                                         double kyx, double kyy, double *stg) {
   constexpr int NN = Dims<P>::NN, CS = Dims<P>::CS;
   const int r0 = w ? b : a, c0 = w ? a : b;
-  double v0 = kxx, v1 = w ? kyx : kxy, v2 = w ? kxy : kyx, v3 = kyy;
+  const double v0 = kxx, v1 = w ? kyx : kxy, v2 = w ? kxy : kyx, v3 = kyy;
   if constexpr (PLAN) {
-    if (carry_block<P>(pc, r0, c0, v0, v1, v2, v3)) return;
     const uint8_t code = O.codes[el * CS + r0 * NN + c0];
     if (code & 0x80) {
       store_block(O.mat + 4 * ((int64_t)O.rbase[el * NN + r0] + (code & 0x7f)), v0, v1, v2, v3);
@@ -323,6 +251,19 @@ __device__ __forceinline__ void frag_put(const Out &O, int el, int a, int b, int
   }
   reinterpret_cast<double2 *>(stg)[0] = make_double2(v0, v1);
   reinterpret_cast<double2 *>(stg)[1] = make_double2(v2, v3);
+}
+
+// Before the second element of a step writes.  In a plan's pair layout it shares an
+// edge with the first: where the first stored a shared block (a generic-proxy
+// 256-bit store) the second adds to it with a bulk reduction (async proxy, maybe
+// another lane), and where both add (an earlier colour stored it) the first one's
+// reduction must land first, or the two would round in either order.  So: wait
+// for this lane's reductions to complete, order the lanes, order the proxies.
+// Residual rows go generic store or atomic, then atomics: the barrier orders them.
+__device__ __forceinline__ void pair_order_fence() {
+  asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+  __syncwarp();
+  asm volatile("fence.proxy.async.global;" ::: "memory");
 }
 
 __device__ __forceinline__ void bulk_add(double *gdst, const double *src, int bytes) {
@@ -338,8 +279,7 @@ __device__ __forceinline__ void bulk_add(double *gdst, const double *src, int by
 // when all four are added and adjacent in the matrix, else 32 bytes per block
 // (four FP64 atomics for a block whose address is not 16-byte aligned).
 template <int P, bool PLAN>
-__device__ __forceinline__ void frag_issue_run(const Out &O, int el, int sl, int r, const double *redsW,
-                                               const PairCarry &pc) {
+__device__ __forceinline__ void frag_issue_run(const Out &O, int el, int sl, int r, const double *redsW) {
   constexpr int NN = Dims<P>::NN, CS = Dims<P>::CS;
   const int k = sl < 2 ? 0 : (sl < 6 ? 1 : 2);
   const int h = sl < 2 ? sl : (sl < 6 ? (sl - 2) >> 1 : sl - 6);
@@ -368,8 +308,7 @@ __device__ __forceinline__ void frag_issue_run(const Out &O, int el, int sl, int
     if (add[j]) {
       if constexpr (PLAN) {
         const uint8_t code = O.codes[el * CS + row * NN + col];
-        // a block handed to the pair's second element was not staged
-        add[j] = !(code & 0x80) && !(((pc.out >> row) & (pc.out >> col)) & 1u);
+        add[j] = !(code & 0x80);
         dst[j] = O.mat + 4 * ((int64_t)O.rbase[el * NN + row] + (code & 0x7f));
       } else {
         dst[j] = O.mat + O.map[(el * NN + row) * NN + col];
@@ -405,11 +344,10 @@ __device__ __forceinline__ void frag_issue_run(const Out &O, int el, int sl, int
 // slot's previous bulk read).  `which` = 1 writes the transposed block (b, a).
 template <int P>
 __device__ __forceinline__ void frag_write(const Out &O, int el, int a, int b, int which, double kxx, double kxy,
-                                           double kyx, double kyy, double *slot, const PairCarry &pc) {
+                                           double kyx, double kyy, double *slot) {
   constexpr int NN = Dims<P>::NN, CS = Dims<P>::CS;
   const int r0 = which ? b : a, c0 = which ? a : b;
-  double v0 = kxx, v1 = which ? kyx : kxy, v2 = which ? kxy : kyx, v3 = kyy;
-  if (carry_block<P>(pc, r0, c0, v0, v1, v2, v3)) return;
+  const double v0 = kxx, v1 = which ? kyx : kxy, v2 = which ? kxy : kyx, v3 = kyy;
   const uint8_t code = O.codes[el * CS + r0 * NN + c0];
   double *blk = O.mat + 4 * ((int64_t)O.rbase[el * NN + r0] + (code & 0x7f));
   if (code & 0x80) {
@@ -659,8 +597,6 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
   unsigned char *stage = ws + L::STAGE;
   double *redsW = reinterpret_cast<double *>(ws + L::REDS);  // staging slot s at redsW + 128 s
   double *ATs = reinterpret_cast<double *>(ws + L::AT);      // NONLINEAR tangent
-  double *carryBlk = reinterpret_cast<double *>(ws + L::CARRY);       // pair layout: handed-over blocks
-  double2 *carryRes = reinterpret_cast<double2 *>(ws + L::CARRY_RES);  // ... and residual rows
 
   // Mesh arguments are read through `mtab` (for one mesh, a pointer to the kernel
   // parameter).  At p = 4 it is laundered once per step: the compiler then reloads
@@ -889,9 +825,8 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
       constexpr int NPAIR = NTM * (NTM + 1) / 2;
       const int pa = 4 * (g & 1) + (g >> 1);  // pi(g)
       for (int el = 0; el < ne; el++) {
-        // pair carry: the first element's rows and blocks are in place
+        // pair layout: the first element's residual writes before the second's
         if (PLAN && el > 0) __syncwarp();
-        const PairCarry pc = PLAN ? pair_carry<P>(O, el, lane, carryBlk, carryRes) : PairCarry{};
         if constexpr (B16) {
           // BF16x6 element stiffness: M_ij = sum_q s G_i(q, a) G_j(q, b) as m16n8k16
           // products (k = quadrature points 0-15; rows a and columns b of the two node
@@ -936,10 +871,10 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
               ry[h] += __shfl_xor_sync(0xffffffffu, ry[h], 2);
             }
             const int a = 8 * t + pa;
-            double sx = t ? rx[1] : rx[0], sy = t ? ry[1] : ry[0];
-            if (t < 2 && a < NN && (!PLAN || carry_residual<P>(pc, a, sx, sy))) {
+            if (t < 2 && a < NN) {
+              const double sx = t ? rx[1] : rx[0], sy = t ? ry[1] : ry[0];
               double *dst = M.residual + 2 * (int64_t)nid[el * NN + a];
-              if (PLAN && (O.codes[el * CS + NN * NN + a] & 1)) {
+              if (PLAN && O.codes[el * CS + NN * NN + a]) {
                 *reinterpret_cast<double2 *>(dst) = make_double2(sx, sy);
               } else {
                 atomicAdd(dst, sx);
@@ -994,6 +929,7 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
             // 2x2 blocks, four consecutive columns across the lanes t.  Blocks to add go
             // to the staging slots of the FP64 layout (node-tile pair (r, h) = (TA, TB);
             // the pair (1, 0) is the transposed half of (0, 1)) and leave as row runs.
+            if (PLAN && el > 0) pair_order_fence();
             asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
             __syncwarp();
 #pragma unroll
@@ -1010,7 +946,7 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
                     const double kyx = lam * myx + mu * mxy, kyy = c11 * myy + mu * mxx;
                     const int sl = (r == 1 && h == 0) ? frag_slot(1, g & 1, 1) : frag_slot(r + h, u, 0);
                     const int pos = (r == 1 && h == 0) ? 8 * (g >> 1) + 4 * u + t : 4 * g + t;
-                    frag_put<P, PLAN>(O, el, a, b, 0, kxx, kxy, kyx, kyy, redsW + 128 * sl + 4 * pos, pc);
+                    frag_put<P, PLAN>(O, el, a, b, 0, kxx, kxy, kyx, kyy, redsW + 128 * sl + 4 * pos);
                   }
                 }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -1018,7 +954,7 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
 #pragma unroll
             for (int v = 0; v < 2; v++) {
               const int run = lane + 32 * v;
-              frag_issue_run<P, PLAN>(O, el, run >> 3, run & 7, redsW, pc);
+              frag_issue_run<P, PLAN>(O, el, run >> 3, run & 7, redsW);
             }
             asm volatile("cp.async.bulk.commit_group;" ::: "memory");
           }
@@ -1132,9 +1068,9 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
           sx += __shfl_xor_sync(0xffffffffu, sx, 1);
           sy += __shfl_xor_sync(0xffffffffu, sy, 1);
           const int a = 8 * Tm + pa;
-          if ((t & 1) == 0 && a < NN && (!PLAN || carry_residual<P>(pc, a, sx, sy))) {
+          if ((t & 1) == 0 && a < NN) {
             double *dst = M.residual + 2 * (int64_t)nid[el * NN + a];
-            if (PLAN && (O.codes[el * CS + NN * NN + a] & 1)) {
+            if (PLAN && O.codes[el * CS + NN * NN + a]) {
               *reinterpret_cast<double2 *>(dst) = make_double2(sx, sy);
             } else {
               atomicAdd(dst, sx);
@@ -1150,6 +1086,7 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
         // reduced with one 128-byte bulk operation per run whose four blocks are adjacent in
         // the matrix, else one 32-byte operation per block.
         if constexpr (JAC && RUNS) {
+          if (PLAN && el > 0) pair_order_fence();
           // every lane's previous bulk reads of the staging slots are complete
           asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
           __syncwarp();
@@ -1172,19 +1109,19 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
                   const int s0 = frag_slot(k, h, 0);
                   if (TA < TB) {
                     const int s1 = frag_slot(k, h, 1);
-                    frag_put<P, PLAN>(O, el, a, b, 0, kxx, kxy, kyx, kyy, redsW + 128 * s0 + 4 * (4 * g + t), pc);
-                    frag_put<P, PLAN>(O, el, a, b, 1, kxx, kxy, kyx, kyy, redsW + 128 * s1 + 4 * (8 * t + pa), pc);
+                    frag_put<P, PLAN>(O, el, a, b, 0, kxx, kxy, kyx, kyy, redsW + 128 * s0 + 4 * (4 * g + t));
+                    frag_put<P, PLAN>(O, el, a, b, 1, kxx, kxy, kyx, kyy, redsW + 128 * s1 + 4 * (8 * t + pa));
                   } else if (!NL) {
-                    frag_put<P, PLAN>(O, el, a, b, 0, kxx, kxy, kyx, kyy, redsW + 128 * s0 + 4 * (4 * g + t), pc);
+                    frag_put<P, PLAN>(O, el, a, b, 0, kxx, kxy, kyx, kyy, redsW + 128 * s0 + 4 * (4 * g + t));
                   } else if (a <= b) {
                     // NONLINEAR diagonal tile: (a, b) for a <= b and, for a < b, its exact
                     // transpose (b, a) at the staging position the (b, a) lane would use
-                    frag_put<P, PLAN>(O, el, a, b, 0, kxx, kxy, kyx, kyy, redsW + 128 * s0 + 4 * (4 * g + t), pc);
+                    frag_put<P, PLAN>(O, el, a, b, 0, kxx, kxy, kyx, kyy, redsW + 128 * s0 + 4 * (4 * g + t));
                     if (a < b) {
                       const int xb = b - 8 * TA, xa = a - 8 * TA;  // pi(g') = xb; a = 8T + 4h' + t'
                       const int gb = 2 * (xb & 3) + (xb >> 2);
                       const int st = frag_slot(k, xa >> 2, 0);
-                      frag_put<P, PLAN>(O, el, a, b, 1, kxx, kxy, kyx, kyy, redsW + 128 * st + 4 * (4 * gb + (xa & 3)), pc);
+                      frag_put<P, PLAN>(O, el, a, b, 1, kxx, kxy, kyx, kyy, redsW + 128 * st + 4 * (4 * gb + (xa & 3)));
                     }
                   }
                 }
@@ -1197,15 +1134,15 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
   #pragma unroll
           for (int u = 0; u < 2; u++) {
             const int run = lane + 32 * u;
-            frag_issue_run<P, PLAN>(O, el, run >> 3, run & 7, redsW, pc);
+            frag_issue_run<P, PLAN>(O, el, run >> 3, run & 7, redsW);
           }
           asm volatile("cp.async.bulk.commit_group;" ::: "memory");
         }
         // stiffness blocks, order 2: lane (g, t) holds (a = 8TA + pi(g), b = 8TB + 4h + t),
         // each written (or added) on its own
         if constexpr (JAC && !RUNS) {
+          if (PLAN && el > 0) pair_order_fence();
           asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
-          __syncwarp();  // pair carry: the first element's blocks are in place
           int k = 0, slot = 0;
           double *reds = redsW + 4 * lane;
   #pragma unroll
@@ -1227,8 +1164,8 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
                   const bool dir = TA < TB || !NL || a <= b;
                   const bool trn = TA < TB || (NL && a < b);
                   if constexpr (PLAN) {
-                    if (dir) frag_write<P>(O, el, a, b, 0, kxx, kxy, kyx, kyy, reds + 128 * slot++, pc);
-                    if (trn) frag_write<P>(O, el, a, b, 1, kxx, kxy, kyx, kyy, reds + 128 * slot++, pc);
+                    if (dir) frag_write<P>(O, el, a, b, 0, kxx, kxy, kyx, kyy, reds + 128 * slot++);
+                    if (trn) frag_write<P>(O, el, a, b, 1, kxx, kxy, kyx, kyy, reds + 128 * slot++);
                   } else {
                     if (dir) frag_add_mapped<P>(O, el, a, b, 0, kxx, kxy, kyx, kyy, reds + 128 * slot++);
                     if (trn) frag_add_mapped<P>(O, el, a, b, 1, kxx, kxy, kyx, kyy, reds + 128 * slot++);
@@ -1257,7 +1194,7 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
               const double kyy = NL ? myy : c11 * myy + mu * mxx;
               const int b = diag ? 8 : pa, w = diag ? 0 : t;
               if constexpr (PLAN) {
-                frag_write<P>(O, el, 8, b, w, kxx, kxy, kyx, kyy, reds + 128 * slot, pc);
+                frag_write<P>(O, el, 8, b, w, kxx, kxy, kyx, kyy, reds + 128 * slot);
               } else {
                 frag_add_mapped<P>(O, el, 8, b, w, kxx, kxy, kyx, kyy, reds + 128 * slot);
               }
@@ -1277,9 +1214,7 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
       double *reds = redsW + 4 * lane;
       int nw = 0;  // writes so far: ring position of the staging slot
       for (int el = 0; el < ne; el++) {
-        // pair carry: the first element's blocks and rows are in place
-        if (PLAN && el > 0) __syncwarp();
-        const PairCarry pc = PLAN ? pair_carry<P>(O, el, lane, carryBlk, carryRes) : PairCarry{};
+        if (PLAN && el > 0) pair_order_fence();
         // residual R_(a,i'): lane partials rp over its quadrature points (with the
         // Jacobian, accumulated by the first three stiffness groups, which between them
         // form every column tile's fragments; alone, in a pass of its own), then a full
@@ -1308,14 +1243,13 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
 #pragma unroll
           for (int mm = 0; mm < 2; mm++) {
             const int a = 4 * (2 * t + mm) + ah;
-            double zx = z[mm][0], zy = z[mm][1];
-            if (ii == 0 && a < NN && (!PLAN || carry_residual<P>(pc, a, zx, zy))) {
+            if (ii == 0 && a < NN) {
               double *dst = M.residual + 2 * (int64_t)nid[el * NN + a];
-              if (PLAN && (O.codes[el * CS + NN * NN + a] & 1)) {
-                *reinterpret_cast<double2 *>(dst) = make_double2(zx, zy);
+              if (PLAN && O.codes[el * CS + NN * NN + a]) {
+                *reinterpret_cast<double2 *>(dst) = make_double2(z[mm][0], z[mm][1]);
               } else {
-                atomicAdd(dst, zx);
-                atomicAdd(dst + 1, zy);
+                atomicAdd(dst, z[mm][0]);
+                atomicAdd(dst + 1, z[mm][1]);
               }
             }
           }
@@ -1401,7 +1335,7 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
                 double *slot = reds + 128 * (nw % L::NSLOT);
                 nw++;
                 if constexpr (PLAN) {
-                  frag_write<P>(O, el, a, b, ii, kxx, kxy, kyx, kyy, slot, pc);
+                  frag_write<P>(O, el, a, b, ii, kxx, kxy, kyx, kyy, slot);
                 } else {
                   frag_add_mapped<P>(O, el, a, b, ii, kxx, kxy, kyx, kyy, slot);
                 }

@@ -180,12 +180,8 @@ static void build_row_plan(HostPlan &hp) {
 // a = ly (P + 1) + lx); elements are paired greedily in id order.  Units (pairs
 // and unpaired elements) are coloured greedily like the elements of the colour
 // layout; codes are computed per colour with the units in parallel (they share no
-// node) and the two elements of a pair in order.  The first element of a pair
-// writes neither its blocks between right-edge nodes nor its right-edge residual
-// rows (residual byte bit 1): it hands them to the second, which adds them to its
-// own (bit 2 on its left-edge nodes), so that no block or row receives two
-// contributions in one launch.  Leaves the layout empty when the units need more
-// than 64 colours.
+// node) and the two elements of a pair in order.  Leaves the layout empty when
+// the units need more than 64 colours.
 static void build_pair_plan(const int *connPtr, const int *conn, HostPlan &hp) {
   const int P = hp.order, P1 = P + 1, nn = hp.nn, nE = hp.numElements;
   auto node = [&](int e, int lx, int ly) { return conn[connPtr[e] + ly * P1 + lx]; };
@@ -277,25 +273,13 @@ static void build_pair_plan(const int *connPtr, const int *conn, HostPlan &hp) {
         int *cl = &hp.pairConnList[(size_t)k * nn];
         uint8_t *rec = &hp.pairCode[(size_t)k * hp.codeStride];
         for (int a = 0; a < nn; a++) cl[a] = en[a];
-        // a pair's first element hands its right edge (lx = P) over to the second,
-        // which takes it on its left edge (lx = 0): residual byte bits 1 / 2
-        auto out = [&](int a) { return n == 2 && w == 0 && a % P1 == P; };
-        auto in = [&](int a) { return n == 2 && w == 1 && a % P1 == 0; };
         for (int a = 0; a < nn; a++) {
           const int r = en[a];
-          if (out(a)) {
-            rec[nn * nn + a] = 2;  // the second element writes the row
-          } else {
-            rec[nn * nn + a] = (uint8_t)((nodeWritten[r] ? 0 : 1) | (in(a) ? 4 : 0));
-            nodeWritten[r] = 1;
-          }
+          rec[nn * nn + a] = nodeWritten[r] ? 0 : 1;
+          nodeWritten[r] = 1;
           const int *c0 = hp.cols.data() + hp.rowp[r], *c1 = hp.cols.data() + hp.rowp[r + 1];
           for (int b = 0; b < nn; b++) {
             const int *pos = std::lower_bound(c0, c1, en[b]);  // present: the colour layout found it
-            if (out(a) && out(b)) {
-              rec[a * nn + b] = (uint8_t)(pos - c0);  // handed over: the second element writes it
-              continue;
-            }
             uint8_t &bf = blockWritten[(size_t)(pos - hp.cols.data())];
             rec[a * nn + b] = (uint8_t)((pos - c0) | (bf ? 0 : 0x80));
             bf = 1;

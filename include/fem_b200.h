@@ -134,11 +134,8 @@ int fem_colour_elements(int numNodes, const int *connPtr, const int *conn, int n
  * colourPtr[numColours + 1] (at most 65 entries), the pairs formed and, when
  * codes != NULL, the code records (numElements * codeStride bytes: per listed
  * element, [a*nn + b] = rank of block (a, b) in row conn[a] | 0x80 for its first
- * contributor, [nn*nn + a] bit 0 for the first writer of node a's residual, bit 1
- * on a pair's first element for the right-edge nodes whose rows and blocks among
- * them it hands to the second element instead of writing them, bit 2 on the
- * second element's left-edge nodes that take them).  numColours = 0: no pair
- * layout (more than 64 colours).  (No reference counterpart.) */
+ * contributor, [nn*nn + a] = 1 for the first writer of node a's residual).
+ * numColours = 0: no pair layout (more than 64 colours).  (No reference counterpart.) */
 int fem_pair_layout(int elementOrder, int numNodes, const int *connPtr, const int *conn, int numElements,
                     int *elemList, int *colourPtr, int *numColours, int64_t *numPairs, uint8_t *codes,
                     int *codeStride);
@@ -175,9 +172,8 @@ int fem_plan_row_chunks(const fem_plan *plan, int *numChunks);
  *                       node for node); pairs are coloured so that one colour's
  *                       pairs share no node, and a warp assembles a pair in one
  *                       step, the second element adding to the shared edge's
- *                       blocks the first one hands over (no block or residual
- *                       row gets two contributions in one launch), so that the
- *                       rows the two share are written while their lines are in L2;
+ *                       blocks the first one stored, so that the rows the two
+ *                       share are written while their lines are in L2;
  *   FEM_LAYOUT_COLOURS  the element colouring above (what every other path runs).
  * The results agree to rounding: a block's contributions are added in another
  * order where more than two elements share it.  fem_plan_get_layout also reports

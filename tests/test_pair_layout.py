@@ -4,9 +4,7 @@ permutation, that each listed pair shares its edge node for node (the first
 element's right edge is the second's left edge), that the units of a colour share
 no node, and replays the write protocol of the code records: in list order,
 colour after colour, every block and residual row is stored exactly once, by its
-first contributor, before any element adds to it, where a pair's first element
-hands the blocks between its right-edge nodes and its right-edge rows to the
-second instead of writing them."""
+first contributor, before any element adds to it."""
 import numpy as np
 import pytest
 
@@ -52,35 +50,20 @@ def _check(fem, mesh, expect_pairs=None, expect_colours=None):
             assert not (un & used), (c, u)
             used |= un
         for u in units:
-            for w, k in enumerate(u):
+            for k in u:
                 en = nodes(elist[k])
                 rec = codes[k]
-                flags = rec[nn * nn:nn * nn + nn]
-                out = (flags & 2) != 0
-                inn = (flags & 4) != 0
-                # hand-over flags: a pair's first element on its right edge, the
-                # second on its left edge; nothing on unpaired elements
-                edge_r = np.arange(nn) % (P + 1) == P
-                edge_l = np.arange(nn) % (P + 1) == 0
-                assert np.array_equal(out, edge_r & (len(u) == 2) & (w == 0))
-                assert np.array_equal(inn, edge_l & (len(u) == 2) & (w == 1))
                 for a in range(nn):
                     r = en[a]
-                    if out[a]:
-                        assert not (flags[a] & 1)
-                    else:
-                        first = bool(flags[a] & 1)
-                        assert first == (not res_written[r])
-                        res_written[r] = True
+                    first = bool(rec[nn * nn + a])
+                    assert first == (not res_written[r])
+                    res_written[r] = True
                     row = cols[rowp[r]:rowp[r + 1]]
                     for bb in range(nn):
                         code = int(rec[a * nn + bb])
                         rank = code & 0x7F
                         assert row[rank] == en[bb]
                         blk = rowp[r] + rank
-                        if out[a] and out[bb]:
-                            assert not (code & 0x80)  # handed to the second element
-                            continue
                         assert bool(code & 0x80) == (not written[blk])
                         written[blk] = True
     assert seen_pairs == npairs
