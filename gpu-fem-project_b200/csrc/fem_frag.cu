@@ -260,10 +260,16 @@ __device__ __forceinline__ void frag_put(const Out &O, int el, int a, int b, int
 // reduction must land first, or the two would round in either order.  So: wait
 // for this lane's reductions to complete, order the lanes, order the proxies.
 // Residual rows go generic store or atomic, then atomics: the barrier orders them.
+// The order-3 writers, which store first and reduce last, take the two halves
+// apart (pair_first_landed before, pair_first_visible after the barrier that
+// precedes their reductions) so that the first element's reductions have the second
+// element's stores to land in.
+__device__ __forceinline__ void pair_first_landed() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void pair_first_visible() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
 __device__ __forceinline__ void pair_order_fence() {
-  asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+  pair_first_landed();
   __syncwarp();
-  asm volatile("fence.proxy.async.global;" ::: "memory");
+  pair_first_visible();
 }
 
 __device__ __forceinline__ void bulk_add(double *gdst, const double *src, int bytes) {
@@ -929,7 +935,6 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
             // 2x2 blocks, four consecutive columns across the lanes t.  Blocks to add go
             // to the staging slots of the FP64 layout (node-tile pair (r, h) = (TA, TB);
             // the pair (1, 0) is the transposed half of (0, 1)) and leave as row runs.
-            if (PLAN && el > 0) pair_order_fence();
             asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
             __syncwarp();
 #pragma unroll
@@ -949,8 +954,10 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
                     frag_put<P, PLAN>(O, el, a, b, 0, kxx, kxy, kyx, kyy, redsW + 128 * sl + 4 * pos);
                   }
                 }
+            if (PLAN && el > 0) pair_first_landed();
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncwarp();
+            if (PLAN && el > 0) pair_first_visible();
 #pragma unroll
             for (int v = 0; v < 2; v++) {
               const int run = lane + 32 * v;
@@ -1086,7 +1093,6 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
         // reduced with one 128-byte bulk operation per run whose four blocks are adjacent in
         // the matrix, else one 32-byte operation per block.
         if constexpr (JAC && RUNS) {
-          if (PLAN && el > 0) pair_order_fence();
           // every lane's previous bulk reads of the staging slots are complete
           asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
           __syncwarp();
@@ -1128,8 +1134,10 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
               }
             }
           }
+          if (PLAN && el > 0) pair_first_landed();
           asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
           __syncwarp();
+          if (PLAN && el > 0) pair_first_visible();
           // 64 runs (8 slots x 8 runs), two per lane
   #pragma unroll
           for (int u = 0; u < 2; u++) {
