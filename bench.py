@@ -61,12 +61,13 @@ def make_mesh(mesh_mod, name):
 
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per assembly from ncu
-# captures, keyed by workload and kernel label prefix.  The 1024^2 order-3 figure
-# is the sum over the four colour launches of the 512^2 case (2.835 GB; the FP64
-# and BF16x6 kernels move the same bytes) times 4: traffic grows with the element
-# count.
+# captures, keyed by workload, kernel label prefix and element layout.  The 1024^2
+# order-3 figures are the sums over the four colour launches of the 512^2 case
+# (colour layout 2.835 GB, the FP64 and BF16x6 kernels moving the same bytes; pair
+# layout 2.592 GB) times 4: traffic grows with the element count.
 MEASURED_TRAFFIC = {
     ("square1024_p3", "frag_kernel<3", "colours"): 4 * 2.835e9,
+    ("square1024_p3", "frag_kernel<3>", "pairs"): 4 * 2.5917e9,
 }
 
 
