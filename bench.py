@@ -685,7 +685,7 @@ def serve_sweep(fem, srv, ids, meshes, states, outs, rates, seconds, rng):
         per_client = [[] for _ in meshes]
         for t, c in zip(arrivals, who):
             per_client[c].append(t)
-        lat, srv_lat, elems, sizes = [], [], [0], []
+        lat, srv_lat, elems, sizes, arr = [], [], [0], [], []
         lock = threading.Lock()
         t0 = time.perf_counter() + 0.05
         st0 = srv.stats()
@@ -704,6 +704,7 @@ def serve_sweep(fem, srv, ids, meshes, states, outs, rates, seconds, rng):
                     lat.append(done - (t0 + t))
                     srv_lat.append(sl)
                     sizes.append(meshes[c].num_elements)
+                    arr.append(t)
                     elems[0] += meshes[c].num_elements
 
         threads = [threading.Thread(target=client, args=(c,)) for c in range(len(meshes)) if per_client[c]]
@@ -725,7 +726,10 @@ def serve_sweep(fem, srv, ids, meshes, states, outs, rates, seconds, rng):
                       "p50_ms": float(np.percentile(lat_ms, 50)), "p99_ms": float(np.percentile(lat_ms, 99)),
                       "server_p50_ms": float(np.percentile(np.array(srv_lat) * 1e3, 50)),
                       "server_p99_ms": float(np.percentile(np.array(srv_lat) * 1e3, 99)),
-                      "by_request_size": by_size, "waves": st1["waves"] - st0["waves"], "wall_s": wall})
+                      "by_request_size": by_size, "waves": st1["waves"] - st0["waves"], "wall_s": wall,
+                      "slowest": [{"arrival_s": float(arr[i]), "ms": float(lat_ms[i]),
+                                   "server_ms": float(srv_lat[i] * 1e3), "elements": int(sz[i])}
+                                  for i in np.argsort(lat_ms)[::-1][:5]]})
     return sweep
 
 
