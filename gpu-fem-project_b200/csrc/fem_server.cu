@@ -91,6 +91,8 @@ struct fem_server {
   std::unordered_map<int64_t, Request> reqs;
   std::deque<int64_t> pending;
   int64_t nextTicket = 1;
+  int64_t maxMeshElements = 0;  // largest registered mesh
+  int maxMeshColours = 0;
   Lane lanes[kLanes];
   std::thread dispatcher;
   bool stop = false;
@@ -117,6 +119,17 @@ int lane_reserve(Lane &L, size_t nargs, size_t ntiles) {
       return fem::cuda_fail(err, "cudaMalloc(lane tiles)");
   }
   return FEM_SUCCESS;
+}
+
+// Upper bound of the tiles of one wave: at most maxBatch meshes and, past its first
+// request, kWaveElements elements (a single request may exceed it); per mesh and
+// colour one partial tile beyond elements / tile length; order-1 row tiles hold
+// kRowTileChunks chunks of up to kRowChunkRows rows (at least one element per
+// chunk row band), plus one partial tile per mesh.
+size_t lane_tile_bound(const fem_server *S) {
+  const int64_t ne = std::max<int64_t>(kWaveElements, S->maxMeshElements);
+  const int64_t perTile = std::max<int64_t>(1, S->tileBatches);  // the smallest tile: EPG >= 1
+  return (size_t)(ne / perTile + ne / fem::kRowTileChunks + (int64_t)S->maxBatch * (S->maxMeshColours + 2) + 1);
 }
 
 // Issues one wave on lane L (called by the dispatcher without the server lock;
@@ -445,6 +458,22 @@ int fem_server_add_mesh(fem_server *S, int elementOrder, int numNodes, const int
     return fem::cuda_fail(err, "fem_server_add_mesh");
   }
   std::lock_guard<std::mutex> lk(S->mu);
+  // Size the idle lanes' mesh tables and tile lists for any wave the meshes
+  // registered so far can form, so that serving never allocates: a cudaFree in
+  // the dispatcher would synchronise the device under every lane's running wave.
+  S->maxMeshElements = std::max<int64_t>(S->maxMeshElements, numElements);
+  S->maxMeshColours = std::max(S->maxMeshColours, plan->numColours);
+  const size_t tiles = lane_tile_bound(S);
+  for (auto &L : S->lanes)
+    if (!L.busy && (st = lane_reserve(L, (size_t)S->maxBatch, tiles))) {
+      fem_plan_destroy(plan);
+      cudaFree(m.coords);
+      cudaFree(m.states);
+      cudaFree(m.residual);
+      cudaFree(m.mat);
+      S->used -= bytes;
+      return st;
+    }
   for (size_t i = 0; i < S->meshes.size(); i++)
     if (!S->meshes[i].plan) {
       S->meshes[i] = m;
