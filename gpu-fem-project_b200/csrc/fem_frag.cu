@@ -54,6 +54,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <type_traits>
 
@@ -1435,7 +1436,14 @@ int launch_frag_p(const AsmArgs &a, cudaStream_t s) {
   if (st) return st;
   const int64_t pairs = (a.count + 1) / 2;
   const int64_t need = (pairs + F::WARPS - 1) / F::WARPS;
-  const int64_t cap = (int64_t)li.grid_per_sm * li.num_sms;
+  // Order-3 drop-in Jacobian (every block added through the element map, one launch
+  // whose elements share blocks): two CTAs per SM.  At 1024^2 the kernel took 3.90 ms
+  // with two resident CTAs per SM against 4.35 ms with three (the bulk reductions of
+  // more warps contend in L2); at order 2 (four CTAs) halving them cost 2.04 -> 3.46
+  // ms on the 512x2048 annulus, so it keeps its occupancy.
+  const int perSm =
+      (P == 3 && (MODE & kPlan) == 0 && (MODE & kJac) != 0) ? std::min(li.grid_per_sm, 2) : li.grid_per_sm;
+  const int64_t cap = (int64_t)perSm * li.num_sms;
   const int grid = (int)(need < cap ? need : cap);
   if (grid <= 0) return FEM_SUCCESS;
   kernel<<<grid, NT, smem, s>>>(a);
