@@ -52,6 +52,7 @@ struct HostPlan {
   int numPairColours = 0;
   int64_t numPairs = 0;
   std::vector<int> pairColourPtr, pairList, pairConnList;
+  std::vector<int> pairRegionEnd;  // per colour: the end of its pairs (its unpaired elements follow)
   std::vector<uint8_t> pairCode;
 };
 constexpr int kRowChunkRows = 32, kRowChunkBlocks = 320;

@@ -289,6 +289,8 @@ static void build_pair_plan(const int *connPtr, const int *conn, HostPlan &hp) {
     }
   }
   hp.numPairColours = nc;
+  hp.pairRegionEnd.resize((size_t)nc);
+  for (int c = 0; c < nc; c++) hp.pairRegionEnd[c] = hp.pairColourPtr[c] + (int)(2 * pairsOf[c]);
   int64_t np = 0;
   for (int c = 0; c < nc; c++) np += pairsOf[c];
   hp.numPairs = np;

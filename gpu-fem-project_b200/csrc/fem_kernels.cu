@@ -474,6 +474,15 @@ int fem_plan_create(int elementOrder, int numNodes, const int *connPtr, const in
       return st;
     }
     p->pairColourPtr = hp.pairColourPtr;
+    p->pairRegionEnd = hp.pairRegionEnd;
+    p->pairList = hp.pairList;
+    p->pairNodeLo.resize((size_t)hp.numElements);
+    p->pairNodeHi.resize((size_t)hp.numElements);
+    for (int k = 0; k < hp.numElements; k++) {
+      const int *c = &hp.pairConnList[(size_t)k * hp.nn];
+      p->pairNodeLo[k] = *std::min_element(c, c + hp.nn);
+      p->pairNodeHi[k] = *std::max_element(c, c + hp.nn);
+    }
     p->numPairColours = hp.numPairColours;
     p->numPairs = hp.numPairs;
     p->usePairs = true;
@@ -733,7 +742,17 @@ int fem_plan_assemble_host(const fem_plan *plan, const double *hostStates, doubl
       if (err != cudaSuccess) return fem::cuda_fail(err, "cudaStreamCreateWithFlags");
     }
   }
-  const int N = plan->numNodes, nE = plan->numElements, nc = plan->numColours;
+  const bool frag = fem::frag_supported(plan->order, precision, strainType, true);
+  const bool rows = fem::plan_rows(plan) && strainType == FEM_STRAIN_LINEAR;
+  // the fragment kernel runs the pair layout when the plan uses it (each band's pairs
+  // and unpaired elements are two ranges of a colour), else the colour layout
+  const bool pairs = frag && !rows && plan->usePairs && plan->numPairColours > 0;
+  const int N = plan->numNodes, nE = plan->numElements;
+  const int nc = pairs ? plan->numPairColours : plan->numColours;
+  const std::vector<int> &cptr = pairs ? plan->pairColourPtr : plan->colourPtr;
+  const std::vector<int> &list = pairs ? plan->pairList : plan->elemList;
+  const std::vector<int> &nlo = pairs ? plan->pairNodeLo : plan->nodeLo;
+  const std::vector<int> &nhi = pairs ? plan->pairNodeHi : plan->nodeHi;
   const int B = std::min(numBands, std::max(1, std::min(N, nE)));
   // node chunk j = [nstart[j], nstart[j + 1]); chunk_of inverts exactly that split
   std::vector<int64_t> nstart((size_t)B + 1);
@@ -742,33 +761,60 @@ int fem_plan_assemble_host(const fem_plan *plan, const double *hostStates, doubl
     return (int)(std::upper_bound(nstart.begin(), nstart.end(), n) - nstart.begin()) - 1;
   };
   auto node0 = [&](int j) { return nstart[j]; };
-  const bool rows = fem::plan_rows(plan) && strainType == FEM_STRAIN_LINEAR;
 
+  // a (band, colour) cell: list positions [p0, p1) and, in the pair layout, the
+  // band's unpaired elements [q0, q1)
   struct L {
     int t, c, k;
-    int64_t p0, p1;
+    int64_t p0, p1, q0, q1;
     int lo, hi;
   };
   std::vector<L> ls;
   if (rows) {
-    ls.push_back({0, 0, 0, 0, plan->numChunks, 0, N - 1});
+    ls.push_back({0, 0, 0, 0, plan->numChunks, 0, 0, 0, N - 1});
   } else {
     // per (band, colour): list positions and node span; per band: node span
     std::vector<int> blo(B, INT32_MAX), bhi(B, -1);
     std::vector<L> cells((size_t)B * nc);
     for (int c = 0; c < nc; c++) {
-      const int *b0 = plan->elemList.data() + plan->colourPtr[c], *b1 = plan->elemList.data() + plan->colourPtr[c + 1];
+      // colour layout: the colour's elements in ascending id; pair layout: its pairs
+      // in ascending id of their first element (two positions each), then its
+      // unpaired elements in ascending id
+      const int64_t c0 = cptr[c], c1 = cptr[c + 1], pe = pairs ? plan->pairRegionEnd[c] : c1;
+      auto pair_pos = [&](int id) {  // first pair position whose lead id is >= id
+        int64_t lo = 0, hi = (pe - c0) / 2;
+        while (lo < hi) {
+          const int64_t mid = (lo + hi) / 2;
+          if (list[c0 + 2 * mid] < id) lo = mid + 1;
+          else hi = mid;
+        }
+        return c0 + 2 * lo;
+      };
+      const int *s0 = list.data() + pe, *s1 = list.data() + c1;
       for (int k = 0; k < B; k++) {
         L &x = cells[(size_t)k * nc + c];
         x.c = c;
         x.k = k;
-        x.p0 = std::lower_bound(b0, b1, (int)((int64_t)k * nE / B)) - plan->elemList.data();
-        x.p1 = std::lower_bound(b0, b1, (int)((int64_t)(k + 1) * nE / B)) - plan->elemList.data();
+        const int id0 = (int)((int64_t)k * nE / B), id1 = (int)((int64_t)(k + 1) * nE / B);
+        if (pairs) {
+          x.p0 = pair_pos(id0);
+          x.p1 = pair_pos(id1);
+          x.q0 = std::lower_bound(s0, s1, id0) - list.data();
+          x.q1 = std::lower_bound(s0, s1, id1) - list.data();
+        } else {
+          x.p0 = std::lower_bound(list.data() + c0, list.data() + c1, id0) - list.data();
+          x.p1 = std::lower_bound(list.data() + c0, list.data() + c1, id1) - list.data();
+          x.q0 = x.q1 = 0;
+        }
         x.lo = INT32_MAX;
         x.hi = -1;
         for (int64_t q = x.p0; q < x.p1; q++) {
-          x.lo = std::min(x.lo, plan->nodeLo[q]);
-          x.hi = std::max(x.hi, plan->nodeHi[q]);
+          x.lo = std::min(x.lo, nlo[q]);
+          x.hi = std::max(x.hi, nhi[q]);
+        }
+        for (int64_t q = x.q0; q < x.q1; q++) {
+          x.lo = std::min(x.lo, nlo[q]);
+          x.hi = std::max(x.hi, nhi[q]);
         }
         blo[k] = std::min(blo[k], x.lo);
         bhi[k] = std::max(bhi[k], x.hi);
@@ -785,7 +831,7 @@ int fem_plan_assemble_host(const fem_plan *plan, const double *hostStates, doubl
         tcur[k] = tk;
         L &x = cells[(size_t)k * nc + c];
         x.t = tk;
-        if (x.p1 > x.p0) ls.push_back(x);
+        if (x.p1 > x.p0 || x.q1 > x.q0) ls.push_back(x);
       }
       tprev = tcur;
     }
@@ -793,7 +839,6 @@ int fem_plan_assemble_host(const fem_plan *plan, const double *hostStates, doubl
       return a.t != b.t ? a.t < b.t : (a.c != b.c ? a.c < b.c : a.k < b.k);
     });
   }
-  const bool frag = fem::frag_supported(plan->order, precision, strainType, true);
   // launches: the fragment kernel takes the ranges of one schedule step (independent:
   // different bands of different colours, or one colour's bands) in one launch
   struct G {
@@ -802,13 +847,18 @@ int fem_plan_assemble_host(const fem_plan *plan, const double *hostStates, doubl
   };
   std::vector<G> gs;
   for (const L &x : ls) {
-    const bool join = frag && !rows && !gs.empty() && gs.back().r.n < fem::dev::kMaxRanges &&
+    const int nr = (x.p1 > x.p0) + (x.q1 > x.q0);
+    const bool join = frag && !rows && !gs.empty() && gs.back().r.n + nr <= fem::dev::kMaxRanges &&
                       ls[&x - ls.data() - 1].t == x.t;
     if (!join) gs.push_back(G{-1, INT32_MAX, -1, fem::dev::RangeList{0, {}, {}}});
     G &g = gs.back();
-    g.r.begin[g.r.n] = x.p0;
-    g.r.count[g.r.n] = x.p1 - x.p0;
-    g.r.n++;
+    for (int h = 0; h < 2; h++) {
+      const int64_t b0 = h ? x.q0 : x.p0, b1 = h ? x.q1 : x.p1;
+      if (b1 <= b0) continue;
+      g.r.begin[g.r.n] = b0;
+      g.r.count[g.r.n] = b1 - b0;
+      g.r.n++;
+    }
     g.lo = std::min(g.lo, x.lo);
     g.hi = std::max(g.hi, x.hi);
     g.need = rows ? B - 1 : std::max(g.need, chunk_of(x.hi));
@@ -820,6 +870,10 @@ int fem_plan_assemble_host(const fem_plan *plan, const double *hostStates, doubl
 
   fem::dev::AsmArgs a{};
   fem::plan_args(a, plan);
+  if (pairs) {
+    a.connList = plan->d_pairConnList;
+    a.blockCode = plan->d_pairCode;
+  }
   a.states = states;
   a.coords = nodeCoords;
   a.residual = residual;

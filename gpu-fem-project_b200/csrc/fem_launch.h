@@ -202,7 +202,8 @@ struct fem_plan {
   // (HostPlan::pairColourPtr ...); usePairs selects it (fem_plan_set_layout)
   int *d_pairConnList = nullptr;
   uint8_t *d_pairCode = nullptr;
-  std::vector<int> pairColourPtr;
+  std::vector<int> pairColourPtr, pairRegionEnd;
+  std::vector<int> pairList, pairNodeLo, pairNodeHi;  // host copies for the band split of fem_plan_assemble_host
   int numPairColours = 0;
   int64_t numPairs = 0;
   bool usePairs = false;

@@ -32,13 +32,16 @@ CASES = [
 ]
 
 
+@pytest.mark.parametrize("layout", ["pairs", "colours"])
 @pytest.mark.parametrize("name,make,precision,strain,bands", CASES, ids=[c[0] for c in CASES])
-def test_host_assembly_equals_device_assembly(fem, cuda, name, make, precision, strain, bands):
+def test_host_assembly_equals_device_assembly(fem, cuda, name, make, precision, strain, bands, layout):
     import torch
     m = make(fem)
     plan = fem.Plan(m.order, m.num_nodes, m.conn_ptr, m.conn)
     if m.order > 1:
-        plan.set_layout("colours")  # the band-split launches run the colour layout
+        plan.set_layout(layout)  # the band-split launches run the plan's layout
+    elif layout == "pairs":
+        pytest.skip("order 1: no pair layout")
     d = fem.DeviceMesh(m, cuda)
     res0 = torch.empty(m.num_nodes * 2, dtype=torch.float64, device=cuda)
     mat0 = torch.empty(plan.nnzb * 4, dtype=torch.float64, device=cuda)
