@@ -665,6 +665,10 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
     cp_async_commit();
   };
 
+  // a grid launched after this one with programmatic serialization may start its CTAs
+  // as this one's retire; it waits (griddepcontrol.wait) before it writes
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  bool dep_ready = false;
   PairCursor cur = gen.next(lane);
   PairCursor nxt = gen.next(lane);
   load_nodes(cur, nodeB);
@@ -822,6 +826,12 @@ __device__ __forceinline__ void frag_loop(unsigned char *smem, Gen &gen, const A
     }
     __syncwarp();
 
+    // the warp's first writes wait for the grid launched before this one (programmatic
+    // dependent launch: its gathers and element arithmetic ran while that grid drained)
+    if (!dep_ready) {
+      asm volatile("griddepcontrol.wait;" ::: "memory");
+      dep_ready = true;
+    }
     if constexpr (Gen::kSched) gen.acquire(cur, lane);
     const Out O{M.mat, M.residual, stage + buf * 2 * STG, rb, reinterpret_cast<const int *>(stage + buf * 2 * STG)};
     if constexpr (!F::IL) {
@@ -1425,8 +1435,31 @@ __global__ void __launch_bounds__(32 * FragDims<P>::WARPS, FEM_FRAG_MINB)
   frag_loop<P, MODE>(smem, gen, meshes[0], meshes);
 }
 
+// A launch whose grid may begin while the kernel before it on the stream drains
+// (programmatic dependent launch): consecutive colour or band launches of one
+// assembly overlap one's tail with the next one's table setup, gathers and element
+// arithmetic; the fragment kernel waits for the previous grid before it writes.
+template <typename K, typename... Args>
+cudaError_t pdl_launch(K kernel, int grid, int nt, size_t smem, cudaStream_t s, const Args &...args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)nt);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
+// chained: the launch follows this assembly's previous fragment-kernel launch on the
+// stream (a later colour or band), whose outputs are the only ones it may read
+// early, so it may start as that one drains; a first launch follows the caller's
+// work, which may have produced its inputs, and launches in stream order.
 template <int P, int MODE>
-int launch_frag_p(const AsmArgs &a, cudaStream_t s) {
+int launch_frag_p(const AsmArgs &a, cudaStream_t s, bool chained) {
   using F = FragDims<P>;
   constexpr int NT = 32 * F::WARPS;
   auto kernel = frag_kernel<P, MODE>;
@@ -1446,14 +1479,19 @@ int launch_frag_p(const AsmArgs &a, cudaStream_t s) {
   const int64_t cap = (int64_t)perSm * li.num_sms;
   const int grid = (int)(need < cap ? need : cap);
   if (grid <= 0) return FEM_SUCCESS;
-  kernel<<<grid, NT, smem, s>>>(a);
-  cudaError_t err = cudaGetLastError();
+  cudaError_t err;
+  if (chained) {
+    err = pdl_launch(kernel, grid, NT, smem, s, a);
+  } else {
+    kernel<<<grid, NT, smem, s>>>(a);
+    err = cudaGetLastError();
+  }
   if (err != cudaSuccess) return cuda_fail(err, "frag_kernel launch");
   return FEM_SUCCESS;
 }
 
 template <int P, int MODE>
-int launch_frag_ranges_p(const AsmArgs &a, const RangeList &r, cudaStream_t s) {
+int launch_frag_ranges_p(const AsmArgs &a, const RangeList &r, cudaStream_t s, bool chained) {
   using F = FragDims<P>;
   constexpr int NT = 32 * F::WARPS;
   auto kernel = frag_ranges_kernel<P, MODE>;
@@ -1467,8 +1505,13 @@ int launch_frag_ranges_p(const AsmArgs &a, const RangeList &r, cudaStream_t s) {
   const int64_t cap = (int64_t)li.grid_per_sm * li.num_sms;
   const int grid = (int)(need < cap ? need : cap);
   if (grid <= 0) return FEM_SUCCESS;
-  kernel<<<grid, NT, smem, s>>>(a, r);
-  cudaError_t err = cudaGetLastError();
+  cudaError_t err;
+  if (chained) {
+    err = pdl_launch(kernel, grid, NT, smem, s, a, r);
+  } else {
+    kernel<<<grid, NT, smem, s>>>(a, r);
+    err = cudaGetLastError();
+  }
   if (err != cudaSuccess) return cuda_fail(err, "frag_ranges_kernel launch");
   return FEM_SUCCESS;
 }
@@ -1512,15 +1555,15 @@ int launch_frag_sched_p(const AsmArgs &a, const SchedArgs &sa, cudaStream_t s) {
 }
 
 template <int MODE>
-int launch_frag_mode(int order, const AsmArgs &a, cudaStream_t s) {
+int launch_frag_mode(int order, const AsmArgs &a, cudaStream_t s, bool chained) {
   switch (order) {
     case 2:
       if constexpr ((MODE & kB16) != 0) return fail(FEM_ERR_INVALID_ORDER, "fragment kernel, BF16x6: order 2");
-      else return launch_frag_p<2, MODE>(a, s);
-    case 3: return launch_frag_p<3, MODE>(a, s);
+      else return launch_frag_p<2, MODE>(a, s, chained);
+    case 3: return launch_frag_p<3, MODE>(a, s, chained);
     case 4:
       if constexpr ((MODE & (kNL | kB16)) != 0) return fail(FEM_ERR_INVALID_ORDER, "fragment kernel, mode %d: order 4", MODE);
-      else return launch_frag_p<4, MODE>(a, s);
+      else return launch_frag_p<4, MODE>(a, s, chained);
     default: return fail(FEM_ERR_INVALID_ORDER, "fragment kernel: order %d", order);
   }
 }
@@ -1554,33 +1597,33 @@ bool frag_supported(int order, int precision, int strain, bool plan) {
   return order == 2 || order == 3 || (order == 4 && plan);
 }
 
-int launch_frag(int order, int precision, int mode, const dev::AsmArgs &a, cudaStream_t s, int strain) {
+int launch_frag(int order, int precision, int mode, const dev::AsmArgs &a, cudaStream_t s, int strain, bool chained) {
   using namespace dev;
   if (strain == FEM_STRAIN_NONLINEAR) mode |= kNL;
   if (b16_stiffness(order, precision, strain) && (mode & kJac)) mode |= kB16;
   switch (mode) {
-    case kPlan | kJac | kB16: return launch_frag_mode<kPlan | kJac | kB16>(order, a, s);
-    case kPlan | kRes | kJac | kB16: return launch_frag_mode<kPlan | kRes | kJac | kB16>(order, a, s);
-    case kJac | kB16: return launch_frag_mode<kJac | kB16>(order, a, s);
-    case kRes | kJac | kB16: return launch_frag_mode<kRes | kJac | kB16>(order, a, s);
-    case kPlan | kRes: return launch_frag_mode<kPlan | kRes>(order, a, s);
-    case kPlan | kJac: return launch_frag_mode<kPlan | kJac>(order, a, s);
-    case kPlan | kRes | kJac: return launch_frag_mode<kPlan | kRes | kJac>(order, a, s);
-    case kRes: return launch_frag_mode<kRes>(order, a, s);
-    case kJac: return launch_frag_mode<kJac>(order, a, s);
-    case kRes | kJac: return launch_frag_mode<kRes | kJac>(order, a, s);
-    case kNL | kPlan | kRes: return launch_frag_mode<kNL | kPlan | kRes>(order, a, s);
-    case kNL | kPlan | kJac: return launch_frag_mode<kNL | kPlan | kJac>(order, a, s);
-    case kNL | kPlan | kRes | kJac: return launch_frag_mode<kNL | kPlan | kRes | kJac>(order, a, s);
-    case kNL | kRes: return launch_frag_mode<kNL | kRes>(order, a, s);
-    case kNL | kJac: return launch_frag_mode<kNL | kJac>(order, a, s);
-    case kNL | kRes | kJac: return launch_frag_mode<kNL | kRes | kJac>(order, a, s);
+    case kPlan | kJac | kB16: return launch_frag_mode<kPlan | kJac | kB16>(order, a, s, chained);
+    case kPlan | kRes | kJac | kB16: return launch_frag_mode<kPlan | kRes | kJac | kB16>(order, a, s, chained);
+    case kJac | kB16: return launch_frag_mode<kJac | kB16>(order, a, s, chained);
+    case kRes | kJac | kB16: return launch_frag_mode<kRes | kJac | kB16>(order, a, s, chained);
+    case kPlan | kRes: return launch_frag_mode<kPlan | kRes>(order, a, s, chained);
+    case kPlan | kJac: return launch_frag_mode<kPlan | kJac>(order, a, s, chained);
+    case kPlan | kRes | kJac: return launch_frag_mode<kPlan | kRes | kJac>(order, a, s, chained);
+    case kRes: return launch_frag_mode<kRes>(order, a, s, chained);
+    case kJac: return launch_frag_mode<kJac>(order, a, s, chained);
+    case kRes | kJac: return launch_frag_mode<kRes | kJac>(order, a, s, chained);
+    case kNL | kPlan | kRes: return launch_frag_mode<kNL | kPlan | kRes>(order, a, s, chained);
+    case kNL | kPlan | kJac: return launch_frag_mode<kNL | kPlan | kJac>(order, a, s, chained);
+    case kNL | kPlan | kRes | kJac: return launch_frag_mode<kNL | kPlan | kRes | kJac>(order, a, s, chained);
+    case kNL | kRes: return launch_frag_mode<kNL | kRes>(order, a, s, chained);
+    case kNL | kJac: return launch_frag_mode<kNL | kJac>(order, a, s, chained);
+    case kNL | kRes | kJac: return launch_frag_mode<kNL | kRes | kJac>(order, a, s, chained);
     default: return fail(FEM_ERR_INVALID_ARGUMENT, "fragment kernel: mode %d", mode);
   }
 }
 
 int launch_frag_ranges(int order, int precision, int mode, const dev::AsmArgs &a, const dev::RangeList &r,
-                       cudaStream_t s, int strain) {
+                       cudaStream_t s, int strain, bool chained) {
   using namespace dev;
   if (strain == FEM_STRAIN_NONLINEAR) mode |= kNL;
   if (b16_stiffness(order, precision, strain) && (mode & kJac)) mode |= kB16;
@@ -1589,11 +1632,11 @@ int launch_frag_ranges(int order, int precision, int mode, const dev::AsmArgs &a
     switch (order) {
       case 2:
         if constexpr ((M & kB16) != 0) return fail(FEM_ERR_INVALID_ORDER, "fragment kernel, BF16x6: order 2");
-        else return launch_frag_ranges_p<2, M>(a, r, s);
-      case 3: return launch_frag_ranges_p<3, M>(a, r, s);
+        else return launch_frag_ranges_p<2, M>(a, r, s, chained);
+      case 3: return launch_frag_ranges_p<3, M>(a, r, s, chained);
       case 4:
         if constexpr ((M & (kNL | kB16)) != 0) return fail(FEM_ERR_INVALID_ORDER, "fragment kernel, mode %d: order 4", M);
-        else return launch_frag_ranges_p<4, M>(a, r, s);
+        else return launch_frag_ranges_p<4, M>(a, r, s, chained);
       default: return fail(FEM_ERR_INVALID_ORDER, "fragment kernel: order %d", order);
     }
   };

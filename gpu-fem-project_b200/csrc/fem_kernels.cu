@@ -681,7 +681,7 @@ int fem_plan_assemble_ex(const fem_plan *plan, const double *states, const doubl
     for (int c = 0; c < ncol; c++) {
       a.begin = cptr[c];
       a.count = cptr[c + 1] - cptr[c];
-      int st = frag ? fem::launch_frag(plan->order, precision, mode, a, s, strainType)
+      int st = frag ? fem::launch_frag(plan->order, precision, mode, a, s, strainType, /*chained=*/c > 0)
                     : fem::launch(plan->order, precision, mode, a, s, strainType);
       if (st) return st;
     }
@@ -917,7 +917,9 @@ int fem_plan_assemble_host(const fem_plan *plan, const double *hostStates, doubl
         a.count = plan->numChunks;
         r = fem::launch_rows(mode, a, s);
       } else if (frag) {
-        r = fem::launch_frag_ranges(plan->order, precision, mode, a, g.r, s, strainType);
+        // after the first launch each one follows this call's previous launch (a state
+        // chunk it waits for still gates it through the stream's event wait)
+        r = fem::launch_frag_ranges(plan->order, precision, mode, a, g.r, s, strainType, /*chained=*/i > 0);
       } else {
         a.begin = g.r.begin[0];
         a.count = g.r.count[0];

@@ -119,12 +119,14 @@ constexpr int kRowTileChunks = 16;
 // products (b16_stiffness); the rest stays FP64.
 bool frag_supported(int order, int precision, int strain, bool plan);
 bool b16_stiffness(int order, int precision, int strain);
+// chained: the launch directly follows this assembly's previous fragment-kernel
+// launch on the stream and may overlap its tail (programmatic dependent launch).
 int launch_frag(int order, int precision, int mode, const dev::AsmArgs &a, cudaStream_t s,
-                int strain = FEM_STRAIN_LINEAR);
+                int strain = FEM_STRAIN_LINEAR, bool chained = false);
 // Its multi-range form (plan mode, residual always, Jacobian optional): up to
 // kMaxRanges list-position ranges of one mesh in one launch.
 int launch_frag_ranges(int order, int precision, int mode, const dev::AsmArgs &a, const dev::RangeList &r,
-                       cudaStream_t s, int strain = FEM_STRAIN_LINEAR);
+                       cudaStream_t s, int strain = FEM_STRAIN_LINEAR, bool chained = false);
 // All colours of one plan in one dependency-ordered persistent launch (plan mode).
 int launch_frag_sched(int order, int precision, int mode, const dev::AsmArgs &a, const dev::SchedArgs &sa,
                       cudaStream_t s, int strain = FEM_STRAIN_LINEAR);
