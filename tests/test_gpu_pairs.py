@@ -91,3 +91,36 @@ def test_layout_errors(fem, cuda):
         plan.set_layout("colours")
     finally:
         plan.close()
+
+
+def test_chained_launches_see_the_callers_writes(fem, cuda):
+    """The later colour launches of an assembly overlap the previous launch's tail
+    (programmatic dependent launch); the first one follows the caller's work in
+    stream order, so states a caller kernel writes just before the call are the
+    states assembled -- on a stream, for several back-to-back calls."""
+    import torch
+    m = fem.square_mesh(24, 20, 3, 1.0, 1.0, 0.15, seed=77)
+    plan = fem.Plan(m.order, m.num_nodes, m.conn_ptr, m.conn)
+    d = fem.DeviceMesh(m, cuda)
+    stream = torch.cuda.Stream(device=cuda)
+    res = torch.empty(m.num_nodes * 2, dtype=torch.float64, device=cuda)
+    mat = torch.empty(plan.nnzb * 4, dtype=torch.float64, device=cuda)
+    base = d.states.clone()
+    refs = []
+    for k in range(3):  # reference results, one call at a time
+        d.states.copy_(base * (1.0 + 0.5 * k))
+        torch.cuda.synchronize()
+        plan.assemble(d.states, d.coords, m.E, m.nu, m.t, res, mat)
+        torch.cuda.synchronize()
+        refs.append((res.clone(), mat.clone()))
+    outs = []
+    with torch.cuda.stream(stream):
+        for k in range(3):
+            d.states.copy_(base)
+            d.states.mul_(1.0 + 0.5 * k)  # a kernel on the same stream right before the call
+            plan.assemble(d.states, d.coords, m.E, m.nu, m.t, res, mat, stream=stream.cuda_stream)
+            outs.append((res.clone(), mat.clone()))
+    stream.synchronize()
+    for (r, a), (r0, a0) in zip(outs, refs):
+        assert torch.equal(r, r0) and torch.equal(a, a0)
+    plan.close()
