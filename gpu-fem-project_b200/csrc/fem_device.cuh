@@ -523,7 +523,11 @@ struct SchedArgs {
 };
 
 // Work source of the batched kernel: groups pull tiles from a per-launch queue
-// (one atomic counter per launch) and walk their batches.
+// (one atomic counter per launch) and walk their batches.  The argument blocks of
+// the meshes the group works on are kept in two shared-memory slots, filled by the
+// thread that takes a tile (at most two meshes are live: the current batch's and
+// the next one's), so that a batch's gathers do not wait on a global load of its
+// mesh's table first.
 struct QueueSource {
   static constexpr bool kBatched = true;
   const Tile *tiles;
@@ -532,6 +536,19 @@ struct QueueSource {
   int *slot;  // one int in the group's shared memory
   int bar, gt, epg;
   int64_t kend;
+  const AsmArgs *meshes;
+  AsmArgs *cache;  // [2] in the group's shared memory
+  int *cacheMesh;  // [2]: the mesh each slot holds (-1: none)
+  __device__ const AsmArgs &args(int m) const { return cacheMesh[0] == m ? cache[0] : cache[1]; }
+  // thread 0: the tile's mesh into the slot that the current batch does not use
+  __device__ void cache_tile(int t, int curMesh) {
+    if (t >= ntiles) return;
+    const int m = tiles[t].mesh;
+    if (cacheMesh[0] == m || cacheMesh[1] == m) return;
+    const int k = cacheMesh[0] == curMesh ? 1 : 0;
+    cache[k] = meshes[m];
+    cacheMesh[k] = m;
+  }
   __device__ Cursor from_tile(int t) {
     Cursor c{0, 0, 0};
     if (t < ntiles) {
@@ -548,7 +565,11 @@ struct QueueSource {
   // it: a group whose threads took different tiles would mix two meshes' staged
   // block codes and row bases.
   __device__ Cursor first(int tg, int) {
-    if (tg == 0) *slot = atomicAdd(counter, 1);
+    if (tg == 0) {
+      cacheMesh[0] = cacheMesh[1] = -1;
+      *slot = atomicAdd(counter, 1);
+      cache_tile(*slot, -1);
+    }
     group_sync(bar, gt);
     const Cursor c = from_tile(*slot);
     group_sync(bar, gt);
@@ -557,7 +578,10 @@ struct QueueSource {
   // Before the group barrier that precedes next(): grab the following tile when
   // this is the tile's last batch.
   __device__ void request(const Cursor &c, int tg) {
-    if (tg == 0 && c.k0 + epg >= kend) *slot = atomicAdd(counter, 1);
+    if (tg == 0 && c.k0 + epg >= kend) {
+      *slot = atomicAdd(counter, 1);
+      cache_tile(*slot, c.mesh);
+    }
   }
   __device__ Cursor next(const Cursor &c) {
     if (c.k0 + epg >= kend) return from_tile(*slot);
@@ -665,7 +689,7 @@ __device__ __forceinline__ void group_loop(unsigned char *smem, Src &src, const 
   double2 pf_x = make_double2(0, 0), pf_u = make_double2(0, 0);
   auto args = [&](const Cursor &c) -> const AsmArgs & {
     if constexpr (Src::kBatched) {
-      return meshes[c.mesh];
+      return src.args(c.mesh);
     } else {
       return single;
     }
@@ -1195,9 +1219,11 @@ __global__ void __launch_bounds__(ShapeSel<P, MODE>::GT *ShapeSel<P, MODE>::GPC,
   using S = ShapeSel<P, MODE>;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int slots[S::GPC];
+  __shared__ AsmArgs argCache[S::GPC][2];
+  __shared__ int argMesh[S::GPC][2];
   cta_prologue<P, T, MODE>(smem);
   const int g = threadIdx.x / S::GT;
-  QueueSource src{tiles, ntiles, counter, &slots[g], 1 + g, S::GT, S::EPG, 0};
+  QueueSource src{tiles, ntiles, counter, &slots[g], 1 + g, S::GT, S::EPG, 0, meshes, argCache[g], argMesh[g]};
   group_loop<P, T, MODE>(smem, src, meshes[0], meshes);
 }
 
