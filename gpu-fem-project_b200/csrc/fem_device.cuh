@@ -539,6 +539,10 @@ struct QueueSource {
   const AsmArgs *meshes;
   AsmArgs *cache;  // [2] in the group's shared memory
   int *cacheMesh;  // [2]: the mesh each slot holds (-1: none)
+  // thread 0: the tile after the current one, taken when the current one starts so
+  // that the queue atomic's latency -- long behind a later colour's matrix
+  // reductions in L2 -- is hidden by the current tile's work
+  int ahead = 0;
   __device__ const AsmArgs &args(int m) const { return cacheMesh[0] == m ? cache[0] : cache[1]; }
   // thread 0: the tile's mesh into the slot that the current batch does not use
   __device__ void cache_tile(int t, int curMesh) {
@@ -568,6 +572,7 @@ struct QueueSource {
     if (tg == 0) {
       cacheMesh[0] = cacheMesh[1] = -1;
       *slot = atomicAdd(counter, 1);
+      ahead = atomicAdd(counter, 1);
       cache_tile(*slot, -1);
     }
     group_sync(bar, gt);
@@ -579,8 +584,9 @@ struct QueueSource {
   // this is the tile's last batch.
   __device__ void request(const Cursor &c, int tg) {
     if (tg == 0 && c.k0 + epg >= kend) {
-      *slot = atomicAdd(counter, 1);
-      cache_tile(*slot, c.mesh);
+      *slot = ahead;
+      cache_tile(ahead, c.mesh);
+      if (ahead < ntiles) ahead = atomicAdd(counter, 1);
     }
   }
   __device__ Cursor next(const Cursor &c) {

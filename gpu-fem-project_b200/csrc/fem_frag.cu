@@ -452,11 +452,17 @@ struct PairQueue {
   int mesh;
   int64_t pos, tend;
   bool done;
+  // lane 0: the tile after the current one, taken one tile ahead so that the queue
+  // atomic's latency (long behind a later colour's reductions in L2) is hidden
+  int ahead = -1;
   __device__ PairCursor next(int lane) {
     PairCursor c{0, 0, 0};
     while (!done && pos >= tend) {
       int t = 0;
-      if (lane == 0) t = atomicAdd(counter, 1);
+      if (lane == 0) {
+        t = ahead < 0 ? atomicAdd(counter, 1) : ahead;
+        ahead = t < ntiles ? atomicAdd(counter, 1) : ntiles;
+      }
       t = __shfl_sync(0xffffffffu, t, 0);
       if (t >= ntiles) {
         done = true;

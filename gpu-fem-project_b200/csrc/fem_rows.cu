@@ -208,9 +208,13 @@ __global__ void __launch_bounds__(32 * kRowWarps, 3) rows_p1_batched_kernel(cons
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double NP, NM;
   p1_basis(NP, NM);
+  int ahead = -1;  // lane 0: the next tile, taken one tile ahead (hides the queue atomic's latency)
   for (;;) {
     int t = 0;
-    if (lane == 0) t = atomicAdd(counter, 1);
+    if (lane == 0) {
+      t = ahead < 0 ? atomicAdd(counter, 1) : ahead;
+      ahead = t < ntiles ? atomicAdd(counter, 1) : ntiles;
+    }
     t = __shfl_sync(0xffffffffu, t, 0);
     if (t >= ntiles) break;
     const Tile tl = tiles[t];
