@@ -5,12 +5,17 @@
 // stay on the device; admission is refused with FEM_ERR_BUDGET when the device
 // bytes would exceed the server's budget) and then submit requests, each with a
 // new host state and a host buffer for the residual.  A dispatcher thread takes
-// pending requests in arrival order (up to maxBatch requests and, past the first
-// one, up to kWaveElements elements, so that one large mesh does not hold a crowd
-// of small ones) whenever one of the server's kLanes lanes is free, and issues on
-// that lane's stream: the state copies, one batched persistent launch per (order,
-// colour) over the requested meshes' tiles, and the residual copies, smallest
-// first, each followed by an event of its request.  Requests that arrive while
+// pending requests whenever one of the server's kLanes lanes is free: the small
+// ones (meshes of at most kSmallRequest elements) first, in arrival order, up to
+// kSmallWave elements, so that a small request never waits inside a large wave;
+// else all of them in arrival order (also once the oldest has waited kMaxWait),
+// up to maxBatch requests and, past the first one, kWaveElements elements.  It
+// issues on that lane's stream: the wave's mesh table and tile list, the state
+// copies, one batched persistent launch per (order, colour) over the requested
+// meshes' tiles, and the residual copies, smallest first, each followed by an
+// event of its request.  Each lane has a high- and a low-priority stream: waves
+// of at most kSmallWave elements run on the high-priority one, so that the block
+// scheduler starts their kernels ahead of the queued launches of larger waves.  Requests that arrive while
 // lanes are busy go to the next free lane, so waves overlap on the device; a
 // waiter thread per lane completes each request as soon as its own residual has
 // arrived.  Results do not depend on which requests share a wave (see the batched
@@ -36,6 +41,9 @@ namespace {
 constexpr int kLanes = 4;
 constexpr int kMaxColoursS = 64;
 constexpr int64_t kWaveElements = 1 << 21;  // element cap of a wave past its first request
+constexpr int64_t kSmallRequest = 1 << 15;  // requests taken first
+constexpr int64_t kSmallWave = 1 << 17;     // waves up to this many elements run at high priority
+constexpr double kMaxWait = 0.01;           // seconds: past this the oldest request goes first
 
 double now_seconds() {
   using namespace std::chrono;
@@ -60,7 +68,8 @@ struct Request {
 };
 
 struct Lane {
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;  // the current wave's stream: hi or lo
+  cudaStream_t hi = nullptr, lo = nullptr;
   cudaEvent_t done = nullptr;
   std::vector<cudaEvent_t> reqDone;  // per request of the wave, after its residual copy (maxBatch events)
   std::vector<int> doneOrder;        // wave positions in the order their events were recorded
@@ -200,13 +209,13 @@ int issue_wave(fem_server *S, Lane &L, const std::vector<ServerMesh> &wm, const 
   off.push_back((int)L.tiles.size());
   int st = lane_reserve(L, n, std::max<size_t>(L.tiles.size(), 1));
   if (st) return st;
-  // inputs: new states
-  for (int i = 0; i < n; i++) {
-    const ServerMesh &m = wm[i];
-    err = cudaMemcpyAsync(m.states, rq[i]->hostStates, sizeof(double) * 2 * m.plan->numNodes, cudaMemcpyHostToDevice,
-                          L.stream);
-    if (err != cudaSuccess) return fem::cuda_fail(err, "state upload");
-  }
+  int64_t waveElements = 0;
+  for (int i = 0; i < n; i++) waveElements += wm[i].plan->numElements;
+  L.stream = waveElements <= kSmallWave ? L.hi : L.lo;
+  // The mesh table and tile list come from pageable vectors: a pageable upload
+  // first waits for the stream's earlier work, so it goes before the state
+  // uploads, on the lane's idle stream (after them it would hold the dispatcher
+  // until the states had crossed PCIe).
   err = cudaMemcpyAsync(L.d_args, L.args.data(), sizeof(fem::dev::AsmArgs) * n, cudaMemcpyHostToDevice, L.stream);
   if (err == cudaSuccess && !L.tiles.empty())
     err = cudaMemcpyAsync(L.d_tiles, L.tiles.data(), sizeof(fem::dev::Tile) * L.tiles.size(), cudaMemcpyHostToDevice,
@@ -214,6 +223,13 @@ int issue_wave(fem_server *S, Lane &L, const std::vector<ServerMesh> &wm, const 
   if (err == cudaSuccess)
     err = cudaMemsetAsync(L.d_counters, 0, sizeof(int) * 5 * kMaxColoursS, L.stream);
   if (err != cudaSuccess) return fem::cuda_fail(err, "wave staging");
+  // inputs: new states
+  for (int i = 0; i < n; i++) {
+    const ServerMesh &m = wm[i];
+    err = cudaMemcpyAsync(m.states, rq[i]->hostStates, sizeof(double) * 2 * m.plan->numNodes, cudaMemcpyHostToDevice,
+                          L.stream);
+    if (err != cudaSuccess) return fem::cuda_fail(err, "state upload");
+  }
   for (size_t j = 0; j < keys.size(); j++) {
     const int p = keys[j].first, c = keys[j].second;
     if (c < 0) {  // row assembly, queue counter [0][0]
@@ -269,13 +285,25 @@ void dispatcher_main(fem_server *S) {
     std::vector<ServerMesh> wm;
     std::vector<Request *> rq;
     L.reqs.clear();
+    auto elements_of = [&](int64_t tk) { return S->meshes[S->reqs[tk].mesh].plan->numElements; };
+    bool smallFirst = false;
+    if (now_seconds() - S->reqs[S->pending.front()].tSubmit < kMaxWait)
+      for (int64_t tk : S->pending)
+        if (elements_of(tk) <= kSmallRequest) {
+          smallFirst = true;
+          break;
+        }
     int64_t waveElements = 0;
-    while (!S->pending.empty() && (int)L.reqs.size() < S->maxBatch) {
-      const int64_t tk = S->pending.front();
-      const int64_t ne = S->meshes[S->reqs[tk].mesh].plan->numElements;
-      if (!L.reqs.empty() && waveElements + ne > kWaveElements) break;
+    for (auto it = S->pending.begin(); it != S->pending.end() && (int)L.reqs.size() < S->maxBatch;) {
+      const int64_t tk = *it;
+      const int64_t ne = elements_of(tk);
+      if (smallFirst && ne > kSmallRequest) {
+        ++it;
+        continue;
+      }
+      if (!L.reqs.empty() && waveElements + ne > (smallFirst ? kSmallWave : kWaveElements)) break;
       waveElements += ne;
-      S->pending.pop_front();
+      it = S->pending.erase(it);
       Request &r = S->reqs[tk];
       L.reqs.push_back(tk);
       wm.push_back(S->meshes[r.mesh]);
@@ -285,6 +313,9 @@ void dispatcher_main(fem_server *S) {
     S->waves++;
     lk.unlock();
     int st = issue_wave(S, L, wm, rq);
+    // a failed wave may have left work on its stream; the lane's next wave (on
+    // either stream) reuses the mesh table and tile buffers
+    if (st) cudaStreamSynchronize(L.stream);
     lk.lock();
     if (st) {
       for (int64_t tk : L.reqs) {
@@ -353,13 +384,15 @@ void server_free(fem_server *S) {
   cudaGetDevice(&cur);
   cudaSetDevice(S->device);
   for (auto &L : S->lanes) {
-    if (L.stream) cudaStreamSynchronize(L.stream);
+    if (L.hi) cudaStreamSynchronize(L.hi);
+    if (L.lo) cudaStreamSynchronize(L.lo);
     cudaFree(L.d_args);
     cudaFree(L.d_tiles);
     cudaFree(L.d_counters);
     if (L.done) cudaEventDestroy(L.done);
     for (cudaEvent_t e : L.reqDone) cudaEventDestroy(e);
-    if (L.stream) cudaStreamDestroy(L.stream);
+    if (L.hi) cudaStreamDestroy(L.hi);
+    if (L.lo) cudaStreamDestroy(L.lo);
   }
   for (auto &m : S->meshes) {
     if (!m.plan) continue;
@@ -389,9 +422,12 @@ int fem_server_create(int64_t budgetBytes, int precision, int maxBatch, fem_serv
   S->budget = budgetBytes;
   S->precision = precision;
   S->maxBatch = maxBatch;
-  cudaError_t err = cudaSuccess;
+  int leastPri = 0, greatestPri = 0;
+  cudaError_t err = cudaDeviceGetStreamPriorityRange(&leastPri, &greatestPri);
   for (auto &L : S->lanes) {
-    if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking);
+    if (err == cudaSuccess) err = cudaStreamCreateWithPriority(&L.hi, cudaStreamNonBlocking, greatestPri);
+    if (err == cudaSuccess) err = cudaStreamCreateWithPriority(&L.lo, cudaStreamNonBlocking, leastPri);
+    L.stream = L.lo;
     if (err == cudaSuccess) err = cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming);
     if (err == cudaSuccess) err = cudaMalloc(&L.d_counters, sizeof(int) * 5 * kMaxColoursS);
     L.reqDone.assign((size_t)maxBatch, nullptr);

@@ -321,11 +321,16 @@ int fem_batch_replay(fem_batch *batch, void *stream, double *elapsedSeconds);
 /* ---- serving: continuous batching over device-resident meshes ------------------------- */
 /* A server keeps client meshes resident (plan, coordinates, state, residual and
  * matrix) within a device-memory budget and assembles submitted requests in
- * waves: whenever one of its four lanes is free, the pending requests in arrival
- * order (up to maxBatch, and past the first up to 2^21 elements) are copied in,
- * assembled by the batched persistent kernels and their residuals copied back,
- * smallest first, while other lanes may still be running; each request completes
- * as soon as its own residual has arrived.  (No reference counterpart.) */
+ * waves: whenever one of its four lanes is free, the pending requests of meshes
+ * with at most 2^15 elements (in arrival order, up to 2^17 elements per wave),
+ * or, when there are none or the oldest request has waited 10 ms, all pending
+ * requests in arrival order (up to maxBatch, and past the first up to 2^21
+ * elements) are copied in, assembled by the batched persistent kernels (waves
+ * of at most 2^17 elements on a high-priority stream) and their residuals copied
+ * back, smallest first, while other lanes may still be running; each request
+ * completes as soon as its own residual has arrived.  Host state and residual
+ * buffers should be page-locked: a pageable one makes its copy synchronous.
+ * (No reference counterpart.) */
 typedef struct fem_server fem_server;
 
 int fem_server_create(int64_t budgetBytes, int precision, int maxBatch, fem_server **server);
