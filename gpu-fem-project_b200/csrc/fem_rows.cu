@@ -38,51 +38,94 @@ constexpr int kRowWarps = 4;
 __device__ __forceinline__ int acc_pos(int i) { return 2 * i + i / 9; }
 constexpr int kAccUnits = 2 * kRowChunkBlocks + kRowChunkBlocks / 9 + 1;  // double2 per warp
 
-// One chunk c of mesh M, by the calling warp; acc is the warp's kAccUnits double2
-// of shared memory.  NP, NM: the 1D basis values at the Gauss point on the node's
-// own side / the opposite side, fma(0.5, g, 0.5) and fma(-0.5, g, 0.5) as in
-// lagrangePoly1dDeriv<double,1>.  For the bilinear element the xi-column of
-// J = sum_b x_b (x) dN_b depends on the point's eta only and the eta-column on its
-// xi only: with the edge vectors e0 = x1 - x0, e1 = x3 - x2, f0 = x2 - x0,
-// f1 = x3 - x1, dx/dxi(qy) = (NP e_qy + NM e_(1-qy)) / 2 and
-// dx/deta(qx) = (NP f_qx + NM f_(1-qx)) / 2 (likewise for the states).
-template <int MODE>
-__device__ __forceinline__ void row_chunk(const AsmArgs &M, int64_t c, double2 *acc, int lane, double NP, double NM) {
-  const int r0 = __ldg(M.rowChunk + c), r1 = __ldg(M.rowChunk + c + 1);
-  const int blk0 = __ldg(M.rowp + r0), nb = __ldg(M.rowp + r1) - blk0;
-  if constexpr ((MODE & kJac) != 0) {
-    for (int i = lane; i < nb; i += 32) {
-      acc[acc_pos(i)] = make_double2(0.0, 0.0);
-      acc[acc_pos(i) + 1] = make_double2(0.0, 0.0);
-    }
+// A chunk's header as one lane sees it: the chunk's rows [r0, r1) and blocks
+// [blk0, blk0 + nb), the lane's row r0 + lane, its first block relative to blk0
+// and its rowElem entries [j0, j1) (empty past r1).
+struct RowHead {
+  int r0, r1, blk0, nb, base, j0, j1;
+};
+
+__device__ __forceinline__ RowHead row_head(const AsmArgs &M, int r0, int r1, int lane) {
+  RowHead h{r0, r1, 0, 0, 0, 0, 0};
+  h.blk0 = __ldg(M.rowp + r0);
+  h.nb = __ldg(M.rowp + r1) - h.blk0;
+  const int r = r0 + lane;
+  if (r < r1) {
+    h.base = __ldg(M.rowp + r) - h.blk0;
+    h.j0 = __ldg(M.rowElemPtr + r);
+    h.j1 = __ldg(M.rowElemPtr + r + 1);
   }
-  __syncwarp();
+  return h;
+}
+
+// Chunks c, c + stride, ... < end of mesh M, by the calling warp; acc is the
+// warp's kAccUnits double2 of shared memory.  NP, NM: the 1D basis values at the
+// Gauss point on the node's own side / the opposite side, fma(0.5, g, 0.5) and
+// fma(-0.5, g, 0.5) as in lagrangePoly1dDeriv<double,1>.  For the bilinear
+// element the xi-column of J = sum_b x_b (x) dN_b depends on the point's eta only
+// and the eta-column on its xi only: with the edge vectors e0 = x1 - x0,
+// e1 = x3 - x2, f0 = x2 - x0, f1 = x3 - x1, dx/dxi(qy) = (NP e_qy + NM e_(1-qy)) / 2
+// and dx/deta(qx) = (NP f_qx + NM f_(1-qx)) / 2 (likewise for the states).
+//
+// The loads run ahead of the arithmetic across chunk boundaries, so that a chunk
+// does not start with its dependent chain (row range -> row pointers and element
+// ranges -> rowElem entry -> node ids -> coordinates and states) exposed: the row
+// range of the chunk after next and the header of the next chunk are loaded when a
+// chunk starts, and each lane's element pipeline (nodal data one entry ahead,
+// rowElem entry and node ids two ahead) runs over the lane's entries of the
+// current chunk followed by those of the next.
+template <int MODE>
+__device__ __forceinline__ void row_stream(const AsmArgs &M, int64_t c, int64_t end, int64_t stride, double2 *acc,
+                                           int lane, double NP, double NM) {
+  if (c >= end) return;
   const double mu = M.mu, lam = M.lam, thick = M.t, c11 = lam + 2.0 * mu;
   const double hP = 0.5 * NP, hM = 0.5 * NM;
   const int2 *rowElem = reinterpret_cast<const int2 *>(M.rowElem);
   const int4 *conn4 = reinterpret_cast<const int4 *>(M.connList);
   const double2 *X2 = reinterpret_cast<const double2 *>(M.coords);
   const double2 *U2 = reinterpret_cast<const double2 *>(M.states);
-  const int r = r0 + lane;
-  double rx = 0.0, ry = 0.0;
-  if (r < r1) {
-    const int base = __ldg(M.rowp + r) - blk0;
-    const int j0 = __ldg(M.rowElemPtr + r), j1 = __ldg(M.rowElemPtr + r + 1);
-    // software pipeline: nodal data of entry j in x/u, header of j+1 in enN/ndN
-    int2 enC = make_int2(0, 0), enN = make_int2(0, 0);
-    int4 ndN = make_int4(0, 0, 0, 0);
-    double2 x[4], u[4];
-    if (j0 < j1) {
-      enC = __ldg(rowElem + j0);
-      const int4 nd = __ldg(conn4 + (enC.x >> 2));
-      x[0] = __ldg(X2 + nd.x), x[1] = __ldg(X2 + nd.y), x[2] = __ldg(X2 + nd.z), x[3] = __ldg(X2 + nd.w);
-      u[0] = __ldg(U2 + nd.x), u[1] = __ldg(U2 + nd.y), u[2] = __ldg(U2 + nd.z), u[3] = __ldg(U2 + nd.w);
-    }
-    if (j0 + 1 < j1) {
-      enN = __ldg(rowElem + j0 + 1);
+  RowHead h = row_head(M, __ldg(M.rowChunk + c), __ldg(M.rowChunk + c + 1), lane);
+  int64_t cn = c + stride;
+  int n0 = 0, n1 = 0;  // row range of chunk cn
+  if (cn < end) n0 = __ldg(M.rowChunk + cn), n1 = __ldg(M.rowChunk + cn + 1);
+  // element pipeline over this lane's entries (current chunk, then next chunk):
+  // nodal data of entry k in x/u and its rowElem entry in enC, entry k + 1 in enN/ndN
+  int2 enC = make_int2(0, 0), enN = make_int2(0, 0);
+  int4 ndN = make_int4(0, 0, 0, 0);
+  double2 x[4], u[4];
+  auto load_nodes = [&](int4 nd) {
+    x[0] = __ldg(X2 + nd.x), x[1] = __ldg(X2 + nd.y), x[2] = __ldg(X2 + nd.z), x[3] = __ldg(X2 + nd.w);
+    u[0] = __ldg(U2 + nd.x), u[1] = __ldg(U2 + nd.y), u[2] = __ldg(U2 + nd.z), u[3] = __ldg(U2 + nd.w);
+  };
+  int lenC = h.j1 - h.j0;
+  if (lenC > 0) {
+    enC = __ldg(rowElem + h.j0);
+    load_nodes(__ldg(conn4 + (enC.x >> 2)));
+  }
+  if (lenC > 1) {
+    enN = __ldg(rowElem + h.j0 + 1);
+    ndN = __ldg(conn4 + (enN.x >> 2));
+  }
+  for (;;) {
+    const bool hasN = cn < end;
+    RowHead hn{0, 0, 0, 0, 0, 0, 0};
+    if (hasN) hn = row_head(M, n0, n1, lane);
+    const int64_t cnn = cn + stride;
+    if (hasN && cnn < end) n0 = __ldg(M.rowChunk + cnn), n1 = __ldg(M.rowChunk + cnn + 1);
+    const int lenN = hn.j1 - hn.j0, tot = lenC + lenN;
+    if (lenC == 1 && lenN > 0) {  // entry 1 is the next chunk's first
+      enN = __ldg(rowElem + hn.j0);
       ndN = __ldg(conn4 + (enN.x >> 2));
     }
-    for (int j = j0; j < j1; j++) {
+    if constexpr ((MODE & kJac) != 0) {
+      for (int i = lane; i < h.nb; i += 32) {
+        acc[acc_pos(i)] = make_double2(0.0, 0.0);
+        acc[acc_pos(i) + 1] = make_double2(0.0, 0.0);
+      }
+    }
+    __syncwarp();
+    double rx = 0.0, ry = 0.0;
+    for (int k = 0; k < lenC; k++) {
       // J and grad-u columns at the two eta (xi-derivative) and two xi (eta-derivative) values
       double2 Jxi[2], Jeta[2], Uxi[2], Ueta[2];
       {
@@ -104,14 +147,13 @@ __device__ __forceinline__ void row_chunk(const AsmArgs &M, int64_t c, double2 *
         Ueta[1] = make_double2(hM * b0.x + hP * b1.x, hM * b0.y + hP * b1.y);
       }
       const int2 en = enC;
-      // prefetch: nodal data of entry j+1, header of entry j+2
-      if (j + 1 < j1) {
-        x[0] = __ldg(X2 + ndN.x), x[1] = __ldg(X2 + ndN.y), x[2] = __ldg(X2 + ndN.z), x[3] = __ldg(X2 + ndN.w);
-        u[0] = __ldg(U2 + ndN.x), u[1] = __ldg(U2 + ndN.y), u[2] = __ldg(U2 + ndN.z), u[3] = __ldg(U2 + ndN.w);
+      // prefetch: nodal data of entry k + 1, rowElem entry and node ids of entry k + 2
+      if (k + 1 < tot) {
+        load_nodes(ndN);
         enC = enN;
       }
-      if (j + 2 < j1) {
-        enN = __ldg(rowElem + j + 2);
+      if (k + 2 < tot) {
+        enN = __ldg(rowElem + (k + 2 < lenC ? h.j0 + k + 2 : hn.j0 + (k + 2 - lenC)));
         ndN = __ldg(conn4 + (enN.x >> 2));
       }
       const int a = en.x & 3, ax = a & 1, ay = a >> 1;
@@ -161,26 +203,38 @@ __device__ __forceinline__ void row_chunk(const AsmArgs &M, int64_t c, double2 *
           const double kxy = lam * Mm[b][1] + mu * Mm[b][2];
           const double kyx = lam * Mm[b][2] + mu * Mm[b][1];
           const double kyy = c11 * Mm[b][3] + mu * Mm[b][0];
-          double2 *sp = acc + acc_pos(base + ((en.y >> (8 * b)) & 0xff));
+          double2 *sp = acc + acc_pos(h.base + ((en.y >> (8 * b)) & 0xff));
           const double2 p0 = sp[0], p1 = sp[1];
           sp[0] = make_double2(p0.x + kxx, p0.y + kxy);
           sp[1] = make_double2(p1.x + kyx, p1.y + kyy);
         }
       }
     }
-  }
-  __syncwarp();
-  if constexpr ((MODE & kRes) != 0) {
-    if (r < r1) reinterpret_cast<double2 *>(M.residual)[r] = make_double2(rx, ry);
-  }
-  if constexpr ((MODE & kJac) != 0) {
-    double *dst = M.mat + 4 * (int64_t)blk0;
-    for (int i = lane; i < nb; i += 32) {
-      const double2 p0 = acc[acc_pos(i)], p1 = acc[acc_pos(i) + 1];
-      store_block(dst + 4 * i, p0.x, p0.y, p1.x, p1.y);
+    __syncwarp();
+    if constexpr ((MODE & kRes) != 0) {
+      if (h.r0 + lane < h.r1) reinterpret_cast<double2 *>(M.residual)[h.r0 + lane] = make_double2(rx, ry);
     }
+    if constexpr ((MODE & kJac) != 0) {
+      double *dst = M.mat + 4 * (int64_t)h.blk0;
+      for (int i = lane; i < h.nb; i += 32) {
+        const double2 p0 = acc[acc_pos(i)], p1 = acc[acc_pos(i) + 1];
+        store_block(dst + 4 * i, p0.x, p0.y, p1.x, p1.y);
+      }
+    }
+    __syncwarp();
+    if (!hasN) break;
+    if (lenC == 0 && lenN > 0) {  // this lane's pipeline starts in the next chunk
+      enC = __ldg(rowElem + hn.j0);
+      load_nodes(__ldg(conn4 + (enC.x >> 2)));
+      if (lenN > 1) {
+        enN = __ldg(rowElem + hn.j0 + 1);
+        ndN = __ldg(conn4 + (enN.x >> 2));
+      }
+    }
+    h = hn;
+    lenC = lenN;
+    cn = cnn;
   }
-  __syncwarp();
 }
 
 __device__ __forceinline__ void p1_basis(double &NP, double &NM) {
@@ -195,9 +249,8 @@ __global__ void __launch_bounds__(32 * kRowWarps, 3) rows_p1_kernel(const __grid
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double NP, NM;
   p1_basis(NP, NM);
-  const int64_t end = A.begin + A.count, stride = (int64_t)gridDim.x * kRowWarps;
-  for (int64_t c = A.begin + (int64_t)blockIdx.x * kRowWarps + warp; c < end; c += stride)
-    row_chunk<MODE>(A, c, acc[warp], lane, NP, NM);
+  row_stream<MODE>(A, A.begin + (int64_t)blockIdx.x * kRowWarps + warp, A.begin + A.count,
+                   (int64_t)gridDim.x * kRowWarps, acc[warp], lane, NP, NM);
 }
 
 // Many meshes: warps pull tiles (mesh, `count` chunks from `begin`) from the queue.
@@ -219,7 +272,7 @@ __global__ void __launch_bounds__(32 * kRowWarps, 3) rows_p1_batched_kernel(cons
     if (t >= ntiles) break;
     const Tile tl = tiles[t];
     const AsmArgs &M = meshes[tl.mesh];
-    for (int64_t c = tl.begin; c < tl.begin + tl.count; c++) row_chunk<kRes | kJac>(M, c, acc[warp], lane, NP, NM);
+    row_stream<kRes | kJac>(M, tl.begin, tl.begin + tl.count, 1, acc[warp], lane, NP, NM);
   }
 }
 
