@@ -321,7 +321,7 @@ int fem_batch_replay(fem_batch *batch, void *stream, double *elapsedSeconds);
 /* ---- serving: continuous batching over device-resident meshes ------------------------- */
 /* A server keeps client meshes resident (plan, coordinates, state, residual and
  * matrix) within a device-memory budget and assembles submitted requests in
- * waves: whenever one of its four lanes is free, the pending requests of meshes
+ * waves: whenever one of its eight lanes is free, the pending requests of meshes
  * with at most 2^15 elements (in arrival order, up to 2^17 elements per wave),
  * or, when there are none or the oldest request has waited 10 ms, all pending
  * requests in arrival order (up to maxBatch, and past the first up to 2^21
