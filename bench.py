@@ -156,7 +156,7 @@ def reference_sample(mesh_mod, orc, args):
     """The bounded CPU sample of the workload: its first elements, with the pattern
     and element map from the oracle's own builders (nothing from the library)."""
     mesh = make_mesh(mesh_mod, args.workload)
-    sample = min(mesh.num_elements, args.ref_elements)
+    sample = min(mesh.num_elements, args.ref_elements or 131072)
     sub = mesh_mod.submesh(mesh, 0, sample)
     rowp, cols = orc.bsr_pattern(sub.num_nodes, sub.conn_ptr, sub.conn)
     mp = orc.element_bsr_map(sub.conn_ptr, sub.conn, sub.nodes_per_element, rowp, cols)
@@ -202,6 +202,8 @@ def run_reference(args):
     import fem_pkg
     import oracle as orc
     mesh_mod = fem_pkg.load_module("mesh")
+    if args.ref_elements is None:  # each step a bounded sample: about 20 x 131072 elements in all
+        args.ref_elements = max(32768, min(131072, 131072 * 20 // max(1, args.steps)))
     mesh, sub, mp, nnzb = reference_sample(mesh_mod, orc, args)
     threads = os.cpu_count() or 1
     kind, what, run = reference_assembler(orc, threads)
@@ -909,7 +911,7 @@ def measure_peaks():
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=400, help="timed steps (400 x ~2.6 ms: a region of about 1 s)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="square1024_p3", choices=sorted(WORKLOADS) + ["batch256", "serve64"])
@@ -926,7 +928,9 @@ def main():
     ap.add_argument("--leg-steps", type=int, default=10)
     ap.add_argument("--leg-rates", type=lambda v: [float(x) for x in v.split(",")], default=[1000, 5000])
     ap.add_argument("--leg-serve-seconds", type=float, default=2.0)
-    ap.add_argument("--ref-elements", type=int, default=131072)
+    ap.add_argument("--ref-elements", type=int, default=None,
+                    help="elements of the CPU sample (default 131072; in --impl reference scaled down with "
+                         "--steps so that the run stays near 20 steps of 131072 elements, at least 32768)")
     ap.add_argument("--bands", type=int, default=32, help="element bands / node chunks of the end-to-end call")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
