@@ -564,7 +564,8 @@ def batched_measure(fem, dev, waves, steps, warmup, precisions):
     stream = torch.cuda.Stream(device=dev)
     sptr = stream.cuda_stream
     out = {"elements": 0, "ms": {p: 0.0 for p in precisions}, "ms_plain": 0.0, "launches": {p: 0 for p in precisions},
-           "tiles": {p: [] for p in precisions}, "kernels": {p: [] for p in precisions}, "errs": [],
+           "tiles": {p: [] for p in precisions}, "kernels": {p: [] for p in precisions},
+           "ordered": {p: [] for p in precisions}, "errs": [],
            "wave_ms": {p: [] for p in precisions}}
 
     def ev_time(fn, reps):
@@ -591,6 +592,7 @@ def batched_measure(fem, dev, waves, steps, warmup, precisions):
             batch.tune(precision=prec, stream=sptr, reps=2)
             out["tiles"][prec].append(batch.info()["tile_batches"])
             out["kernels"][prec].append(batch.kernels(prec))
+            out["ordered"][prec].append(batch.ordered())
             batch.capture(precision=prec, stream=sptr)
             for _ in range(warmup):
                 batch.replay(stream=sptr)
@@ -663,9 +665,11 @@ def batch_leg(fem, dev, args, plain_single):
                      f"first in draw order within {args.leg_batch_gb:g} GB, one captured graph per precision"),
         "meshes": len(chosen), "elements": el, "elements_per_order": per_order,
         "fp64": {"elements_per_s": el / (r["ms"]["fp64"] * 1e-3), "ms_per_step": r["ms"]["fp64"],
-                 "tuned_tile_batches": r["tiles"]["fp64"][0], "tuned_kernels": r["kernels"]["fp64"][0]},
+                 "tuned_tile_batches": r["tiles"]["fp64"][0], "tuned_kernels": r["kernels"]["fp64"][0],
+                 "tuned_ordered": r["ordered"]["fp64"][0]},
         "mixed": {"elements_per_s": el / (r["ms"]["mixed"] * 1e-3), "ms_per_step": r["ms"]["mixed"],
                   "tuned_tile_batches": r["tiles"]["mixed"][0], "tuned_kernels": r["kernels"]["mixed"][0],
+                  "tuned_ordered": r["ordered"]["mixed"][0],
                   "rel_frobenius_err_vs_fp64_max": max(r["errs"]) if r["errs"] else None},
         "plain_fp64_dropin_same_meshes": {"elements_per_s": el / (r["ms_plain"] * 1e-3), "ms_per_step": r["ms_plain"],
                                           "note": "zero the outputs, fem_run_jacobian per mesh"},
@@ -848,6 +852,7 @@ def run_batch(args):
         "batched_over_plain": r["ms_plain"] / r["ms"][prec],
         "wave_graph_ms": r["wave_ms"][prec], "tuned_tile_batches": r["tiles"][prec],
         "tuned_kernels": r["kernels"][prec],
+        "tuned_ordered": r["ordered"][prec],
         "mixed_rel_frobenius_err_max": max(r["errs"]) if r["errs"] else None,
         "gpu_launches": r["launches"][prec],
     }

@@ -96,6 +96,10 @@ SIGNATURES = {
     "fem_batch_tune": (_i, [_p, _i, _p, _i, _pd]),
     "fem_batch_get_kernels": (_i, [_p, _i, _p]),
     "fem_batch_set_kernels": (_i, [_p, _i, _p]),
+    "fem_batch_set_ordered": (_i, [_p, _p]),
+    "fem_batch_get_ordered": (_i, [_p, _p]),
+    "fem_batch_wait_status": (_i, [_p, _p, _pi64]),
+    "fem_batch_set_schedule_waits": (_i, [_p, _i64, _i, _i]),
     "fem_batch_capture": (_i, [_p, _i, _p]),
     "fem_batch_replay": (_i, [_p, _p, _pd]),
 }

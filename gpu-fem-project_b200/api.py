@@ -345,7 +345,30 @@ class Batch:
         tiles = (C.c_int * 4)()
         check(lib.fem_batch_get_tiles(self._h, tiles), "fem_batch_get_tiles")
         return {"elements": ne.value, "tiles": nt.value, "launches": nl.value, "device_bytes": bytes_.value,
-                "tile_batches": list(tiles), "kernels_fp64": self.kernels("fp64"), "kernels_mixed": self.kernels("mixed")}
+                "tile_batches": list(tiles), "kernels_fp64": self.kernels("fp64"), "kernels_mixed": self.kernels("mixed"),
+                "ordered": self.ordered()}
+
+    def ordered(self):
+        """Per order (1..4): 1 where its colours run as one dependency-ordered launch."""
+        arr = (C.c_int * 4)()
+        check(lib.fem_batch_get_ordered(self._h, arr), "fem_batch_get_ordered")
+        return list(arr)
+
+    def set_ordered(self, ordered):
+        """Per order (1..4; order 1 must be 0): one dependency-ordered launch for all colours."""
+        arr = (C.c_int * 4)(*[int(x) for x in ordered])
+        check(lib.fem_batch_set_ordered(self._h, arr), "fem_batch_set_ordered")
+
+    def wait_status(self, *, stream=None):
+        """Bounded in-kernel waits of the dependency-ordered launches that ran out (cleared)."""
+        n = C.c_int64(0)
+        check(lib.fem_batch_wait_status(self._h, _stream(stream), C.byref(n)), "fem_batch_wait_status")
+        return n.value
+
+    def set_schedule_waits(self, order, wait_limit_ns=0, stall_group=-1):
+        """Failure injection: wait limit and a group whose completion no wait observes."""
+        check(lib.fem_batch_set_schedule_waits(self._h, int(wait_limit_ns), int(order), int(stall_group)),
+              "fem_batch_set_schedule_waits")
 
     def kernels(self, precision="fp64"):
         """Kernel variant per order (1..4) for `precision`, by name (FEM_KERNEL_*)."""

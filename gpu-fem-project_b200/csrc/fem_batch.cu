@@ -18,7 +18,9 @@
 // FP64 or, MIXED, FP32 element products, at order 4 MIXED also with its stiffness
 // as BF16x6 tcgen05 MMAs), or order-1 row assembly.  MIXED may run
 // any FP64 variant (FP64 is within its error bound); FP64 runs FP64 variants only.
-// The tuner also picks the tile length of the order's work queues.
+// The tuner also picks the tile length of the order's work queues and, for the
+// fragment kernels, whether an order's colours run as one launch each or all in
+// one dependency-ordered persistent launch (fem_batch_set_ordered).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -175,6 +177,13 @@ struct fem_batch {
   size_t d_tiles_cap = 0;
   bool tiles_dirty = true;
   int *d_counters = nullptr;  // [kOrders][kMaxColours]
+  // per order: 1 = its colours in one dependency-ordered launch (fragment variants)
+  int ordered[kOrders] = {};
+  unsigned char *d_sched[kOrders] = {};
+  fem::dev::SchedArgs sched[kOrders] = {};
+  int schedGroups[kOrders] = {};
+  int64_t schedBytes[kOrders] = {};
+  bool sched_dirty = true;
   cudaStream_t streams[kOrders] = {};  // [0]: capture stream, [1..4]: one per order
   cudaEvent_t fork = nullptr, join[kOrders] = {};
   cudaGraph_t graph = nullptr;
@@ -203,6 +212,7 @@ void batch_free(fem_batch *b) {
   cudaFree(b->d_args);
   cudaFree(b->d_tiles);
   cudaFree(b->d_counters);
+  for (int p = 0; p < kOrders; p++) cudaFree(b->d_sched[p]);
   for (int p = 0; p < kOrders; p++) {
     if (b->streams[p]) cudaStreamDestroy(b->streams[p]);
     if (b->join[p]) cudaEventDestroy(b->join[p]);
@@ -257,11 +267,92 @@ void build_tiles(fem_batch *b) {
   }
   b->rowTile1 = (int)b->tiles.size();
   b->tiles_dirty = true;
+  b->sched_dirty = true;
+}
+
+// The dependency-ordered launch of order p: one group per (mesh, colour), listed
+// colours outermost (every mesh's colour 0, then every mesh's colour 1, ...), each
+// cut into tiles of the order's tile length; a group waits for its mesh's previous
+// colour, so every block still receives its contributions in colour order (the
+// result equals the colour launches' bit for bit).  A warp holds only tiles it has
+// pulled, in dispatch order, and every dependency is an earlier group: the
+// earliest unfinished tile can always proceed.
+int build_sched(fem_batch *b, int p) {
+  cudaFree(b->d_sched[p]);
+  b->d_sched[p] = nullptr;
+  b->sched[p] = fem::dev::SchedArgs{};
+  b->schedGroups[p] = 0;
+  b->schedBytes[p] = 0;
+  const int C = b->maxColours;
+  const int64_t len = (int64_t)b->tileBatches[p] * fem::epg_of(p);
+  std::vector<fem::dev::SchedTile> tiles;
+  std::vector<int> groupTiles, depPtr(1, 0), deps, last(b->plans.size(), -1);
+  for (int c = 0; c < C; c++)
+    for (size_t m = 0; m < b->plans.size(); m++) {
+      const fem_plan *pl = b->plans[m];
+      if (pl->order != p || c >= pl->numColours || fem::plan_rows(pl)) continue;
+      const int g = (int)groupTiles.size();
+      int n = 0;
+      for (int64_t k = pl->colourPtr[c]; k < pl->colourPtr[c + 1]; k += len, n++) {
+        fem::dev::SchedTile t;
+        t.begin = k;
+        t.count = (int)std::min<int64_t>(len, pl->colourPtr[c + 1] - k);
+        t.group = g;
+        t.mesh = (int)m;
+        tiles.push_back(t);
+      }
+      groupTiles.push_back(n);
+      if (last[m] >= 0) deps.push_back(last[m]);
+      depPtr.push_back((int)deps.size());
+      last[m] = g;
+    }
+  const int G = (int)groupTiles.size();
+  if (tiles.empty()) return FEM_SUCCESS;
+  // one allocation: tiles | groupTiles | depPtr | deps | status (2 + G words)
+  auto al = [](size_t x) { return (x + 15) & ~(size_t)15; };
+  const size_t oT = 0, oG = al(oT + tiles.size() * sizeof(fem::dev::SchedTile)), oP = al(oG + 4 * (size_t)G),
+               oD = al(oP + 4 * ((size_t)G + 1)), oS = al(oD + 4 * std::max<size_t>(deps.size(), 1)),
+               total = oS + 4 * ((size_t)G + 2);
+  cudaError_t err = cudaMalloc(&b->d_sched[p], total);
+  if (err != cudaSuccess) return fem::cuda_fail(err, "cudaMalloc(batch schedule)");
+  unsigned char *d = b->d_sched[p];
+  err = cudaMemcpy(d + oT, tiles.data(), tiles.size() * sizeof(fem::dev::SchedTile), cudaMemcpyHostToDevice);
+  if (err == cudaSuccess) err = cudaMemcpy(d + oG, groupTiles.data(), 4 * (size_t)G, cudaMemcpyHostToDevice);
+  if (err == cudaSuccess) err = cudaMemcpy(d + oP, depPtr.data(), 4 * ((size_t)G + 1), cudaMemcpyHostToDevice);
+  if (err == cudaSuccess && !deps.empty()) err = cudaMemcpy(d + oD, deps.data(), 4 * deps.size(), cudaMemcpyHostToDevice);
+  if (err == cudaSuccess) err = cudaMemset(d + oS, 0, 4 * ((size_t)G + 2));
+  if (err != cudaSuccess) return fem::cuda_fail(err, "batch schedule upload");
+  fem::dev::SchedArgs &a = b->sched[p];
+  a.tiles = reinterpret_cast<const fem::dev::SchedTile *>(d + oT);
+  a.groupTiles = reinterpret_cast<const int *>(d + oG);
+  a.depPtr = reinterpret_cast<const int *>(d + oP);
+  a.deps = reinterpret_cast<const int *>(d + oD);
+  a.status = reinterpret_cast<int *>(d + oS);
+  a.ntiles = (int)tiles.size();
+  a.stallGroup = -1;
+  a.waitLimitNs = 500000000LL;
+  b->schedGroups[p] = G;
+  b->schedBytes[p] = (int64_t)total;
+  return FEM_SUCCESS;
 }
 
 int sync_device_state(fem_batch *b) {
   cudaError_t err;
-  const bool any = b->args_dirty || b->tiles_dirty;
+  const bool any = b->args_dirty || b->tiles_dirty || b->sched_dirty;
+  if (b->sched_dirty) {
+    for (int p = 2; p < kOrders; p++) {
+      int st = b->ordered[p] ? build_sched(b, p) : FEM_SUCCESS;
+      if (!b->ordered[p] && b->d_sched[p]) {
+        cudaFree(b->d_sched[p]);
+        b->d_sched[p] = nullptr;
+        b->sched[p] = fem::dev::SchedArgs{};
+        b->schedGroups[p] = 0;
+        b->schedBytes[p] = 0;
+      }
+      if (st) return st;
+    }
+    b->sched_dirty = false;
+  }
   if (b->args_dirty) {
     err = cudaMemcpy(b->d_args, b->args.data(), sizeof(fem::dev::AsmArgs) * b->args.size(), cudaMemcpyHostToDevice);
     if (err != cudaSuccess) return fem::cuda_fail(err, "cudaMemcpy(mesh table)");
@@ -296,9 +387,25 @@ int variant_of(const fem_batch *b, int p, int precision) {
 // The colour chain of one order on stream s (counters reset by the caller).  Order
 // 1 with FEM_KERNEL_ROWS: one row-assembly launch (queue counter [0][0]) for the
 // meshes with row tables, colour launches of the element kernel for the others.
+// Whether order p runs its colours as one dependency-ordered launch with variant v.
+bool sched_launch(const fem_batch *b, int p, int v) {
+  const int C = b->maxColours;
+  return p >= 2 && b->ordered[p] && b->tileOff[p * (C + 1) + C] > b->tileOff[p * (C + 1)] &&
+         (v == FEM_KERNEL_FRAGMENT_FP64 || v == FEM_KERNEL_FRAGMENT_BF16X6);
+}
+
 int enqueue_order(fem_batch *b, int p, int precision, cudaStream_t s) {
   const int C = b->maxColours;
   const int v = variant_of(b, p, precision);
+  if (sched_launch(b, p, v)) {
+    if (b->sched[p].ntiles == 0) return FEM_SUCCESS;
+    // the tile dispenser and group counters start at zero; the sticky count of
+    // waits that ran out (word 0) is kept for fem_batch_wait_status
+    cudaError_t err = cudaMemsetAsync(b->sched[p].status + 1, 0, sizeof(int) * ((size_t)b->schedGroups[p] + 1), s);
+    if (err != cudaSuccess) return fem::cuda_fail(err, "cudaMemsetAsync(schedule counters)");
+    return fem::launch_frag_batched_sched(p, v == FEM_KERNEL_FRAGMENT_BF16X6 ? FEM_PRECISION_MIXED : FEM_PRECISION_FP64,
+                                          b->d_args, b->sched[p], s);
+  }
   const bool rows = p == 1 && v == FEM_KERNEL_ROWS;
   if (rows && b->rowTile1 > b->rowTile0) {
     int st = fem::launch_rows_batched(b->d_args, b->d_tiles + b->rowTile0, b->rowTile1 - b->rowTile0,
@@ -433,6 +540,10 @@ int fem_batch_info(const fem_batch *b, int64_t *totalElements, int64_t *numTiles
     int n = 0;
     const int C = b->maxColours;
     for (int p = 1; p < kOrders; p++) {
+      if (sched_launch(b, p, variant_of(b, p, FEM_PRECISION_FP64))) {
+        n++;
+        continue;
+      }
       const bool rows = p == 1 && variant_of(b, p, FEM_PRECISION_FP64) == FEM_KERNEL_ROWS;
       if (rows) n += b->rowTile1 > b->rowTile0;
       for (int c = 0; c < C; c++)
@@ -440,7 +551,10 @@ int fem_batch_info(const fem_batch *b, int64_t *totalElements, int64_t *numTiles
     }
     *numLaunches = n;
   }
-  if (deviceBytes) *deviceBytes = b->deviceBytes + (int64_t)(sizeof(fem::dev::Tile) * b->d_tiles_cap);
+  if (deviceBytes) {
+    *deviceBytes = b->deviceBytes + (int64_t)(sizeof(fem::dev::Tile) * b->d_tiles_cap);
+    for (int p = 0; p < kOrders; p++) *deviceBytes += b->schedBytes[p];
+  }
   return FEM_SUCCESS;
 }
 
@@ -546,6 +660,55 @@ int fem_batch_set_kernels(fem_batch *b, int precision, const int *kernels) {
   return FEM_SUCCESS;
 }
 
+int fem_batch_set_ordered(fem_batch *b, const int *ordered) {
+  fem::clear_error();
+  if (!b || !ordered) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (ordered[0] != 0) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "order 1 has no dependency-ordered launch");
+  for (int p = 2; p < kOrders; p++) b->ordered[p] = ordered[p - 1] != 0;
+  b->sched_dirty = true;
+  drop_graph(b);
+  return FEM_SUCCESS;
+}
+
+int fem_batch_get_ordered(const fem_batch *b, int *ordered) {
+  fem::clear_error();
+  if (!b || !ordered) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "NULL argument");
+  for (int p = 1; p < kOrders; p++) ordered[p - 1] = b->ordered[p];
+  return FEM_SUCCESS;
+}
+
+int fem_batch_wait_status(fem_batch *b, void *stream, int64_t *timedOutWaits) {
+  fem::clear_error();
+  if (!b || !timedOutWaits) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "NULL argument");
+  *timedOutWaits = 0;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  int v[kOrders] = {};
+  cudaError_t err = cudaSuccess;
+  for (int p = 2; p < kOrders && err == cudaSuccess; p++)
+    if (b->d_sched[p]) err = cudaMemcpyAsync(&v[p], b->sched[p].status, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+  for (int p = 2; p < kOrders && err == cudaSuccess; p++)
+    if (v[p]) err = cudaMemsetAsync(b->sched[p].status, 0, sizeof(int), s);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+  if (err != cudaSuccess) return fem::cuda_fail(err, "reading the batch's wait status");
+  for (int p = 2; p < kOrders; p++) *timedOutWaits += v[p];
+  return FEM_SUCCESS;
+}
+
+int fem_batch_set_schedule_waits(fem_batch *b, int64_t waitLimitNs, int order, int stallGroup) {
+  fem::clear_error();
+  if (!b) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "batch is NULL");
+  if (order < 2 || order > 4) return fem::fail(FEM_ERR_INVALID_ORDER, "order %d", order);
+  int st = sync_device_state(b);
+  if (st) return st;
+  if (stallGroup != -1 && (stallGroup < 0 || stallGroup >= b->schedGroups[order]))
+    return fem::fail(FEM_ERR_INVALID_ARGUMENT, "stallGroup %d of %d groups", stallGroup, b->schedGroups[order]);
+  if (waitLimitNs > 0) b->sched[order].waitLimitNs = waitLimitNs;
+  b->sched[order].stallGroup = stallGroup;
+  drop_graph(b);
+  return FEM_SUCCESS;
+}
+
 int fem_batch_tune(fem_batch *b, int precision, void *stream, int reps, double *bestSeconds) {
   fem::clear_error();
   if (!b) return fem::fail(FEM_ERR_INVALID_ARGUMENT, "batch is NULL");
@@ -561,11 +724,14 @@ int fem_batch_tune(fem_batch *b, int precision, void *stream, int reps, double *
   for (int p = 1; p < kOrders; p++) {
     if (!order_has_work(b, p)) continue;
     double best = 1e30;
-    int bestLen = b->tileBatches[p], bestVar = kern[p];
+    int bestLen = b->tileBatches[p], bestVar = kern[p], bestOrd = b->ordered[p];
     for (int v : variants) {
       if (!variant_allowed(p, precision, v)) continue;
       kern[p] = v;
+      const bool frag = v == FEM_KERNEL_FRAGMENT_FP64 || v == FEM_KERNEL_FRAGMENT_BF16X6;
+      for (int ord = 0; ord <= (frag && p >= 2 ? 1 : 0); ord++)
       for (int len : lens) {
+        b->ordered[p] = ord;
         b->tileBatches[p] = len;
         build_tiles(b);
         if ((st = sync_device_state(b))) return st;
@@ -585,11 +751,13 @@ int fem_batch_tune(fem_batch *b, int precision, void *stream, int reps, double *
           best = secs;
           bestLen = len;
           bestVar = v;
+          bestOrd = ord;
         }
       }
     }
     b->tileBatches[p] = bestLen;
     kern[p] = bestVar;
+    b->ordered[p] = bestOrd;
     total += best;
   }
   build_tiles(b);

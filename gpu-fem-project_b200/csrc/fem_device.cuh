@@ -510,6 +510,7 @@ struct SchedTile {
   int64_t begin;  // first list position
   int count;      // list positions (even except at the end of a group)
   int group;
+  int mesh = 0;   // batches: the mesh's index in the launch's mesh table
 };
 struct SchedArgs {
   const SchedTile *tiles;

@@ -515,18 +515,20 @@ __device__ __noinline__ void sched_wait(const SchedArgs *S, int g) {
   }
 }
 
-// One mesh, dependency-ordered: warps pull tiles in dispatch order from one counter
-// (status[1]).  Before the first write of a tile's pairs the warp waits for the
+// Dependency-ordered: warps pull tiles in dispatch order from one counter
+// (status[1]); one mesh, or (BATCHED) the tiles of many meshes of one order, each
+// tile naming its mesh.  Before the first write of a tile's pairs the warp waits for the
 // groups its tile's group depends on (acquire); after the last pair of a tile it
 // completes its writes -- the asynchronous bulk reductions included -- and counts
 // the tile in its group (release).  A warp holds at most the tiles it has pulled,
 // in dispatch order, and every dependency of a tile is an earlier group, so the
 // earliest unfinished tile can always proceed: no wait is circular, whether or not
 // every CTA of the grid is resident.
-struct PairSched {
-  static constexpr bool kBatched = false, kSched = true;
+template <bool BATCHED>
+struct PairSchedT {
+  static constexpr bool kBatched = BATCHED, kSched = true;
   const SchedArgs *S;  // the kernel's __grid_constant__ parameter
-  int tile = -1, held = -1;
+  int tile = -1, held = -1, mesh = 0;
   int64_t pos = 0, tend = 0;
   bool done = false;
   __device__ PairCursor next(int lane) {
@@ -540,11 +542,13 @@ struct PairSched {
       } else {
         const SchedTile tl = S->tiles[t];
         tile = t;
+        if (BATCHED) mesh = tl.mesh;
         pos = tl.begin;
         tend = tl.begin + tl.count;
       }
     }
     if (done) return c;
+    c.mesh = mesh;
     c.k0 = pos;
     c.ne = (int)min((int64_t)2, tend - pos);
     c.tile = tile;
@@ -572,6 +576,7 @@ struct PairSched {
     if (lane == 0) atomicAdd(S->status + 2 + S->tiles[c.tile].group, 1);
   }
 };
+using PairSched = PairSchedT<false>;
 
 // One warp's assembly loop over the pairs its generator yields.  `single` is the
 // single-mesh kernel's argument block; batched generators read meshes[c.mesh].
@@ -1431,6 +1436,18 @@ __global__ void __launch_bounds__(32 * FragDims<P>::WARPS, FEM_FRAG_MINB)
   frag_loop<P, MODE>(smem, gen, A, &A);
 }
 
+// Many meshes of one order, all colours in one dependency-ordered persistent launch:
+// the tiles of every (mesh, colour) group, colours outermost, each group waiting
+// for its mesh's previous colour.
+template <int P, int MODE>
+__global__ void __launch_bounds__(32 * FragDims<P>::WARPS, FEM_FRAG_MINB)
+    frag_batched_sched_kernel(const AsmArgs *__restrict__ meshes, const __grid_constant__ SchedArgs S) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  frag_prologue<P, (MODE & kB16) != 0>(smem);
+  PairSchedT<true> gen{&S};
+  frag_loop<P, MODE>(smem, gen, meshes[0], meshes);
+}
+
 // Many meshes of one order (one colour each): warps pull tiles from the launch's queue.
 template <int P, int MODE>
 __global__ void __launch_bounds__(32 * FragDims<P>::WARPS, FEM_FRAG_MINB)
@@ -1538,6 +1555,25 @@ int launch_frag_batched_p(const AsmArgs *meshes, const Tile *tiles, int ntiles, 
   kernel<<<grid, NT, smem, s>>>(meshes, tiles, ntiles, counter);
   cudaError_t err = cudaGetLastError();
   if (err != cudaSuccess) return cuda_fail(err, "frag_batched_kernel launch");
+  return FEM_SUCCESS;
+}
+
+template <int P, int MODE>
+int launch_frag_batched_sched_p(const AsmArgs *meshes, const SchedArgs &sa, cudaStream_t s) {
+  using F = FragDims<P>;
+  constexpr int NT = 32 * F::WARPS;
+  auto kernel = frag_batched_sched_kernel<P, MODE>;
+  const size_t smem = FragLayout<P, false, false, (MODE & kB16) != 0>::total;
+  LaunchInfo li;
+  int st = launch_info(kernel, NT, smem, li);
+  if (st) return st;
+  const int64_t need = ((int64_t)sa.ntiles + F::WARPS - 1) / F::WARPS;
+  const int64_t cap = (int64_t)li.grid_per_sm * li.num_sms;
+  const int grid = (int)(need < cap ? need : cap);
+  if (grid <= 0) return FEM_SUCCESS;
+  kernel<<<grid, NT, smem, s>>>(meshes, sa);
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return cuda_fail(err, "frag_batched_sched_kernel launch");
   return FEM_SUCCESS;
 }
 
@@ -1684,6 +1720,20 @@ int launch_frag_sched(int order, int precision, int mode, const dev::AsmArgs &a,
     case kNL | kPlan | kJac: return go(IC<kNL | kPlan | kJac>{});
     case kNL | kPlan | kRes | kJac: return go(IC<kNL | kPlan | kRes | kJac>{});
     default: return fail(FEM_ERR_INVALID_ARGUMENT, "fragment kernel, schedule: mode %d", mode);
+  }
+}
+
+int launch_frag_batched_sched(int order, int precision, const dev::AsmArgs *meshes, const dev::SchedArgs &sa,
+                              cudaStream_t s) {
+  using namespace dev;
+  constexpr int M = kPlan | kRes | kJac;
+  const bool b16 = b16_stiffness(order, precision, FEM_STRAIN_LINEAR);
+  switch (order) {
+    case 2: return launch_frag_batched_sched_p<2, M>(meshes, sa, s);
+    case 3: return b16 ? launch_frag_batched_sched_p<3, M | kB16>(meshes, sa, s)
+                       : launch_frag_batched_sched_p<3, M>(meshes, sa, s);
+    case 4: return launch_frag_batched_sched_p<4, M>(meshes, sa, s);
+    default: return fail(FEM_ERR_INVALID_ORDER, "fragment kernel: order %d", order);
   }
 }
 

@@ -137,6 +137,10 @@ int launch_batched_variant(int p, int variant, const dev::AsmArgs *meshes, const
 // Its tile-queue form for batches and the server (residual and Jacobian).
 int launch_frag_batched(int order, int precision, const dev::AsmArgs *meshes, const dev::Tile *tiles, int ntiles,
                         int *counter, cudaStream_t s);
+// All colours of a batch's order-p meshes in one dependency-ordered persistent
+// launch (sa.tiles name their meshes; residual and Jacobian).
+int launch_frag_batched_sched(int order, int precision, const dev::AsmArgs *meshes, const dev::SchedArgs &sa,
+                              cudaStream_t s);
 
 // A synchronous cudaMemcpy from pageable host memory returns once the data is staged,
 // before the DMA has landed, and a synchronous cudaMemset only enqueues; both run on

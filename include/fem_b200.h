@@ -253,9 +253,10 @@ int fem_plan_assemble_host(const fem_plan *plan, const double *hostStates, doubl
 
 /* ---- batched assembly of many meshes (config: 256 meshes, mixed orders) --------------- */
 /* A batch references existing plans (they must outlive it) and assembles all of
- * their meshes with one persistent kernel per (order, colour) whose thread groups
- * pull element tiles from that launch's work queue; the orders run concurrently on
- * internal streams.  Outputs follow fem_plan_assemble (complete overwrite).
+ * their meshes with one persistent kernel per (order, colour) -- or, per order,
+ * one for all colours (fem_batch_set_ordered) -- whose thread groups pull element
+ * tiles from that launch's work queue; the orders run concurrently on internal
+ * streams.  Outputs follow fem_plan_assemble (complete overwrite).
  * (No reference counterpart: the reference assembles one mesh per call.) */
 typedef struct fem_batch fem_batch;
 
@@ -302,12 +303,32 @@ int fem_batch_set_tiles(fem_batch *batch, const int *tileBatches);
  * FEM_ERR_INVALID_ARGUMENT for a variant that cannot serve its order at `precision`. */
 int fem_batch_get_kernels(const fem_batch *batch, int precision, int *kernels);
 int fem_batch_set_kernels(fem_batch *batch, int precision, const int *kernels);
+/* Per order (index 0..3 = order 1..4; order 1 must be 0): 1 runs the order's
+ * colours, when its variant is a fragment kernel, as ONE dependency-ordered
+ * persistent launch instead of one launch per colour: the tiles of every (mesh,
+ * colour) group are dispatched colours outermost, and a tile waits (in the kernel,
+ * bounded) until its mesh's previous colour has finished, so every block still
+ * receives its contributions in colour order and the result is the same bit for
+ * bit.  Batches start with 0; fem_batch_tune chooses per order. */
+int fem_batch_set_ordered(fem_batch *batch, const int *ordered);
+int fem_batch_get_ordered(const fem_batch *batch, int *ordered);
+/* Waits for `stream`, then returns (and clears) the number of bounded in-kernel
+ * waits of the batch's dependency-ordered launches that ran out (each gives up
+ * after waitLimitNs, default 0.5 s); an assembly with a wait that ran out has
+ * invalid results. */
+int fem_batch_wait_status(fem_batch *batch, void *stream, int64_t *timedOutWaits);
+/* Failure injection for tests of the bounded waits of order `order`'s
+ * dependency-ordered launch: waitLimitNs > 0 sets the wait limit; stallGroup >= 0
+ * makes every wait on that group (0 = the first mesh's colour 0) run out, -1
+ * restores normal waits. */
+int fem_batch_set_schedule_waits(fem_batch *batch, int64_t waitLimitNs, int order, int stallGroup);
 /* One assembly of every mesh, stream-ordered on `stream`. */
 int fem_batch_assemble(fem_batch *batch, int precision, void *stream, double *elapsedSeconds);
 /* Autotuner: per order, times the order's launches for every kernel variant the
- * precision allows and every candidate tile length (1, 4, 16, 64, 256 element
- * batches; reps repetitions after a warm-up) and keeps the fastest pair
- * (fem_batch_get_kernels / fem_batch_get_tiles report it).  Replaces the
+ * precision allows, every candidate tile length (1, 4, 16, 64, 256 element
+ * batches; reps repetitions after a warm-up) and, for the fragment kernels, both
+ * launch forms (per colour, dependency-ordered), and keeps the fastest
+ * (fem_batch_get_kernels / fem_batch_get_tiles / fem_batch_get_ordered report it).  Replaces the
  * (order, precision) reference tables of hand-tuned elements per block
  * (element/FEKernels.h:1009-1028, 1104-1123). */
 int fem_batch_tune(fem_batch *batch, int precision, void *stream, int reps, double *bestSeconds);
