@@ -46,11 +46,13 @@ extern "C" {
 
 #define FEM_PRECISION_FP64 0  /* all element arithmetic in FP64                               */
 #define FEM_PRECISION_MIXED 1 /* FP64 J/detJ/J^-1, weak stress and accumulate; element
-                               stiffness in reduced precision where that kernel is the
-                               faster one: order 3 as BF16 tensor-core products of
-                               three-way split operands (FP32 accumulate), order 4 and the
-                               order-1 drop-in as FP32 element products; elsewhere the
-                               faster FP64 kernel runs and the result is FP64 */
+                               stiffness in reduced precision: order 3 as BF16 tensor-core
+                               products of three-way split operands (FP32 accumulate;
+                               as fast as FP64 in the colour layout, ~12 % slower than
+                               FP64 in a plan's pair layout, whose gain it does not
+                               share), order 4 and the order-1 drop-in as FP32 element
+                               products; orders 1-2 (plans) run the faster FP64 kernel
+                               and the result is FP64 */
 
 /* Strain measure of the weak residual: the reference's A2D::GreenStrainType
  * template option of planeStressWeakRes and the four assembly kernels
